@@ -1,0 +1,68 @@
+"""Build libcalculator.so (the C-ABI + sm_100a kernels) in-tree with nvcc.
+
+    python -m rover_b200.build          # -> rover_b200/lib/libcalculator.so
+
+Compiled for sm_100a only.  -fmad=false keeps every floating-point multiply
+and add separately rounded, as the reference's host build does; the kernels
+also spell those steps with _rn intrinsics.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+LIB_DIR = HERE / "lib"
+LIB = LIB_DIR / "libcalculator.so"
+HOST_DIR = HERE / "host"
+
+SOURCES = ["calculator.cu", "pq_search.cu", "sq_search.cu", "distance.cu", "rpcmem_compat.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    LIB_DIR.mkdir(exist_ok=True)
+    obj_dir = HERE / "_build"
+    obj_dir.mkdir(exist_ok=True)
+    headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list((HERE.parent / "include").glob("*.h"))
+    objs = []
+    for src in SOURCES:
+        s = CSRC / src
+        o = obj_dir / (s.stem + ".o")
+        objs.append(o)
+        if not force and not _stale(o, [s, *headers]):
+            continue
+        cmd = [nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2",
+               "--expt-relaxed-constexpr", "-I", str(CSRC), "-I", str(HERE.parent / "include"), "-c", str(s),
+               "-o", str(o)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        subprocess.run(cmd, check=True)
+    if force or _stale(LIB, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-Xlinker", "-Bsymbolic",
+               "-lcudart_static", "-lpthread", "-ldl", "-lrt"]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,298 @@
+"""Python binding of libcalculator.so (ctypes), the host-side mirror of the
+reference's accelerator interface.
+
+``Calculator`` exposes the reference entry points of inc/calculator.idl
+(``retrieval_load`` / ``retrieval_search`` / ...) under their own names, plus
+the batched extension of include/rover_b200.h.  It holds no search logic:
+every call goes through the C-ABI into the CUDA library, and the library must
+be present -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "lib" / "libcalculator.so"
+
+AEE_SUCCESS = 0
+AEE_EFAILED = 1
+AEE_ENOMEMORY = 2
+AEE_EBADPARM = 14
+AEE_EUNSUPPORTED = 20
+
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_u64p = C.POINTER(C.c_uint64)
+_f32p = C.POINTER(C.c_float)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class CalculatorError(RuntimeError):
+    def __init__(self, call: str, code: int, detail: str = ""):
+        super().__init__(f"{call} returned {code}" + (f": {detail}" if detail else ""))
+        self.code = code
+
+
+class PqIndexDesc(C.Structure):
+    _fields_ = [("graph", _i32p), ("num_vectors", C.c_int32), ("graph_degree", C.c_int32),
+                ("graph_entry", C.c_int32), ("dim", C.c_int32), ("codes", _u8p), ("codebook", _f32p),
+                ("m", C.c_int32), ("ks", C.c_int32), ("subdim", C.c_int32), ("code_bytes", C.c_int32),
+                ("residual_blocks", _u8p), ("residual_blocks_bytes", C.c_int64),
+                ("residual_bits", C.c_int32), ("residual_qparams", _f32p)]
+
+
+class SqIndexDesc(C.Structure):
+    _fields_ = [("graph", _i32p), ("num_vectors", C.c_int32), ("graph_degree", C.c_int32),
+                ("graph_entry", C.c_int32), ("dim", C.c_int32), ("l1_codes", _u8p), ("l1_bits", C.c_int32),
+                ("l1_scale", C.c_float), ("l1_zero", C.c_float), ("residual_rows", _u8p),
+                ("residual_bits", C.c_int32), ("residual_qparams", _f32p)]
+
+
+class SearchParams(C.Structure):
+    _fields_ = [("size", C.c_int32), ("mode", C.c_int32), ("entry_points", C.c_int32), ("seed", C.c_uint32),
+                ("expand_count", C.c_int32), ("correction", C.c_int32), ("refine_budget", C.c_int32),
+                ("top_k", C.c_int32), ("pool_stride", C.c_int32), ("sq_mode", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
+
+
+class SearchOutputs(C.Structure):
+    _fields_ = [("ids", _i32p), ("dists", _f32p), ("counts", _i32p), ("out_stride", C.c_int32),
+                ("pool_ids", _i32p), ("pool_dists", _f32p), ("pool_counts", _i32p), ("stats", _u64p),
+                ("status", _i32p)]
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def _dp(t, ptr):
+    """A raw device pointer (int) as a ctypes pointer."""
+    return C.cast(C.c_void_p(int(ptr)), t) if ptr else None
+
+
+def load_library(path: str | Path | None = None) -> C.CDLL:
+    path = Path(path or LIB_PATH)
+    if not path.is_file():
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m rover_b200.build`")
+    return C.CDLL(str(path))
+
+
+class Calculator:
+    """One session handle on the process-wide device state."""
+
+    def __init__(self, lib_path: str | Path | None = None):
+        self.lib = load_library(lib_path)
+        L = self.lib
+        L.calculator_open.argtypes = [C.c_char_p, C.POINTER(C.c_uint64)]
+        L.calculator_close.argtypes = [C.c_uint64]
+        L.calculator_rover_configure.argtypes = [C.c_uint64, C.c_int32, C.c_int32]
+        L.calculator_retrieval_load.argtypes = [C.c_uint64, _i32p, C.c_int, _u8p, C.c_int, C.c_int32, C.c_int32,
+                                                C.c_int32, C.c_int32, C.c_float, C.c_float]
+        L.calculator_retrieval_search.argtypes = [C.c_uint64, _f32p, C.c_int, C.c_int32, C.c_int32, C.c_int32,
+                                                  C.c_int32, _i32p, C.c_int, _f32p, C.c_int, _i32p]
+        L.calculator_retrieval_unload.argtypes = [C.c_uint64]
+        L.calculator_rover_last_error.restype = C.c_char_p
+        L.calculator_rover_pq_load.argtypes = [C.c_uint64, C.POINTER(PqIndexDesc)]
+        L.calculator_rover_pq_unload.argtypes = [C.c_uint64]
+        L.calculator_rover_pq_search.argtypes = [C.c_uint64, C.POINTER(SearchParams), _f32p, C.c_int32, _i32p,
+                                                 _i32p, C.POINTER(SearchOutputs)]
+        L.calculator_rover_pq_search_device.argtypes = [C.c_uint64, C.POINTER(SearchParams), _f32p, C.c_int32,
+                                                        _i32p, _i32p, C.POINTER(SearchOutputs), C.c_void_p]
+        L.calculator_rover_score.argtypes = [C.c_uint64, C.c_int32, _f32p, C.c_int32, _i32p, _i64p, _f32p, _i32p]
+        L.calculator_rover_pq_lut.argtypes = [C.c_uint64, _f32p, C.c_int32, _f32p, _i32p]
+        L.calculator_rover_refine.argtypes = [C.c_uint64, C.c_int32, _f32p, C.c_int32, _i32p, C.c_int32, _i32p,
+                                              C.c_int32, _i32p, _f32p, _i32p, _i32p]
+        L.calculator_rover_sq_load.argtypes = [C.c_uint64, C.POINTER(SqIndexDesc)]
+        L.calculator_rover_sq_unload.argtypes = [C.c_uint64]
+        L.calculator_rover_sq_search.argtypes = [C.c_uint64, C.POINTER(SearchParams), _f32p, C.c_int32, _i32p,
+                                                 C.POINTER(SearchOutputs)]
+        self.handle = C.c_uint64(0)
+        self._check("calculator_open", L.calculator_open(b"file:///libcalculator_skel.so", C.byref(self.handle)))
+        self._keep = {}
+
+    # -- helpers
+    def last_error(self) -> str:
+        return (self.lib.calculator_rover_last_error() or b"").decode()
+
+    def _check(self, call, rc):
+        if rc != AEE_SUCCESS:
+            raise CalculatorError(call, rc, self.last_error())
+        return rc
+
+    def close(self):
+        if self.handle.value:
+            self.lib.calculator_close(self.handle)
+            self.handle = C.c_uint64(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference entry points (calculator.idl)
+    def rover_configure(self, abi_version: int, l1_bits: int) -> int:
+        return self.lib.calculator_rover_configure(self.handle, abi_version, l1_bits)
+
+    def retrieval_load(self, graph, l1_codes, num_vectors, dim, graph_k, graph_entry, l1_scale, l1_zero) -> int:
+        g = np.ascontiguousarray(graph, dtype=np.int32).reshape(-1)
+        c = np.ascontiguousarray(l1_codes, dtype=np.uint8).reshape(-1)
+        return self.lib.calculator_retrieval_load(self.handle, _p(g, _i32p), g.size, _p(c, _u8p), c.size,
+                                                  num_vectors, dim, graph_k, graph_entry, l1_scale, l1_zero)
+
+    def retrieval_search(self, query, entry_points, expand_count, pool_size, num_out):
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        ids = np.full(num_out, -1, dtype=np.int32)
+        d = np.zeros(num_out, dtype=np.float32)
+        actual = C.c_int32(0)
+        rc = self.lib.calculator_retrieval_search(self.handle, _p(q, _f32p), q.size, entry_points, expand_count,
+                                                  pool_size, num_out, _p(ids, _i32p), num_out, _p(d, _f32p),
+                                                  num_out, C.byref(actual))
+        return rc, ids[:actual.value], d[:actual.value]
+
+    def retrieval_unload(self) -> int:
+        return self.lib.calculator_retrieval_unload(self.handle)
+
+    # -- extension: PQ
+    def pq_load(self, graph, graph_entry: int, bundle) -> None:
+        """graph: [n][degree] int32 or None; bundle: rover_b200.bundle.PqBundle."""
+        md = bundle.meta
+        g = None if graph is None else np.ascontiguousarray(graph, dtype=np.int32)
+        codes = np.ascontiguousarray(bundle.codes, dtype=np.uint8)
+        book = np.ascontiguousarray(bundle.codebook, dtype=np.float32)
+        res = np.ascontiguousarray(bundle.residual_blocks, dtype=np.uint8) if bundle.residual_bits else None
+        qp = np.ascontiguousarray(bundle.qparams, dtype=np.float32) if bundle.residual_bits else None
+        desc = PqIndexDesc(_p(g, _i32p), md.num_vectors, 0 if g is None else g.shape[1], graph_entry, md.dim,
+                           _p(codes, _u8p), _p(book, _f32p), md.m, md.ks, md.subdim, md.code_bytes,
+                           _p(res, _u8p), 0 if res is None else res.size, bundle.residual_bits, _p(qp, _f32p))
+        self._check("calculator_rover_pq_load", self.lib.calculator_rover_pq_load(self.handle, C.byref(desc)))
+        self.pq_dim = md.dim
+
+    def pq_unload(self):
+        self.lib.calculator_rover_pq_unload(self.handle)
+
+    @staticmethod
+    def params(entry_points=1, expand_count=32, correction=1, refine_budget=0, top_k=10, seed=42,
+               pool_stride=0, sq_mode=0, mode=0) -> SearchParams:
+        p = SearchParams()
+        p.size = C.sizeof(SearchParams)
+        p.mode = mode
+        p.entry_points = entry_points
+        p.seed = seed
+        p.expand_count = expand_count
+        p.correction = correction
+        p.refine_budget = refine_budget
+        p.top_k = top_k
+        p.pool_stride = pool_stride
+        p.sq_mode = sq_mode
+        return p
+
+    def pq_search(self, queries, pool_sizes, top_k=10, top_ks=None, pool_stride=0, stats=True, check=True,
+                  **kw) -> dict:
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        nq = q.shape[0]
+        pools = np.ascontiguousarray(np.broadcast_to(np.asarray(pool_sizes, dtype=np.int32), (nq,)))
+        tks = None if top_ks is None else np.ascontiguousarray(np.broadcast_to(np.asarray(top_ks, dtype=np.int32), (nq,)))
+        stride = top_k if tks is None else int(tks.max())
+        p = self.params(top_k=top_k, pool_stride=pool_stride, **kw)
+        r = dict(ids=np.full((nq, stride), -1, np.int32), dists=np.zeros((nq, stride), np.float32),
+                 counts=np.zeros(nq, np.int32), status=np.zeros(nq, np.int32))
+        if pool_stride:
+            r.update(pool_ids=np.full((nq, pool_stride), -1, np.int32),
+                     pool_dists=np.zeros((nq, pool_stride), np.float32), pool_counts=np.zeros(nq, np.int32))
+        if stats:
+            r["stats"] = np.zeros((nq, 4), np.uint64)
+        o = SearchOutputs(_p(r["ids"], _i32p), _p(r["dists"], _f32p), _p(r["counts"], _i32p), stride,
+                          _p(r.get("pool_ids"), _i32p), _p(r.get("pool_dists"), _f32p),
+                          _p(r.get("pool_counts"), _i32p), _p(r.get("stats"), _u64p), _p(r["status"], _i32p))
+        rc = self.lib.calculator_rover_pq_search(self.handle, C.byref(p), _p(q, _f32p), nq, _p(pools, _i32p),
+                                                 _p(tks, _i32p), C.byref(o))
+        r["rc"] = rc
+        if check:
+            self._check("calculator_rover_pq_search", rc)
+        return r
+
+    def pq_search_device(self, queries_ptr: int, nq: int, pool_ptr: int, out: dict, topk_ptr: int = 0,
+                         stream_ptr: int = 0, check=True, **kw) -> int:
+        """Device-resident variant: pointers are raw CUDA device addresses
+        (e.g. torch tensor .data_ptr()).  out holds device pointers for the
+        keys ids, dists, counts, stride and optionally pool_*, stats, status."""
+        p = self.params(**kw)
+        o = SearchOutputs(_dp(_i32p, out.get("ids")), _dp(_f32p, out.get("dists")), _dp(_i32p, out.get("counts")),
+                          out.get("stride", 0), _dp(_i32p, out.get("pool_ids")), _dp(_f32p, out.get("pool_dists")),
+                          _dp(_i32p, out.get("pool_counts")), _dp(_u64p, out.get("stats")),
+                          _dp(_i32p, out.get("status")))
+        rc = self.lib.calculator_rover_pq_search_device(self.handle, C.byref(p), _dp(_f32p, queries_ptr), nq,
+                                                        _dp(_i32p, pool_ptr), _dp(_i32p, topk_ptr), C.byref(o),
+                                                        C.c_void_p(stream_ptr or None))
+        if check:
+            self._check("calculator_rover_pq_search_device", rc)
+        return rc
+
+    def pq_lut(self, queries, m, ks):
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        out = np.zeros((q.shape[0], m * ks), np.float32)
+        st = np.zeros(q.shape[0], np.int32)
+        self._check("calculator_rover_pq_lut",
+                    self.lib.calculator_rover_pq_lut(self.handle, _p(q, _f32p), q.shape[0], _p(out, _f32p),
+                                                     _p(st, _i32p)))
+        return out
+
+    def score(self, kind: int, queries, id_lists):
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        offsets = np.zeros(len(id_lists) + 1, np.int64)
+        offsets[1:] = np.cumsum([len(x) for x in id_lists])
+        ids = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32) for x in id_lists])
+                                   if len(id_lists) else np.zeros(0, np.int32), dtype=np.int32)
+        out = np.zeros(max(1, int(offsets[-1])), np.float32)
+        st = np.zeros(q.shape[0], np.int32)
+        self._check("calculator_rover_score",
+                    self.lib.calculator_rover_score(self.handle, kind, _p(q, _f32p), q.shape[0], _p(ids, _i32p),
+                                                    _p(offsets, _i64p), _p(out, _f32p), _p(st, _i32p)))
+        return [out[offsets[i]:offsets[i + 1]] for i in range(len(id_lists))]
+
+    def refine(self, kind, queries, cand_ids, cand_counts, top_k):
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        ids = np.ascontiguousarray(cand_ids, dtype=np.int32)
+        counts = np.ascontiguousarray(cand_counts, dtype=np.int32)
+        nq = q.shape[0]
+        oi = np.full((nq, top_k), -1, np.int32)
+        od = np.zeros((nq, top_k), np.float32)
+        oc = np.zeros(nq, np.int32)
+        st = np.zeros(nq, np.int32)
+        self._check("calculator_rover_refine",
+                    self.lib.calculator_rover_refine(self.handle, kind, _p(q, _f32p), nq, _p(ids, _i32p),
+                                                     ids.shape[1], _p(counts, _i32p), top_k, _p(oi, _i32p),
+                                                     _p(od, _f32p), _p(oc, _i32p), _p(st, _i32p)))
+        return oi, od, oc
+
+    # -- extension: SQ
+    def sq_load(self, graph, graph_entry: int, b) -> None:
+        g = None if graph is None else np.ascontiguousarray(graph, dtype=np.int32)
+        l1 = np.ascontiguousarray(b.l1, dtype=np.uint8)
+        res = np.ascontiguousarray(b.residual_rows, dtype=np.uint8)
+        qp = np.ascontiguousarray(b.qparams, dtype=np.float32)
+        self._keep["sq"] = (g, l1, res, qp)
+        desc = SqIndexDesc(_p(g, _i32p), b.num_vectors, 0 if g is None else g.shape[1], graph_entry, b.dim,
+                           _p(l1, _u8p), b.l1_bits, b.l1_scale, b.l1_zero, _p(res, _u8p), b.residual_bits,
+                           _p(qp, _f32p))
+        self._check("calculator_rover_sq_load", self.lib.calculator_rover_sq_load(self.handle, C.byref(desc)))
+
+    def sq_search(self, queries, pool_sizes, out_stride, sq_mode=1, num_out=None, check=True, **kw) -> dict:
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        nq = q.shape[0]
+        pools = np.ascontiguousarray(np.broadcast_to(np.asarray(pool_sizes, dtype=np.int32), (nq,)))
+        p = self.params(sq_mode=sq_mode, top_k=num_out or out_stride, **kw)
+        r = dict(ids=np.full((nq, out_stride), -1, np.int32), dists=np.zeros((nq, out_stride), np.float32),
+                 counts=np.zeros(nq, np.int32), status=np.zeros(nq, np.int32), stats=np.zeros((nq, 4), np.uint64))
+        o = SearchOutputs(_p(r["ids"], _i32p), _p(r["dists"], _f32p), _p(r["counts"], _i32p), out_stride,
+                          None, None, None, _p(r["stats"], _u64p), _p(r["status"], _i32p))
+        rc = self.lib.calculator_rover_sq_search(self.handle, C.byref(p), _p(q, _f32p), nq, _p(pools, _i32p),
+                                                 C.byref(o))
+        r["rc"] = rc
+        if check:
+            self._check("calculator_rover_sq_search", rc)
+        return r

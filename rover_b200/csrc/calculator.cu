@@ -1,0 +1,1018 @@
+// calculator.cu -- libcalculator.so: Rover's accelerator C-ABI on a B200.
+//
+// The reference serves these entry points from a Hexagon DSP skeleton whose
+// state is module-global (src/dsp_demo/retrieval_async_dsp_search.c:44-76:
+// one loaded index per process).  This library keeps the same model: one
+// process-wide device state guarded by a mutex, shared by every session
+// handle.  Index buffers are uploaded to HBM once at load time; searches run
+// as the kernels in pq_search.cu / sq_search.cu / distance.cu.
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/calculator.h"
+#include "../../include/rover_b200.h"
+#include "kernels.h"
+#include "rpcmem_compat.h"
+
+using namespace rover;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+#define CK(expr)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (expr);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      set_error("%s failed: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return AEE_EFAILED;                                                            \
+    }                                                                                \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b ? b : 16);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct PqDevice {
+  DevBuf graph, codes, codebook, residual, qparams;
+  PqIndexView view{};
+  int32_t graph_entry = -1;
+  bool loaded = false;
+  bool has_graph = false;
+  void release() {
+    graph.release(); codes.release(); codebook.release(); residual.release(); qparams.release();
+    loaded = false;
+    has_graph = false;
+  }
+};
+
+struct SqDevice {
+  DevBuf graph, l1, residual, qparams;
+  SqIndexView view{};
+  int32_t graph_entry = -1;
+  bool loaded = false;
+  void release() {
+    graph.release(); l1.release(); residual.release(); qparams.release();
+    loaded = false;
+  }
+};
+
+struct State {
+  std::mutex mu;
+  bool init = false;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  int32_t l1_bits = 4;           // calculator_rover_configure
+  PqDevice pq;                    // extension PQ index / pure-PQ DMA index
+  SqDevice sq;                    // extension SQ index
+  SqDevice legacy;                // calculator_retrieval_load(_dma) index
+  bool legacy_dma = false;
+  // scratch
+  DevBuf visited, heaps, counter, status, stats, luts;
+  uint32_t visited_mask = 0;
+  size_t visited_slots = 0;
+  uint32_t gen_next = 1;
+  DevBuf in_queries, in_pool, in_topk, in_ids, in_offsets;
+  DevBuf out_ids, out_dists, out_counts, pool_ids, pool_dists, pool_counts;
+  std::vector<int32_t> h_status;
+};
+
+State& st() {
+  static State s;
+  return s;
+}
+
+int open_count = 0;
+
+AEEResult ensure_init(State& s) {
+  if (s.init) return AEE_SUCCESS;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+  s.init = true;
+  return AEE_SUCCESS;
+}
+
+template <class T>
+AEEResult upload(DevBuf& b, const T* src, size_t count, cudaStream_t s) {
+  CK(b.ensure(count * sizeof(T)));
+  if (count) CK(cudaMemcpyAsync(b.p, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  return AEE_SUCCESS;
+}
+
+uint32_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return static_cast<uint32_t>(p > 0x80000000ull ? 0x80000000ull : p);
+}
+
+// Reserve `entries` visited-table entries for each of `slots` warp slots and
+// a generation range of `queries` queries.
+AEEResult reserve_visited(State& s, size_t slots, uint32_t entries, uint32_t queries, uint32_t* gen_base) {
+  const size_t need = slots * static_cast<size_t>(entries) * 8u;
+  const bool regrow = need > s.visited.bytes || entries != s.visited_mask + 1u || slots > s.visited_slots;
+  if (regrow || static_cast<uint64_t>(s.gen_next) + queries >= 0xffffffffull) {
+    if (need > s.visited.bytes) CK(s.visited.ensure(need));
+    CK(cudaMemsetAsync(s.visited.p, 0, need, s.stream));
+    s.visited_mask = entries - 1u;
+    s.visited_slots = slots;
+    s.gen_next = 1;
+  }
+  *gen_base = s.gen_next;
+  s.gen_next += queries;
+  return AEE_SUCCESS;
+}
+
+int resident_blocks(const void* kernel, int threads, size_t smem, int sms) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return per_sm * sms;
+}
+
+bool valid_params(const RoverSearchParams* p) {
+  return p && p->size >= static_cast<int32_t>(offsetof(RoverSearchParams, reserved)) && p->entry_points > 0 &&
+         p->expand_count > 0 && p->refine_budget >= 0 && p->refine_budget <= 2000;
+}
+
+// Core PQ search on device buffers.  Retries queries whose visited table
+// overflowed with a 4x larger table.
+AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_queries, int nq,
+                         const int32_t* d_pool, const int32_t* d_topk, const std::vector<int32_t>& h_pool,
+                         const RoverSearchOutputs& d_out, cudaStream_t stream) {
+  const PqDevice& pq = s.pq;
+  if (!pq.loaded || !pq.has_graph) { set_error("no PQ index with a graph is loaded"); return AEE_EFAILED; }
+  int max_pool = 0;
+  for (int32_t v : h_pool) max_pool = std::max(max_pool, v);
+  if (max_pool <= 0 || max_pool > 4096) { set_error("pool sizes must be in 1..4096"); return AEE_EBADPARM; }
+  if (p->correction && pq.view.residual_bits == 0) { set_error("correction needs residuals"); return AEE_EBADPARM; }
+  if (p->refine_budget > 0 && pq.view.residual_bits == 0) { set_error("refine needs residuals"); return AEE_EBADPARM; }
+  const int expand = std::min(p->expand_count, pq.view.degree);
+  if (expand > kMaxBatch) { set_error("expand_count above %d", kMaxBatch); return AEE_EBADPARM; }
+
+  PqSearchArgs a{};
+  a.ix = pq.view;
+  a.queries = d_queries;
+  a.nq = nq;
+  a.pool_sizes = d_pool;
+  a.top_ks = d_topk;
+  a.top_k = p->top_k;
+  a.entry_points = p->entry_points;
+  a.graph_entry = pq.graph_entry;
+  a.seed = p->seed;
+  a.expand_count = p->expand_count;
+  a.correction = p->correction;
+  a.refine_budget = p->refine_budget;
+  a.max_pool = max_pool;
+  a.pool_ids = d_out.pool_ids;
+  a.pool_dists = d_out.pool_dists;
+  a.pool_stride = p->pool_stride;
+  a.pool_counts = d_out.pool_counts;
+  a.out_ids = d_out.ids;
+  a.out_dists = d_out.dists;
+  a.out_stride = d_out.out_stride;
+  a.out_counts = d_out.counts;
+  a.stats = reinterpret_cast<unsigned long long*>(d_out.stats);
+  a.status = d_out.status;
+  pq_search_layout(&a, p->refine_budget);
+  const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
+  if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, max_pool); return AEE_EBADPARM; }
+  CK(cudaFuncSetAttribute(pq_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  const int max_blocks = resident_blocks(reinterpret_cast<const void*>(pq_search_kernel), kSearchWarps * 32, smem, s.sms);
+  const int blocks = std::max(1, std::min(max_blocks, (nq + kSearchWarps - 1) / kSearchWarps));
+  const size_t slots = static_cast<size_t>(blocks) * kSearchWarps;
+  const uint64_t est = static_cast<uint64_t>(std::min(p->entry_points, pq.view.n)) +
+                       (2ull * max_pool + 64ull) * static_cast<uint64_t>(expand);
+  uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * est));
+  CK(s.counter.ensure(sizeof(unsigned int)));
+  CK(cudaMemsetAsync(d_out.status, 0, nq * sizeof(int32_t), stream));
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    uint32_t gen_base = 0;
+    if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    if (stream != s.stream) {
+      CK(cudaStreamSynchronize(s.stream));
+    }
+    a.visited = s.visited.as<unsigned long long>();
+    a.visited_mask = s.visited_mask;
+    a.gen_base = gen_base;
+    a.next_query = s.counter.as<unsigned int>();
+    CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
+    pq_search_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
+    CK(cudaGetLastError());
+    s.h_status.resize(nq);
+    CK(cudaMemcpyAsync(s.h_status.data(), d_out.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    bool retry = false;
+    for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
+    if (!retry) break;
+    // Re-run everything with a larger table: the outputs of successful
+    // queries are rewritten with identical values.
+    entries = next_pow2(static_cast<uint64_t>(entries) * 4);
+    CK(cudaMemsetAsync(d_out.status, 0, nq * sizeof(int32_t), stream));
+  }
+  for (int i = 0; i < nq; ++i)
+    if (s.h_status[i] != kStatusOk) {
+      set_error("query %d failed with status %d", i, s.h_status[i]);
+      return AEE_EFAILED;
+    }
+  return AEE_SUCCESS;
+}
+
+template <class T>
+AEEResult download(T* dst, const void* src, size_t count, cudaStream_t s) {
+  if (dst && count) CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+  return AEE_SUCCESS;
+}
+
+AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSearchParams* p,
+                         const float* d_queries, int nq, const int32_t* d_pool,
+                         const std::vector<int32_t>& h_pool, int num_out, int32_t* d_ids, float* d_dists,
+                         int32_t out_stride, int32_t* d_counts, unsigned long long* d_stats,
+                         int32_t* d_status, cudaStream_t stream) {
+  if (!sq.loaded) { set_error("no SQ index is loaded"); return AEE_EFAILED; }
+  int max_pool = 0;
+  for (int32_t v : h_pool) max_pool = std::max(max_pool, mode == kSqModeDsp ? std::min(v, 2000) : v);
+  if (max_pool <= 0 || max_pool > 4096) { set_error("pool sizes must be in 1..4096"); return AEE_EBADPARM; }
+  const int expand = std::min(p->expand_count, sq.view.degree);
+  const long long fbound = mode == kSqModeSqmd
+                               ? static_cast<long long>(p->entry_points) + static_cast<long long>(max_pool) * p->expand_count
+                               : static_cast<long long>(p->entry_points) + static_cast<long long>(max_pool) * expand;
+  const int fcap = static_cast<int>(std::min<long long>(fbound, 1 << 20));
+  SqSearchArgs a{};
+  a.ix = sq.view;
+  a.queries = d_queries;
+  a.nq = nq;
+  a.pool_sizes = d_pool;
+  a.mode = mode;
+  a.entry_points = p->entry_points;
+  a.graph_entry = sq.graph_entry;
+  a.seed = p->seed;
+  a.expand_count = p->expand_count;
+  a.correction = p->correction;
+  a.num_out = num_out;
+  a.max_pool = max_pool;
+  a.frontier_cap = fcap;
+  a.out_ids = d_ids;
+  a.out_dists = d_dists;
+  a.out_stride = out_stride;
+  a.out_counts = d_counts;
+  a.stats = d_stats;
+  a.status = d_status;
+  const size_t per_warp = ((sq.view.dim * 4 + 15) & ~15) + ((sq.view.dim + 15) & ~15) + 64 * 8;
+  const size_t smem = per_warp * kSearchWarps;
+  CK(cudaFuncSetAttribute(sq_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  int blocks = std::max(1, std::min(resident_blocks(reinterpret_cast<const void*>(sq_search_kernel), kSearchWarps * 32, smem, s.sms),
+                                    (nq + kSearchWarps - 1) / kSearchWarps));
+  // keep the heap scratch under 4 GiB
+  const size_t heap_per_slot = static_cast<size_t>(max_pool + fcap) * 8u;
+  while (blocks > 1 && static_cast<size_t>(blocks) * kSearchWarps * heap_per_slot > (4ull << 30)) blocks >>= 1;
+  const size_t slots = static_cast<size_t>(blocks) * kSearchWarps;
+  CK(s.heaps.ensure(slots * heap_per_slot));
+  a.heaps = s.heaps.as<uint64_t>();
+  const uint64_t est = static_cast<uint64_t>(p->entry_points) * 2 + (2ull * max_pool + 64ull) * static_cast<uint64_t>(std::max(expand, 1));
+  uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * est));
+  CK(s.counter.ensure(sizeof(unsigned int)));
+  CK(cudaMemsetAsync(d_status, 0, nq * sizeof(int32_t), stream));
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    uint32_t gen_base = 0;
+    if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    a.visited = s.visited.as<unsigned long long>();
+    a.visited_mask = s.visited_mask;
+    a.gen_base = gen_base;
+    a.next_query = s.counter.as<unsigned int>();
+    CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
+    sq_search_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
+    CK(cudaGetLastError());
+    s.h_status.resize(nq);
+    CK(cudaMemcpyAsync(s.h_status.data(), d_status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    bool retry = false;
+    for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
+    if (!retry) break;
+    entries = next_pow2(static_cast<uint64_t>(entries) * 4);
+    CK(cudaMemsetAsync(d_status, 0, nq * sizeof(int32_t), stream));
+  }
+  for (int i = 0; i < nq; ++i)
+    if (s.h_status[i] != kStatusOk) {
+      set_error("query %d failed with status %d", i, s.h_status[i]);
+      return AEE_EFAILED;
+    }
+  return AEE_SUCCESS;
+}
+
+AEEResult load_sq(State& s, SqDevice& d, const RoverSqIndexDesc* desc, int l1_bits) {
+  if (!desc || desc->num_vectors <= 0 || desc->dim <= 0 || desc->dim > 1024 || desc->graph_degree <= 0 ||
+      (l1_bits != 4 && l1_bits != 8) || !desc->l1_codes)
+    return AEE_EBADPARM;
+  d.release();
+  const size_t n = desc->num_vectors;
+  const int l1cb = l1_bits == 4 ? (desc->dim + 1) / 2 : desc->dim;
+  if (desc->graph) {
+    if (upload(d.graph, desc->graph, n * desc->graph_degree, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  }
+  if (upload(d.l1, desc->l1_codes, n * l1cb, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  int rcb = 0;
+  if (desc->residual_rows && desc->residual_qparams) {
+    if (desc->residual_bits != 4 && desc->residual_bits != 8) return AEE_EBADPARM;
+    rcb = desc->residual_bits == 4 ? (desc->dim + 1) / 2 : desc->dim;
+    if (upload(d.residual, desc->residual_rows, n * rcb, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    if (upload(d.qparams, desc->residual_qparams, n * 2, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  }
+  CK(cudaStreamSynchronize(s.stream));
+  SqIndexView& v = d.view;
+  v.graph = d.graph.as<int32_t>();
+  v.n = desc->num_vectors;
+  v.degree = desc->graph_degree;
+  v.dim = desc->dim;
+  v.l1 = d.l1.as<uint8_t>();
+  v.l1_bits = l1_bits;
+  v.l1_code_bytes = l1cb;
+  v.l1_scale = desc->l1_scale;
+  v.l1_zero = desc->l1_zero;
+  v.residual = rcb ? d.residual.as<uint8_t>() : nullptr;
+  v.residual_bits = rcb ? desc->residual_bits : 0;
+  v.rcb = rcb;
+  v.qparams = rcb ? d.qparams.as<float>() : nullptr;
+  d.graph_entry = desc->graph_entry;
+  d.loaded = true;
+  return AEE_SUCCESS;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Extension entry points (include/rover_b200.h)
+
+extern "C" const char* calculator_rover_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" AEEResult calculator_rover_pq_load(remote_handle64 h, const RoverPqIndexDesc* d) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!d || d->num_vectors <= 0 || d->dim <= 0 || d->dim > 1024 || d->m <= 0 ||
+      (d->ks != 16 && d->ks != 256) || d->subdim <= 0 || d->m * d->subdim != d->dim ||
+      d->code_bytes != (d->ks == 16 ? (d->m + 1) / 2 : d->m) || !d->codes || !d->codebook) {
+    set_error("invalid PQ index description");
+    return AEE_EBADPARM;
+  }
+  const size_t n = d->num_vectors;
+  const size_t book = static_cast<size_t>(d->m) * d->ks * d->subdim;
+  for (size_t i = 0; i < book; ++i)
+    if (!std::isfinite(d->codebook[i])) { set_error("codebook is not finite"); return AEE_EBADPARM; }
+  PqDevice& pq = s.pq;
+  pq.release();
+  AEEResult r = AEE_SUCCESS;
+  if (d->graph) {
+    if (d->graph_degree <= 0) return AEE_EBADPARM;
+    r = upload(pq.graph, d->graph, n * d->graph_degree, s.stream);
+    pq.has_graph = r == AEE_SUCCESS;
+  }
+  if (r == AEE_SUCCESS) r = upload(pq.codes, d->codes, n * d->code_bytes, s.stream);
+  if (r == AEE_SUCCESS) r = upload(pq.codebook, d->codebook, book, s.stream);
+  int rcb = 0, vpb = 0;
+  if (r == AEE_SUCCESS && d->residual_bits) {
+    if ((d->residual_bits != 4 && d->residual_bits != 8) || !d->residual_blocks || !d->residual_qparams) {
+      set_error("invalid residual description");
+      return AEE_EBADPARM;
+    }
+    rcb = d->residual_bits == 4 ? (d->dim + 1) / 2 : d->dim;
+    vpb = 4096 / rcb;
+    const int64_t blocks = (static_cast<int64_t>(n) + vpb - 1) / vpb;
+    if (d->residual_blocks_bytes != blocks * 4096) {
+      set_error("residual payload must be %lld bytes", static_cast<long long>(blocks * 4096));
+      return AEE_EBADPARM;
+    }
+    r = upload(pq.residual, d->residual_blocks, static_cast<size_t>(d->residual_blocks_bytes), s.stream);
+    if (r == AEE_SUCCESS) r = upload(pq.qparams, d->residual_qparams, n * 2, s.stream);
+  }
+  if (r != AEE_SUCCESS) { pq.release(); return AEE_ENOMEMORY; }
+  CK(cudaStreamSynchronize(s.stream));
+  PqIndexView& v = pq.view;
+  v.graph = pq.graph.as<int32_t>();
+  v.n = d->num_vectors;
+  v.degree = d->graph ? d->graph_degree : 0;
+  v.dim = d->dim;
+  v.codes = pq.codes.as<uint8_t>();
+  v.codebook = pq.codebook.as<float>();
+  v.m = d->m;
+  v.ks = d->ks;
+  v.subdim = d->subdim;
+  v.code_bytes = d->code_bytes;
+  v.residual = rcb ? pq.residual.as<uint8_t>() : nullptr;
+  v.residual_bits = rcb ? d->residual_bits : 0;
+  v.rcb = rcb;
+  v.vpb = vpb;
+  v.qparams = rcb ? pq.qparams.as<float>() : nullptr;
+  pq.graph_entry = d->graph_entry;
+  pq.loaded = true;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_pq_unload(remote_handle64 h) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  s.pq.release();
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_pq_search_device(remote_handle64 h, const RoverSearchParams* p,
+                                                       const float* queries, int32_t nq,
+                                                       const int32_t* pool_sizes, const int32_t* top_ks,
+                                                       const RoverSearchOutputs* out, void* stream) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!valid_params(p) || nq < 0 || !out || !queries || !pool_sizes || (out->ids && !out->counts)) return AEE_EBADPARM;
+  if (nq == 0) return AEE_SUCCESS;
+  cudaStream_t strm = stream ? static_cast<cudaStream_t>(stream) : s.stream;
+  std::vector<int32_t> h_pool(nq);
+  CK(cudaMemcpyAsync(h_pool.data(), pool_sizes, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, strm));
+  CK(cudaStreamSynchronize(strm));
+  RoverSearchOutputs o = *out;
+  if (!o.status) {
+    CK(s.status.ensure(nq * sizeof(int32_t)));
+    o.status = s.status.as<int32_t>();
+  }
+  return pq_search_core(s, p, queries, nq, pool_sizes, top_ks, h_pool, o, strm);
+}
+
+extern "C" AEEResult calculator_rover_pq_search(remote_handle64 h, const RoverSearchParams* p,
+                                                const float* queries, int32_t nq, const int32_t* pool_sizes,
+                                                const int32_t* top_ks, const RoverSearchOutputs* out) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!valid_params(p) || nq < 0 || !out || !queries || !pool_sizes || (out->ids && !out->counts)) return AEE_EBADPARM;
+  if (nq == 0) return AEE_SUCCESS;
+  if (!s.pq.loaded) { set_error("no PQ index loaded"); return AEE_EFAILED; }
+  cudaStream_t strm = s.stream;
+  const int dim = s.pq.view.dim;
+  std::vector<int32_t> h_pool(pool_sizes, pool_sizes + nq);
+  int max_pool = 0;
+  for (int v : h_pool) max_pool = std::max(max_pool, v);
+  const int k_stride = out->ids ? out->out_stride : 0;
+  const int p_stride = out->pool_ids ? p->pool_stride : 0;
+  if (upload(s.in_queries, queries, static_cast<size_t>(nq) * dim, strm) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  if (upload(s.in_pool, pool_sizes, nq, strm) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  if (top_ks && upload(s.in_topk, top_ks, nq, strm) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  RoverSearchOutputs d{};
+  if (k_stride) {
+    CK(s.out_ids.ensure(static_cast<size_t>(nq) * k_stride * 4));
+    CK(s.out_dists.ensure(static_cast<size_t>(nq) * k_stride * 4));
+    CK(s.out_counts.ensure(static_cast<size_t>(nq) * 4));
+    d.ids = s.out_ids.as<int32_t>();
+    d.dists = s.out_dists.as<float>();
+    d.counts = s.out_counts.as<int32_t>();
+    d.out_stride = k_stride;
+  }
+  if (p_stride) {
+    CK(s.pool_ids.ensure(static_cast<size_t>(nq) * p_stride * 4));
+    CK(s.pool_dists.ensure(static_cast<size_t>(nq) * p_stride * 4));
+    CK(s.pool_counts.ensure(static_cast<size_t>(nq) * 4));
+    d.pool_ids = s.pool_ids.as<int32_t>();
+    d.pool_dists = s.pool_dists.as<float>();
+    d.pool_counts = s.pool_counts.as<int32_t>();
+  }
+  if (out->stats) {
+    CK(s.stats.ensure(static_cast<size_t>(nq) * 32));
+    d.stats = s.stats.as<uint64_t>();
+  }
+  CK(s.status.ensure(static_cast<size_t>(nq) * 4));
+  d.status = s.status.as<int32_t>();
+  RoverSearchParams pp = *p;
+  pp.pool_stride = p_stride;
+  AEEResult r = pq_search_core(s, &pp, s.in_queries.as<float>(), nq, s.in_pool.as<int32_t>(),
+                               top_ks ? s.in_topk.as<int32_t>() : nullptr, h_pool, d, strm);
+  if (out->status) {
+    std::copy(s.h_status.begin(), s.h_status.begin() + nq, out->status);
+  }
+  if (r != AEE_SUCCESS) return r;
+  if (k_stride) {
+    if (download(out->ids, d.ids, static_cast<size_t>(nq) * k_stride, strm) ||
+        download(out->dists, d.dists, static_cast<size_t>(nq) * k_stride, strm) ||
+        download(out->counts, d.counts, nq, strm))
+      return AEE_EFAILED;
+  }
+  if (p_stride) {
+    if (download(out->pool_ids, d.pool_ids, static_cast<size_t>(nq) * p_stride, strm) ||
+        download(out->pool_dists, d.pool_dists, static_cast<size_t>(nq) * p_stride, strm) ||
+        download(out->pool_counts, d.pool_counts, nq, strm))
+      return AEE_EFAILED;
+  }
+  if (out->stats && download(out->stats, d.stats, static_cast<size_t>(nq) * 4, strm)) return AEE_EFAILED;
+  CK(cudaStreamSynchronize(strm));
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_pq_lut(remote_handle64 h, const float* queries, int32_t nq, float* out_luts,
+                                             int32_t* out_status) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!s.pq.loaded) { set_error("no PQ index loaded"); return AEE_EFAILED; }
+  if (nq <= 0 || !queries || !out_luts) return AEE_EBADPARM;
+  const PqIndexView& v = s.pq.view;
+  const size_t lut = static_cast<size_t>(v.m) * v.ks;
+  if (upload(s.in_queries, queries, static_cast<size_t>(nq) * v.dim, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  CK(s.luts.ensure(nq * lut * 4));
+  CK(s.status.ensure(nq * 4));
+  CK(cudaMemsetAsync(s.status.p, 0, nq * 4, s.stream));
+  launch_pq_lut(v, s.in_queries.as<float>(), nq, s.luts.as<float>(), s.status.as<int32_t>(), s.stream);
+  CK(cudaGetLastError());
+  std::vector<int32_t> hs(nq);
+  if (download(out_luts, s.luts.p, nq * lut, s.stream) || download(hs.data(), s.status.p, nq, s.stream)) return AEE_EFAILED;
+  CK(cudaStreamSynchronize(s.stream));
+  if (out_status) std::copy(hs.begin(), hs.end(), out_status);
+  for (int32_t x : hs) if (x) return AEE_EFAILED;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, const float* queries, int32_t nq,
+                                            const int32_t* ids, const int64_t* offsets, float* out_dists,
+                                            int32_t* out_status) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (nq <= 0 || !queries || !offsets || !out_dists || kind < 0 || kind > 3) return AEE_EBADPARM;
+  const bool pqk = kind <= 1;
+  if (pqk && !s.pq.loaded) { set_error("no PQ index loaded"); return AEE_EFAILED; }
+  if (!pqk && !s.sq.loaded) { set_error("no SQ index loaded"); return AEE_EFAILED; }
+  if (kind == 1 && !s.pq.view.residual_bits) return AEE_EBADPARM;
+  const int dim = pqk ? s.pq.view.dim : s.sq.view.dim;
+  const int64_t total = offsets[nq];
+  for (int i = 0; i < nq; ++i)
+    if (offsets[i + 1] < offsets[i] || offsets[0] != 0) return AEE_EBADPARM;
+  if (upload(s.in_queries, queries, static_cast<size_t>(nq) * dim, s.stream) ||
+      upload(s.in_offsets, offsets, nq + 1, s.stream) || upload(s.in_ids, ids, static_cast<size_t>(total), s.stream))
+    return AEE_ENOMEMORY;
+  CK(s.out_dists.ensure(std::max<int64_t>(total, 1) * 4));
+  CK(s.status.ensure(nq * 4));
+  CK(cudaMemsetAsync(s.status.p, 0, nq * 4, s.stream));
+  const int32_t* di = s.in_ids.as<int32_t>();
+  const int64_t* dof = s.in_offsets.as<int64_t>();
+  float* dout = s.out_dists.as<float>();
+  int32_t* dst = s.status.as<int32_t>();
+  if (kind == 0) {
+    const size_t lut = static_cast<size_t>(s.pq.view.m) * s.pq.view.ks;
+    CK(s.luts.ensure(nq * lut * 4));
+    launch_pq_lut(s.pq.view, s.in_queries.as<float>(), nq, s.luts.as<float>(), dst, s.stream);
+    launch_pq_adc(s.pq.view, s.luts.as<float>(), nq, di, dof, dout, dst, s.stream);
+  } else if (kind == 1) {
+    launch_pq_residual(s.pq.view, s.in_queries.as<float>(), nq, di, dof, dout, dst, s.stream);
+  } else if (kind == 2) {
+    launch_sq_coarse(s.sq.view, s.in_queries.as<float>(), nq, di, dof, dout, dst, s.stream);
+  } else {
+    launch_sq_exact(s.sq.view, s.in_queries.as<float>(), nq, di, dof, dout, dst, s.stream);
+  }
+  CK(cudaGetLastError());
+  std::vector<int32_t> hs(nq);
+  if (download(out_dists, dout, static_cast<size_t>(total), s.stream) || download(hs.data(), dst, nq, s.stream))
+    return AEE_EFAILED;
+  CK(cudaStreamSynchronize(s.stream));
+  if (out_status) std::copy(hs.begin(), hs.end(), out_status);
+  for (int32_t x : hs) if (x) { set_error("score failed with status %d", x); return AEE_EFAILED; }
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, const float* queries, int32_t nq,
+                                             const int32_t* cand_ids, int32_t cand_stride,
+                                             const int32_t* cand_counts, int32_t top_k, int32_t* out_ids,
+                                             float* out_dists, int32_t* out_counts, int32_t* out_status) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (nq <= 0 || !queries || !cand_ids || !cand_counts || top_k <= 0 || cand_stride <= 0 || (kind != 0 && kind != 1))
+    return AEE_EBADPARM;
+  if (kind == 1 && (!s.pq.loaded || !s.pq.view.residual_bits)) { set_error("no PQ residual index"); return AEE_EFAILED; }
+  if (kind == 0 && (!s.sq.loaded || !s.sq.view.residual)) { set_error("no SQ residual index"); return AEE_EFAILED; }
+  const int dim = kind == 1 ? s.pq.view.dim : s.sq.view.dim;
+  int cap = 1;
+  for (int i = 0; i < nq; ++i) {
+    if (cand_counts[i] < 0 || cand_counts[i] > cand_stride || cand_counts[i] > 2048) return AEE_EBADPARM;
+    cap = std::max(cap, cand_counts[i]);
+  }
+  if (upload(s.in_queries, queries, static_cast<size_t>(nq) * dim, s.stream) ||
+      upload(s.in_ids, cand_ids, static_cast<size_t>(nq) * cand_stride, s.stream) ||
+      upload(s.in_pool, cand_counts, nq, s.stream))
+    return AEE_ENOMEMORY;
+  CK(s.out_ids.ensure(static_cast<size_t>(nq) * top_k * 4));
+  CK(s.out_dists.ensure(static_cast<size_t>(nq) * top_k * 4));
+  CK(s.out_counts.ensure(nq * 4));
+  CK(s.status.ensure(nq * 4));
+  CK(cudaMemsetAsync(s.status.p, 0, nq * 4, s.stream));
+  launch_refine(kind, s.pq.view, s.sq.view, s.in_queries.as<float>(), nq, s.in_ids.as<int32_t>(), cand_stride,
+                s.in_pool.as<int32_t>(), top_k, cap, s.out_ids.as<int32_t>(), s.out_dists.as<float>(),
+                s.out_counts.as<int32_t>(), s.status.as<int32_t>(), s.stream);
+  CK(cudaGetLastError());
+  std::vector<int32_t> hs(nq);
+  if (download(out_ids, s.out_ids.p, static_cast<size_t>(nq) * top_k, s.stream) ||
+      download(out_dists, s.out_dists.p, static_cast<size_t>(nq) * top_k, s.stream) ||
+      download(out_counts, s.out_counts.p, nq, s.stream) || download(hs.data(), s.status.p, nq, s.stream))
+    return AEE_EFAILED;
+  CK(cudaStreamSynchronize(s.stream));
+  if (out_status) std::copy(hs.begin(), hs.end(), out_status);
+  for (int32_t x : hs) if (x) { set_error("refine failed with status %d", x); return AEE_EFAILED; }
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_sq_load(remote_handle64 h, const RoverSqIndexDesc* desc) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!desc) return AEE_EBADPARM;
+  return load_sq(s, s.sq, desc, desc->l1_bits);
+}
+
+extern "C" AEEResult calculator_rover_sq_unload(remote_handle64 h) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  s.sq.release();
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSearchParams* p, const float* queries,
+                                                int32_t nq, const int32_t* pool_sizes, const RoverSearchOutputs* out) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!valid_params(p) || nq < 0 || !out || !out->ids || !out->dists || !out->counts || out->out_stride <= 0 ||
+      !queries || !pool_sizes)
+    return AEE_EBADPARM;
+  if (nq == 0) return AEE_SUCCESS;
+  if (!s.sq.loaded || !s.sq.view.graph) { set_error("no SQ index with a graph loaded"); return AEE_EFAILED; }
+  if (p->sq_mode == 1 && p->correction && !s.sq.view.residual) { set_error("correction needs residuals"); return AEE_EBADPARM; }
+  const int dim = s.sq.view.dim;
+  std::vector<int32_t> h_pool(pool_sizes, pool_sizes + nq);
+  const int stride = out->out_stride;
+  if (upload(s.in_queries, queries, static_cast<size_t>(nq) * dim, s.stream) ||
+      upload(s.in_pool, pool_sizes, nq, s.stream))
+    return AEE_ENOMEMORY;
+  CK(s.out_ids.ensure(static_cast<size_t>(nq) * stride * 4));
+  CK(s.out_dists.ensure(static_cast<size_t>(nq) * stride * 4));
+  CK(s.out_counts.ensure(nq * 4));
+  CK(s.stats.ensure(static_cast<size_t>(nq) * 32));
+  CK(s.status.ensure(nq * 4));
+  AEEResult r = sq_search_core(s, s.sq, p->sq_mode == 1 ? kSqModeSqmd : kSqModeDsp, p, s.in_queries.as<float>(), nq,
+                               s.in_pool.as<int32_t>(), h_pool, p->sq_mode == 1 ? stride : std::min(stride, p->top_k),
+                               s.out_ids.as<int32_t>(), s.out_dists.as<float>(), stride, s.out_counts.as<int32_t>(),
+                               s.stats.as<unsigned long long>(), s.status.as<int32_t>(), s.stream);
+  if (out->status) std::copy(s.h_status.begin(), s.h_status.begin() + nq, out->status);
+  if (r != AEE_SUCCESS) return r;
+  if (download(out->ids, s.out_ids.p, static_cast<size_t>(nq) * stride, s.stream) ||
+      download(out->dists, s.out_dists.p, static_cast<size_t>(nq) * stride, s.stream) ||
+      download(out->counts, s.out_counts.p, nq, s.stream) ||
+      (out->stats && download(out->stats, s.stats.p, static_cast<size_t>(nq) * 4, s.stream)))
+    return AEE_EFAILED;
+  CK(cudaStreamSynchronize(s.stream));
+  return AEE_SUCCESS;
+}
+
+// ===========================================================================
+// Reference interface (include/calculator.h)
+
+extern "C" int calculator_open(const char* uri, remote_handle64* handle) {
+  (void)uri;
+  if (!handle) return AEE_EBADPARM;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  ++open_count;
+  *handle = static_cast<remote_handle64>(open_count);
+  return AEE_SUCCESS;
+}
+
+extern "C" int calculator_close(remote_handle64 handle) {
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (handle && open_count > 0) --open_count;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_configure(remote_handle64 h, int32 abi_version, int32 l1_bits) {
+  (void)h;
+  if (abi_version != 1 || (l1_bits != 4 && l1_bits != 8)) return AEE_EBADPARM;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  s.l1_bits = l1_bits;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_retrieval_load(remote_handle64 h, const int* graph, int graphLen, const uint8* l1_codes,
+                                               int l1_codesLen, int32 num_vectors, int32 dim, int32 graph_k,
+                                               int32 graph_entry_point, float l1_scale, float l1_zero_point) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  s.legacy.release();
+  s.legacy_dma = false;
+  if (num_vectors <= 0 || dim <= 0 || graph_k <= 0 || dim > 1024) return AEE_EBADPARM;
+  const int cb = s.l1_bits == 4 ? (dim + 1) / 2 : dim;
+  if (graphLen < static_cast<int64_t>(num_vectors) * graph_k || l1_codesLen < static_cast<int64_t>(num_vectors) * cb)
+    return AEE_EBADPARM;
+  RoverSqIndexDesc d{};
+  d.graph = graph;
+  d.num_vectors = num_vectors;
+  d.graph_degree = graph_k;
+  d.graph_entry = (graph_entry_point >= 0 && graph_entry_point < num_vectors) ? graph_entry_point : -1;
+  d.dim = dim;
+  d.l1_codes = l1_codes;
+  d.l1_scale = l1_scale;
+  d.l1_zero = l1_zero_point;
+  return load_sq(s, s.legacy, &d, s.l1_bits) == AEE_SUCCESS ? AEE_SUCCESS : AEE_ENOMEMORY;
+}
+
+extern "C" AEEResult calculator_retrieval_search(remote_handle64 h, const float* query, int queryLen,
+                                                 int32 entry_points, int32 expand_count, int32 pool_size,
+                                                 int32 num_out, int* candidate_ids, int candidate_idsLen,
+                                                 float* candidate_dists, int candidate_distsLen,
+                                                 int32* actual_count) {
+  (void)h;
+  if (!actual_count) return AEE_EBADPARM;
+  *actual_count = 0;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (!s.legacy.loaded || !s.legacy.view.graph) return AEE_EFAILED;
+  if (queryLen < s.legacy.view.dim || pool_size <= 0 || num_out <= 0) return AEE_EBADPARM;
+  if (candidate_idsLen < num_out || candidate_distsLen < num_out) return AEE_EBADPARM;
+  if (std::min(expand_count, s.legacy.view.degree) <= 0) return AEE_EBADPARM;
+  // with no entry points the reference's loop seeds nothing and returns an
+  // empty result (retrieval_async_dsp_search.c:438)
+  if (entry_points <= 0) return AEE_SUCCESS;
+  RoverSearchParams p{};
+  p.size = sizeof(p);
+  p.entry_points = entry_points;
+  p.seed = 42u;
+  p.expand_count = expand_count;
+  const int pool = std::min(pool_size, 2000);
+  std::vector<int32_t> h_pool(1, pool);
+  if (upload(s.in_queries, query, s.legacy.view.dim, s.stream) || upload(s.in_pool, h_pool.data(), 1, s.stream))
+    return AEE_ENOMEMORY;
+  CK(s.out_ids.ensure(num_out * 4));
+  CK(s.out_dists.ensure(num_out * 4));
+  CK(s.out_counts.ensure(4));
+  CK(s.status.ensure(4));
+  AEEResult r = sq_search_core(s, s.legacy, kSqModeDsp, &p, s.in_queries.as<float>(), 1, s.in_pool.as<int32_t>(),
+                               h_pool, num_out, s.out_ids.as<int32_t>(), s.out_dists.as<float>(), num_out,
+                               s.out_counts.as<int32_t>(), nullptr, s.status.as<int32_t>(), s.stream);
+  if (r != AEE_SUCCESS) return AEE_EFAILED;
+  int32_t count = 0;
+  if (download(&count, s.out_counts.p, 1, s.stream)) return AEE_EFAILED;
+  CK(cudaStreamSynchronize(s.stream));
+  if (download(candidate_ids, s.out_ids.p, count, s.stream) ||
+      download(candidate_dists, s.out_dists.p, count, s.stream))
+    return AEE_EFAILED;
+  CK(cudaStreamSynchronize(s.stream));
+  *actual_count = count;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_retrieval_unload(remote_handle64 h) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  s.legacy.release();
+  s.legacy_dma = false;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_retrieval_load_dma(remote_handle64 h, int32 fd_graph, const int32* fd_l1_codes,
+                                                   int fd_l1_codesLen, int32 l1_chunk_vectors, int32 num_vectors,
+                                                   int32 dim, int32 graph_k, int32 graph_entry_point, float l1_scale,
+                                                   float l1_zero_point) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  s.legacy.release();
+  s.legacy_dma = false;
+  if (fd_graph < -1 || num_vectors <= 0 || dim <= 0 || graph_k <= 0 || dim > 1024) return AEE_EBADPARM;
+  if (!fd_l1_codes || fd_l1_codesLen < 1 || fd_l1_codesLen > 16 || l1_chunk_vectors <= 0) return AEE_EBADPARM;
+  const int cb = s.l1_bits == 4 ? (dim + 1) / 2 : dim;
+  std::vector<uint8_t> codes(static_cast<size_t>(num_vectors) * cb);
+  size_t done = 0;
+  for (int c = 0; c < fd_l1_codesLen; ++c) {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    if (rover_rpcmem_lookup(fd_l1_codes[c], &ptr, &bytes) != 0) return AEE_EFAILED;
+    const size_t want = std::min(static_cast<size_t>(l1_chunk_vectors) * cb, codes.size() - done);
+    if (bytes < want) return AEE_EFAILED;
+    std::memcpy(codes.data() + done, ptr, want);
+    done += want;
+  }
+  if (done != codes.size()) return AEE_EBADPARM;
+  RoverSqIndexDesc d{};
+  void* gptr = nullptr;
+  size_t gbytes = 0;
+  if (fd_graph != -1) {
+    if (rover_rpcmem_lookup(fd_graph, &gptr, &gbytes) != 0 ||
+        gbytes < static_cast<size_t>(num_vectors) * graph_k * sizeof(int32_t))
+      return AEE_EFAILED;
+    d.graph = static_cast<const int32_t*>(gptr);
+  }
+  d.num_vectors = num_vectors;
+  d.graph_degree = graph_k;
+  d.graph_entry = (graph_entry_point >= 0 && graph_entry_point < num_vectors) ? graph_entry_point : -1;
+  d.dim = dim;
+  d.l1_codes = codes.data();
+  d.l1_scale = l1_scale;
+  d.l1_zero = l1_zero_point;
+  if (load_sq(s, s.legacy, &d, s.l1_bits) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  s.legacy_dma = true;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_retrieval_unload_dma(remote_handle64 h) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (!s.legacy_dma) return AEE_SUCCESS;
+  s.legacy.release();
+  s.legacy_dma = false;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_retrieval_pure_pq_load_dma(
+    remote_handle64 h, const int32* fd_pq_codes, int fd_pq_codesLen, const int32* pq_chunk_vector_counts,
+    int pq_chunk_vector_countsLen, int32 pq_chunk_vectors, const float* pq_codebook, int pq_codebookLen,
+    int32 num_vectors, int32 dim, int32 pq_m, int32 pq_ks, int32 pq_subdim, int32 pq_code_bytes,
+    const uint8* index_uuid, int index_uuidLen) {
+  (void)h;
+  // argument checks of retrieval_async_dsp_search.c:713-751
+  if (!fd_pq_codes || !pq_chunk_vector_counts || !pq_codebook || !index_uuid || fd_pq_codesLen <= 0 ||
+      fd_pq_codesLen > 64 || pq_chunk_vector_countsLen != fd_pq_codesLen || pq_chunk_vectors <= 0 ||
+      num_vectors <= 0 || dim <= 0 || pq_m <= 0 || (pq_ks != 16 && pq_ks != 256) || pq_subdim <= 0 ||
+      pq_m > INT32_MAX / pq_subdim || pq_m * pq_subdim != dim ||
+      pq_code_bytes != (pq_ks == 16 ? pq_m / 2 + pq_m % 2 : pq_m) || index_uuidLen != 16)
+    return AEE_EBADPARM;
+  const size_t book = static_cast<size_t>(pq_m) * pq_ks * pq_subdim;
+  if (book > static_cast<size_t>(INT32_MAX) || pq_codebookLen != static_cast<int>(book)) return AEE_EBADPARM;
+  uint64_t total = 0;
+  for (int i = 0; i < fd_pq_codesLen; ++i) {
+    const int count = pq_chunk_vector_counts[i];
+    if (fd_pq_codes[i] < 0 || count <= 0 || count > pq_chunk_vectors ||
+        total > static_cast<uint64_t>(num_vectors) - static_cast<uint64_t>(count))
+      return AEE_EBADPARM;
+    if (i + 1 < fd_pq_codesLen && count != pq_chunk_vectors) return AEE_EBADPARM;
+    total += count;
+  }
+  if (total != static_cast<uint64_t>(num_vectors)) return AEE_EBADPARM;
+  for (size_t i = 0; i < book; ++i)
+    if (!(pq_codebook[i] == pq_codebook[i]) || pq_codebook[i] > 3.402823466e+38F || pq_codebook[i] < -3.402823466e+38F)
+      return AEE_EBADPARM;
+  std::vector<uint8_t> codes(static_cast<size_t>(num_vectors) * pq_code_bytes);
+  size_t done = 0;
+  for (int i = 0; i < fd_pq_codesLen; ++i) {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    const size_t want = static_cast<size_t>(pq_chunk_vector_counts[i]) * pq_code_bytes;
+    if (rover_rpcmem_lookup(fd_pq_codes[i], &ptr, &bytes) != 0 || bytes < want) return AEE_EFAILED;
+    std::memcpy(codes.data() + done, ptr, want);
+    done += want;
+  }
+  RoverPqIndexDesc d{};
+  d.num_vectors = num_vectors;
+  d.graph_entry = -1;
+  d.dim = dim;
+  d.codes = codes.data();
+  d.codebook = pq_codebook;
+  d.m = pq_m;
+  d.ks = pq_ks;
+  d.subdim = pq_subdim;
+  d.code_bytes = pq_code_bytes;
+  return calculator_rover_pq_load(h, &d);
+}
+
+extern "C" AEEResult calculator_retrieval_pure_pq_unload_dma(remote_handle64 h) {
+  return calculator_rover_pq_unload(h);
+}
+
+// Lane-protocol sessions and the remaining legacy services.
+extern "C" AEEResult calculator_retrieval_pure_pq_sqmd_run(remote_handle64 h, int32 fd_sqmd_ctrl, int32 fd_query_lut,
+                                                           int32 lane_count, int32 work_items_cap) {
+  (void)h; (void)fd_sqmd_ctrl; (void)fd_query_lut; (void)lane_count; (void)work_items_cap;
+  set_error("pure-PQ lane sessions are not available in this build");
+  return AEE_EUNSUPPORTED;
+}
+
+extern "C" AEEResult calculator_retrieval_expand_sqmd(remote_handle64 h, const float* query, int queryLen,
+                                                      int32 query_dim, int32 fd_sqmd_ctrl, int32 lane_count,
+                                                      int32 work_items_cap) {
+  (void)h; (void)query; (void)queryLen; (void)query_dim; (void)fd_sqmd_ctrl; (void)lane_count; (void)work_items_cap;
+  set_error("SQMD lane sessions are not available in this build");
+  return AEE_EUNSUPPORTED;
+}
+
+extern "C" AEEResult calculator_retrieval_expand_sqmd_run(remote_handle64 h, int32 fd_sqmd_ctrl, int32 lane_count,
+                                                          int32 work_items_cap) {
+  (void)h; (void)fd_sqmd_ctrl; (void)lane_count; (void)work_items_cap;
+  set_error("SQMD lane sessions are not available in this build");
+  return AEE_EUNSUPPORTED;
+}
+
+extern "C" AEEResult calculator_retrieval_search_db(remote_handle64 h, const float* query_a, int query_aLen,
+                                                    const float* query_b, int query_bLen, int32 fd_expansion_buf,
+                                                    int32 entry_points, int32 expand_count, int32 pool_size,
+                                                    int32 num_out, int* candidate_ids_a, int candidate_ids_aLen,
+                                                    float* candidate_dists_a, int candidate_dists_aLen,
+                                                    int32* actual_count_a, int* candidate_ids_b, int candidate_ids_bLen,
+                                                    float* candidate_dists_b, int candidate_dists_bLen,
+                                                    int32* actual_count_b) {
+  (void)h; (void)query_a; (void)query_aLen; (void)query_b; (void)query_bLen; (void)fd_expansion_buf;
+  (void)entry_points; (void)expand_count; (void)pool_size; (void)num_out; (void)candidate_ids_a;
+  (void)candidate_ids_aLen; (void)candidate_dists_a; (void)candidate_dists_aLen; (void)candidate_ids_b;
+  (void)candidate_ids_bLen; (void)candidate_dists_b; (void)candidate_dists_bLen;
+  if (actual_count_a) *actual_count_a = 0;
+  if (actual_count_b) *actual_count_b = 0;
+  set_error("DB-pair search is not available in this build");
+  return AEE_EUNSUPPORTED;
+}
+
+extern "C" AEEResult calculator_retrieval_async_submit(remote_handle64 h, const float* query, int queryLen,
+                                                       const int* candidate_ids, int candidate_idsLen,
+                                                       const uint8* compressed_batch, int compressed_batchLen,
+                                                       int32 dim, int32 num_candidates, float scale, float zero_point,
+                                                       int32* task_id) {
+  (void)h; (void)query; (void)queryLen; (void)candidate_ids; (void)candidate_idsLen; (void)compressed_batch;
+  (void)compressed_batchLen; (void)dim; (void)num_candidates; (void)scale; (void)zero_point;
+  if (task_id) *task_id = -1;
+  return AEE_EUNSUPPORTED;
+}
+
+extern "C" AEEResult calculator_retrieval_async_poll(remote_handle64 h, int32 task_id, int32* status, int* result_ids,
+                                                     int result_idsLen, float* distances, int distancesLen,
+                                                     int32* num_results) {
+  (void)h; (void)task_id; (void)result_ids; (void)result_idsLen; (void)distances; (void)distancesLen;
+  if (status) *status = 4;  // RETRIEVAL_ASYNC_DEMO_STATUS_NOT_FOUND
+  if (num_results) *num_results = 0;
+  return AEE_EUNSUPPORTED;
+}
+
+extern "C" AEEResult calculator_retrieval_async_reset(remote_handle64 h) {
+  (void)h;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_retrieval_rnn_l2_load_dma(remote_handle64 h, int32 fd_base, int32 num_vectors,
+                                                          int32 dim) {
+  (void)h; (void)fd_base; (void)num_vectors; (void)dim;
+  return AEE_EUNSUPPORTED;
+}
+
+extern "C" AEEResult calculator_retrieval_rnn_l2_batch(remote_handle64 h, const int* ids_a, int ids_aLen,
+                                                       const int* ids_b, int ids_bLen, int32 pair_count,
+                                                       float* distances, int distancesLen) {
+  (void)h; (void)ids_a; (void)ids_aLen; (void)ids_b; (void)ids_bLen; (void)pair_count; (void)distances;
+  (void)distancesLen;
+  return AEE_EUNSUPPORTED;
+}
+
+extern "C" AEEResult calculator_retrieval_rnn_l2_unload_dma(remote_handle64 h) {
+  (void)h;
+  return AEE_SUCCESS;
+}

@@ -1,0 +1,387 @@
+// distance.cu -- batched distance kernels (the standalone K1/K2/K3/K5/K6
+// kernels) for scoring explicit (query, id) lists: the lane-protocol
+// sessions, the score-ids entry points and the re-rank of host-supplied
+// candidate lists use them.
+//
+//  pq_lut_kernel       retrieval_pq_build_lut      (retrieval_pq_core.c:362)
+//  pq_adc_kernel       retrieval_pq_adc_ids_batch  (retrieval_pq_core.c:280-360)
+//  pq_residual_kernel  retrieval_pq_residual_query_evaluate (retrieval_pq_residual.c:983)
+//  sq_coarse_kernel    retrieval_compute_int8_native_distance_u8 / int4 (l1_int8_core.c:119-169)
+//  sq_exact_kernel     retrieval_demo_exact_distance_residual (retrieval_rpc_demo_support.c:1397)
+//  refine_kernel       refine_impl (retrieval_final_refine.c:256-292)
+//
+// Each query's id list is offsets[q] .. offsets[q+1] of a flat id array.
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace rover {
+
+__device__ __forceinline__ const uint8_t* residual_row(const PqIndexView& ix, int32_t id) {
+  const uint32_t u = static_cast<uint32_t>(id);
+  const uint32_t block = u / static_cast<uint32_t>(ix.vpb);
+  return ix.residual + static_cast<size_t>(block) * 4096u +
+         (u - block * static_cast<uint32_t>(ix.vpb)) * static_cast<uint32_t>(ix.rcb);
+}
+
+__global__ void pq_lut_kernel(PqIndexView ix, const float* __restrict__ queries, int nq,
+                              float* __restrict__ luts, int32_t* status) {
+  const int qi = blockIdx.x;
+  const float* q = queries + static_cast<size_t>(qi) * ix.dim;
+  const int entries = ix.m * ix.ks;
+  bool bad = false;
+  for (int e = threadIdx.x; e < entries; e += blockDim.x) {
+    const int m = e / ix.ks;
+    const float* cen = ix.codebook + static_cast<size_t>(e) * ix.subdim;
+    const float* qs = q + m * ix.subdim;
+    float acc = 0.0f;
+    for (int j = 0; j < ix.subdim; ++j) {
+      const float diff = fsub(__ldg(qs + j), __ldg(cen + j));
+      acc = fadd(acc, fmul(diff, diff));
+    }
+    bad |= !isfinite(acc);
+    luts[static_cast<size_t>(qi) * entries + e] = acc;
+  }
+  if (bad) status[qi] = kStatusNumeric;
+}
+
+// One CTA per query: the query's LUT is staged in shared memory, then each
+// thread gathers one candidate's code row and sums its M LUT entries in
+// subspace order.
+__global__ void pq_adc_kernel(PqIndexView ix, const float* __restrict__ luts, int nq,
+                              const int32_t* __restrict__ ids, const int64_t* __restrict__ offsets,
+                              float* __restrict__ out, int32_t* status) {
+  extern __shared__ __align__(16) float lut[];
+  const int qi = blockIdx.y;
+  const int entries = ix.m * ix.ks;
+  const float* src = luts + static_cast<size_t>(qi) * entries;
+  for (int e = threadIdx.x; e < entries; e += blockDim.x) lut[e] = __ldg(src + e);
+  __syncthreads();
+  const int64_t begin = offsets[qi], end = offsets[qi + 1];
+  bool bad = false;
+  for (int64_t i = begin + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < end;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t id = __ldg(ids + i);
+    if (id < 0 || id >= ix.n) { bad = true; continue; }
+    const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
+    float acc = 0.0f;
+    if (ix.ks == 256 && (ix.code_bytes & 15) == 0) {
+      for (int w = 0; w < ix.code_bytes; w += 16) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(code + w));
+        const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int m = w + k;
+          const uint32_t c = (words[k >> 2] >> (8 * (k & 3))) & 255u;
+          acc = fadd(acc, lut[m * 256 + c]);
+        }
+      }
+    } else {
+      for (int m = 0; m < ix.m; ++m) {
+        const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
+        acc = fadd(acc, lut[m * ix.ks + c]);
+      }
+    }
+    if (!isfinite(acc)) bad = true;
+    out[i] = acc;
+  }
+  if (bad) status[qi] = kStatusNumeric;
+}
+
+__global__ void pq_residual_kernel(PqIndexView ix, const float* __restrict__ queries, int nq,
+                                   const int32_t* __restrict__ ids,
+                                   const int64_t* __restrict__ offsets, float* __restrict__ out,
+                                   int32_t* status) {
+  extern __shared__ __align__(16) float qs[];
+  const int qi = blockIdx.y;
+  for (int d = threadIdx.x; d < ix.dim; d += blockDim.x)
+    qs[d] = queries[static_cast<size_t>(qi) * ix.dim + d];
+  __syncthreads();
+  const int64_t begin = offsets[qi], end = offsets[qi + 1];
+  bool bad = false;
+  for (int64_t i = begin + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < end;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t id = __ldg(ids + i);
+    if (id < 0 || id >= ix.n) { bad = true; continue; }
+    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+    if (!isfinite(qp.x) || !isfinite(qp.y) || !(qp.x > 0.0f)) { bad = true; continue; }
+    const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
+    const uint8_t* res = residual_row(ix, id);
+    float acc = 0.0f;
+    int dim = 0;
+    for (int m = 0; m < ix.m; ++m) {
+      const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
+      const float* cen = ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim;
+      for (int j = 0; j < ix.subdim; ++j, ++dim) {
+        const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, dim))
+                                                 : static_cast<uint32_t>(__ldg(res + dim));
+        const float x = fadd(fadd(__ldg(cen + j), fmul(u8f(r), qp.x)), qp.y);
+        const float dq = fsub(qs[dim], x);
+        acc = fadd(acc, fmul(dq, dq));
+      }
+    }
+    if (!isfinite(acc)) bad = true;
+    out[i] = acc;
+  }
+  if (bad) status[qi] = kStatusNumeric;
+}
+
+// Query codes as retrieval_quantize_query_u8/_u4 produce them
+// (l1_int8_core.c:13-63): roundf((q - zero) * (1 / scale)), clamped.
+__device__ __forceinline__ void quantize_query(const SqIndexView& ix, const float* q, uint8_t* qc) {
+  const float inv = __frcp_rn(ix.l1_scale);
+  const int levels = ix.l1_bits == 4 ? 15 : 255;
+  for (int d = threadIdx.x; d < ix.dim; d += blockDim.x) {
+    int c = static_cast<int>(roundf(fmul(fsub(q[d], ix.l1_zero), inv)));
+    qc[d] = static_cast<uint8_t>(c < 0 ? 0 : (c > levels ? levels : c));
+  }
+}
+
+__global__ void sq_coarse_kernel(SqIndexView ix, const float* __restrict__ queries, int nq,
+                                 const int32_t* __restrict__ ids, const int64_t* __restrict__ offsets,
+                                 float* __restrict__ out, int32_t* status) {
+  extern __shared__ __align__(16) uint8_t qc[];
+  const int qi = blockIdx.y;
+  quantize_query(ix, queries + static_cast<size_t>(qi) * ix.dim, qc);
+  __syncthreads();
+  const int64_t begin = offsets[qi], end = offsets[qi + 1];
+  const float scale_sq = fmul(ix.l1_scale, ix.l1_scale);
+  bool bad = false;
+  for (int64_t i = begin + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < end;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t id = __ldg(ids + i);
+    if (id < 0 || id >= ix.n) { bad = true; continue; }
+    const uint8_t* x = ix.l1 + static_cast<size_t>(id) * ix.l1_code_bytes;
+    long long acc = 0;
+    if (ix.l1_bits == 8 && (ix.dim & 15) == 0) {
+      int iacc = 0;
+      for (int d = 0; d < ix.dim; d += 16) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(x + d));
+        const uint4 w = *reinterpret_cast<const uint4*>(qc + d);
+        iacc += __dp4a(w.x, w.x, 0u) - 2 * static_cast<int>(__dp4a(w.x, v.x, 0u)) + __dp4a(v.x, v.x, 0u);
+        iacc += __dp4a(w.y, w.y, 0u) - 2 * static_cast<int>(__dp4a(w.y, v.y, 0u)) + __dp4a(v.y, v.y, 0u);
+        iacc += __dp4a(w.z, w.z, 0u) - 2 * static_cast<int>(__dp4a(w.z, v.z, 0u)) + __dp4a(v.z, v.z, 0u);
+        iacc += __dp4a(w.w, w.w, 0u) - 2 * static_cast<int>(__dp4a(w.w, v.w, 0u)) + __dp4a(v.w, v.w, 0u);
+        if ((d & 1023) == 1008) { acc += iacc; iacc = 0; }
+      }
+      acc += iacc;
+    } else if (ix.l1_bits == 8) {
+      for (int d = 0; d < ix.dim; ++d) {
+        const int df = static_cast<int>(qc[d]) - static_cast<int>(__ldg(x + d));
+        acc += df * df;
+      }
+    } else {
+      for (int d = 0; d < ix.dim; ++d) {
+        const int df = static_cast<int>(qc[d] & 15) - nibble(x, d);
+        acc += df * df;
+      }
+    }
+    out[i] = fmul(__ll2float_rn(acc), scale_sq);
+  }
+  if (bad) status[qi] = kStatusBadParam;
+}
+
+__global__ void sq_exact_kernel(SqIndexView ix, const float* __restrict__ queries, int nq,
+                                const int32_t* __restrict__ ids, const int64_t* __restrict__ offsets,
+                                float* __restrict__ out, int32_t* status) {
+  extern __shared__ __align__(16) float qv[];
+  const int qi = blockIdx.y;
+  for (int d = threadIdx.x; d < ix.dim; d += blockDim.x) qv[d] = queries[static_cast<size_t>(qi) * ix.dim + d];
+  __syncthreads();
+  const int64_t begin = offsets[qi], end = offsets[qi + 1];
+  bool bad = false;
+  for (int64_t i = begin + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < end;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t id = __ldg(ids + i);
+    if (id < 0 || id >= ix.n) { bad = true; continue; }
+    const uint8_t* l1 = ix.l1 + static_cast<size_t>(id) * ix.l1_code_bytes;
+    const uint8_t* res = ix.residual ? ix.residual + static_cast<size_t>(id) * ix.rcb : nullptr;
+    float rs = 0.0f, rz = 0.0f, dist = 0.0f;
+    if (res) {
+      const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+      rs = qp.x;
+      rz = qp.y;
+    }
+    for (int d = 0; d < ix.dim; ++d) {
+      const uint32_t c = ix.l1_bits == 4 ? static_cast<uint32_t>(nibble(l1, d)) : __ldg(l1 + d);
+      float value = fadd(fmul(u8f(c), ix.l1_scale), ix.l1_zero);
+      if (res) {
+        const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, d)) : __ldg(res + d);
+        value = fadd(value, fadd(fmul(u8f(r), rs), rz));
+      }
+      const float diff = fsub(qv[d], value);
+      dist = fadd(dist, fmul(diff, diff));
+    }
+    out[i] = dist;
+  }
+  if (bad) status[qi] = kStatusBadParam;
+}
+
+// Decode of one vector for the final refine: PQ  ((c + code*s) + z), SQ
+// (l1*ls + lz) + (r*rs + rz), each product and sum rounded to float
+// (pq_residual_decode_value :946, retrieval_final_refine_decode_sq :55).
+__device__ __forceinline__ bool refine_value(int kind, const PqIndexView& pq, const SqIndexView& sq,
+                                             int32_t id, int d, const uint8_t* a, const uint8_t* b,
+                                             float2 qp, float* out) {
+  float x;
+  if (kind == 1) {
+    const int m = d / pq.subdim, j = d - m * pq.subdim;
+    const int c = pq.ks == 16 ? nibble(a, m) : __ldg(a + m);
+    const uint32_t r = pq.residual_bits == 4 ? static_cast<uint32_t>(nibble(b, d)) : __ldg(b + d);
+    x = fadd(fadd(__ldg(pq.codebook + (static_cast<size_t>(m) * pq.ks + c) * pq.subdim + j),
+                  fmul(u8f(r), qp.x)), qp.y);
+  } else {
+    const uint32_t c = sq.l1_bits == 4 ? static_cast<uint32_t>(nibble(a, d)) : __ldg(a + d);
+    const uint32_t r = sq.residual_bits == 4 ? static_cast<uint32_t>(nibble(b, d)) : __ldg(b + d);
+    x = fadd(fadd(fmul(u8f(c), sq.l1_scale), sq.l1_zero), fadd(fmul(u8f(r), qp.x), qp.y));
+  }
+  *out = x;
+  return isfinite(x);
+}
+
+// One warp per query: FP64 distances of the candidates on their decoded
+// vectors, sorted by (distance, id), top k kept.
+__global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const float* __restrict__ queries,
+                              int nq, const int32_t* __restrict__ cand_ids, int cand_stride,
+                              const int32_t* __restrict__ cand_counts, int top_k, int capacity,
+                              int32_t* out_ids, float* out_dists, int32_t* out_counts, int32_t* status) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (qi >= nq) return;
+  const int dim = kind == 1 ? pq.dim : sq.dim;
+  const int n = kind == 1 ? pq.n : sq.n;
+  double* sd = reinterpret_cast<double*>(smem) + static_cast<size_t>(warp) * capacity;
+  int32_t* si = reinterpret_cast<int32_t*>(reinterpret_cast<double*>(smem) + static_cast<size_t>(blockDim.x >> 5) * capacity) +
+                static_cast<size_t>(warp) * capacity;
+  const float* q = queries + static_cast<size_t>(qi) * dim;
+  const int count = cand_counts[qi];
+  int np2 = 1;
+  while (np2 < count) np2 <<= 1;
+  bool bad = count < 0 || count > capacity;
+  for (int d = lane; d < dim; d += kWarp) bad |= !isfinite(q[d]);
+  if (!__any_sync(kFullMask, bad)) {
+    for (int i = lane; i < np2; i += kWarp) {
+      if (i < count) {
+        const int32_t id = cand_ids[static_cast<size_t>(qi) * cand_stride + i];
+        if (id < 0 || id >= n) { bad = true; continue; }
+        const uint8_t* a;
+        const uint8_t* b;
+        float2 qp;
+        if (kind == 1) {
+          a = pq.codes + static_cast<size_t>(id) * pq.code_bytes;
+          b = residual_row(pq, id);
+          qp = __ldg(reinterpret_cast<const float2*>(pq.qparams) + id);
+          if (!isfinite(qp.x) || !(qp.x > 0.0f) || !isfinite(qp.y)) bad = true;
+        } else {
+          a = sq.l1 + static_cast<size_t>(id) * sq.l1_code_bytes;
+          b = sq.residual + static_cast<size_t>(id) * sq.rcb;
+          qp = __ldg(reinterpret_cast<const float2*>(sq.qparams) + id);
+          if (!isfinite(sq.l1_scale) || !(sq.l1_scale > 0.0f) || !isfinite(sq.l1_zero) ||
+              !isfinite(qp.x) || qp.x < 0.0f || !isfinite(qp.y)) bad = true;
+        }
+        double dist = 0.0;
+        for (int d = 0; d < dim; ++d) {
+          float x;
+          if (!refine_value(kind, pq, sq, id, d, a, b, qp, &x)) bad = true;
+          const double delta = __dsub_rn(static_cast<double>(q[d]), static_cast<double>(x));
+          dist = __dadd_rn(dist, __dmul_rn(delta, delta));
+        }
+        if (!isfinite(dist) || dist >= 3.4028234663852886e38) bad = true;
+        sd[i] = dist;
+        si[i] = id;
+      } else {
+        sd[i] = __longlong_as_double(0x7ff0000000000000ll);
+        si[i] = 0x7fffffff;
+      }
+    }
+  }
+  if (__any_sync(kFullMask, bad)) {
+    if (lane == 0) status[qi] = kStatusNumeric;
+    return;
+  }
+  __syncwarp();
+  // duplicate ids are rejected by the reference (refine_impl :269)
+  for (int kk = 2; kk <= np2; kk <<= 1) {
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < np2; i += kWarp) {
+        const int p = i ^ j;
+        if (p > i) {
+          const bool up = (i & kk) == 0;
+          const double x = sd[i], y = sd[p];
+          const int32_t ix = si[i], iy = si[p];
+          const bool gt = (x > y) || (x == y && ix > iy);
+          if (up == gt) { sd[i] = y; sd[p] = x; si[i] = iy; si[p] = ix; }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  bool dup = false;
+  for (int i = lane + 1; i < count; i += kWarp) dup |= (si[i] == si[i - 1] && sd[i] == sd[i - 1]);
+  if (__any_sync(kFullMask, dup)) {
+    if (lane == 0) status[qi] = kStatusBadParam;
+    return;
+  }
+  const int outn = count < top_k ? count : top_k;
+  for (int i = lane; i < outn; i += kWarp) {
+    out_ids[static_cast<size_t>(qi) * top_k + i] = si[i];
+    out_dists[static_cast<size_t>(qi) * top_k + i] = static_cast<float>(sd[i]);
+  }
+  if (lane == 0) out_counts[qi] = outn;
+}
+
+// ---------------------------------------------------------------------------
+
+void launch_pq_lut(const PqIndexView& ix, const float* queries, int nq, float* luts,
+                   int32_t* status, cudaStream_t s) {
+  if (nq <= 0) return;
+  pq_lut_kernel<<<nq, 256, 0, s>>>(ix, queries, nq, luts, status);
+}
+
+void launch_pq_adc(const PqIndexView& ix, const float* luts, int nq, const int32_t* ids,
+                   const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
+  if (nq <= 0) return;
+  const size_t smem = static_cast<size_t>(ix.m) * ix.ks * sizeof(float);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(pq_adc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  dim3 grid(8, nq);
+  pq_adc_kernel<<<grid, 256, smem, s>>>(ix, luts, nq, ids, offsets, out, status);
+}
+
+void launch_pq_residual(const PqIndexView& ix, const float* queries, int nq, const int32_t* ids,
+                        const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
+  if (nq <= 0) return;
+  dim3 grid(8, nq);
+  pq_residual_kernel<<<grid, 128, ix.dim * sizeof(float), s>>>(ix, queries, nq, ids, offsets, out, status);
+}
+
+void launch_sq_coarse(const SqIndexView& ix, const float* queries, int nq, const int32_t* ids,
+                      const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
+  if (nq <= 0) return;
+  dim3 grid(8, nq);
+  sq_coarse_kernel<<<grid, 128, (ix.dim + 15) & ~15, s>>>(ix, queries, nq, ids, offsets, out, status);
+}
+
+void launch_sq_exact(const SqIndexView& ix, const float* queries, int nq, const int32_t* ids,
+                     const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
+  if (nq <= 0) return;
+  dim3 grid(8, nq);
+  sq_exact_kernel<<<grid, 128, ix.dim * sizeof(float), s>>>(ix, queries, nq, ids, offsets, out, status);
+}
+
+void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const float* queries,
+                   int nq, const int32_t* cand_ids, int cand_stride, const int32_t* cand_counts,
+                   int top_k, int capacity, int32_t* out_ids, float* out_dists,
+                   int32_t* out_counts, int32_t* status, cudaStream_t s) {
+  if (nq <= 0) return;
+  int cap = 1;
+  while (cap < capacity) cap <<= 1;
+  const int warps = 4;
+  const size_t smem = static_cast<size_t>(warps) * cap * 12;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  refine_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, s>>>(kind, pq, sq, queries, nq, cand_ids, cand_stride,
+                                                                   cand_counts, top_k, cap, out_ids, out_dists,
+                                                                   out_counts, status);
+}
+
+}  // namespace rover

@@ -1,0 +1,102 @@
+// kernels.h -- launch-side view of the search and distance kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace rover {
+
+constexpr int kSearchWarps = 4;   // query warps per CTA
+constexpr int kMaxBatch = 128;    // max neighbours scored per expansion
+
+struct PqSearchArgs {
+  PqIndexView ix;
+  const float* queries;          // [nq][dim], device
+  int32_t nq;
+  const int32_t* pool_sizes;     // [nq] beam width L per query
+  const int32_t* top_ks;         // [nq] or null (then top_k)
+  int32_t top_k;
+  int32_t entry_points, graph_entry;
+  uint32_t seed;
+  int32_t expand_count;
+  int32_t correction;
+  int32_t refine_budget;         // 0 = no final refine
+  int32_t max_pool;              // list capacity per warp (>= every pool size)
+  // outputs (device)
+  int32_t* pool_ids; float* pool_dists; int32_t pool_stride; int32_t* pool_counts;
+  int32_t* out_ids; float* out_dists; int32_t out_stride; int32_t* out_counts;
+  unsigned long long* stats;     // [nq][4] {scored, corrected, expanded, dedup}
+  int32_t* status;               // [nq]
+  // scratch (device)
+  unsigned long long* visited;   // per warp slot: visited_mask + 1 entries
+  uint32_t visited_mask;
+  uint32_t gen_base;             // generation of query 0 (queries use gen_base + qi)
+  unsigned int* next_query;      // work counter, zero at launch
+  // shared-memory layout per warp
+  int32_t smem_per_warp, smem_query_bytes, smem_refine_offset, refine_capacity;
+};
+
+__global__ void pq_search_kernel(PqSearchArgs a);
+
+// Layout of the per-warp shared-memory slice of pq_search_kernel.
+inline void pq_search_layout(PqSearchArgs* a, int refine_budget) {
+  const int qbytes = ((a->ix.dim * 4) + 15) & ~15;
+  a->smem_query_bytes = qbytes;
+  int off = qbytes + a->max_pool * 8 + kMaxBatch * 8 + kMaxBatch * 4;
+  off = (off + 15) & ~15;
+  a->smem_refine_offset = off;
+  int cap = 0;
+  if (refine_budget > 0) {
+    cap = 1;
+    while (cap < refine_budget) cap <<= 1;
+  }
+  a->refine_capacity = cap;
+  a->smem_per_warp = (off + cap * 12 + 15) & ~15;
+}
+
+// ---- SQ search (heap-exact) ----------------------------------------------
+
+enum SqSearchMode : int32_t { kSqModeDsp = 0, kSqModeSqmd = 1 };
+
+struct SqSearchArgs {
+  SqIndexView ix;
+  const float* queries; int32_t nq;
+  const int32_t* pool_sizes;
+  int32_t mode;                  // kSqModeDsp (a15) or kSqModeSqmd (a12)
+  int32_t entry_points, graph_entry;
+  uint32_t seed;
+  int32_t expand_count;
+  int32_t correction;            // SQMD only
+  int32_t num_out;               // DSP mode: outputs per query
+  int32_t max_pool;              // pool heap capacity per slot
+  int32_t frontier_cap;          // frontier heap capacity per slot
+  int32_t* out_ids; float* out_dists; int32_t out_stride; int32_t* out_counts;
+  unsigned long long* stats;     // [nq][4]
+  int32_t* status;
+  unsigned long long* visited; uint32_t visited_mask; uint32_t gen_base;
+  uint64_t* heaps;               // per slot: max_pool + frontier_cap entries
+  unsigned int* next_query;
+};
+
+__global__ void sq_search_kernel(SqSearchArgs a);
+
+// ---- batched distance kernels ---------------------------------------------
+
+void launch_pq_lut(const PqIndexView& ix, const float* queries, int nq, float* luts,
+                   int32_t* status, cudaStream_t s);
+void launch_pq_adc(const PqIndexView& ix, const float* luts, int nq, const int32_t* ids,
+                   const int64_t* offsets, float* out, int32_t* status, cudaStream_t s);
+void launch_pq_residual(const PqIndexView& ix, const float* queries, int nq, const int32_t* ids,
+                        const int64_t* offsets, float* out, int32_t* status, cudaStream_t s);
+void launch_sq_coarse(const SqIndexView& ix, const float* queries, int nq, const int32_t* ids,
+                      const int64_t* offsets, float* out, int32_t* status, cudaStream_t s);
+void launch_sq_exact(const SqIndexView& ix, const float* queries, int nq, const int32_t* ids,
+                     const int64_t* offsets, float* out, int32_t* status, cudaStream_t s);
+void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const float* queries,
+                   int nq, const int32_t* cand_ids, int cand_stride, const int32_t* cand_counts,
+                   int top_k, int capacity, int32_t* out_ids, float* out_dists,
+                   int32_t* out_counts, int32_t* status, cudaStream_t s);
+
+}  // namespace rover

@@ -1,0 +1,437 @@
+// pq_search.cu -- pure-PQ beam search on sm_100a, one warp per query.
+//
+// Semantics follow retrieval_pure_pq_search_scalar_with_policy
+// (src/dsp_demo/retrieval_sqmd_pure_pq.c:793-969) with the ONLINE residual
+// policy (retrieval_pq_residual_query_evaluate, retrieval_pq_residual.c:983)
+// and the final refine (refine_impl, retrieval_final_refine.c:256-292).
+//
+// The reference keeps a bounded max-heap pool and a min-heap frontier under
+// the strict total order (distance, id).  Because that order is total, the
+// pool after any sequence of inserts is the top-L of everything scored, and
+// the frontier pop that survives the pool-membership check is always the best
+// not-yet-expanded pool entry.  The kernel therefore keeps the pool as a
+// sorted list of 64-bit keys in shared memory with an "expanded" bit and
+// expands the first unexpanded entry each step; this yields the same pool,
+// the same expansion sequence and the same statistics as the heaps.
+//
+// Per expansion the warp reads the adjacency row, checks the valid-prefix
+// rule (pure_pq_graph_row_count, :59-87), claims first visits in a per-warp
+// visited table, scores the new neighbours (one lane each: ADC from the
+// codebook in the reference's order plus the residual correction), sorts them
+// with a warp bitonic network and merges them into the list.
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace rover {
+
+// Residual row address inside the .pqresN block payload
+// (pq_residual_query_block, retrieval_pq_residual.c:914-924).
+__device__ __forceinline__ const uint8_t* pq_residual_row(const PqIndexView& ix, int32_t id) {
+  const uint32_t u = static_cast<uint32_t>(id);
+  const uint32_t block = u / static_cast<uint32_t>(ix.vpb);
+  const uint32_t within = (u - block * static_cast<uint32_t>(ix.vpb)) * static_cast<uint32_t>(ix.rcb);
+  return ix.residual + static_cast<size_t>(block) * 4096u + within;
+}
+
+// One candidate's ADC distance (retrieval_pq_build_lut entries recomputed in
+// place, then the sequential sum of retrieval_pq_adc_scalar) and, when
+// correction is on, the residual-corrected distance.  Returns false when the
+// reference would reject the candidate (non-finite or invalid qparams).
+__device__ __forceinline__ bool pq_score(const PqIndexView& ix, const float* __restrict__ q,
+                                         int32_t id, bool correction, float* out_adc,
+                                         float* out_dist) {
+  const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
+  float adc = 0.0f;
+  float acc = 0.0f;
+  float scale = 0.0f, zero = 0.0f;
+  const uint8_t* res = nullptr;
+  if (correction) {
+    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+    scale = qp.x;
+    zero = qp.y;
+    if (!isfinite(scale) || !isfinite(zero) || !(scale > 0.0f)) return false;
+    res = pq_residual_row(ix, id);
+  }
+  int dim = 0;
+  for (int m = 0; m < ix.m; ++m) {
+    const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
+    const float* cen = ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim;
+    float lut = 0.0f;
+    for (int j = 0; j < ix.subdim; ++j, ++dim) {
+      const float cj = __ldg(cen + j);
+      const float qd = q[dim];
+      const float diff = fsub(qd, cj);
+      lut = fadd(lut, fmul(diff, diff));
+      if (correction) {
+        const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, dim))
+                                                 : static_cast<uint32_t>(__ldg(res + dim));
+        const float x = fadd(fadd(cj, fmul(u8f(r), scale)), zero);
+        const float dq = fsub(qd, x);
+        acc = fadd(acc, fmul(dq, dq));
+      }
+    }
+    adc = fadd(adc, lut);
+  }
+  if (!isfinite(adc)) return false;
+  if (correction && !isfinite(acc)) return false;
+  *out_adc = adc;
+  *out_dist = correction ? acc : adc;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Final refine of the first `count` pool entries (refine_impl with the PQ
+// residual decode provider): FP32 decode ((c + code*s) + z), FP64 sum of
+// squared differences in dimension order, sort by (distance, id), keep k.
+__device__ void pq_refine_warp(const PqIndexView& ix, const float* q, const uint64_t* list,
+                               int count, int k, double* sd, int32_t* si, int lane,
+                               int32_t* out_ids, float* out_dists, int32_t* out_count,
+                               int32_t* status) {
+  int np2 = 1;
+  while (np2 < count) np2 <<= 1;
+  bool bad = false;
+  for (int i = lane; i < np2; i += kWarp) {
+    if (i < count) {
+      const int32_t id = key_id(list[i]);
+      const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+      const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
+      const uint8_t* res = pq_residual_row(ix, id);
+      double dist = 0.0;
+      if (!isfinite(qp.x) || !(qp.x > 0.0f) || !isfinite(qp.y)) bad = true;
+      int dim = 0;
+      for (int m = 0; m < ix.m; ++m) {
+        const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
+        const float* cen = ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim;
+        for (int j = 0; j < ix.subdim; ++j, ++dim) {
+          const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, dim))
+                                                   : static_cast<uint32_t>(__ldg(res + dim));
+          const float x = fadd(fadd(__ldg(cen + j), fmul(u8f(r), qp.x)), qp.y);
+          if (!isfinite(x)) bad = true;
+          const double delta = __dsub_rn(static_cast<double>(q[dim]), static_cast<double>(x));
+          dist = __dadd_rn(dist, __dmul_rn(delta, delta));
+        }
+      }
+      if (!isfinite(dist) || dist >= 3.4028234663852886e38) bad = true;
+      sd[i] = dist;
+      si[i] = id;
+    } else {
+      sd[i] = __longlong_as_double(0x7ff0000000000000ll);  // +inf pads sort last
+      si[i] = 0x7fffffff;
+    }
+  }
+  if (__any_sync(kFullMask, bad)) {
+    if (lane == 0) *status = kStatusNumeric;
+    return;
+  }
+  __syncwarp();
+  // bitonic sort of (distance, id) pairs in shared memory
+  for (int kk = 2; kk <= np2; kk <<= 1) {
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < np2; i += kWarp) {
+        const int p = i ^ j;
+        if (p > i) {
+          const bool up = (i & kk) == 0;
+          const double a = sd[i], b = sd[p];
+          const int32_t ia = si[i], ib = si[p];
+          const bool a_gt = (a > b) || (a == b && ia > ib);
+          if (up == a_gt) {
+            sd[i] = b; sd[p] = a; si[i] = ib; si[p] = ia;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  const int outn = count < k ? count : k;
+  for (int i = lane; i < outn; i += kWarp) {
+    out_ids[i] = si[i];
+    out_dists[i] = static_cast<float>(sd[i]);
+  }
+  if (lane == 0) *out_count = outn;
+}
+
+// ---------------------------------------------------------------------------
+
+template <int PER>
+__device__ __forceinline__ int merge_batch(uint64_t* list, int size, int cap, uint64_t* stage,
+                                           uint64_t (&v)[PER], int nb, int lane) {
+  // stage the sorted batch so list elements can rank against it
+#pragma unroll
+  for (int r = 0; r < PER; ++r) stage[lane + 32 * r] = v[r];
+  __syncwarp();
+  int bpos[PER];
+  int min_ins = cap;
+#pragma unroll
+  for (int r = 0; r < PER; ++r) {
+    const int e = lane + 32 * r;
+    bpos[r] = e < nb ? e + count_less(list, size, v[r]) : cap;
+    min_ins = min(min_ins, bpos[r]);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) min_ins = min(min_ins, __shfl_xor_sync(kFullMask, min_ins, off));
+  // shift list elements right, highest chunk first (new position >= old)
+  const int first_chunk = min_ins >> 5;
+  for (int t = (size - 1) >> 5; t >= first_chunk; --t) {
+    const int i = 32 * t + lane;
+    uint64_t key = 0;
+    int pos = cap;
+    if (i < size) {
+      key = list[i];
+      pos = i + count_less(stage, nb, key);
+    }
+    __syncwarp();
+    if (i < size && pos < cap && pos != i) list[pos] = key;
+    __syncwarp();
+  }
+#pragma unroll
+  for (int r = 0; r < PER; ++r)
+    if (bpos[r] < cap) list[bpos[r]] = v[r];
+  __syncwarp();
+  return min_ins;
+}
+
+template <int PER>
+__device__ bool score_and_merge(const PqSearchArgs& a, const float* q, uint64_t* list, int* size,
+                                int cap, uint64_t* stage, const int32_t* batch_ids, int nb,
+                                int* cursor, int lane) {
+  uint64_t v[PER];
+  bool bad = false;
+#pragma unroll
+  for (int r = 0; r < PER; ++r) {
+    const int e = lane + 32 * r;
+    v[r] = kEmptyKey;
+    if (e < nb) {
+      const int32_t id = batch_ids[e];
+      float adc, dist;
+      if (pq_score(a.ix, q, id, a.correction != 0, &adc, &dist)) v[r] = make_key(dist, id);
+      else bad = true;
+    }
+  }
+  if (__any_sync(kFullMask, bad)) return false;
+  warp_bitonic_sort<PER>(v, lane);
+  const int min_ins = merge_batch<PER>(list, *size, cap, stage, v, nb, lane);
+  *size = min(cap, *size + nb);
+  *cursor = min(*cursor, min_ins);
+  return true;
+}
+
+__device__ bool dispatch_batch(const PqSearchArgs& a, const float* q, uint64_t* list, int* size,
+                               int cap, uint64_t* stage, const int32_t* batch_ids, int nb,
+                               int* cursor, int lane) {
+  if (nb <= 32) return score_and_merge<1>(a, q, list, size, cap, stage, batch_ids, nb, cursor, lane);
+  if (nb <= 64) return score_and_merge<2>(a, q, list, size, cap, stage, batch_ids, nb, cursor, lane);
+  return score_and_merge<4>(a, q, list, size, cap, stage, batch_ids, nb, cursor, lane);
+}
+
+__global__ void __launch_bounds__(kSearchWarps * 32)
+pq_search_kernel(PqSearchArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  uint8_t* base = smem + static_cast<size_t>(warp) * a.smem_per_warp;
+  float* q = reinterpret_cast<float*>(base);
+  uint64_t* list = reinterpret_cast<uint64_t*>(base + a.smem_query_bytes);
+  uint64_t* stage = list + a.max_pool;                 // kMaxBatch keys
+  int32_t* batch = reinterpret_cast<int32_t*>(stage + kMaxBatch);  // kMaxBatch ids
+  const int slot = blockIdx.x * kSearchWarps + warp;
+  VisitedTable vt;
+  vt.slots = a.visited + static_cast<size_t>(slot) * (a.visited_mask + 1ull);
+  vt.mask = a.visited_mask;
+  const PqIndexView& ix = a.ix;
+
+  for (;;) {
+    int qi = 0;
+    if (lane == 0) qi = static_cast<int>(atomicAdd(a.next_query, 1u));
+    qi = __shfl_sync(kFullMask, qi, 0);
+    if (qi >= a.nq) break;
+
+    const int cap = a.pool_sizes[qi];
+    int32_t* status = a.status + qi;
+    const int expand = min(a.expand_count, ix.degree);
+    if (cap <= 0 || cap > a.max_pool || expand <= 0 || expand > kMaxBatch || a.entry_points <= 0) {
+      if (lane == 0) *status = kStatusBadParam;
+      continue;
+    }
+    for (int d = lane; d < ix.dim; d += kWarp) q[d] = a.queries[static_cast<size_t>(qi) * ix.dim + d];
+    __syncwarp();
+    // retrieval_pq_build_lut fails the query if any LUT entry is not finite
+    bool bad = false;
+    for (int e = lane; e < ix.m * ix.ks; e += kWarp) {
+      const int m = e / ix.ks;
+      const float* cen = ix.codebook + static_cast<size_t>(e) * ix.subdim;
+      float acc = 0.0f;
+      for (int j = 0; j < ix.subdim; ++j) {
+        const float diff = fsub(q[m * ix.subdim + j], __ldg(cen + j));
+        acc = fadd(acc, fmul(diff, diff));
+      }
+      if (!isfinite(acc)) bad = true;
+    }
+    if (__any_sync(kFullMask, bad)) {
+      if (lane == 0) *status = kStatusNumeric;
+      continue;
+    }
+    vt.gen = a.gen_base + static_cast<uint32_t>(qi);
+    int size = 0, cursor = 0;
+    unsigned long long scored = 0, expanded = 0, dedup = 0;
+    int32_t st = kStatusOk;
+    const uint32_t load_limit = (a.visited_mask + 1u) >> 1;
+
+    // entry ids: graph entry first, then the LCG of pure_pq_make_seed_ids
+    // (retrieval_rpc_demo_pure_pq.c:192-208), processed in chunks of 32.
+    const int entries = min(a.entry_points, ix.n);
+    uint32_t lcg = a.seed;
+    for (int base_e = 0; base_e < entries && st == kStatusOk; base_e += kWarp) {
+      if (lane == 0) {
+        for (int t = 0; t < kWarp && base_e + t < entries; ++t) {
+          const int i = base_e + t;
+          int32_t id;
+          if (i == 0 && a.graph_entry >= 0 && a.graph_entry < ix.n) {
+            id = a.graph_entry;
+          } else {
+            lcg = lcg * 1103515245u + 12345u;
+            id = static_cast<int32_t>((static_cast<uint64_t>(lcg) * static_cast<uint64_t>(ix.n)) >> 32);
+          }
+          stage[t] = static_cast<uint64_t>(id);
+        }
+      }
+      __syncwarp();
+      const int e = base_e + lane;
+      int fresh = 0;
+      int32_t id = -1;
+      if (e < entries) {
+        id = static_cast<int32_t>(stage[lane]);
+        const int r = visited_insert(vt, static_cast<uint32_t>(id));
+        if (r < 0) st = kStatusTableFull;
+        fresh = r == 1;
+        if (r == 0) ++dedup;
+      }
+      __syncwarp();
+      const unsigned fm = __ballot_sync(kFullMask, fresh);
+      const int nb = __popc(fm);
+      if (fresh) batch[__popc(fm & ((1u << lane) - 1u))] = id;
+      __syncwarp();
+      if (__any_sync(kFullMask, st != kStatusOk)) { st = kStatusTableFull; break; }
+      scored += nb;
+      if (nb > 0 && !score_and_merge<1>(a, q, list, &size, cap, stage, batch, nb, &cursor, lane)) {
+        st = kStatusNumeric;
+        break;
+      }
+    }
+
+    // expansion loop
+    while (st == kStatusOk) {
+      int pos = -1;
+      for (int b = cursor & ~31; b < size; b += kWarp) {
+        const int i = b + lane;
+        const bool cand = i >= cursor && i < size && !(list[i] & kExpandedBit);
+        const unsigned m = __ballot_sync(kFullMask, cand);
+        if (m) { pos = b + __ffs(m) - 1; break; }
+      }
+      if (pos < 0) break;
+      cursor = pos + 1;
+      const int32_t src = key_id(list[pos]);
+      __syncwarp();
+      if (lane == 0) list[pos] |= kExpandedBit;
+      const int32_t* row = ix.graph + static_cast<size_t>(src) * ix.degree;
+      // valid-prefix rule (pure_pq_graph_row_count)
+      int first_pad = expand;
+      bool row_bad = false;
+      for (int b = 0; b < expand; b += kWarp) {
+        const int j = b + lane;
+        const int32_t nid = j < expand ? __ldg(row + j) : -1;
+        const unsigned pad = __ballot_sync(kFullMask, j < expand && nid == -1);
+        if (pad && first_pad == expand) first_pad = b + __ffs(pad) - 1;
+      }
+      for (int b = 0; b < expand; b += kWarp) {
+        const int j = b + lane;
+        if (j < expand) {
+          const int32_t nid = __ldg(row + j);
+          if (j < first_pad) row_bad |= (nid < 0 || nid >= ix.n);
+          else row_bad |= (nid != -1);
+        }
+      }
+      if (__any_sync(kFullMask, row_bad)) { st = kStatusBadRow; break; }
+      // first visits, in row order
+      int nb = 0;
+      bool full = false;
+      for (int b = 0; b < first_pad; b += kWarp) {
+        const int j = b + lane;
+        int fresh = 0;
+        int32_t nid = -1;
+        if (j < first_pad) {
+          nid = __ldg(row + j);
+          const int r = visited_insert(vt, static_cast<uint32_t>(nid));
+          full |= r < 0;
+          fresh = r == 1;
+          if (r == 0) ++dedup;
+        }
+        const unsigned fm = __ballot_sync(kFullMask, fresh);
+        if (fresh) batch[nb + __popc(fm & ((1u << lane) - 1u))] = nid;
+        nb += __popc(fm);
+      }
+      ++expanded;
+      if (__any_sync(kFullMask, full) || scored + nb > load_limit) { st = kStatusTableFull; break; }
+      __syncwarp();
+      if (nb == 0) continue;
+      scored += nb;
+      if (!dispatch_batch(a, q, list, &size, cap, stage, batch, nb, &cursor, lane)) {
+        st = kStatusNumeric;
+        break;
+      }
+    }
+
+    // dedup counts were per lane: reduce
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) dedup += __shfl_xor_sync(kFullMask, dedup, off);
+    if (st != kStatusOk) {
+      if (lane == 0) *status = st;
+      continue;
+    }
+    __syncwarp();
+    if (a.pool_ids) {
+      const int pc = min(size, a.pool_stride);  // pool_stride > 0 when pool_ids is set
+      for (int i = lane; i < pc; i += kWarp) {
+        const uint64_t k = list[i];
+        a.pool_ids[static_cast<size_t>(qi) * a.pool_stride + i] = key_id(k);
+        a.pool_dists[static_cast<size_t>(qi) * a.pool_stride + i] = key_dist(k);
+      }
+      if (lane == 0) a.pool_counts[qi] = pc;
+    }
+    if (lane == 0 && a.stats) {
+      unsigned long long* s = a.stats + static_cast<size_t>(qi) * 4;
+      s[0] = scored;
+      s[1] = a.correction ? scored : 0ull;
+      s[2] = expanded;
+      s[3] = dedup;
+    }
+    if (a.out_ids) {
+      const int k = min(a.top_ks ? a.top_ks[qi] : a.top_k, a.out_stride);
+      const int budget = a.refine_budget;
+      int32_t* oi = a.out_ids + static_cast<size_t>(qi) * a.out_stride;
+      float* od = a.out_dists + static_cast<size_t>(qi) * a.out_stride;
+      if (budget > 0) {
+        const int cnt = min(size, budget);
+        // refine scratch reuses the batch/stage area and the tail of the warp
+        // slice; it is sized for max refine budget by the host.
+        double* sd = reinterpret_cast<double*>(base + a.smem_refine_offset);
+        int32_t* si = reinterpret_cast<int32_t*>(sd + a.refine_capacity);
+        int32_t rs = kStatusOk;
+        pq_refine_warp(ix, q, list, cnt, k, sd, si, lane, oi, od, a.out_counts + qi, &rs);
+        rs = __shfl_sync(kFullMask, rs, 0);
+        if (rs != kStatusOk && lane == 0) *status = rs;
+      } else {
+        const int outn = min(size, k);
+        for (int i = lane; i < outn; i += kWarp) {
+          const uint64_t kk = list[i];
+          oi[i] = key_id(kk);
+          od[i] = key_dist(kk);
+        }
+        if (lane == 0) a.out_counts[qi] = outn;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace rover

@@ -1,0 +1,114 @@
+"""Synthetic stand-ins for the Rover benchmark configurations.
+
+The reference measures on SIFT-like datasets that are not part of this
+project; seeded Gaussian mixtures with the configured sizes, dimensions and
+value distributions stand in for them (rover_b200.datasets).  A workload is
+built once per process (and optionally cached on local disk as .npy files),
+then loaded into the library.
+
+``pq_1m_d128``: base n=1,000,000 d=128 from a 1,024-component mixture
+(centres N(0, 4I), sigma 0.5) clipped to >= 0; 10,000 queries from the same
+mixture; a degree-48 graph = 64-NN pruned by the alpha=1.2 occlusion rule;
+entry = medoid; PQ M=16 x 256 (k-means, 25 iterations, 100,000 uniform-stride
+training samples); 8-bit residuals; exact top-100 ground truth.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import time
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from . import bundle as B
+from . import datasets as D
+
+
+@dataclass
+class PqWorkload:
+    name: str
+    base_shape: tuple
+    queries: np.ndarray
+    gt: np.ndarray            # [nq][gt_k] exact neighbours
+    graph: np.ndarray         # [n][degree]
+    entry: int
+    bundle: B.PqBundle
+    build_seconds: float = 0.0
+
+
+CONFIGS = {
+    "pq_1m_d128": dict(n=1_000_000, dim=128, comps=1024, clip=True, normalize=False, nq=10_000,
+                       cand=64, degree=48, alpha=1.2, m=16, ks=256, iters=25, rbits=8, seed=2024),
+    "pq_100k_d128": dict(n=100_000, dim=128, comps=256, clip=True, normalize=False, nq=2_000,
+                         cand=64, degree=48, alpha=1.2, m=16, ks=256, iters=10, rbits=8, seed=2024),
+    "pq_1m_d96": dict(n=1_000_000, dim=96, comps=512, clip=False, normalize=True, nq=20_000,
+                      cand=48, degree=32, alpha=1.2, m=24, ks=256, iters=25, rbits=8, seed=2025),
+}
+
+
+def _key(cfg: dict) -> str:
+    return hashlib.sha256(json.dumps(cfg, sort_keys=True).encode()).hexdigest()[:16]
+
+
+def build_pq(name: str, cache_dir: str | Path | None = None, device=None, gt_k: int = 100,
+             nq: int | None = None, verbose: bool = True) -> PqWorkload:
+    cfg = dict(CONFIGS[name])
+    if nq is not None:
+        cfg["nq"] = nq
+    t0 = time.time()
+    cache = None
+    if cache_dir:
+        cache = Path(cache_dir) / f"{name}-{_key(cfg)}"
+        if (cache / "done").exists():
+            return _load_cache(name, cache, cfg, time.time() - t0)
+    log = (lambda *a: print(f"[workload {name} {time.time() - t0:6.1f}s]", *a, flush=True)) if verbose else (lambda *a: None)
+    base = D.gmm(cfg["n"], cfg["dim"], cfg["comps"], cfg["seed"], clip_nonneg=cfg["clip"],
+                 normalize=cfg["normalize"])
+    queries = D.gmm(cfg["nq"], cfg["dim"], cfg["comps"], cfg["seed"] + 1, centers_seed=cfg["seed"],
+                    clip_nonneg=cfg["clip"], normalize=cfg["normalize"])
+    log("vectors")
+    gt = D.exact_knn(queries, base, gt_k, device=device)
+    log("ground truth")
+    graph = D.pruned_graph(base, cfg["cand"], cfg["degree"], cfg["alpha"], device=device)
+    entry = D.medoid(base, device=device)
+    log("graph", f"mean degree {float((graph >= 0).sum(1).mean()):.1f}")
+    book, codes, rows, qp = D.pq_prepare(base, cfg["m"], cfg["ks"], cfg["iters"], cfg["rbits"], device=device)
+    log("pq codes + residuals")
+    md = B.PqMeta(hashlib.sha256(name.encode()).digest()[:16], cfg["n"], cfg["dim"], cfg["m"], cfg["ks"],
+                  cfg["dim"] // cfg["m"], B.pq_code_bytes(cfg["m"], cfg["ks"]),
+                  train_count=min(cfg["n"], 100000), kmeans_iters=cfg["iters"], seed=cfg["seed"])
+    bundle = B.PqBundle(md, book, codes, cfg["rbits"], B.pack_residual_blocks(rows), qp)
+    w = PqWorkload(name, base.shape, queries, gt, graph, entry, bundle, time.time() - t0)
+    if cache:
+        cache.mkdir(parents=True, exist_ok=True)
+        for k, v in dict(queries=queries, gt=gt, graph=graph, book=book, codes=codes,
+                         blocks=bundle.residual_blocks, qparams=qp).items():
+            np.save(cache / f"{k}.npy", v)
+        (cache / "meta.json").write_text(json.dumps(dict(entry=entry, cfg=cfg)))
+        (cache / "done").write_text("1")
+    return w
+
+
+def _load_cache(name, cache: Path, cfg, seconds) -> PqWorkload:
+    meta = json.loads((cache / "meta.json").read_text())
+    ld = lambda k: np.load(cache / f"{k}.npy")
+    book, codes = ld("book"), ld("codes")
+    md = B.PqMeta(hashlib.sha256(name.encode()).digest()[:16], cfg["n"], cfg["dim"], cfg["m"], cfg["ks"],
+                  cfg["dim"] // cfg["m"], B.pq_code_bytes(cfg["m"], cfg["ks"]),
+                  train_count=min(cfg["n"], 100000), kmeans_iters=cfg["iters"], seed=cfg["seed"])
+    bundle = B.PqBundle(md, book, codes, cfg["rbits"], ld("blocks"), ld("qparams"))
+    return PqWorkload(name, (cfg["n"], cfg["dim"]), ld("queries"), ld("gt"), ld("graph"), meta["entry"], bundle,
+                      seconds)
+
+
+def recall_at_k(ids: np.ndarray, counts: np.ndarray, gt: np.ndarray, k: int) -> float:
+    """demo_recall_hits_at_k (retrieval_rpc_demo_support.c:1709) averaged:
+    hits among the first k results that appear in the first k truth ids."""
+    hits = 0
+    for i in range(ids.shape[0]):
+        c = min(int(counts[i]), k)
+        hits += len(np.intersect1d(ids[i, :c], gt[i, :k]))
+    return hits / (ids.shape[0] * k)
