@@ -1,0 +1,405 @@
+#!/usr/bin/env python3
+"""Benchmark: QPS at recall@10 >= 0.95 of Rover's pure-PQ graph search on
+the 1M x 128 PQ workload (M=16 x 256, 8-bit residuals, degree-48 alpha=1.2
+graph, 10,000 queries per step, top-10 after the FP64 re-rank of 20).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one batched search of the 10,000 queries at the operating point
+picked by the calibration (entry points as multiples of the mixture's cluster
+count x beam width L in {32, 64, 128, 256}: the least-work point whose
+recall@10 reaches 0.95).  ``value`` is device-timed with inputs resident in
+HBM; ``e2e`` is the same step through the host-buffer C-ABI call with the
+host->device query copy and the device->host result copy inside the timed
+region.  Multi-GPU runs are replicas (each rank searches its own 10,000
+queries; no collective on the data path) and report weak scaling.
+
+``--impl reference`` times the reference's own CPU search code
+(oracle/_ref: retrieval_pure_pq_search_scalar_with_policy + residual
+correction + final refine, compiled from the reference sources) with all host
+threads on bounded query samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "pq_1m_d128"
+L_SWEEP = (32, 64, 128, 256)
+EP_MULTIPLES = (0.25, 1, 2, 4)   # entry points as multiples of the mixture's cluster count
+TOP_K = 10
+REFINE_BUDGET = 20      # refine_factor 2 x top_k
+TARGET_RECALL = 0.95
+CALIBRATION_QUERIES = 2000
+
+
+def log(*a):
+    print("[bench]", *a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(stats: np.ndarray, counts: np.ndarray, md, rcb: int, expand: int, dim: int) -> int:
+    """Per launch: E*4*expand (adjacency rows read) + S*c (codes of scored
+    candidates) + C*(r + 8) (residual row + qparams of corrected candidates)
+    + F*(c + r + 8) (refined candidates) + 4*d per query."""
+    s = stats.astype(np.int64)
+    refined = np.minimum(counts.astype(np.int64), REFINE_BUDGET)
+    b = (s[:, 2] * 4 * expand + s[:, 0] * md.code_bytes + s[:, 1] * (rcb + 8)
+         + refined * (md.code_bytes + rcb + 8) + 4 * dim)
+    return int(b.sum())
+
+
+def calibrate(search, w, comps, log_prefix=""):
+    """Operating point: for each entry-point count (multiples of the mixture's
+    cluster count) the smallest L of the sweep whose recall@10 on the first
+    CALIBRATION_QUERIES queries reaches the target; among those, the point
+    with the fewest scored candidates per query (the least work).  The rule
+    only uses recall and the search's own statistics, so the reference and
+    this library -- whose searches are identical -- choose the same point."""
+    from rover_b200.workloads import recall_at_k
+    nc = min(CALIBRATION_QUERIES, len(w.queries))
+    qs, gt = w.queries[:nc], w.gt[:nc]
+    table, chosen = [], None
+    for mult in EP_MULTIPLES:
+        ep = max(1, int(round(mult * comps)))
+        for L in L_SWEEP:
+            r = search(qs, L, ep)
+            rec = recall_at_k(r["ids"], r["counts"], gt, TOP_K)
+            work = float(r["stats"][:, 0].mean())
+            table.append({"entry_points": ep, "L": L, "recall_at_10": rec, "scored": work})
+            log(f"{log_prefix}calibration ep={ep} L={L} recall@10={rec:.4f} scored={work:.0f}")
+            if rec >= TARGET_RECALL:
+                if chosen is None or work < chosen[2]:
+                    chosen = (ep, L, work)
+                break
+    if chosen is None:   # target not reached: the highest-recall point
+        best = max(table, key=lambda t: t["recall_at_10"])
+        chosen = (best["entry_points"], best["L"], best["scored"])
+    return chosen[0], chosen[1], table
+
+
+def reference_arm(args, w, rank) -> dict:
+    """The reference's CPU path on bounded samples (oracle/_ref)."""
+    from oracle import bindings
+    from rover_b200 import bundle as B
+    if not bindings.reference_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent at build)"}
+    ref = bindings.Reference()
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = Path(tmp) / "index"
+        B.write_pq_bundle(prefix, w.bundle.codebook, w.bundle.codes, w.bundle.residual_rows(), w.bundle.qparams,
+                          w.bundle.residual_bits, index_uuid=w.bundle.meta.index_uuid)
+        h = ref.pq_open(prefix, w.bundle.residual_bits)
+        expand = w.graph.shape[1]
+        from rover_b200.workloads import CONFIGS
+        def search(qs, L, ep):
+            return ref.pq_search(h, w.graph, w.entry, qs, L, ep, expand, correction=1,
+                                 refine_budget=REFINE_BUDGET, top_k=TOP_K, threads=threads)
+        ep_chosen, chosen, table = calibrate(search, w, CONFIGS[args.workload]["comps"], "reference ")
+        # size the per-step sample to ~5 s of work
+        probe = w.queries[:max(threads * 2, 64)]
+        t0 = time.perf_counter()
+        search(probe, chosen, ep_chosen)
+        rate = len(probe) / (time.perf_counter() - t0)
+        sample = int(min(len(w.queries), max(threads, rate * 5.0)))
+        times = []
+        for step in range(args.warmup + args.steps):
+            off = (step * sample) % max(1, len(w.queries) - sample + 1)
+            qs = w.queries[off:off + sample]
+            t0 = time.perf_counter()
+            search(qs, chosen, ep_chosen)
+            if step >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        ref.pq_close(h)
+    elapsed = sum(times)
+    qps = sample * len(times) / elapsed
+    return {
+        "metric": "QPS at recall@10>=0.95 (pure-PQ graph search, 1M x 128)",
+        "value": qps, "unit": "queries/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * elapsed / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture)", "impl": "reference",
+        "config": {"workload": args.workload, "queries_per_step": sample, "beam_L": chosen,
+                   "entry_points": ep_chosen, "calibration": table, "top_k": TOP_K,
+                   "refine_budget": REFINE_BUDGET, "expand_count": expand, "correction": "online"},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "reference",
+                         "sample": f"{sample} queries per step x {len(times)} steps at L={chosen}, ep={ep_chosen} "
+                                   "(retrieval_pure_pq_search_scalar_with_policy + ONLINE residual policy + "
+                                   "retrieval_final_refine, reference sources compiled -O2 -ffp-contract=off)"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def cpu_baseline(w, L, ep, expand, budget_s=12.0) -> dict:
+    from oracle import bindings
+    from rover_b200 import bundle as B
+    threads = os.cpu_count() or 1
+    if not bindings.reference_available():
+        return {"value": None, "unit": "queries/s", "cores": threads, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    ref = bindings.Reference()
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = Path(tmp) / "index"
+        B.write_pq_bundle(prefix, w.bundle.codebook, w.bundle.codes, w.bundle.residual_rows(), w.bundle.qparams,
+                          w.bundle.residual_bits, index_uuid=w.bundle.meta.index_uuid)
+        h = ref.pq_open(prefix, w.bundle.residual_bits)
+        probe = w.queries[:max(threads * 2, 64)]
+        t0 = time.perf_counter()
+        ref.pq_search(h, w.graph, w.entry, probe, L, ep, expand, correction=1,
+                      refine_budget=REFINE_BUDGET, top_k=TOP_K, threads=threads)
+        rate = len(probe) / (time.perf_counter() - t0)
+        sample = int(min(len(w.queries), max(threads, rate * budget_s)))
+        qs = w.queries[:sample]
+        t0 = time.perf_counter()
+        ref.pq_search(h, w.graph, w.entry, qs, L, ep, expand, correction=1,
+                      refine_budget=REFINE_BUDGET, top_k=TOP_K, threads=threads)
+        el = time.perf_counter() - t0
+        ref.pq_close(h)
+    return {"value": sample / el, "unit": "queries/s", "cores": threads, "kind": "reference",
+            "sample": f"{sample} queries at L={L}, ep={ep} through the reference's own search, correction and refine "
+                      f"(oracle/_ref), {threads} threads"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--cache-dir", default=os.environ.get("ROVER_BENCH_CACHE", "/tmp/rover_bench_cache"))
+    ap.add_argument("--L", type=int, default=0, help="with --ep: skip calibration, use this beam width")
+    ap.add_argument("--ep", type=int, default=0, help="with --L: skip calibration, use this many entry points")
+    ap.add_argument("--workload", default=WORKLOAD, help="workload name (rover_b200.workloads.CONFIGS)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference" and rank != 0:
+        return 0
+    dist = None
+    if world > 1 and args.impl == "ours":
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+
+    from rover_b200 import workloads
+    w = workloads.build_pq(args.workload, cache_dir=args.cache_dir, verbose=rank == 0)
+    log(f"workload ready in {w.build_seconds:.1f}s")
+    if args.impl == "reference":
+        print(json.dumps(reference_arm(args, w, rank)), flush=True)
+        return 0
+
+    from rover_b200.calculator import Calculator
+    calc = Calculator()
+    calc.pq_load(w.graph, w.entry, w.bundle)
+    md = w.bundle.meta
+    expand = w.graph.shape[1]
+    nq = len(w.queries)
+    from rover_b200.workloads import CONFIGS
+    if args.L and args.ep:
+        L, ep, table = args.L, args.ep, []
+    else:
+        def search(qs, L_, ep_):
+            return calc.pq_search(qs, L_, top_k=TOP_K, entry_points=ep_, expand_count=expand, correction=1,
+                                  refine_budget=REFINE_BUDGET)
+        ep, L, table = calibrate(search, w, CONFIGS[args.workload]["comps"])
+    kw = dict(entry_points=ep, expand_count=expand, correction=1, refine_budget=REFINE_BUDGET)
+    final = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
+    recall = workloads.recall_at_k(final["ids"], final["counts"], w.gt, TOP_K)
+    # the calibration subset can pass while the full set falls just short:
+    # widen the beam until the full query set meets the target
+    while recall < TARGET_RECALL and not (args.L and args.ep):
+        wider = [x for x in L_SWEEP + (512, 1024) if x > L]
+        if not wider:
+            break
+        L = wider[0]
+        final = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
+        recall = workloads.recall_at_k(final["ids"], final["counts"], w.gt, TOP_K)
+    stats = final["stats"]
+    bytes_per_launch = algorithmic_bytes(stats, final["counts"], md, w.bundle.residual_code_bytes, expand, md.dim)
+
+    # device-resident inputs and outputs
+    dev = torch.device("cuda", local)
+    q_d = torch.from_numpy(w.queries).to(dev)
+    pool_d = torch.full((nq,), L, dtype=torch.int32, device=dev)
+    out = dict(ids=torch.empty((nq, TOP_K), dtype=torch.int32, device=dev),
+               dists=torch.empty((nq, TOP_K), dtype=torch.float32, device=dev),
+               counts=torch.empty(nq, dtype=torch.int32, device=dev),
+               status=torch.empty(nq, dtype=torch.int32, device=dev))
+    ptrs = {k: v.data_ptr() for k, v in out.items()}
+    ptrs["stride"] = TOP_K
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        calc.pq_search_device(q_d.data_ptr(), nq, pool_d.data_ptr(), ptrs, stream_ptr=stream.cuda_stream,
+                              top_k=TOP_K, **kw)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = calc.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for i in range(args.steps):
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    launches = calc.launch_count() - launches0
+    total_ms = t0.elapsed_time(t1)
+    per_launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = nq * args.steps * world / (total_ms / 1e3)
+    avg_launch_s = statistics.mean(per_launch_ms) / 1e3
+    peak, peak_kind = measured_peak()
+    achieved = bytes_per_launch / avg_launch_s / 1e9
+    clock = clocks.summary()
+
+    # end to end through the host-buffer entry point (pinned host memory)
+    q_h = torch.from_numpy(w.queries).pin_memory().numpy()
+    for _ in range(2):
+        calc.pq_search(q_h, L, top_k=TOP_K, stats=False, **kw)
+    torch.cuda.synchronize()
+    e2e_times = []
+    for _ in range(args.steps):
+        t_e = time.perf_counter()
+        calc.pq_search(q_h, L, top_k=TOP_K, stats=False, **kw)
+        e2e_times.append(time.perf_counter() - t_e)
+    e2e_qps = nq * len(e2e_times) * world / sum(e2e_times)
+    h2d = nq * md.dim * 4 + nq * 4
+    d2h = nq * TOP_K * 8 + nq * 8
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, L, ep, expand)
+
+    line = {
+        "metric": "QPS at recall@10>=0.95 (pure-PQ graph search, 1M x 128)",
+        "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Gaussian mixture stand-in for the dataset)",
+        "config": {"workload": args.workload, "n": md.num_vectors, "dim": md.dim, "pq": f"M={md.m}x{md.ks}",
+                   "residual_bits": w.bundle.residual_bits, "graph_degree": int(w.graph.shape[1]),
+                   "queries_per_step": nq, "beam_L": L, "recall_at_10": recall,
+                   "calibration": table, "top_k": TOP_K,
+                   "refine_budget": REFINE_BUDGET, "expand_count": expand, "entry_points": ep,
+                   "mode": "exact (reference expansion order)", "parallelism": f"replicas x{world}",
+                   "l2": "index (>300 MB) larger than L2; no flush"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "pq_search_kernel", "algorithmic_bytes_per_launch": bytes_per_launch},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clock,
+        "stats_mean": {"scored": float(stats[:, 0].mean()), "expanded": float(stats[:, 2].mean()),
+                       "dedup": float(stats[:, 3].mean())},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    calc.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

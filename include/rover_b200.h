@@ -152,6 +152,9 @@ AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSearchParams 
 /* Last CUDA / library error as text (thread-local). */
 const char *calculator_rover_last_error(void);
 
+/* Number of CUDA kernels this library has launched in this process. */
+uint64_t calculator_rover_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,7 @@ class Calculator:
                                                   C.c_int32, _i32p, C.c_int, _f32p, C.c_int, _i32p]
         L.calculator_retrieval_unload.argtypes = [C.c_uint64]
         L.calculator_rover_last_error.restype = C.c_char_p
+        L.calculator_rover_launch_count.restype = C.c_uint64
         L.calculator_rover_pq_load.argtypes = [C.c_uint64, C.POINTER(PqIndexDesc)]
         L.calculator_rover_pq_unload.argtypes = [C.c_uint64]
         L.calculator_rover_pq_search.argtypes = [C.c_uint64, C.POINTER(SearchParams), _f32p, C.c_int32, _i32p,
@@ -121,6 +122,9 @@ class Calculator:
         if rc != AEE_SUCCESS:
             raise CalculatorError(call, rc, self.last_error())
         return rc
+
+    def launch_count(self) -> int:
+        return int(self.lib.calculator_rover_launch_count())
 
     def close(self):
         if self.handle.value:

@@ -118,6 +118,7 @@ State& st() {
 }
 
 int open_count = 0;
+std::atomic<unsigned long long> g_launches{0};  // kernels this library launched
 
 AEEResult ensure_init(State& s) {
   if (s.init) return AEE_SUCCESS;
@@ -235,6 +236,7 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
     CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
     pq_search_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
     CK(cudaGetLastError());
+    ++g_launches;
     s.h_status.resize(nq);
     CK(cudaMemcpyAsync(s.h_status.data(), d_out.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
@@ -319,6 +321,7 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
     CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
     sq_search_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
     CK(cudaGetLastError());
+    ++g_launches;
     s.h_status.resize(nq);
     CK(cudaMemcpyAsync(s.h_status.data(), d_status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
@@ -380,6 +383,8 @@ AEEResult load_sq(State& s, SqDevice& d, const RoverSqIndexDesc* desc, int l1_bi
 // Extension entry points (include/rover_b200.h)
 
 extern "C" const char* calculator_rover_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" uint64_t calculator_rover_launch_count(void) { return g_launches.load(); }
 
 extern "C" AEEResult calculator_rover_pq_load(remote_handle64 h, const RoverPqIndexDesc* d) {
   (void)h;
@@ -560,6 +565,7 @@ extern "C" AEEResult calculator_rover_pq_lut(remote_handle64 h, const float* que
   CK(cudaMemsetAsync(s.status.p, 0, nq * 4, s.stream));
   launch_pq_lut(v, s.in_queries.as<float>(), nq, s.luts.as<float>(), s.status.as<int32_t>(), s.stream);
   CK(cudaGetLastError());
+  ++g_launches;
   std::vector<int32_t> hs(nq);
   if (download(out_luts, s.luts.p, nq * lut, s.stream) || download(hs.data(), s.status.p, nq, s.stream)) return AEE_EFAILED;
   CK(cudaStreamSynchronize(s.stream));
@@ -599,6 +605,7 @@ extern "C" AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, con
     CK(s.luts.ensure(nq * lut * 4));
     launch_pq_lut(s.pq.view, s.in_queries.as<float>(), nq, s.luts.as<float>(), dst, s.stream);
     launch_pq_adc(s.pq.view, s.luts.as<float>(), nq, di, dof, dout, dst, s.stream);
+    ++g_launches;
   } else if (kind == 1) {
     launch_pq_residual(s.pq.view, s.in_queries.as<float>(), nq, di, dof, dout, dst, s.stream);
   } else if (kind == 2) {
@@ -607,6 +614,7 @@ extern "C" AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, con
     launch_sq_exact(s.sq.view, s.in_queries.as<float>(), nq, di, dof, dout, dst, s.stream);
   }
   CK(cudaGetLastError());
+  ++g_launches;
   std::vector<int32_t> hs(nq);
   if (download(out_dists, dout, static_cast<size_t>(total), s.stream) || download(hs.data(), dst, nq, s.stream))
     return AEE_EFAILED;
@@ -647,6 +655,7 @@ extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, co
                 s.in_pool.as<int32_t>(), top_k, cap, s.out_ids.as<int32_t>(), s.out_dists.as<float>(),
                 s.out_counts.as<int32_t>(), s.status.as<int32_t>(), s.stream);
   CK(cudaGetLastError());
+  ++g_launches;
   std::vector<int32_t> hs(nq);
   if (download(out_ids, s.out_ids.p, static_cast<size_t>(nq) * top_k, s.stream) ||
       download(out_dists, s.out_dists.p, static_cast<size_t>(nq) * top_k, s.stream) ||

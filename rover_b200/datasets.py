@@ -269,3 +269,129 @@ def pq_prepare(base: np.ndarray, m: int, ks: int, iters: int, residual_bits: int
     codes = pq_encode(base, book, device=device)
     rows, qp = quantize_residual_rint(base - pq_reconstruct(codes, book), residual_bits)
     return book, codes, rows, qp
+
+
+def kmeans_centroids(base: np.ndarray, k: int, iters: int = 10, device=None, seed: int = 0):
+    """Plain Lloyd k-means (uniform-stride init); returns (centroids, labels)."""
+    dev = _device(device)
+    with torch.no_grad():
+        x = torch.from_numpy(np.ascontiguousarray(base)).to(dev)
+        # k-means++ seeding (D^2 sampling): separated clusters each get a centre
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(seed)
+        first = int(torch.randint(0, x.shape[0], (1,), generator=gen, device=dev).item())
+        picks = [first]
+        dmin = ((x - x[first]) ** 2).sum(1)
+        for _ in range(1, k):
+            r = torch.rand(1, generator=gen, device=dev) * dmin.sum()
+            nxt = int(torch.searchsorted(torch.cumsum(dmin, 0), r).clamp_max(x.shape[0] - 1).item())
+            picks.append(nxt)
+            dmin = torch.minimum(dmin, ((x - x[nxt]) ** 2).sum(1))
+        cent = x[torch.tensor(picks, device=dev)].clone()
+        labels = None
+        for _ in range(iters + 1):
+            cn = (cent * cent).sum(1)
+            parts = []
+            for s in range(0, x.shape[0], 65536):
+                xs = x[s:s + 65536]
+                parts.append(torch.argmin(cn[None, :] - 2.0 * (xs @ cent.T), dim=1))
+            labels = torch.cat(parts)
+            sums = torch.zeros_like(cent).index_add_(0, labels, x)
+            cnt = torch.bincount(labels, minlength=k).to(x.dtype)
+            pop = cnt > 0
+            cent[pop] = sums[pop] / cnt[pop, None]
+        return cent.cpu().numpy(), labels.cpu().numpy()
+
+
+def navigable_graph(base: np.ndarray, candidates: int, degree: int, alpha: float, long_edges: int = 8,
+                    clusters: int | None = None, device=None, chunk: int = 16384) -> np.ndarray:
+    """Occlusion-pruned k-NN graph plus long-range edges.
+
+    A k-NN graph of well separated mixture data falls apart into one component
+    per cluster, which no beam search can cross.  Here each node keeps at most
+    ``degree - long_edges`` neighbours from its alpha-pruned k-NN list and
+    spends the remaining slots on representatives (the member nearest the
+    centroid) of the nearest other k-means clusters, each admitted only if no
+    already kept neighbour occludes it (alpha * d(k, c) <= d(p, c))."""
+    dev = _device(device)
+    n = base.shape[0]
+    clusters = clusters or max(16, int(np.sqrt(n)))
+    intra = pruned_graph(base, candidates, degree - long_edges, alpha, device=device)
+    cent, labels = kmeans_centroids(base, clusters, device=device)
+    out = np.full((n, degree), -1, dtype=np.int32)
+    out[:, :degree - long_edges] = intra
+    with torch.no_grad():
+        x = torch.from_numpy(np.ascontiguousarray(base)).to(dev)
+        c = torch.from_numpy(cent).to(dev)
+        lab = torch.from_numpy(labels).to(dev).long()
+        # representative of each cluster: member nearest its centroid
+        dc = ((x - c[lab]) ** 2).sum(1)
+        rep = torch.full((clusters,), -1, dtype=torch.long, device=dev)
+        order = torch.argsort(dc, descending=True)
+        rep[lab[order]] = order            # last write wins = nearest member
+        cn = (c * c).sum(1)
+        a2 = float(alpha) * float(alpha)
+        want = long_edges + 1
+        for s in range(0, n, chunk):
+            xs = x[s:s + chunk]
+            b = xs.shape[0]
+            near = torch.topk(cn[None, :] - 2.0 * (xs @ c.T), min(want, clusters), dim=1, largest=False).indices
+            cand = rep[near]                                          # (b, want)
+            ids = torch.arange(s, s + b, device=dev)
+            cand = torch.where((cand == ids[:, None]) | (lab[s:s + b, None] == near), -1, cand)
+            kept = torch.from_numpy(out[s:s + b]).to(dev).long()     # (b, degree)
+            dpc = ((x[cand.clamp_min(0)] - xs[:, None, :]) ** 2).sum(2)  # (b, want)
+            cnt = (kept >= 0).sum(1)
+            for i in range(cand.shape[1]):
+                ci = cand[:, i]
+                cv = x[ci.clamp_min(0)]
+                kv = x[kept.clamp_min(0)]
+                dkc = ((kv - cv[:, None, :]) ** 2).sum(2)             # (b, degree)
+                occl = ((kept >= 0) & (a2 * dkc <= dpc[:, i:i + 1])).any(1)
+                dup = (kept == ci[:, None]).any(1)
+                take = (ci >= 0) & ~occl & ~dup & (cnt < degree)
+                rows = torch.nonzero(take, as_tuple=True)[0]
+                kept[rows, cnt[rows]] = ci[rows]
+                cnt = cnt + take.long()
+            out[s:s + b] = kept.int().cpu().numpy()
+    return out
+
+
+def routed_graph(base: np.ndarray, candidates: int, degree: int, alpha: float, long_edges: int = 8,
+                 clusters: int | None = None, entry: int | None = None, device=None) -> tuple[np.ndarray, int]:
+    """``navigable_graph`` plus a two-level routing structure so that a beam
+    search from the entry can reach every cluster.  Routing rows hold only
+    cluster representatives (the member nearest each k-means centroid): the
+    entry's row lists ``degree`` hub nodes, each hub's row lists its share of
+    all representatives.  Hubs are ordinary nodes that are not
+    representatives; their clusters stay connected through the other members.
+    Returns (graph, entry)."""
+    dev = _device(device)
+    n = base.shape[0]
+    clusters = clusters or max(16, int(np.sqrt(n)))
+    graph = navigable_graph(base, candidates, degree, alpha, long_edges, clusters, device)
+    cent, labels = kmeans_centroids(base, clusters, device=device)
+    entry = medoid(base, device) if entry is None else entry
+    with torch.no_grad():
+        x = torch.from_numpy(np.ascontiguousarray(base)).to(dev)
+        c = torch.from_numpy(cent).to(dev)
+        lab = torch.from_numpy(labels).to(dev).long()
+        dc = ((x - c[lab]) ** 2).sum(1)
+        order = torch.argsort(dc, descending=True)
+        rep = torch.full((clusters,), -1, dtype=torch.long, device=dev)
+        rep[lab[order]] = order
+        reps = [int(r) for r in rep.cpu().numpy() if r >= 0 and r != entry]
+        # hubs: the nodes nearest the entry that are not representatives
+        taken = set(reps) | {entry}
+        near = torch.argsort(((x - x[entry]) ** 2).sum(1))[: degree + len(taken) + 1].cpu().numpy()
+        hubs = [int(v) for v in near if int(v) not in taken][:degree]
+    per = (len(reps) + len(hubs) - 1) // max(1, len(hubs))
+    if per > degree:
+        raise ValueError("too many clusters for a two-level routing of this degree")
+    graph[entry, :] = -1
+    graph[entry, :len(hubs)] = hubs
+    for h_i, h in enumerate(hubs):
+        mine = reps[h_i * per:(h_i + 1) * per]
+        graph[h, :] = -1
+        graph[h, :len(mine)] = mine
+    return graph, entry

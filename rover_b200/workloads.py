@@ -8,8 +8,10 @@ then loaded into the library.
 
 ``pq_1m_d128``: base n=1,000,000 d=128 from a 1,024-component mixture
 (centres N(0, 4I), sigma 0.5) clipped to >= 0; 10,000 queries from the same
-mixture; a degree-48 graph = 64-NN pruned by the alpha=1.2 occlusion rule;
-entry = medoid; PQ M=16 x 256 (k-means, 25 iterations, 100,000 uniform-stride
+mixture; a degree-48 graph = 64-NN pruned by the alpha=1.2 occlusion rule to
+40 neighbours plus up to 8 long-range edges to representatives of the nearest
+k-means clusters (rover_b200.datasets.navigable_graph: a pure k-NN graph of
+this mixture splits into one component per cluster); entry = medoid; PQ M=16 x 256 (k-means, 25 iterations, 100,000 uniform-stride
 training samples); 8-bit residuals; exact top-100 ground truth.
 """
 from __future__ import annotations
@@ -72,7 +74,8 @@ def build_pq(name: str, cache_dir: str | Path | None = None, device=None, gt_k: 
     log("vectors")
     gt = D.exact_knn(queries, base, gt_k, device=device)
     log("ground truth")
-    graph = D.pruned_graph(base, cfg["cand"], cfg["degree"], cfg["alpha"], device=device)
+    graph = D.navigable_graph(base, cfg["cand"], cfg["degree"], cfg["alpha"], long_edges=8,
+                              clusters=cfg["comps"], device=device)
     entry = D.medoid(base, device=device)
     log("graph", f"mean degree {float((graph >= 0).sum(1).mean()):.1f}")
     book, codes, rows, qp = D.pq_prepare(base, cfg["m"], cfg["ks"], cfg["iters"], cfg["rbits"], device=device)
