@@ -119,6 +119,28 @@ AEEResult calculator_rover_pq_search_device(remote_handle64 h, const RoverSearch
                                             const int32_t *pool_sizes, const int32_t *top_ks,
                                             const RoverSearchOutputs *out, void *stream);
 
+/* Allocation-free variant of calculator_rover_pq_search_device.  It has no
+ * counterpart in the reference: it exists for callers that cannot allocate
+ * device memory while they search -- a server whose memory pool already owns
+ * the GPU, or a latency-bound loop that must not take cudaMalloc/cudaFree's
+ * implicit synchronization.  Nothing is allocated per call: the kernel's
+ * visited tables, work counter and error flag live in a fixed 64 MiB device
+ * array inside the library (held by every GPU that loads the library until
+ * the process exits).  All pointers are device pointers; out->status is
+ * required; max_pool must bound every pool_sizes[i] (the sizes are not read
+ * back).  A request whose visited tables cannot fit the array is rejected
+ * with AEE_EBADPARM, and a query that overflows its table fails the call
+ * (AEE_EFAILED) instead of being retried.  The first call on each device
+ * resolves the array's device address (cudaGetSymbolAddress) and clears it;
+ * make that first call before any stream capture.  Calls share the array:
+ * two calls whose kernels overlap on the GPU race, so issue them one after
+ * another.  stream is a cudaStream_t (NULL = the legacy default stream). */
+AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const RoverSearchParams *params,
+                                             const float *queries, int32_t num_queries,
+                                             const int32_t *pool_sizes, int32_t max_pool,
+                                             const int32_t *top_ks, const RoverSearchOutputs *out,
+                                             void *stream);
+
 /* Distances for explicit (query, id) lists: ids[offsets[q] .. offsets[q+1]).
  * kind 0 = PQ ADC (retrieval_pq_adc_ids_batch, retrieval_pq_core.c:332),
  * 1 = PQ residual-corrected (retrieval_pq_residual_query_evaluate,

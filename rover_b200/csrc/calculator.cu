@@ -1025,3 +1025,165 @@ extern "C" AEEResult calculator_retrieval_rnn_l2_unload_dma(remote_handle64 h) {
   (void)h;
   return AEE_SUCCESS;
 }
+
+// ===========================================================================
+// Allocation-free batched PQ search.
+//
+// For callers that may not allocate device memory at search time: a serving
+// process whose memory pool already owns the whole GPU (a cudaMalloc there
+// fails or fragments the pool), or a latency-critical loop that must not
+// take cudaMalloc/cudaFree's implicit device synchronization.  The search
+// kernel's scratch (the per-warp visited tables, the work counter and an
+// error flag) lives in the fixed array below instead of library
+// allocations.  The array is a static device variable: every GPU that loads
+// this library holds its kNoAllocScratchBytes until the process exits.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // 64 MiB per device
+constexpr size_t kNoAllocHeaderBytes = 256;           // work counter + error flag
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};   // device address of the array, per device
+uint32_t g_noalloc_gen[kNoAllocMaxDevices] = {};         // next visited-table generation, per device
+int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+// ORs every query status into one flag word.
+__global__ void noalloc_status_any(const int32_t* status, int nq, unsigned int* flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+    const int32_t s = status[i];
+    if (s != kStatusOk) atomicOr(flag, 1u << (s & 31));
+  }
+}
+
+}  // namespace
+
+extern "C" AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const RoverSearchParams* p,
+                                                        const float* queries, int32_t nq,
+                                                        const int32_t* pool_sizes, int32_t max_pool,
+                                                        const int32_t* top_ks, const RoverSearchOutputs* out,
+                                                        void* stream) {
+  (void)h;
+  if (!valid_params(p) || nq < 0 || !out || !queries || !pool_sizes || !out->status ||
+      (out->ids && (!out->dists || !out->counts || out->out_stride <= 0)) ||
+      (out->pool_ids && (!out->pool_dists || !out->pool_counts || p->pool_stride <= 0))) {
+    set_error("invalid arguments: params, queries, pool_sizes and out->status are required, "
+              "and each requested output needs its arrays and a positive stride");
+    return AEE_EBADPARM;
+  }
+  if (nq == 0) return AEE_SUCCESS;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  std::lock_guard<std::mutex> nlock(g_noalloc_mu);
+  const PqDevice& pq = s.pq;
+  if (!pq.loaded || !pq.has_graph) { set_error("no PQ index with a graph is loaded"); return AEE_EFAILED; }
+  if (max_pool <= 0 || max_pool > 4096) { set_error("max_pool must be in 1..4096"); return AEE_EBADPARM; }
+  if (p->correction && pq.view.residual_bits == 0) { set_error("correction needs residuals"); return AEE_EBADPARM; }
+  if (p->refine_budget > 0 && pq.view.residual_bits == 0) { set_error("refine needs residuals"); return AEE_EBADPARM; }
+  const int expand = std::min(p->expand_count, pq.view.degree);
+  if (expand > kMaxBatch) { set_error("expand_count above %d", kMaxBatch); return AEE_EBADPARM; }
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) { set_error("device %d out of range", dev); return AEE_EFAILED; }
+  cudaStream_t strm = static_cast<cudaStream_t>(stream);
+
+  // Set-up, once per device, with that device current: the array's name is
+  // a host-side stand-in in this code, so its device address must come from
+  // cudaGetSymbolAddress before any kernel may be given it.
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+      set_error("cudaGetSymbolAddress(no-alloc scratch) failed: %s", cudaGetErrorString(e));
+      return AEE_EFAILED;
+    }
+    CK(cudaDeviceGetAttribute(&g_noalloc_sms[dev], cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaMemsetAsync(ptr, 0, kNoAllocScratchBytes, strm));
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(ptr);
+    g_noalloc_gen[dev] = 1;
+  }
+  unsigned char* base = g_noalloc_ptr[dev];
+
+  PqSearchArgs a{};
+  a.ix = pq.view;
+  a.queries = queries;
+  a.nq = nq;
+  a.pool_sizes = pool_sizes;
+  a.top_ks = top_ks;
+  a.top_k = p->top_k;
+  a.entry_points = p->entry_points;
+  a.graph_entry = pq.graph_entry;
+  a.seed = p->seed;
+  a.expand_count = p->expand_count;
+  a.correction = p->correction;
+  a.refine_budget = p->refine_budget;
+  a.max_pool = max_pool;
+  a.pool_ids = out->pool_ids;
+  a.pool_dists = out->pool_dists;
+  a.pool_stride = p->pool_stride;
+  a.pool_counts = out->pool_counts;
+  a.out_ids = out->ids;
+  a.out_dists = out->dists;
+  a.out_stride = out->out_stride;
+  a.out_counts = out->counts;
+  a.stats = reinterpret_cast<unsigned long long*>(out->stats);
+  a.status = out->status;
+  pq_search_layout(&a, p->refine_budget);
+  const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
+  if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, max_pool); return AEE_EBADPARM; }
+  CK(cudaFuncSetAttribute(pq_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+
+  // Visited-table geometry: the same per-slot capacity rule as the
+  // allocating path; the number of warp slots is what fits in the array.
+  const uint64_t est = static_cast<uint64_t>(std::min(p->entry_points, pq.view.n)) +
+                       (2ull * max_pool + 64ull) * static_cast<uint64_t>(expand);
+  const uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * est));
+  const size_t per_slot = static_cast<size_t>(entries) * 8u;
+  const size_t fit_slots = (kNoAllocScratchBytes - kNoAllocHeaderBytes) / per_slot;
+  if (fit_slots < static_cast<size_t>(kSearchWarps)) {
+    set_error("request needs %zu bytes of visited table per warp; the no-alloc scratch holds %zu bytes "
+              "(%d warps minimum): lower pool/entry_points/expand_count or use calculator_rover_pq_search_device",
+              per_slot, kNoAllocScratchBytes - kNoAllocHeaderBytes, kSearchWarps);
+    return AEE_EBADPARM;
+  }
+  const int max_blocks = resident_blocks(reinterpret_cast<const void*>(pq_search_kernel), kSearchWarps * 32, smem,
+                                         g_noalloc_sms[dev]);
+  int blocks = std::min<int>(max_blocks, static_cast<int>(fit_slots / kSearchWarps));
+  blocks = std::max(1, std::min(blocks, (nq + kSearchWarps - 1) / kSearchWarps));
+
+  // Generations make stale entries of earlier calls read as empty; when the
+  // 32-bit range would wrap, the tables are cleared and numbering restarts.
+  if (static_cast<uint64_t>(g_noalloc_gen[dev]) + static_cast<uint64_t>(nq) >= 0xffffffffull) {
+    CK(cudaMemsetAsync(base + kNoAllocHeaderBytes, 0, kNoAllocScratchBytes - kNoAllocHeaderBytes, strm));
+    g_noalloc_gen[dev] = 1;
+  }
+  a.visited = reinterpret_cast<unsigned long long*>(base + kNoAllocHeaderBytes);
+  a.visited_mask = entries - 1u;
+  a.gen_base = g_noalloc_gen[dev];
+  g_noalloc_gen[dev] += static_cast<uint32_t>(nq);
+  a.next_query = reinterpret_cast<unsigned int*>(base);
+  unsigned int* flag = reinterpret_cast<unsigned int*>(base + 4);
+  // the counter and the flag keep the last call's values: start them at zero
+  CK(cudaMemsetAsync(base, 0, 8, strm));
+  CK(cudaMemsetAsync(out->status, 0, static_cast<size_t>(nq) * sizeof(int32_t), strm));
+  pq_search_kernel<<<blocks, kSearchWarps * 32, smem, strm>>>(a);
+  CK(cudaGetLastError());
+  noalloc_status_any<<<std::min(64, (nq + 255) / 256), 256, 0, strm>>>(out->status, nq, flag);
+  CK(cudaGetLastError());
+  g_launches += 2;
+  unsigned int any = 0;
+  CK(cudaMemcpyAsync(&any, flag, sizeof(any), cudaMemcpyDeviceToHost, strm));
+  CK(cudaStreamSynchronize(strm));
+  if (any) {
+    if (any & (1u << kStatusTableFull))
+      set_error("a query exceeded its visited table (%u entries per warp) in the no-alloc scratch; "
+                "rerun it with calculator_rover_pq_search_device", entries);
+    else
+      set_error("some queries failed: status bits 0x%x (see out->status)", any);
+    return AEE_EFAILED;
+  }
+  return AEE_SUCCESS;
+}
