@@ -214,8 +214,10 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
   pq_search_layout(&a, p->refine_budget);
   const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, max_pool); return AEE_EBADPARM; }
-  CK(cudaFuncSetAttribute(pq_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  const int max_blocks = resident_blocks(reinterpret_cast<const void*>(pq_search_kernel), kSearchWarps * 32, smem, s.sms);
+  const PqSearchFn kernel = pq_search_kernel_for(pq.view, p->correction != 0);
+  CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          static_cast<int>(smem)));
+  const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
   const int blocks = std::max(1, std::min(max_blocks, (nq + kSearchWarps - 1) / kSearchWarps));
   const size_t slots = static_cast<size_t>(blocks) * kSearchWarps;
   const uint64_t est = static_cast<uint64_t>(std::min(p->entry_points, pq.view.n)) +
@@ -234,7 +236,7 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
     a.gen_base = gen_base;
     a.next_query = s.counter.as<unsigned int>();
     CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
-    pq_search_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
+    kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
     CK(cudaGetLastError());
     ++g_launches;
     s.h_status.resize(nq);
@@ -1134,7 +1136,9 @@ extern "C" AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const
   pq_search_layout(&a, p->refine_budget);
   const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, max_pool); return AEE_EBADPARM; }
-  CK(cudaFuncSetAttribute(pq_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  const PqSearchFn kernel = pq_search_kernel_for(pq.view, p->correction != 0);
+  CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          static_cast<int>(smem)));
 
   // Visited-table geometry: the same per-slot capacity rule as the
   // allocating path; the number of warp slots is what fits in the array.
@@ -1149,7 +1153,7 @@ extern "C" AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const
               per_slot, kNoAllocScratchBytes - kNoAllocHeaderBytes, kSearchWarps);
     return AEE_EBADPARM;
   }
-  const int max_blocks = resident_blocks(reinterpret_cast<const void*>(pq_search_kernel), kSearchWarps * 32, smem,
+  const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem,
                                          g_noalloc_sms[dev]);
   int blocks = std::min<int>(max_blocks, static_cast<int>(fit_slots / kSearchWarps));
   blocks = std::max(1, std::min(blocks, (nq + kSearchWarps - 1) / kSearchWarps));
@@ -1169,7 +1173,7 @@ extern "C" AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const
   // the counter and the flag keep the last call's values: start them at zero
   CK(cudaMemsetAsync(base, 0, 8, strm));
   CK(cudaMemsetAsync(out->status, 0, static_cast<size_t>(nq) * sizeof(int32_t), strm));
-  pq_search_kernel<<<blocks, kSearchWarps * 32, smem, strm>>>(a);
+  kernel<<<blocks, kSearchWarps * 32, smem, strm>>>(a);
   CK(cudaGetLastError());
   noalloc_status_any<<<std::min(64, (nq + 255) / 256), 256, 0, strm>>>(out->status, nq, flag);
   CK(cudaGetLastError());

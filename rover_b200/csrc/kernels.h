@@ -38,7 +38,10 @@ struct PqSearchArgs {
   int32_t smem_per_warp, smem_query_bytes, smem_refine_offset, refine_capacity;
 };
 
-__global__ void pq_search_kernel(PqSearchArgs a);
+using PqSearchFn = void (*)(PqSearchArgs);
+// The pq_search kernel instantiated for this index shape (a __global__
+// function; launch with fn<<<grid, kSearchWarps * 32, smem, stream>>>(args)).
+PqSearchFn pq_search_kernel_for(const PqIndexView& ix, bool correction);
 
 // Layout of the per-warp shared-memory slice of pq_search_kernel.
 inline void pq_search_layout(PqSearchArgs* a, int refine_budget) {

@@ -80,6 +80,96 @@ __device__ __forceinline__ bool pq_score(const PqIndexView& ix, const float* __r
   return true;
 }
 
+// Shape-specialised scorer for Ks=256 codebooks: the candidate's whole code
+// row and residual row are fetched up front with 16-byte (or 8/4-byte)
+// vector loads and every loop is unrolled, so a candidate costs one round
+// of independent memory requests instead of one per subspace or dimension.
+// The floating-point operations and their order are those of pq_score.
+template <int M, int SUB, int RBITS>
+__device__ __forceinline__ bool pq_score_fixed(const PqIndexView& ix, const float* __restrict__ q, int32_t id,
+                                               bool correction, float* out_adc, float* out_dist) {
+  constexpr int DIM = M * SUB;
+  constexpr int RCB = RBITS == 8 ? DIM : DIM / 2;
+  constexpr int CW = (M + 3) / 4;      // code words
+  constexpr int RW = RCB / 4;          // residual words
+  uint32_t cw[CW];
+  const uint8_t* crow = ix.codes + static_cast<size_t>(id) * M;
+  if constexpr (M % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < M / 16; ++i) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(crow) + i);
+      cw[4 * i] = v.x; cw[4 * i + 1] = v.y; cw[4 * i + 2] = v.z; cw[4 * i + 3] = v.w;
+    }
+  } else if constexpr (M % 8 == 0) {
+#pragma unroll
+    for (int i = 0; i < M / 8; ++i) {
+      const uint2 v = __ldg(reinterpret_cast<const uint2*>(crow) + i);
+      cw[2 * i] = v.x; cw[2 * i + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < CW; ++i) cw[i] = __ldg(reinterpret_cast<const uint32_t*>(crow) + i);
+  }
+  uint32_t rw[RW];
+  float scale = 0.0f, zero = 0.0f;
+  if (correction) {
+    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+    scale = qp.x;
+    zero = qp.y;
+    const uint8_t* res = pq_residual_row(ix, id);
+    if constexpr (RCB % 16 == 0) {
+#pragma unroll
+      for (int i = 0; i < RCB / 16; ++i) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(res) + i);
+        rw[4 * i] = v.x; rw[4 * i + 1] = v.y; rw[4 * i + 2] = v.z; rw[4 * i + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < RW; ++i) rw[i] = __ldg(reinterpret_cast<const uint32_t*>(res) + i);
+    }
+    if (!isfinite(scale) || !isfinite(zero) || !(scale > 0.0f)) return false;
+  }
+  float adc = 0.0f, acc = 0.0f;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const uint32_t c = (cw[m >> 2] >> (8 * (m & 3))) & 255u;
+    const float* cen = ix.codebook + (static_cast<size_t>(m) * 256u + c) * SUB;
+    float cv[SUB];
+    if constexpr (SUB % 4 == 0) {
+#pragma unroll
+      for (int t = 0; t < SUB / 4; ++t) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(cen) + t);
+        cv[4 * t] = v.x; cv[4 * t + 1] = v.y; cv[4 * t + 2] = v.z; cv[4 * t + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int t = 0; t < SUB; ++t) cv[t] = __ldg(cen + t);
+    }
+    float lut = 0.0f;
+#pragma unroll
+    for (int j = 0; j < SUB; ++j) {
+      const int d = m * SUB + j;
+      const float qd = q[d];
+      const float diff = fsub(qd, cv[j]);
+      lut = fadd(lut, fmul(diff, diff));
+      if (correction) {
+        uint32_t r;
+        if constexpr (RBITS == 8) r = (rw[d >> 2] >> (8 * (d & 3))) & 255u;
+        else r = (rw[d >> 3] >> (4 * (d & 7))) & 15u;
+        const float x = fadd(fadd(cv[j], fmul(u8f(r), scale)), zero);
+        const float dq = fsub(qd, x);
+        acc = fadd(acc, fmul(dq, dq));
+      }
+    }
+    adc = fadd(adc, lut);
+  }
+  if (!isfinite(adc)) return false;
+  if (correction && !isfinite(acc)) return false;
+  *out_adc = adc;
+  *out_dist = correction ? acc : adc;
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // Final refine of the first `count` pool entries (refine_impl with the PQ
 // residual decode provider): FP32 decode ((c + code*s) + z), FP64 sum of
@@ -191,41 +281,59 @@ __device__ __forceinline__ int merge_batch(uint64_t* list, int size, int cap, ui
   return min_ins;
 }
 
-template <int PER>
-__device__ bool score_and_merge(const PqSearchArgs& a, const float* q, uint64_t* list, int* size,
-                                int cap, uint64_t* stage, const int32_t* batch_ids, int nb,
-                                int* cursor, int lane) {
-  uint64_t v[PER];
+template <int M, int SUB, int RBITS>
+__device__ __forceinline__ bool score_one(const PqIndexView& ix, const float* __restrict__ q, int32_t id,
+                                          bool correction, float* adc, float* dist) {
+  if constexpr (M == 0) return pq_score(ix, q, id, correction, adc, dist);
+  else return pq_score_fixed<M, SUB, RBITS>(ix, q, id, correction, adc, dist);
+}
+
+// Score batch_ids[0..nb) (one lane per candidate) into keys[0..nb).
+// Returns false when the reference would reject any candidate.
+template <int M, int SUB, int RBITS>
+__device__ __noinline__ bool score_batch(const PqSearchArgs& a, const float* q, const int32_t* batch_ids, int nb,
+                                         uint64_t* keys, int lane) {
   bool bad = false;
+  for (int e = lane; e < nb; e += kWarp) {
+    const int32_t id = batch_ids[e];
+    float adc, dist;
+    if (score_one<M, SUB, RBITS>(a.ix, q, id, a.correction != 0, &adc, &dist)) keys[e] = make_key(dist, id);
+    else bad = true;
+  }
+  __syncwarp();
+  return !__any_sync(kFullMask, bad);
+}
+
+// Sort the scored batch (keys in `stage`) and merge it into the list.
+template <int PER>
+__device__ __forceinline__ void sort_and_merge(uint64_t* list, int* size, int cap, uint64_t* stage, int nb,
+                                               int* cursor, int lane) {
+  uint64_t v[PER];
 #pragma unroll
   for (int r = 0; r < PER; ++r) {
     const int e = lane + 32 * r;
-    v[r] = kEmptyKey;
-    if (e < nb) {
-      const int32_t id = batch_ids[e];
-      float adc, dist;
-      if (pq_score(a.ix, q, id, a.correction != 0, &adc, &dist)) v[r] = make_key(dist, id);
-      else bad = true;
-    }
+    v[r] = e < nb ? stage[e] : kEmptyKey;
   }
-  if (__any_sync(kFullMask, bad)) return false;
+  __syncwarp();
   warp_bitonic_sort<PER>(v, lane);
   const int min_ins = merge_batch<PER>(list, *size, cap, stage, v, nb, lane);
   *size = min(cap, *size + nb);
   *cursor = min(*cursor, min_ins);
+}
+
+template <int M, int SUB, int RBITS>
+__device__ bool score_and_merge(const PqSearchArgs& a, const float* q, uint64_t* list, int* size, int cap,
+                                uint64_t* stage, const int32_t* batch_ids, int nb, int* cursor, int lane) {
+  if (!score_batch<M, SUB, RBITS>(a, q, batch_ids, nb, stage, lane)) return false;
+  if (nb <= 32) sort_and_merge<1>(list, size, cap, stage, nb, cursor, lane);
+  else if (nb <= 64) sort_and_merge<2>(list, size, cap, stage, nb, cursor, lane);
+  else sort_and_merge<4>(list, size, cap, stage, nb, cursor, lane);
   return true;
 }
 
-__device__ bool dispatch_batch(const PqSearchArgs& a, const float* q, uint64_t* list, int* size,
-                               int cap, uint64_t* stage, const int32_t* batch_ids, int nb,
-                               int* cursor, int lane) {
-  if (nb <= 32) return score_and_merge<1>(a, q, list, size, cap, stage, batch_ids, nb, cursor, lane);
-  if (nb <= 64) return score_and_merge<2>(a, q, list, size, cap, stage, batch_ids, nb, cursor, lane);
-  return score_and_merge<4>(a, q, list, size, cap, stage, batch_ids, nb, cursor, lane);
-}
-
+template <int M, int SUB, int RBITS>
 __global__ void __launch_bounds__(kSearchWarps * 32)
-pq_search_kernel(PqSearchArgs a) {
+pq_search_kernel_t(PqSearchArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -313,7 +421,7 @@ pq_search_kernel(PqSearchArgs a) {
       __syncwarp();
       if (__any_sync(kFullMask, st != kStatusOk)) { st = kStatusTableFull; break; }
       scored += nb;
-      if (nb > 0 && !score_and_merge<1>(a, q, list, &size, cap, stage, batch, nb, &cursor, lane)) {
+      if (nb > 0 && !score_and_merge<M, SUB, RBITS>(a, q, list, &size, cap, stage, batch, nb, &cursor, lane)) {
         st = kStatusNumeric;
         break;
       }
@@ -375,7 +483,7 @@ pq_search_kernel(PqSearchArgs a) {
       __syncwarp();
       if (nb == 0) continue;
       scored += nb;
-      if (!dispatch_batch(a, q, list, &size, cap, stage, batch, nb, &cursor, lane)) {
+      if (!score_and_merge<M, SUB, RBITS>(a, q, list, &size, cap, stage, batch, nb, &cursor, lane)) {
         st = kStatusNumeric;
         break;
       }
@@ -432,6 +540,27 @@ pq_search_kernel(PqSearchArgs a) {
     }
     __syncwarp();
   }
+}
+
+// Kernel instantiation for an index shape: Ks=256 shapes with a specialised
+// scorer, the generic kernel otherwise.
+PqSearchFn pq_search_kernel_for(const PqIndexView& ix, bool correction) {
+  if (ix.ks == 256 && ix.code_bytes == ix.m) {
+    const bool r8 = !correction || ix.residual_bits == 8;
+    const bool r4 = correction && ix.residual_bits == 4;
+    if (r8 || r4) {
+#define ROVER_PQ_SHAPE(MM, SS)                                                 \
+  if (ix.m == MM && ix.subdim == SS)                                           \
+    return r8 ? pq_search_kernel_t<MM, SS, 8> : pq_search_kernel_t<MM, SS, 4>;
+      ROVER_PQ_SHAPE(16, 8)
+      ROVER_PQ_SHAPE(32, 4)
+      ROVER_PQ_SHAPE(24, 4)
+      ROVER_PQ_SHAPE(8, 8)
+      ROVER_PQ_SHAPE(16, 4)
+#undef ROVER_PQ_SHAPE
+    }
+  }
+  return pq_search_kernel_t<0, 0, 0>;
 }
 
 }  // namespace rover
