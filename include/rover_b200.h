@@ -32,6 +32,12 @@ extern "C" {
 /* Search modes. */
 #define ROVER_MODE_EXACT 0   /* reference expansion order, bit-exact results */
 
+/* Residual layouts for PQ searches with correction (RoverSearchParams.layout).
+ * Both give identical results; they trade device memory for arithmetic. */
+#define ROVER_LAYOUT_AUTO 0     /* decoded when it fits, else packed */
+#define ROVER_LAYOUT_PACKED 1   /* .pqresN rows decoded per candidate */
+#define ROVER_LAYOUT_DECODED 2  /* FP32 rows ((c + code*s) + z) built once per index */
+
 /* A pure-PQ index held in host memory (layouts of the reference bundle:
  * graph.rover rows, .pqcodes / .pqbook payloads, .pqresN block payload,
  * .pqresN.qparams payload).  Loaded once; the library keeps a device copy. */
@@ -75,7 +81,8 @@ typedef struct RoverSearchParams {
     int32_t pool_stride;     /* columns of the optional pool output */
     int32_t sq_mode;         /* SQ only: 0 = device search (calculator_retrieval_search),
                                 1 = SQMD session semantics */
-    int32_t reserved[6];
+    int32_t layout;          /* PQ with correction: ROVER_LAYOUT_* */
+    int32_t reserved[5];
 } RoverSearchParams;
 
 /* Per-call outputs.  Host pointers for calculator_rover_*_search, device

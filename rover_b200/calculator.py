@@ -55,7 +55,7 @@ class SearchParams(C.Structure):
     _fields_ = [("size", C.c_int32), ("mode", C.c_int32), ("entry_points", C.c_int32), ("seed", C.c_uint32),
                 ("expand_count", C.c_int32), ("correction", C.c_int32), ("refine_budget", C.c_int32),
                 ("top_k", C.c_int32), ("pool_stride", C.c_int32), ("sq_mode", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("layout", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class SearchOutputs(C.Structure):
@@ -180,7 +180,7 @@ class Calculator:
 
     @staticmethod
     def params(entry_points=1, expand_count=32, correction=1, refine_budget=0, top_k=10, seed=42,
-               pool_stride=0, sq_mode=0, mode=0) -> SearchParams:
+               pool_stride=0, sq_mode=0, mode=0, layout=0) -> SearchParams:
         p = SearchParams()
         p.size = C.sizeof(SearchParams)
         p.mode = mode
@@ -192,6 +192,7 @@ class Calculator:
         p.top_k = top_k
         p.pool_stride = pool_stride
         p.sq_mode = sq_mode
+        p.layout = layout
         return p
 
     def pq_search(self, queries, pool_sizes, top_k=10, top_ks=None, pool_stride=0, stats=True, check=True,

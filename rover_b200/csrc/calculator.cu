@@ -68,14 +68,33 @@ struct DevBuf {
   template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// The entry seeds of one (entry_points, seed) request: the distinct ids in
+// draw order plus a bitmap of them.  Queries share them.
+struct SeedSet {
+  bool valid = false;
+  int32_t entries = 0;
+  uint32_t seed = 0;
+  int32_t count = 0, dups = 0;
+  DevBuf ids, bits;
+  void release() {
+    ids.release(); bits.release();
+    valid = false;
+  }
+};
+
 struct PqDevice {
   DevBuf graph, codes, codebook, residual, qparams;
+  DevBuf decoded;                 // [n][dim] FP32 reconstructions, built on first use
+  bool decoded_ready = false;
+  SeedSet seeds;
   PqIndexView view{};
   int32_t graph_entry = -1;
   bool loaded = false;
   bool has_graph = false;
   void release() {
     graph.release(); codes.release(); codebook.release(); residual.release(); qparams.release();
+    decoded.release(); seeds.release();
+    decoded_ready = false;
     loaded = false;
     has_graph = false;
   }
@@ -103,7 +122,7 @@ struct State {
   SqDevice legacy;                // calculator_retrieval_load(_dma) index
   bool legacy_dma = false;
   // scratch
-  DevBuf visited, heaps, counter, status, stats, luts;
+  DevBuf visited, heaps, counter, status, stats, luts, seed_dists;
   uint32_t visited_mask = 0;
   size_t visited_slots = 0;
   uint32_t gen_next = 1;
@@ -169,7 +188,145 @@ int resident_blocks(const void* kernel, int threads, size_t smem, int sms) {
 
 bool valid_params(const RoverSearchParams* p) {
   return p && p->size >= static_cast<int32_t>(offsetof(RoverSearchParams, reserved)) && p->entry_points > 0 &&
-         p->expand_count > 0 && p->refine_budget >= 0 && p->refine_budget <= 2000;
+         p->expand_count > 0 && p->refine_budget >= 0 && p->refine_budget <= 2000 &&
+         p->layout >= ROVER_LAYOUT_AUTO && p->layout <= ROVER_LAYOUT_DECODED;
+}
+
+// Entry seeds as pure_pq_make_seed_ids draws them
+// (src/dsp_demo/retrieval_rpc_demo_pure_pq.c:192-208): the graph entry first
+// (when valid), then id = (seed * n) >> 32 after each LCG step; a draw that
+// repeats an earlier id is skipped as the search's visited check skips it
+// (retrieval_sqmd_pure_pq.c:846-850).
+AEEResult ensure_seeds(State& s, PqDevice& pq, int32_t entry_points, uint32_t seed) {
+  const int32_t n = pq.view.n;
+  const int32_t entries = std::min(entry_points, n);
+  SeedSet& ss = pq.seeds;
+  if (ss.valid && ss.entries == entries && ss.seed == seed) return AEE_SUCCESS;
+  ss.valid = false;
+  std::vector<uint32_t> bits((static_cast<size_t>(n) + 31) / 32, 0u);
+  std::vector<int32_t> ids;
+  ids.reserve(entries);
+  int32_t dups = 0;
+  uint32_t lcg = seed;
+  for (int32_t i = 0; i < entries; ++i) {
+    int32_t id;
+    if (i == 0 && pq.graph_entry >= 0 && pq.graph_entry < n) {
+      id = pq.graph_entry;
+    } else {
+      lcg = lcg * 1103515245u + 12345u;
+      id = static_cast<int32_t>((static_cast<uint64_t>(lcg) * static_cast<uint64_t>(n)) >> 32);
+    }
+    uint32_t& w = bits[static_cast<uint32_t>(id) >> 5];
+    const uint32_t bit = 1u << (static_cast<uint32_t>(id) & 31u);
+    if (w & bit) {
+      ++dups;
+    } else {
+      w |= bit;
+      ids.push_back(id);
+    }
+  }
+  if (upload(ss.ids, ids.data(), ids.size(), s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  if (upload(ss.bits, bits.data(), bits.size(), s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  CK(cudaStreamSynchronize(s.stream));
+  ss.entries = entries;
+  ss.seed = seed;
+  ss.count = static_cast<int32_t>(ids.size());
+  ss.dups = dups;
+  ss.valid = true;
+  return AEE_SUCCESS;
+}
+
+// Builds the decoded rows once per loaded index.  *ok = false when they do
+// not fit (the caller then uses the packed layout).
+AEEResult ensure_decoded(State& s, PqDevice& pq, bool* ok) {
+  *ok = false;
+  if (pq.decoded_ready) { *ok = true; return AEE_SUCCESS; }
+  const size_t bytes = static_cast<size_t>(pq.view.n) * pq.view.dim * sizeof(float);
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  if (bytes > free_b / 2) return AEE_SUCCESS;
+  if (pq.decoded.ensure(bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return AEE_SUCCESS;
+  }
+  launch_pq_decode(pq.view, pq.decoded.as<float>(), s.stream);
+  CK(cudaGetLastError());
+  ++g_launches;
+  CK(cudaStreamSynchronize(s.stream));
+  pq.decoded_ready = true;
+  *ok = true;
+  return AEE_SUCCESS;
+}
+
+constexpr int kSharedVisitedSlots = 2048;             // per warp, 8 KB
+constexpr size_t kSeedDistBudget = 512ull << 20;      // bytes of query x seed distances per launch
+
+// Exact PQ search over decoded rows (pq_decoded.cu): per query chunk, the
+// all-seeds distance pass, then the search kernel.
+AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p, int nq, int expand,
+                            cudaStream_t stream) {
+  PqDevice& pq = s.pq;
+  if (ensure_seeds(s, pq, p->entry_points, p->seed) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  const SeedSet& ss = pq.seeds;
+  PqDecodedArgs b{};
+  b.decoded = pq.decoded.as<float>();
+  b.seed_ids = ss.ids.as<int32_t>();
+  b.n_seeds = ss.count;
+  b.seed_dups = ss.dups;
+  b.seed_bits = ss.bits.as<uint32_t>();
+  pq_decoded_layout(&a, &b, p->refine_budget, kSharedVisitedSlots);
+  const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
+  if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, a.max_pool); return AEE_EBADPARM; }
+  const PqDecodedFn kernel = pq_decoded_kernel_for(pq.view.dim);
+  CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          static_cast<int>(smem)));
+  const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
+  const int chunk = static_cast<int>(std::max<size_t>(
+      1, std::min<size_t>(nq, kSeedDistBudget / (static_cast<size_t>(ss.count) * sizeof(float)))));
+  CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
+  b.seed_dists = s.seed_dists.as<float>();
+  const int blocks_cap = std::max(1, std::min(max_blocks, (chunk + kSearchWarps - 1) / kSearchWarps));
+  const size_t slots = static_cast<size_t>(blocks_cap) * kSearchWarps;
+  uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * (2ull * a.max_pool + 64ull) * expand));
+  CK(s.counter.ensure(sizeof(unsigned int)));
+  CK(cudaMemsetAsync(a.status, 0, nq * sizeof(int32_t), stream));
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    uint32_t gen_base = 0;
+    if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    if (stream != s.stream) CK(cudaStreamSynchronize(s.stream));
+    a.visited = s.visited.as<unsigned long long>();
+    a.visited_mask = s.visited_mask;
+    a.gen_base = gen_base;
+    a.next_query = s.counter.as<unsigned int>();
+    for (int q0 = 0; q0 < nq; q0 += chunk) {
+      const int q1 = std::min(nq, q0 + chunk);
+      launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
+                           s.seed_dists.as<float>(), stream);
+      CK(cudaGetLastError());
+      ++g_launches;
+      b.q_begin = q0;
+      b.q_end = q1;
+      CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
+      const int blocks = std::max(1, std::min(blocks_cap, (q1 - q0 + kSearchWarps - 1) / kSearchWarps));
+      kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a, b);
+      CK(cudaGetLastError());
+      ++g_launches;
+    }
+    s.h_status.resize(nq);
+    CK(cudaMemcpyAsync(s.h_status.data(), a.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    bool retry = false;
+    for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
+    if (!retry) break;
+    entries = next_pow2(static_cast<uint64_t>(entries) * 4);
+    CK(cudaMemsetAsync(a.status, 0, nq * sizeof(int32_t), stream));
+  }
+  for (int i = 0; i < nq; ++i)
+    if (s.h_status[i] != kStatusOk) {
+      set_error("query %d failed with status %d", i, s.h_status[i]);
+      return AEE_EFAILED;
+    }
+  return AEE_SUCCESS;
 }
 
 // Core PQ search on device buffers.  Retries queries whose visited table
@@ -211,6 +368,19 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
   a.out_counts = d_out.counts;
   a.stats = reinterpret_cast<unsigned long long*>(d_out.stats);
   a.status = d_out.status;
+  // residual layout: decoded rows when correction is on and they fit
+  const bool decodable = p->correction != 0 && pq.view.dim % 4 == 0 &&
+                         reinterpret_cast<uintptr_t>(d_queries) % 16 == 0;
+  if (p->layout == ROVER_LAYOUT_DECODED && !decodable) {
+    set_error("the decoded layout needs correction on, dim %% 4 == 0 and 16-byte aligned queries");
+    return AEE_EBADPARM;
+  }
+  if (decodable && p->layout != ROVER_LAYOUT_PACKED) {
+    bool ok = false;
+    if (ensure_decoded(s, s.pq, &ok) != AEE_SUCCESS) return AEE_EFAILED;
+    if (ok) return pq_search_decoded(s, a, p, nq, expand, stream);
+    if (p->layout == ROVER_LAYOUT_DECODED) { set_error("decoded rows do not fit in device memory"); return AEE_ENOMEMORY; }
+  }
   pq_search_layout(&a, p->refine_budget);
   const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, max_pool); return AEE_EBADPARM; }

@@ -59,6 +59,43 @@ inline void pq_search_layout(PqSearchArgs* a, int refine_budget) {
   a->smem_per_warp = (off + cap * 12 + 15) & ~15;
 }
 
+// ---- PQ search over decoded rows (correction on) ---------------------------
+//
+// The decoded layout stores every vector's residual reconstruction
+// x = (c + code*s) + z as FP32 (NaN rows where the qparams are invalid), so a
+// corrected distance is the plain sequential sum of (q - x)^2.  The entry
+// seeds are the same for every query; their distances come from
+// pq_seed_dists_kernel, a tiled all-queries x all-seeds pass.
+
+struct PqDecodedArgs {
+  const float* decoded;        // [n][dim]
+  const int32_t* seed_ids;     // [n_seeds] distinct entry ids, draw order
+  int32_t n_seeds;
+  int32_t seed_dups;           // draws skipped as already visited
+  const uint32_t* seed_bits;   // [ceil(n/32)] bitmap of seed ids
+  const float* seed_dists;     // [q_end - q_begin][n_seeds]
+  int32_t q_begin, q_end;      // queries served by this launch
+  int32_t vis_cap;             // shared-memory visited slots per warp (power of two)
+  int32_t smem_vis_offset;     // byte offset of that table in the warp slice
+};
+
+using PqDecodedFn = void (*)(PqSearchArgs, PqDecodedArgs);
+// The decoded-layout kernel for this dimension (dim % 4 == 0 required).
+PqDecodedFn pq_decoded_kernel_for(int dim);
+
+// Warp slice: query | list | stage | batch | refine scratch | visited table.
+inline void pq_decoded_layout(PqSearchArgs* a, PqDecodedArgs* b, int refine_budget, int vis_cap) {
+  pq_search_layout(a, refine_budget);
+  const int off = (a->smem_per_warp + 15) & ~15;
+  b->smem_vis_offset = off;
+  b->vis_cap = vis_cap;
+  a->smem_per_warp = (off + vis_cap * 4 + 15) & ~15;
+}
+
+void launch_pq_decode(const PqIndexView& ix, float* decoded, cudaStream_t s);
+void launch_pq_seed_dists(const float* queries, int q_begin, int q_end, int dim, const float* decoded,
+                          const int32_t* seed_ids, int n_seeds, float* out, cudaStream_t s);
+
 // ---- SQ search (heap-exact) ----------------------------------------------
 
 enum SqSearchMode : int32_t { kSqModeDsp = 0, kSqModeSqmd = 1 };

@@ -1,0 +1,431 @@
+// pq_decoded.cu -- PQ beam search with the ONLINE residual policy over
+// decoded rows, on sm_100a.
+//
+// Same search as pq_search.cu (retrieval_pure_pq_search_scalar_with_policy,
+// src/dsp_demo/retrieval_sqmd_pure_pq.c:793-969, with
+// retrieval_pq_residual_query_evaluate, retrieval_pq_residual.c:983, as the
+// distance policy), restructured around two facts:
+//
+// 1. The corrected distance of a candidate is sum_j (q_j - x_j)^2 in
+//    dimension order, with x_j = (c_j + code_j * s) + z rounded per step.  x
+//    does not depend on the query, so pq_decode_kernel writes it once per
+//    index (FP32, n x dim).  A candidate then costs one 4*dim-byte row and
+//    three FP32 operations per dimension instead of about eight.  A vector
+//    whose qparams the reference rejects gets a NaN row: its distance is
+//    non-finite and the query fails exactly where the reference's would.
+//    The ADC distance only decides failure (non-finite ADC fails the query);
+//    when every LUT entry is at most FLT_MAX / (2 m) no ADC sum can overflow,
+//    so the kernel computes ADC only for queries whose LUT is that large.
+//
+// 2. The entry seeds (graph entry, then the LCG of pure_pq_make_seed_ids,
+//    src/dsp_demo/retrieval_rpc_demo_pure_pq.c:192-208) are identical for
+//    every query.  The host draws them once; pq_seed_dists_kernel computes
+//    all queries x all seeds in one tiled pass (same per-pair operation
+//    order); each search warp then builds its initial pool as the top-L of
+//    its row under (distance, id), which is the state the reference's pool
+//    reaches after inserting the seeds one by one.
+//
+// Visited ids: seeds are marked in a bitmap shared by all queries; the ids an
+// expansion claims go into a per-warp open-addressing table in shared memory.
+// A query whose expansions claim more than half that table moves its entries
+// into its global generation-tagged table and continues there.
+
+#include <cfloat>
+
+#include "pq_common.cuh"
+
+namespace rover {
+
+constexpr uint32_t kEmptySlot = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// Decoded rows: one thread per (vector, dimension).
+__global__ void pq_decode_kernel(PqIndexView ix, float* __restrict__ out) {
+  const size_t total = static_cast<size_t>(ix.n) * ix.dim;
+  for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int32_t v = static_cast<int32_t>(t / ix.dim);
+    const int d = static_cast<int>(t - static_cast<size_t>(v) * ix.dim);
+    const int m = d / ix.subdim;
+    const int j = d - m * ix.subdim;
+    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + v);
+    const uint8_t* code = ix.codes + static_cast<size_t>(v) * ix.code_bytes;
+    const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
+    const float cj = __ldg(ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim + j);
+    const uint8_t* res = pq_residual_row(ix, v);
+    const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, d))
+                                             : static_cast<uint32_t>(__ldg(res + d));
+    const bool bad = !isfinite(qp.x) || !isfinite(qp.y) || !(qp.x > 0.0f);
+    out[t] = bad ? __int_as_float(0x7fc00000) : fadd(fadd(cj, fmul(u8f(r), qp.x)), qp.y);
+  }
+}
+
+void launch_pq_decode(const PqIndexView& ix, float* decoded, cudaStream_t s) {
+  const size_t total = static_cast<size_t>(ix.n) * ix.dim;
+  const int threads = 256;
+  const int blocks = static_cast<int>(std::min<size_t>((total + threads - 1) / threads, 148ull * 64));
+  pq_decode_kernel<<<blocks, threads, 0, s>>>(ix, decoded);
+}
+
+// ---------------------------------------------------------------------------
+// All queries x all seeds: out[q][u] = sum_d (Q[q][d] - X[seed u][d])^2, each
+// pair summed sequentially in dimension order like the reference's
+// residual evaluation.  64 x 64 tile per CTA, 4 x 4 pairs per thread,
+// dimensions staged 32 at a time (transposed) in shared memory.
+constexpr int kSdTile = 64;
+constexpr int kSdK = 32;
+
+__global__ void __launch_bounds__(256) pq_seed_dists_kernel(const float* __restrict__ queries, int q_begin,
+                                                            int q_end, int dim, const float* __restrict__ decoded,
+                                                            const int32_t* __restrict__ seed_ids, int n_seeds,
+                                                            float* __restrict__ out) {
+  __shared__ __align__(16) float qs[kSdK][kSdTile + 4];
+  __shared__ __align__(16) float xs[kSdK][kSdTile + 4];
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  const int u0 = blockIdx.x * kSdTile;
+  const int q0 = q_begin + blockIdx.y * kSdTile;
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+  // rows this thread stages (two per operand per chunk)
+  const float* qrow[2];
+  const float* xrow[2];
+  int srow[2], scol[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int idx = tid + 256 * i;
+    srow[i] = idx >> 3;
+    scol[i] = (idx & 7) * 4;
+    const int qq = q0 + srow[i];
+    const int uu = u0 + srow[i];
+    qrow[i] = qq < q_end ? queries + static_cast<size_t>(qq) * dim : nullptr;
+    xrow[i] = uu < n_seeds ? decoded + static_cast<size_t>(__ldg(seed_ids + uu)) * dim : nullptr;
+  }
+  for (int k0 = 0; k0 < dim; k0 += kSdK) {
+    const int kc = min(kSdK, dim - k0);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int c = scol[i];
+      if (c < kc) {
+        float4 qv = make_float4(0.f, 0.f, 0.f, 0.f), xv = qv;
+        if (qrow[i]) qv = __ldg(reinterpret_cast<const float4*>(qrow[i] + k0 + c));
+        if (xrow[i]) xv = __ldg(reinterpret_cast<const float4*>(xrow[i] + k0 + c));
+        const int r = srow[i];
+        qs[c][r] = qv.x; qs[c + 1][r] = qv.y; qs[c + 2][r] = qv.z; qs[c + 3][r] = qv.w;
+        xs[c][r] = xv.x; xs[c + 1][r] = xv.y; xs[c + 2][r] = xv.z; xs[c + 3][r] = xv.w;
+      }
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < kc; ++kk) {
+      const float4 a = *reinterpret_cast<const float4*>(&qs[kk][ty * 4]);
+      const float4 b = *reinterpret_cast<const float4*>(&xs[kk][tx * 4]);
+      const float av[4] = {a.x, a.y, a.z, a.w};
+      const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float dl = fsub(av[i], bv[j]);
+          acc[i][j] = fadd(acc[i][j], fmul(dl, dl));
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int qq = q0 + ty * 4 + i;
+    if (qq >= q_end) continue;
+    float* orow = out + static_cast<size_t>(qq - q_begin) * n_seeds;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int uu = u0 + tx * 4 + j;
+      if (uu < n_seeds) orow[uu] = acc[i][j];
+    }
+  }
+}
+
+void launch_pq_seed_dists(const float* queries, int q_begin, int q_end, int dim, const float* decoded,
+                          const int32_t* seed_ids, int n_seeds, float* out, cudaStream_t s) {
+  const dim3 grid((n_seeds + kSdTile - 1) / kSdTile, (q_end - q_begin + kSdTile - 1) / kSdTile);
+  pq_seed_dists_kernel<<<grid, 256, 0, s>>>(queries, q_begin, q_end, dim, decoded, seed_ids, n_seeds, out);
+}
+
+// ---------------------------------------------------------------------------
+
+// Shared-memory visited insert: 1 = first visit, 0 = seen, -1 = no slot.
+__device__ __forceinline__ int smem_visit(uint32_t* tab, uint32_t mask, uint32_t id) {
+  uint32_t h = hash_id(id) & mask;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint32_t prev = atomicCAS(tab + h, kEmptySlot, id);
+    if (prev == kEmptySlot) return 1;
+    if (prev == id) return 0;
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// Corrected distance of one decoded row; false if non-finite.
+template <int D>
+__device__ __forceinline__ bool decoded_dist(const float* __restrict__ xrow, const float* q, int dim, float* out) {
+  const float4* x4 = reinterpret_cast<const float4*>(xrow);
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  const int n4 = D ? D / 4 : dim / 4;
+  float acc = 0.0f;
+#pragma unroll 8
+  for (int t = 0; t < n4; ++t) {
+    const float4 x = __ldg(x4 + t);
+    const float4 qq = q4[t];
+    float dl = fsub(qq.x, x.x); acc = fadd(acc, fmul(dl, dl));
+    dl = fsub(qq.y, x.y); acc = fadd(acc, fmul(dl, dl));
+    dl = fsub(qq.z, x.z); acc = fadd(acc, fmul(dl, dl));
+    dl = fsub(qq.w, x.w); acc = fadd(acc, fmul(dl, dl));
+  }
+  *out = acc;
+  return isfinite(acc);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kSearchWarps * 32, 4)
+pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  uint8_t* base = smem + static_cast<size_t>(warp) * a.smem_per_warp;
+  float* q = reinterpret_cast<float*>(base);
+  uint64_t* list = reinterpret_cast<uint64_t*>(base + a.smem_query_bytes);
+  uint64_t* stage = list + a.max_pool;
+  int32_t* batch = reinterpret_cast<int32_t*>(stage + kMaxBatch);
+  uint32_t* vis = reinterpret_cast<uint32_t*>(base + b.smem_vis_offset);
+  const uint32_t vmask = static_cast<uint32_t>(b.vis_cap - 1);
+  const int slot = blockIdx.x * kSearchWarps + warp;
+  VisitedTable vt;
+  vt.slots = a.visited + static_cast<size_t>(slot) * (a.visited_mask + 1ull);
+  vt.mask = a.visited_mask;
+  const PqIndexView& ix = a.ix;
+  const int dim = D ? D : ix.dim;
+  const float adc_bound = FLT_MAX / static_cast<float>(2 * ix.m);
+
+  for (;;) {
+    int qi = 0;
+    if (lane == 0) qi = b.q_begin + static_cast<int>(atomicAdd(a.next_query, 1u));
+    qi = __shfl_sync(kFullMask, qi, 0);
+    if (qi >= b.q_end) break;
+
+    const int cap = a.pool_sizes[qi];
+    int32_t* status = a.status + qi;
+    const int expand = min(a.expand_count, ix.degree);
+    if (cap <= 0 || cap > a.max_pool || expand <= 0 || expand > kMaxBatch || a.entry_points <= 0) {
+      if (lane == 0) *status = kStatusBadParam;
+      continue;
+    }
+    {
+      const float4* src = reinterpret_cast<const float4*>(a.queries + static_cast<size_t>(qi) * dim);
+      for (int t = lane; t < dim / 4; t += kWarp) reinterpret_cast<float4*>(q)[t] = __ldg(src + t);
+    }
+    for (int i = lane; i < b.vis_cap; i += kWarp) vis[i] = kEmptySlot;
+    __syncwarp();
+    // retrieval_pq_build_lut fails the query if any LUT entry is not finite;
+    // the largest entry decides whether ADC sums need checking at all.
+    bool bad = false;
+    float lmax = 0.0f;
+    for (int e = lane; e < ix.m * ix.ks; e += kWarp) {
+      const int m = e / ix.ks;
+      const float* cen = ix.codebook + static_cast<size_t>(e) * ix.subdim;
+      float acc = 0.0f;
+      for (int j = 0; j < ix.subdim; ++j) {
+        const float diff = fsub(q[m * ix.subdim + j], __ldg(cen + j));
+        acc = fadd(acc, fmul(diff, diff));
+      }
+      if (!isfinite(acc)) bad = true;
+      else lmax = fmaxf(lmax, acc);
+    }
+    if (__any_sync(kFullMask, bad)) {
+      if (lane == 0) *status = kStatusNumeric;
+      continue;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFullMask, lmax, off));
+    const bool check_adc = !(lmax <= adc_bound);
+    vt.gen = a.gen_base + static_cast<uint32_t>(qi);
+    int size = 0, cursor = 0;
+    unsigned long long scored = static_cast<unsigned long long>(b.n_seeds), expanded = 0;
+    unsigned long long dedup = lane == 0 ? static_cast<unsigned long long>(b.seed_dups) : 0ull;
+    int32_t st = kStatusOk;
+
+    // ---- initial pool: top-L of the seed row under (distance, id)
+    const float* drow = b.seed_dists + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
+    for (int e0 = 0; e0 < b.n_seeds; e0 += kMaxBatch) {
+      const uint64_t thr = size == cap ? key_cmp(list[cap - 1]) : kEmptyKey;
+      int cnt = 0;
+      bool nonfinite = false;
+#pragma unroll
+      for (int r = 0; r < kMaxBatch / kWarp; ++r) {
+        const int e = e0 + r * kWarp + lane;
+        uint64_t k = kEmptyKey;
+        if (e < b.n_seeds) {
+          const float d = drow[e];
+          if (!isfinite(d)) nonfinite = true;
+          else k = make_key(d, __ldg(b.seed_ids + e));
+        }
+        const bool keep = k < thr;
+        const unsigned km = __ballot_sync(kFullMask, keep);
+        if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = k;
+        cnt += __popc(km);
+      }
+      if (__any_sync(kFullMask, nonfinite)) { st = kStatusNumeric; break; }
+      __syncwarp();
+      if (cnt == 0) continue;
+      if (cnt <= 32) sort_and_merge<1>(list, &size, cap, stage, cnt, &cursor, lane);
+      else if (cnt <= 64) sort_and_merge<2>(list, &size, cap, stage, cnt, &cursor, lane);
+      else sort_and_merge<4>(list, &size, cap, stage, cnt, &cursor, lane);
+    }
+    if (st == kStatusOk && check_adc) {
+      bool adc_bad = false;
+      for (int e = lane; e < b.n_seeds; e += kWarp) {
+        float adc, dist;
+        if (!pq_score(ix, q, __ldg(b.seed_ids + e), false, &adc, &dist)) adc_bad = true;
+      }
+      if (__any_sync(kFullMask, adc_bad)) st = kStatusNumeric;
+    }
+
+    // ---- expansion loop (first unexpanded list entry, as pq_search.cu)
+    bool global_mode = false;
+    int claimed = 0;  // ids claimed by expansions of this query
+    const uint32_t load_limit = (a.visited_mask + 1u) >> 1;
+    while (st == kStatusOk) {
+      int pos = -1;
+      for (int b0 = cursor & ~31; b0 < size; b0 += kWarp) {
+        const int i = b0 + lane;
+        const bool cand = i >= cursor && i < size && !(list[i] & kExpandedBit);
+        const unsigned m = __ballot_sync(kFullMask, cand);
+        if (m) { pos = b0 + __ffs(m) - 1; break; }
+      }
+      if (pos < 0) break;
+      cursor = pos + 1;
+      const int32_t src = key_id(list[pos]);
+      __syncwarp();
+      if (lane == 0) list[pos] |= kExpandedBit;
+      const int32_t* row = ix.graph + static_cast<size_t>(src) * ix.degree;
+      // valid-prefix rule (pure_pq_graph_row_count)
+      int first_pad = expand;
+      bool row_bad = false;
+      int32_t nid_r[kMaxBatch / kWarp];
+#pragma unroll
+      for (int r = 0; r < kMaxBatch / kWarp; ++r) {
+        const int j = r * kWarp + lane;
+        nid_r[r] = -1;
+        if (r * kWarp < expand) {
+          const int32_t nid = j < expand ? __ldg(row + j) : -1;
+          nid_r[r] = nid;
+          const unsigned pad = __ballot_sync(kFullMask, j < expand && nid == -1);
+          if (pad && first_pad == expand) first_pad = r * kWarp + __ffs(pad) - 1;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kMaxBatch / kWarp; ++r) {
+        const int j = r * kWarp + lane;
+        if (j < expand) {
+          const int32_t nid = nid_r[r];
+          if (j < first_pad) row_bad |= (nid < 0 || nid >= ix.n);
+          else row_bad |= (nid != -1);
+        }
+      }
+      if (__any_sync(kFullMask, row_bad)) { st = kStatusBadRow; break; }
+      // move to the global table before this row could push the shared one
+      // past half load
+      bool full = false;
+      if (!global_mode && claimed + first_pad > b.vis_cap / 2) {
+        for (int i = lane; i < b.vis_cap; i += kWarp) {
+          const uint32_t id = vis[i];
+          if (id != kEmptySlot && visited_insert(vt, id) < 0) full = true;
+        }
+        global_mode = true;
+        __syncwarp();
+      }
+      // first visits, in row order
+      int nb = 0;
+#pragma unroll
+      for (int r = 0; r < kMaxBatch / kWarp; ++r) {
+        if (r * kWarp < first_pad) {
+          const int j = r * kWarp + lane;
+          int fresh = 0;
+          const int32_t nid = nid_r[r];
+          if (j < first_pad) {
+            const uint32_t u = static_cast<uint32_t>(nid);
+            if (__ldg(b.seed_bits + (u >> 5)) & (1u << (u & 31))) {
+              ++dedup;
+            } else {
+              const int rr = global_mode ? visited_insert(vt, u) : smem_visit(vis, vmask, u);
+              full |= rr < 0;
+              fresh = rr == 1;
+              if (rr == 0) ++dedup;
+            }
+          }
+          const unsigned fm = __ballot_sync(kFullMask, fresh);
+          if (fresh) batch[nb + __popc(fm & ((1u << lane) - 1u))] = nid;
+          nb += __popc(fm);
+        }
+      }
+      ++expanded;
+      claimed += nb;
+      if (__any_sync(kFullMask, full) || (global_mode && static_cast<uint32_t>(claimed) > load_limit)) {
+        st = kStatusTableFull;
+        break;
+      }
+      __syncwarp();
+      if (nb == 0) continue;
+      scored += nb;
+      // score: one lane per candidate, rows prefetched first
+      for (int e = lane; e < nb; e += kWarp) {
+        const float* xr = b.decoded + static_cast<size_t>(batch[e]) * dim;
+        for (int off = 0; off < dim; off += 32) prefetch_l1(xr + off);
+      }
+      bool sbad = false;
+      for (int e = lane; e < nb; e += kWarp) {
+        const int32_t id = batch[e];
+        float dist;
+        if (!decoded_dist<D>(b.decoded + static_cast<size_t>(id) * dim, q, dim, &dist)) sbad = true;
+        if (check_adc) {
+          float adc, unused;
+          if (!pq_score(ix, q, id, false, &adc, &unused)) sbad = true;
+        }
+        stage[e] = make_key(dist, id);
+      }
+      if (__any_sync(kFullMask, sbad)) { st = kStatusNumeric; break; }
+      __syncwarp();
+      if (nb <= 32) sort_and_merge<1>(list, &size, cap, stage, nb, &cursor, lane);
+      else if (nb <= 64) sort_and_merge<2>(list, &size, cap, stage, nb, &cursor, lane);
+      else sort_and_merge<4>(list, &size, cap, stage, nb, &cursor, lane);
+    }
+
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) dedup += __shfl_xor_sync(kFullMask, dedup, off);
+    if (st != kStatusOk) {
+      if (lane == 0) *status = st;
+      continue;
+    }
+    __syncwarp();
+    pq_finish_query(a, q, list, size, qi, lane, base, scored, scored, expanded, dedup);
+    __syncwarp();
+  }
+}
+
+PqDecodedFn pq_decoded_kernel_for(int dim) {
+  if (dim % 4 != 0) return nullptr;
+  switch (dim) {
+    case 128: return pq_decoded_search_kernel<128>;
+    case 96: return pq_decoded_search_kernel<96>;
+    case 64: return pq_decoded_search_kernel<64>;
+    default: return pq_decoded_search_kernel<0>;
+  }
+}
+
+}  // namespace rover

@@ -20,273 +20,9 @@
 // codebook in the reference's order plus the residual correction), sorts them
 // with a warp bitonic network and merges them into the list.
 
-#include "common.cuh"
-#include "kernels.h"
+#include "pq_common.cuh"
 
 namespace rover {
-
-// Residual row address inside the .pqresN block payload
-// (pq_residual_query_block, retrieval_pq_residual.c:914-924).
-__device__ __forceinline__ const uint8_t* pq_residual_row(const PqIndexView& ix, int32_t id) {
-  const uint32_t u = static_cast<uint32_t>(id);
-  const uint32_t block = u / static_cast<uint32_t>(ix.vpb);
-  const uint32_t within = (u - block * static_cast<uint32_t>(ix.vpb)) * static_cast<uint32_t>(ix.rcb);
-  return ix.residual + static_cast<size_t>(block) * 4096u + within;
-}
-
-// One candidate's ADC distance (retrieval_pq_build_lut entries recomputed in
-// place, then the sequential sum of retrieval_pq_adc_scalar) and, when
-// correction is on, the residual-corrected distance.  Returns false when the
-// reference would reject the candidate (non-finite or invalid qparams).
-__device__ __forceinline__ bool pq_score(const PqIndexView& ix, const float* __restrict__ q,
-                                         int32_t id, bool correction, float* out_adc,
-                                         float* out_dist) {
-  const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
-  float adc = 0.0f;
-  float acc = 0.0f;
-  float scale = 0.0f, zero = 0.0f;
-  const uint8_t* res = nullptr;
-  if (correction) {
-    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
-    scale = qp.x;
-    zero = qp.y;
-    if (!isfinite(scale) || !isfinite(zero) || !(scale > 0.0f)) return false;
-    res = pq_residual_row(ix, id);
-  }
-  int dim = 0;
-  for (int m = 0; m < ix.m; ++m) {
-    const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
-    const float* cen = ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim;
-    float lut = 0.0f;
-    for (int j = 0; j < ix.subdim; ++j, ++dim) {
-      const float cj = __ldg(cen + j);
-      const float qd = q[dim];
-      const float diff = fsub(qd, cj);
-      lut = fadd(lut, fmul(diff, diff));
-      if (correction) {
-        const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, dim))
-                                                 : static_cast<uint32_t>(__ldg(res + dim));
-        const float x = fadd(fadd(cj, fmul(u8f(r), scale)), zero);
-        const float dq = fsub(qd, x);
-        acc = fadd(acc, fmul(dq, dq));
-      }
-    }
-    adc = fadd(adc, lut);
-  }
-  if (!isfinite(adc)) return false;
-  if (correction && !isfinite(acc)) return false;
-  *out_adc = adc;
-  *out_dist = correction ? acc : adc;
-  return true;
-}
-
-// Shape-specialised scorer for Ks=256 codebooks: the candidate's whole code
-// row and residual row are fetched up front with 16-byte (or 8/4-byte)
-// vector loads and every loop is unrolled, so a candidate costs one round
-// of independent memory requests instead of one per subspace or dimension.
-// The floating-point operations and their order are those of pq_score.
-template <int M, int SUB, int RBITS>
-__device__ __forceinline__ bool pq_score_fixed(const PqIndexView& ix, const float* __restrict__ q, int32_t id,
-                                               bool correction, float* out_adc, float* out_dist) {
-  constexpr int DIM = M * SUB;
-  constexpr int RCB = RBITS == 8 ? DIM : DIM / 2;
-  constexpr int CW = (M + 3) / 4;      // code words
-  constexpr int RW = RCB / 4;          // residual words
-  uint32_t cw[CW];
-  const uint8_t* crow = ix.codes + static_cast<size_t>(id) * M;
-  if constexpr (M % 16 == 0) {
-#pragma unroll
-    for (int i = 0; i < M / 16; ++i) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(crow) + i);
-      cw[4 * i] = v.x; cw[4 * i + 1] = v.y; cw[4 * i + 2] = v.z; cw[4 * i + 3] = v.w;
-    }
-  } else if constexpr (M % 8 == 0) {
-#pragma unroll
-    for (int i = 0; i < M / 8; ++i) {
-      const uint2 v = __ldg(reinterpret_cast<const uint2*>(crow) + i);
-      cw[2 * i] = v.x; cw[2 * i + 1] = v.y;
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < CW; ++i) cw[i] = __ldg(reinterpret_cast<const uint32_t*>(crow) + i);
-  }
-  uint32_t rw[RW];
-  float scale = 0.0f, zero = 0.0f;
-  if (correction) {
-    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
-    scale = qp.x;
-    zero = qp.y;
-    const uint8_t* res = pq_residual_row(ix, id);
-    if constexpr (RCB % 16 == 0) {
-#pragma unroll
-      for (int i = 0; i < RCB / 16; ++i) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4*>(res) + i);
-        rw[4 * i] = v.x; rw[4 * i + 1] = v.y; rw[4 * i + 2] = v.z; rw[4 * i + 3] = v.w;
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < RW; ++i) rw[i] = __ldg(reinterpret_cast<const uint32_t*>(res) + i);
-    }
-    if (!isfinite(scale) || !isfinite(zero) || !(scale > 0.0f)) return false;
-  }
-  float adc = 0.0f, acc = 0.0f;
-#pragma unroll
-  for (int m = 0; m < M; ++m) {
-    const uint32_t c = (cw[m >> 2] >> (8 * (m & 3))) & 255u;
-    const float* cen = ix.codebook + (static_cast<size_t>(m) * 256u + c) * SUB;
-    float cv[SUB];
-    if constexpr (SUB % 4 == 0) {
-#pragma unroll
-      for (int t = 0; t < SUB / 4; ++t) {
-        const float4 v = __ldg(reinterpret_cast<const float4*>(cen) + t);
-        cv[4 * t] = v.x; cv[4 * t + 1] = v.y; cv[4 * t + 2] = v.z; cv[4 * t + 3] = v.w;
-      }
-    } else {
-#pragma unroll
-      for (int t = 0; t < SUB; ++t) cv[t] = __ldg(cen + t);
-    }
-    float lut = 0.0f;
-#pragma unroll
-    for (int j = 0; j < SUB; ++j) {
-      const int d = m * SUB + j;
-      const float qd = q[d];
-      const float diff = fsub(qd, cv[j]);
-      lut = fadd(lut, fmul(diff, diff));
-      if (correction) {
-        uint32_t r;
-        if constexpr (RBITS == 8) r = (rw[d >> 2] >> (8 * (d & 3))) & 255u;
-        else r = (rw[d >> 3] >> (4 * (d & 7))) & 15u;
-        const float x = fadd(fadd(cv[j], fmul(u8f(r), scale)), zero);
-        const float dq = fsub(qd, x);
-        acc = fadd(acc, fmul(dq, dq));
-      }
-    }
-    adc = fadd(adc, lut);
-  }
-  if (!isfinite(adc)) return false;
-  if (correction && !isfinite(acc)) return false;
-  *out_adc = adc;
-  *out_dist = correction ? acc : adc;
-  return true;
-}
-
-// ---------------------------------------------------------------------------
-// Final refine of the first `count` pool entries (refine_impl with the PQ
-// residual decode provider): FP32 decode ((c + code*s) + z), FP64 sum of
-// squared differences in dimension order, sort by (distance, id), keep k.
-__device__ void pq_refine_warp(const PqIndexView& ix, const float* q, const uint64_t* list,
-                               int count, int k, double* sd, int32_t* si, int lane,
-                               int32_t* out_ids, float* out_dists, int32_t* out_count,
-                               int32_t* status) {
-  int np2 = 1;
-  while (np2 < count) np2 <<= 1;
-  bool bad = false;
-  for (int i = lane; i < np2; i += kWarp) {
-    if (i < count) {
-      const int32_t id = key_id(list[i]);
-      const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
-      const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
-      const uint8_t* res = pq_residual_row(ix, id);
-      double dist = 0.0;
-      if (!isfinite(qp.x) || !(qp.x > 0.0f) || !isfinite(qp.y)) bad = true;
-      int dim = 0;
-      for (int m = 0; m < ix.m; ++m) {
-        const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
-        const float* cen = ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim;
-        for (int j = 0; j < ix.subdim; ++j, ++dim) {
-          const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, dim))
-                                                   : static_cast<uint32_t>(__ldg(res + dim));
-          const float x = fadd(fadd(__ldg(cen + j), fmul(u8f(r), qp.x)), qp.y);
-          if (!isfinite(x)) bad = true;
-          const double delta = __dsub_rn(static_cast<double>(q[dim]), static_cast<double>(x));
-          dist = __dadd_rn(dist, __dmul_rn(delta, delta));
-        }
-      }
-      if (!isfinite(dist) || dist >= 3.4028234663852886e38) bad = true;
-      sd[i] = dist;
-      si[i] = id;
-    } else {
-      sd[i] = __longlong_as_double(0x7ff0000000000000ll);  // +inf pads sort last
-      si[i] = 0x7fffffff;
-    }
-  }
-  if (__any_sync(kFullMask, bad)) {
-    if (lane == 0) *status = kStatusNumeric;
-    return;
-  }
-  __syncwarp();
-  // bitonic sort of (distance, id) pairs in shared memory
-  for (int kk = 2; kk <= np2; kk <<= 1) {
-    for (int j = kk >> 1; j > 0; j >>= 1) {
-      for (int i = lane; i < np2; i += kWarp) {
-        const int p = i ^ j;
-        if (p > i) {
-          const bool up = (i & kk) == 0;
-          const double a = sd[i], b = sd[p];
-          const int32_t ia = si[i], ib = si[p];
-          const bool a_gt = (a > b) || (a == b && ia > ib);
-          if (up == a_gt) {
-            sd[i] = b; sd[p] = a; si[i] = ib; si[p] = ia;
-          }
-        }
-      }
-      __syncwarp();
-    }
-  }
-  const int outn = count < k ? count : k;
-  for (int i = lane; i < outn; i += kWarp) {
-    out_ids[i] = si[i];
-    out_dists[i] = static_cast<float>(sd[i]);
-  }
-  if (lane == 0) *out_count = outn;
-}
-
-// ---------------------------------------------------------------------------
-
-template <int PER>
-__device__ __forceinline__ int merge_batch(uint64_t* list, int size, int cap, uint64_t* stage,
-                                           uint64_t (&v)[PER], int nb, int lane) {
-  // stage the sorted batch so list elements can rank against it
-#pragma unroll
-  for (int r = 0; r < PER; ++r) stage[lane + 32 * r] = v[r];
-  __syncwarp();
-  int bpos[PER];
-  int min_ins = cap;
-#pragma unroll
-  for (int r = 0; r < PER; ++r) {
-    const int e = lane + 32 * r;
-    bpos[r] = e < nb ? e + count_less(list, size, v[r]) : cap;
-    min_ins = min(min_ins, bpos[r]);
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) min_ins = min(min_ins, __shfl_xor_sync(kFullMask, min_ins, off));
-  // shift list elements right, highest chunk first (new position >= old)
-  const int first_chunk = min_ins >> 5;
-  for (int t = (size - 1) >> 5; t >= first_chunk; --t) {
-    const int i = 32 * t + lane;
-    uint64_t key = 0;
-    int pos = cap;
-    if (i < size) {
-      key = list[i];
-      pos = i + count_less(stage, nb, key);
-    }
-    __syncwarp();
-    if (i < size && pos < cap && pos != i) list[pos] = key;
-    __syncwarp();
-  }
-#pragma unroll
-  for (int r = 0; r < PER; ++r)
-    if (bpos[r] < cap) list[bpos[r]] = v[r];
-  __syncwarp();
-  return min_ins;
-}
-
-template <int M, int SUB, int RBITS>
-__device__ __forceinline__ bool score_one(const PqIndexView& ix, const float* __restrict__ q, int32_t id,
-                                          bool correction, float* adc, float* dist) {
-  if constexpr (M == 0) return pq_score(ix, q, id, correction, adc, dist);
-  else return pq_score_fixed<M, SUB, RBITS>(ix, q, id, correction, adc, dist);
-}
 
 // Score batch_ids[0..nb) (one lane per candidate) into keys[0..nb).
 // Returns false when the reference would reject any candidate.
@@ -302,23 +38,6 @@ __device__ __noinline__ bool score_batch(const PqSearchArgs& a, const float* q, 
   }
   __syncwarp();
   return !__any_sync(kFullMask, bad);
-}
-
-// Sort the scored batch (keys in `stage`) and merge it into the list.
-template <int PER>
-__device__ __forceinline__ void sort_and_merge(uint64_t* list, int* size, int cap, uint64_t* stage, int nb,
-                                               int* cursor, int lane) {
-  uint64_t v[PER];
-#pragma unroll
-  for (int r = 0; r < PER; ++r) {
-    const int e = lane + 32 * r;
-    v[r] = e < nb ? stage[e] : kEmptyKey;
-  }
-  __syncwarp();
-  warp_bitonic_sort<PER>(v, lane);
-  const int min_ins = merge_batch<PER>(list, *size, cap, stage, v, nb, lane);
-  *size = min(cap, *size + nb);
-  *cursor = min(*cursor, min_ins);
 }
 
 template <int M, int SUB, int RBITS>
@@ -497,47 +216,7 @@ pq_search_kernel_t(PqSearchArgs a) {
       continue;
     }
     __syncwarp();
-    if (a.pool_ids) {
-      const int pc = min(size, a.pool_stride);  // pool_stride > 0 when pool_ids is set
-      for (int i = lane; i < pc; i += kWarp) {
-        const uint64_t k = list[i];
-        a.pool_ids[static_cast<size_t>(qi) * a.pool_stride + i] = key_id(k);
-        a.pool_dists[static_cast<size_t>(qi) * a.pool_stride + i] = key_dist(k);
-      }
-      if (lane == 0) a.pool_counts[qi] = pc;
-    }
-    if (lane == 0 && a.stats) {
-      unsigned long long* s = a.stats + static_cast<size_t>(qi) * 4;
-      s[0] = scored;
-      s[1] = a.correction ? scored : 0ull;
-      s[2] = expanded;
-      s[3] = dedup;
-    }
-    if (a.out_ids) {
-      const int k = min(a.top_ks ? a.top_ks[qi] : a.top_k, a.out_stride);
-      const int budget = a.refine_budget;
-      int32_t* oi = a.out_ids + static_cast<size_t>(qi) * a.out_stride;
-      float* od = a.out_dists + static_cast<size_t>(qi) * a.out_stride;
-      if (budget > 0) {
-        const int cnt = min(size, budget);
-        // refine scratch reuses the batch/stage area and the tail of the warp
-        // slice; it is sized for max refine budget by the host.
-        double* sd = reinterpret_cast<double*>(base + a.smem_refine_offset);
-        int32_t* si = reinterpret_cast<int32_t*>(sd + a.refine_capacity);
-        int32_t rs = kStatusOk;
-        pq_refine_warp(ix, q, list, cnt, k, sd, si, lane, oi, od, a.out_counts + qi, &rs);
-        rs = __shfl_sync(kFullMask, rs, 0);
-        if (rs != kStatusOk && lane == 0) *status = rs;
-      } else {
-        const int outn = min(size, k);
-        for (int i = lane; i < outn; i += kWarp) {
-          const uint64_t kk = list[i];
-          oi[i] = key_id(kk);
-          od[i] = key_dist(kk);
-        }
-        if (lane == 0) a.out_counts[qi] = outn;
-      }
-    }
+    pq_finish_query(a, q, list, size, qi, lane, base, scored, a.correction ? scored : 0ull, expanded, dedup);
     __syncwarp();
   }
 }

@@ -34,15 +34,21 @@ def test_pq_lut_adc_residual(calc, name):
         assert np.array_equal(bits(res[qi]), bits(g["residual"][qi]))
 
 
+PACKED, DECODED = 1, 2
+
+
 @pytest.mark.parametrize("name", PQ_FIXTURES)
 @pytest.mark.parametrize("tag", ["on", "off", "on_ep8", "on_exp6"])
-def test_pq_search_matches_reference(calc, name, tag):
+@pytest.mark.parametrize("layout", [PACKED, DECODED])
+def test_pq_search_matches_reference(calc, name, tag, layout):
     data, graph, b, g, q = load_fixture(name)
     calc.pq_load(graph, data["graph_entry"], b)
     corr, ep, exp = (int(x) for x in g[f"search_{tag}_params"])
+    if layout == DECODED and not corr:
+        pytest.skip("decoded rows serve the corrected distance only")
     stride = g[f"search_{tag}_pool_ids"].shape[1]
     r = calc.pq_search(q, g["pool_sizes"], top_k=10, pool_stride=stride, entry_points=ep, expand_count=exp,
-                       correction=corr, refine_budget=20 if corr else 0)
+                       correction=corr, refine_budget=20 if corr else 0, layout=layout)
     rows_equal(r["pool_ids"], r["pool_dists"], r["pool_counts"], g[f"search_{tag}_pool_ids"],
                g[f"search_{tag}_pool_dists"], g[f"search_{tag}_pool_counts"])
     rows_equal(r["ids"], r["dists"], r["counts"], g[f"search_{tag}_ids"], g[f"search_{tag}_dists"],
@@ -106,25 +112,68 @@ def test_legacy_retrieval_search(calc, name):
     assert calc.retrieval_unload() == 0
 
 
-def test_pq_search_random_vs_oracle(calc, port):
-    """A larger random index (d=128, M=16, 8-bit residuals, alpha-pruned
-    degree-24 graph) against the oracle restatement, uneven beam widths."""
-    from rover_b200 import bundle as B
-    from rover_b200 import datasets as D
-    n, dim = 12000, 128
-    base = D.gmm(n, dim, 32, 5)
-    queries = D.gmm(200, dim, 32, 6, centers_seed=5)
-    graph = D.pruned_graph(base, 32, 24, 1.2)
-    entry = D.medoid(base)
-    book, codes, rows, qp = D.pq_prepare(base, 16, 256, 6, 8)
-    bundle = B.PqBundle(B.PqMeta(b"\x01" * 16, n, dim, 16, 256, 8, 16), book, codes, 8,
-                        B.pack_residual_blocks(rows), qp)
-    pools = np.random.default_rng(1).choice([16, 32, 64, 100, 128], size=len(queries)).astype(np.int32)
-    calc.pq_load(graph, entry, bundle)
-    r = calc.pq_search(queries, pools, top_k=10, pool_stride=128, entry_points=4, expand_count=24,
-                       correction=1, refine_budget=20)
-    ix = port.pq_index(graph, bundle)
-    o = port.pq_search(ix, entry, queries, pools, 4, 24, correction=1, refine_budget=20, top_k=10)
+_RANDOM = {}
+
+
+def _random_pq_index():
+    """A 12K x 128 random index (M=16, 8-bit residuals, alpha-pruned
+    degree-24 graph) and 200 queries, built once per session."""
+    if not _RANDOM:
+        from rover_b200 import bundle as B
+        from rover_b200 import datasets as D
+        n, dim = 12000, 128
+        base = D.gmm(n, dim, 32, 5)
+        queries = D.gmm(200, dim, 32, 6, centers_seed=5)
+        graph = D.pruned_graph(base, 32, 24, 1.2)
+        entry = D.medoid(base)
+        book, codes, rows, qp = D.pq_prepare(base, 16, 256, 6, 8)
+        bundle = B.PqBundle(B.PqMeta(b"\x01" * 16, n, dim, 16, 256, 8, 16), book, codes, 8,
+                            B.pack_residual_blocks(rows), qp)
+        _RANDOM.update(graph=graph, entry=entry, bundle=bundle, queries=queries)
+    return _RANDOM
+
+
+# (entry points, beam widths): few seeds with uneven beams; many seeds
+# (several 64-seed tiles, LCG repeats) with beams wide enough that some
+# queries overflow the shared-memory visited table into the global one.
+RANDOM_CASES = {"ep4": (4, [16, 32, 64, 100, 128]), "ep700": (700, [32, 64, 512, 1024])}
+
+
+@pytest.mark.parametrize("case", sorted(RANDOM_CASES))
+@pytest.mark.parametrize("layout", [PACKED, DECODED])
+def test_pq_search_random_vs_oracle(calc, port, case, layout):
+    """The CUDA search against the oracle restatement on a larger random
+    index, both residual layouts."""
+    d = _random_pq_index()
+    ep, choices = RANDOM_CASES[case]
+    queries = d["queries"]
+    pools = np.random.default_rng(1).choice(choices, size=len(queries)).astype(np.int32)
+    calc.pq_load(d["graph"], d["entry"], d["bundle"])
+    stride = int(pools.max())
+    r = calc.pq_search(queries, pools, top_k=10, pool_stride=stride, entry_points=ep, expand_count=24,
+                       correction=1, refine_budget=20, layout=layout)
+    ix = port.pq_index(d["graph"], d["bundle"])
+    o = port.pq_search(ix, d["entry"], queries, pools, ep, 24, correction=1, refine_budget=20, top_k=10)
     rows_equal(r["pool_ids"], r["pool_dists"], r["pool_counts"], o["pool_ids"], o["pool_dists"], o["pool_counts"])
     rows_equal(r["ids"], r["dists"], r["counts"], o["ids"], o["dists"], o["counts"])
     assert np.array_equal(r["stats"], o["stats"])
+
+
+@pytest.mark.parametrize("layout", [PACKED, DECODED])
+def test_pq_search_invalid_qparams_fail_like_reference(calc, layout):
+    """A vector with scale <= 0 fails every query that scores it
+    (retrieval_pq_residual_query_evaluate rejects it); other queries are
+    unaffected and the call reports the failure."""
+    from rover_b200 import bundle as B
+    d = _random_pq_index()
+    b0 = d["bundle"]
+    qp = b0.qparams.copy()
+    bad_id = int(d["entry"])
+    qp[bad_id, 0] = 0.0
+    bundle = B.PqBundle(b0.meta, b0.codebook, b0.codes, b0.residual_bits, b0.residual_blocks, qp)
+    calc.pq_load(d["graph"], d["entry"], bundle)
+    queries = d["queries"][:16]
+    r = calc.pq_search(queries, 32, top_k=10, entry_points=4, expand_count=24, correction=1, refine_budget=20,
+                       layout=layout, check=False)
+    assert r["rc"] != 0
+    assert np.all(r["status"] == 2)  # the graph entry is every query's first seed
