@@ -30,7 +30,12 @@ extern "C" {
 #define ROVER_QUERY_FRONTIER_FULL 5
 
 /* Search modes. */
-#define ROVER_MODE_EXACT 0   /* reference expansion order, bit-exact results */
+#define ROVER_MODE_EXACT 0    /* reference expansion order, bit-exact results */
+#define ROVER_MODE_BATCHED 1  /* free-running: beam_width pool entries expanded per step,
+                                 every candidate corrected (PQ with correction only) */
+#define ROVER_MODE_GATED 2    /* batched, with the learned gate choosing which candidates
+                                 are corrected and when a query stops expanding;
+                                 without a loaded gate it runs as ROVER_MODE_BATCHED */
 
 /* Residual layouts for PQ searches with correction (RoverSearchParams.layout).
  * Both give identical results; they trade device memory for arithmetic. */
@@ -82,7 +87,9 @@ typedef struct RoverSearchParams {
     int32_t sq_mode;         /* SQ only: 0 = device search (calculator_retrieval_search),
                                 1 = SQMD session semantics */
     int32_t layout;          /* PQ with correction: ROVER_LAYOUT_* */
-    int32_t reserved[5];
+    int32_t beam_width;      /* BATCHED / GATED: entries expanded per step (0 = largest
+                                that keeps beam_width * expand_count <= 128) */
+    int32_t reserved[4];
 } RoverSearchParams;
 
 /* Per-call outputs.  Host pointers for calculator_rover_*_search, device
@@ -178,11 +185,100 @@ AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSearchParams 
                                      const float *queries, int32_t num_queries,
                                      const int32_t *pool_sizes, const RoverSearchOutputs *out);
 
+/* ---- learned gate (ROVER_MODE_GATED) ----------------------------------
+ * A 5 -> 64 -> 64 -> 2 MLP with ReLU hidden layers.  Inputs per row: log
+ * quantized (ADC) distance, pool rank / L, log worst-in-pool distance,
+ * hop count / L, query norm; each standardised with mu / sigma.  Outputs:
+ * refine-needed logit, stop-expanding logit.  Weights are FP32 row-major
+ * [in][out] here and BF16 on the device; accumulation is FP32. */
+#define ROVER_GATE_IN 5
+#define ROVER_GATE_HIDDEN 64
+#define ROVER_GATE_OUT 2
+/* Packed parameter vector: w1[5][64] b1[64] w2[64][64] b2[64] w3[64][2] b3[2] */
+#define ROVER_GATE_PARAMS (5 * 64 + 64 + 64 * 64 + 64 + 64 * 2 + 2)
+
+typedef struct RoverGateThresholds {
+    float band_lo;       /* quantized / worst ratio at or below which a candidate is corrected */
+    float band_hi;       /* ratio at or above which it keeps its quantized distance */
+    float refine_logit;  /* inside the band: corrected when the refine logit exceeds this */
+    float stop_logit;    /* a query stops when its sources' mean stop logit exceeds this */
+} RoverGateThresholds;
+
+/* Loads a gate (params: ROVER_GATE_PARAMS floats; mu, sigma: 5 each). */
+AEEResult calculator_rover_gate_load(remote_handle64 h, const float *params, const float *mu,
+                                     const float *sigma, const RoverGateThresholds *thresholds);
+AEEResult calculator_rover_gate_unload(remote_handle64 h);
+
+/* One training row per scored candidate or expansion source. */
+typedef struct RoverGateTraceRow {
+    int32_t query, hop, id;
+    int32_t flags;       /* bit0: entered the pool, bit1: expansion source, bit2: entry seed */
+    float quantized;     /* ADC distance (sources: pool distance) */
+    float rank;          /* pool rank / L */
+    float worst;         /* worst pool distance */
+    float qnorm;         /* query L2 norm */
+    float dist;          /* corrected distance */
+    float pad[3];
+} RoverGateTraceRow;
+
+/* Plain search with full correction in the reference's expansion order
+ * (ROVER_MODE_BATCHED with beam width 1), recording trace rows.  Rows beyond
+ * capacity are counted in *count but not written. */
+AEEResult calculator_rover_pq_trace(remote_handle64 h, const RoverSearchParams *params, const float *queries,
+                                    int32_t num_queries, const int32_t *pool_sizes,
+                                    const RoverSearchOutputs *out, RoverGateTraceRow *rows,
+                                    int64_t capacity, int64_t *count);
+
+/* Training on the device (forward / backward / Adam kernels of this
+ * library).  Inputs x[n][5] are the raw gate inputs (log quantized distance,
+ * rank / L, log worst distance, hop / L, query norm); y[n][2] labels in
+ * {0, 1} (refine-needed, stop-expanding); m[n][2] masks (0 = no label for that
+ * head).  Standardisation statistics come from x.  Outputs: the FP32 master
+ * parameters (ROVER_GATE_PARAMS floats), mu / sigma (5 each), and the mean
+ * training loss of each epoch. */
+typedef struct RoverGateTrainParams {
+    int32_t size;            /* sizeof(RoverGateTrainParams) */
+    int32_t epochs;
+    int32_t batch;           /* rows per optimiser step */
+    float lr;                /* Adam step size */
+    float beta1, beta2, eps;
+    float weight_decay;      /* decoupled */
+    uint32_t seed;           /* initialisation and shuffling */
+    float pos_weight[2];     /* positive-class weight per head */
+    int32_t reserved[4];
+} RoverGateTrainParams;
+
+AEEResult calculator_rover_gate_train(remote_handle64 h, const float *x, const float *y, const float *m, int64_t n,
+                                      const RoverGateTrainParams *tp, float *params_out, float *mu_out,
+                                      float *sigma_out, float *epoch_loss);
+
+/* One forward / backward pass over all n rows with the given parameters,
+ * as one training step computes it: the mean loss and the gradient of every
+ * parameter (ROVER_GATE_PARAMS floats), both divided by n. */
+AEEResult calculator_rover_gate_grad(remote_handle64 h, const float *x, const float *y, const float *m, int64_t n,
+                                     const float *params, const float *mu, const float *sigma,
+                                     const float *pos_weight, float *grad_out, float *loss_out);
+
 /* Last CUDA / library error as text (thread-local). */
 const char *calculator_rover_last_error(void);
 
 /* Number of CUDA kernels this library has launched in this process. */
 uint64_t calculator_rover_launch_count(void);
+
+/* Per-kernel device time.  While enabled, each search-path kernel launch is
+ * bracketed by CUDA events on the stream it runs on; the events are read when
+ * the call that launched it synchronizes.  calculator_rover_kernel_times
+ * fills, per kind, the launches and summed milliseconds since the last
+ * calculator_rover_kernel_timing call (which resets them) and returns the
+ * number of kinds written. */
+#define ROVER_KERNEL_PQ_PACKED 0    /* PQ search, packed residual rows */
+#define ROVER_KERNEL_PQ_SEEDS 1     /* all-queries x entry-seeds distances */
+#define ROVER_KERNEL_PQ_DECODED 2   /* PQ search, decoded rows */
+#define ROVER_KERNEL_PQ_BATCHED 3   /* PQ search, batched / gated modes */
+#define ROVER_KERNEL_SQ 4           /* SQ search */
+#define ROVER_KERNEL_KINDS 8
+void calculator_rover_kernel_timing(int32_t enable);
+int32_t calculator_rover_kernel_times(int64_t *launches, double *ms, int32_t kinds);
 
 #ifdef __cplusplus
 }

@@ -55,7 +55,26 @@ class SearchParams(C.Structure):
     _fields_ = [("size", C.c_int32), ("mode", C.c_int32), ("entry_points", C.c_int32), ("seed", C.c_uint32),
                 ("expand_count", C.c_int32), ("correction", C.c_int32), ("refine_budget", C.c_int32),
                 ("top_k", C.c_int32), ("pool_stride", C.c_int32), ("sq_mode", C.c_int32),
-                ("layout", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("layout", C.c_int32), ("beam_width", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+class GateThresholds(C.Structure):
+    _fields_ = [("band_lo", C.c_float), ("band_hi", C.c_float), ("refine_logit", C.c_float),
+                ("stop_logit", C.c_float)]
+
+
+class GateTrainParams(C.Structure):
+    _fields_ = [("size", C.c_int32), ("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("weight_decay", C.c_float),
+                ("seed", C.c_uint32), ("pos_weight", C.c_float * 2), ("reserved", C.c_int32 * 4)]
+
+
+# RoverGateTraceRow as a NumPy record (48 bytes)
+TRACE_DTYPE = np.dtype([("query", np.int32), ("hop", np.int32), ("id", np.int32), ("flags", np.int32),
+                        ("quantized", np.float32), ("rank", np.float32), ("worst", np.float32),
+                        ("qnorm", np.float32), ("dist", np.float32), ("pad", np.float32, 3)])
+GATE_PARAMS = 5 * 64 + 64 + 64 * 64 + 64 + 64 * 2 + 2
+MODE_EXACT, MODE_BATCHED, MODE_GATED = 0, 1, 2
 
 
 class SearchOutputs(C.Structure):
@@ -96,6 +115,17 @@ class Calculator:
         L.calculator_retrieval_unload.argtypes = [C.c_uint64]
         L.calculator_rover_last_error.restype = C.c_char_p
         L.calculator_rover_launch_count.restype = C.c_uint64
+        L.calculator_rover_gate_load.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.POINTER(GateThresholds)]
+        L.calculator_rover_gate_unload.argtypes = [C.c_uint64]
+        L.calculator_rover_gate_train.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.c_int64,
+                                                  C.POINTER(GateTrainParams), _f32p, _f32p, _f32p, _f32p]
+        L.calculator_rover_gate_grad.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.c_int64, _f32p, _f32p, _f32p,
+                                                 _f32p, _f32p, _f32p]
+        L.calculator_rover_pq_trace.argtypes = [C.c_uint64, C.POINTER(SearchParams), _f32p, C.c_int32, _i32p,
+                                                C.POINTER(SearchOutputs), C.c_void_p, C.c_int64, _i64p]
+        L.calculator_rover_kernel_timing.argtypes = [C.c_int32]
+        L.calculator_rover_kernel_times.argtypes = [_i64p, C.POINTER(C.c_double), C.c_int32]
+        L.calculator_rover_kernel_times.restype = C.c_int32
         L.calculator_rover_pq_load.argtypes = [C.c_uint64, C.POINTER(PqIndexDesc)]
         L.calculator_rover_pq_unload.argtypes = [C.c_uint64]
         L.calculator_rover_pq_search.argtypes = [C.c_uint64, C.POINTER(SearchParams), _f32p, C.c_int32, _i32p,
@@ -125,6 +155,92 @@ class Calculator:
 
     def launch_count(self) -> int:
         return int(self.lib.calculator_rover_launch_count())
+
+    KERNEL_KINDS = ("pq_packed", "pq_seeds", "pq_decoded", "pq_batched", "sq")
+
+    # -- learned gate
+    def gate_load(self, params, mu, sigma, band_lo=0.0, band_hi=0.0, refine_logit=0.0, stop_logit=1e30) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        m = np.ascontiguousarray(mu, np.float32)
+        sg = np.ascontiguousarray(sigma, np.float32)
+        t = GateThresholds(band_lo, band_hi, refine_logit, stop_logit)
+        self._check("calculator_rover_gate_load",
+                    self.lib.calculator_rover_gate_load(self.handle, _p(p, _f32p), _p(m, _f32p), _p(sg, _f32p),
+                                                        C.byref(t)))
+
+    def gate_unload(self) -> None:
+        self._check("calculator_rover_gate_unload", self.lib.calculator_rover_gate_unload(self.handle))
+
+    def gate_train(self, x, y, m, epochs=4, batch=4096, lr=2e-3, weight_decay=0.0, seed=1,
+                   pos_weight=(1.0, 1.0)) -> dict:
+        """Trains the gate on the device; returns params, mu, sigma, losses."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        m = np.ascontiguousarray(m, np.float32)
+        n = x.shape[0]
+        tp = GateTrainParams()
+        tp.size = C.sizeof(GateTrainParams)
+        tp.epochs, tp.batch, tp.lr = epochs, batch, lr
+        tp.beta1, tp.beta2, tp.eps, tp.weight_decay, tp.seed = 0.9, 0.999, 1e-8, weight_decay, seed
+        tp.pos_weight[0], tp.pos_weight[1] = pos_weight
+        params = np.zeros(GATE_PARAMS, np.float32)
+        mu = np.zeros(5, np.float32)
+        sigma = np.zeros(5, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        self._check("calculator_rover_gate_train",
+                    self.lib.calculator_rover_gate_train(self.handle, _p(x, _f32p), _p(y, _f32p), _p(m, _f32p), n,
+                                                         C.byref(tp), _p(params, _f32p), _p(mu, _f32p),
+                                                         _p(sigma, _f32p), _p(losses, _f32p)))
+        return dict(params=params, mu=mu, sigma=sigma, losses=losses)
+
+    def gate_grad(self, x, y, m, params, mu, sigma, pos_weight=(1.0, 1.0)):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        m = np.ascontiguousarray(m, np.float32)
+        p = np.ascontiguousarray(params, np.float32)
+        mu = np.ascontiguousarray(mu, np.float32)
+        sg = np.ascontiguousarray(sigma, np.float32)
+        pw = np.ascontiguousarray(pos_weight, np.float32)
+        grad = np.zeros(GATE_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check("calculator_rover_gate_grad",
+                    self.lib.calculator_rover_gate_grad(self.handle, _p(x, _f32p), _p(y, _f32p), _p(m, _f32p),
+                                                        x.shape[0], _p(p, _f32p), _p(mu, _f32p), _p(sg, _f32p),
+                                                        _p(pw, _f32p), _p(grad, _f32p), _p(loss, _f32p)))
+        return float(loss[0]), grad
+
+    def pq_trace(self, queries, pool_sizes, capacity, top_k=10, **kw) -> dict:
+        """Plain search with full correction in the reference's order,
+        returning its results and the gate's trace rows."""
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        nq = q.shape[0]
+        pools = np.ascontiguousarray(np.broadcast_to(np.asarray(pool_sizes, dtype=np.int32), (nq,)))
+        p = self.params(top_k=top_k, **kw)
+        r = dict(ids=np.full((nq, top_k), -1, np.int32), dists=np.zeros((nq, top_k), np.float32),
+                 counts=np.zeros(nq, np.int32), status=np.zeros(nq, np.int32), stats=np.zeros((nq, 4), np.uint64))
+        o = SearchOutputs(_p(r["ids"], _i32p), _p(r["dists"], _f32p), _p(r["counts"], _i32p), top_k, None, None,
+                          None, _p(r["stats"], _u64p), _p(r["status"], _i32p))
+        rows = np.zeros(int(capacity), TRACE_DTYPE)
+        count = C.c_int64(0)
+        self._check("calculator_rover_pq_trace",
+                    self.lib.calculator_rover_pq_trace(self.handle, C.byref(p), _p(q, _f32p), nq, _p(pools, _i32p),
+                                                       C.byref(o), rows.ctypes.data_as(C.c_void_p), int(capacity),
+                                                       C.byref(count)))
+        r["rows"] = rows[:min(int(capacity), count.value)]
+        r["row_count"] = count.value
+        return r
+
+    def kernel_timing(self, enable: bool = True) -> None:
+        """Turn per-kernel event timing on or off (and reset the totals)."""
+        self.lib.calculator_rover_kernel_timing(1 if enable else 0)
+
+    def kernel_times(self) -> dict:
+        """{kind: (launches, total ms)} since the last kernel_timing call."""
+        n = 8
+        launches = np.zeros(n, np.int64)
+        ms = np.zeros(n, np.float64)
+        self.lib.calculator_rover_kernel_times(_p(launches, _i64p), ms.ctypes.data_as(C.POINTER(C.c_double)), n)
+        return {k: (int(launches[i]), float(ms[i])) for i, k in enumerate(self.KERNEL_KINDS)}
 
     def close(self):
         if self.handle.value:
@@ -180,7 +296,7 @@ class Calculator:
 
     @staticmethod
     def params(entry_points=1, expand_count=32, correction=1, refine_budget=0, top_k=10, seed=42,
-               pool_stride=0, sq_mode=0, mode=0, layout=0) -> SearchParams:
+               pool_stride=0, sq_mode=0, mode=0, layout=0, beam_width=0) -> SearchParams:
         p = SearchParams()
         p.size = C.sizeof(SearchParams)
         p.mode = mode
@@ -193,6 +309,7 @@ class Calculator:
         p.pool_stride = pool_stride
         p.sq_mode = sq_mode
         p.layout = layout
+        p.beam_width = beam_width
         return p
 
     def pq_search(self, queries, pool_sizes, top_k=10, top_ks=None, pool_stride=0, stats=True, check=True,

@@ -8,6 +8,7 @@
 // as the kernels in pq_search.cu / sq_search.cu / distance.cu.
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -123,6 +124,12 @@ struct State {
   bool legacy_dma = false;
   // scratch
   DevBuf visited, heaps, counter, status, stats, luts, seed_dists;
+  DevBuf gate_buf;                // BF16 transposed weights + FP32 biases of the loaded gate
+  GateParams gate{};              // enabled == 0: no gate loaded
+  DevBuf trace_rows, trace_count; // calculator_rover_pq_trace
+  GateTraceRow* trace_dev = nullptr;
+  unsigned long long* trace_count_dev = nullptr;
+  int64_t trace_cap = 0;
   uint32_t visited_mask = 0;
   size_t visited_slots = 0;
   uint32_t gen_next = 1;
@@ -138,6 +145,75 @@ State& st() {
 
 int open_count = 0;
 std::atomic<unsigned long long> g_launches{0};  // kernels this library launched
+
+// Optional per-kernel event timing (calculator_rover_kernel_timing).
+struct KernelTimer {
+  std::mutex mu;
+  bool on = false;
+  struct Pending { int kind; cudaEvent_t start, stop; };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> spare;
+  int64_t launches[ROVER_KERNEL_KINDS] = {};
+  double ms[ROVER_KERNEL_KINDS] = {};
+  cudaEvent_t take() {
+    if (!spare.empty()) {
+      cudaEvent_t e = spare.back();
+      spare.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+  }
+};
+
+KernelTimer& timer() {
+  static KernelTimer t;
+  return t;
+}
+
+// Brackets one launch with events when timing is on.
+class TimedLaunch {
+ public:
+  TimedLaunch(int kind, cudaStream_t s) : kind_(kind), s_(s) {
+    KernelTimer& t = timer();
+    std::lock_guard<std::mutex> g(t.mu);
+    if (!t.on) return;
+    start_ = t.take();
+    stop_ = t.take();
+    if (start_ && stop_) cudaEventRecord(start_, s_);
+  }
+  ~TimedLaunch() {
+    if (!start_ || !stop_) return;
+    cudaEventRecord(stop_, s_);
+    KernelTimer& t = timer();
+    std::lock_guard<std::mutex> g(t.mu);
+    t.pending.push_back({kind_, start_, stop_});
+  }
+  TimedLaunch(const TimedLaunch&) = delete;
+  TimedLaunch& operator=(const TimedLaunch&) = delete;
+
+ private:
+  int kind_;
+  cudaStream_t s_;
+  cudaEvent_t start_ = nullptr, stop_ = nullptr;
+};
+
+// Reads the events of finished launches (call after the stream synchronized).
+void collect_timings() {
+  KernelTimer& t = timer();
+  std::lock_guard<std::mutex> g(t.mu);
+  for (const auto& p : t.pending) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+      t.launches[p.kind] += 1;
+      t.ms[p.kind] += ms;
+    }
+    t.spare.push_back(p.start);
+    t.spare.push_back(p.stop);
+  }
+  t.pending.clear();
+}
 
 AEEResult ensure_init(State& s) {
   if (s.init) return AEE_SUCCESS;
@@ -300,21 +376,28 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
     a.next_query = s.counter.as<unsigned int>();
     for (int q0 = 0; q0 < nq; q0 += chunk) {
       const int q1 = std::min(nq, q0 + chunk);
-      launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
-                           s.seed_dists.as<float>(), stream);
+      {
+        TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream);
+        launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
+                             s.seed_dists.as<float>(), stream);
+      }
       CK(cudaGetLastError());
       ++g_launches;
       b.q_begin = q0;
       b.q_end = q1;
       CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
       const int blocks = std::max(1, std::min(blocks_cap, (q1 - q0 + kSearchWarps - 1) / kSearchWarps));
-      kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a, b);
+      {
+        TimedLaunch tl(ROVER_KERNEL_PQ_DECODED, stream);
+        kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a, b);
+      }
       CK(cudaGetLastError());
       ++g_launches;
     }
     s.h_status.resize(nq);
     CK(cudaMemcpyAsync(s.h_status.data(), a.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
+    collect_timings();
     bool retry = false;
     for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
     if (!retry) break;
@@ -328,6 +411,9 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
     }
   return AEE_SUCCESS;
 }
+
+AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p, int nq, int expand,
+                            cudaStream_t stream);
 
 // Core PQ search on device buffers.  Retries queries whose visited table
 // overflowed with a 4x larger table.
@@ -375,6 +461,17 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
     set_error("the decoded layout needs correction on, dim %% 4 == 0 and 16-byte aligned queries");
     return AEE_EBADPARM;
   }
+  if (p->mode == ROVER_MODE_BATCHED || p->mode == ROVER_MODE_GATED || s.trace_dev) {
+    if (!decodable || p->layout == ROVER_LAYOUT_PACKED) {
+      set_error("batched and gated searches need correction on, decoded rows, dim %% 4 == 0 and aligned queries");
+      return AEE_EBADPARM;
+    }
+    bool ok = false;
+    if (ensure_decoded(s, s.pq, &ok) != AEE_SUCCESS) return AEE_EFAILED;
+    if (!ok) { set_error("decoded rows do not fit in device memory"); return AEE_ENOMEMORY; }
+    return pq_search_batched(s, a, p, nq, expand, stream);
+  }
+  if (p->mode != ROVER_MODE_EXACT) { set_error("unknown mode %d", p->mode); return AEE_EBADPARM; }
   if (decodable && p->layout != ROVER_LAYOUT_PACKED) {
     bool ok = false;
     if (ensure_decoded(s, s.pq, &ok) != AEE_SUCCESS) return AEE_EFAILED;
@@ -406,12 +503,16 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
     a.gen_base = gen_base;
     a.next_query = s.counter.as<unsigned int>();
     CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
-    kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
+    {
+      TimedLaunch tl(ROVER_KERNEL_PQ_PACKED, stream);
+      kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
+    }
     CK(cudaGetLastError());
     ++g_launches;
     s.h_status.resize(nq);
     CK(cudaMemcpyAsync(s.h_status.data(), d_out.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
+    collect_timings();
     bool retry = false;
     for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
     if (!retry) break;
@@ -419,6 +520,107 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
     // queries are rewritten with identical values.
     entries = next_pow2(static_cast<uint64_t>(entries) * 4);
     CK(cudaMemsetAsync(d_out.status, 0, nq * sizeof(int32_t), stream));
+  }
+  for (int i = 0; i < nq; ++i)
+    if (s.h_status[i] != kStatusOk) {
+      set_error("query %d failed with status %d", i, s.h_status[i]);
+      return AEE_EFAILED;
+    }
+  return AEE_SUCCESS;
+}
+
+// Batched / gated PQ search (pq_batched.cu): per query chunk, the
+// all-seeds distance pass (not needed by the gate, which ranks seeds by ADC)
+// and the batched kernel.  A trace request (s.trace_dev) records the gate's
+// training rows.
+AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p, int nq, int expand,
+                            cudaStream_t stream) {
+  PqDevice& pq = s.pq;
+  const bool tracing = s.trace_dev != nullptr;
+  const bool gated = p->mode == ROVER_MODE_GATED && s.gate.enabled && !tracing;
+  int W = tracing ? 1 : p->beam_width;
+  if (W == 0) W = std::max(1, std::min(kMaxBeamWidth, kMaxBatch / std::max(1, expand)));
+  if (W < 1 || W > kMaxBeamWidth || W * expand > kMaxBatch) {
+    set_error("beam_width %d: need 1..%d with beam_width * expand_count <= %d", W, kMaxBeamWidth, kMaxBatch);
+    return AEE_EBADPARM;
+  }
+  if (ensure_seeds(s, pq, p->entry_points, p->seed) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  const SeedSet& ss = pq.seeds;
+  PqDecodedArgs b{};
+  b.decoded = pq.decoded.as<float>();
+  b.seed_ids = ss.ids.as<int32_t>();
+  b.n_seeds = ss.count;
+  b.seed_dups = ss.dups;
+  b.seed_bits = ss.bits.as<uint32_t>();
+  PqBatchArgs c{};
+  c.beam_width = W;
+  c.gate = s.gate;
+  c.gate.enabled = gated ? 1 : 0;
+  c.trace = s.trace_dev;
+  c.trace_count = s.trace_count_dev;
+  c.trace_cap = s.trace_cap;
+  c.short_cap = 2 * a.max_pool;
+  const bool lut = gated || tracing;
+  // the LUT takes 4 * m * ks bytes per warp: a smaller visited table keeps
+  // two CTAs per SM
+  pq_batched_layout(&a, &b, &c, p->refine_budget, lut ? kSharedVisitedSlots / 2 : kSharedVisitedSlots, lut);
+  const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
+  if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, a.max_pool); return AEE_EBADPARM; }
+  const PqBatchFn kernel = pq_batched_kernel_for(pq.view.dim, gated ? kBatchGated : kBatchFull);
+  CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          static_cast<int>(smem)));
+  const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
+  const bool seed_pass = !gated;
+  const int chunk = seed_pass ? static_cast<int>(std::max<size_t>(
+                                    1, std::min<size_t>(nq, kSeedDistBudget / (static_cast<size_t>(ss.count) * sizeof(float)))))
+                              : nq;
+  if (seed_pass) CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
+  b.seed_dists = seed_pass ? s.seed_dists.as<float>() : nullptr;
+  const int blocks_cap = std::max(1, std::min(max_blocks, (chunk + kSearchWarps - 1) / kSearchWarps));
+  const size_t slots = static_cast<size_t>(blocks_cap) * kSearchWarps;
+  uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * (2ull * a.max_pool + 64ull) * expand * W));
+  CK(s.counter.ensure(sizeof(unsigned int)));
+  CK(cudaMemsetAsync(a.status, 0, nq * sizeof(int32_t), stream));
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    uint32_t gen_base = 0;
+    if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    if (stream != s.stream) CK(cudaStreamSynchronize(s.stream));
+    if (tracing) CK(cudaMemsetAsync(s.trace_count_dev, 0, sizeof(unsigned long long), stream));
+    a.visited = s.visited.as<unsigned long long>();
+    a.visited_mask = s.visited_mask;
+    a.gen_base = gen_base;
+    a.next_query = s.counter.as<unsigned int>();
+    for (int q0 = 0; q0 < nq; q0 += chunk) {
+      const int q1 = std::min(nq, q0 + chunk);
+      if (seed_pass) {
+        {
+          TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream);
+          launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
+                               s.seed_dists.as<float>(), stream);
+        }
+        CK(cudaGetLastError());
+        ++g_launches;
+      }
+      b.q_begin = q0;
+      b.q_end = q1;
+      CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
+      const int blocks = std::max(1, std::min(blocks_cap, (q1 - q0 + kSearchWarps - 1) / kSearchWarps));
+      {
+        TimedLaunch tl(ROVER_KERNEL_PQ_BATCHED, stream);
+        kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a, b, c);
+      }
+      CK(cudaGetLastError());
+      ++g_launches;
+    }
+    s.h_status.resize(nq);
+    CK(cudaMemcpyAsync(s.h_status.data(), a.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    collect_timings();
+    bool retry = false;
+    for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
+    if (!retry) break;
+    entries = next_pow2(static_cast<uint64_t>(entries) * 4);
+    CK(cudaMemsetAsync(a.status, 0, nq * sizeof(int32_t), stream));
   }
   for (int i = 0; i < nq; ++i)
     if (s.h_status[i] != kStatusOk) {
@@ -491,12 +693,16 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
     a.gen_base = gen_base;
     a.next_query = s.counter.as<unsigned int>();
     CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
-    sq_search_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
+    {
+      TimedLaunch tl(ROVER_KERNEL_SQ, stream);
+      sq_search_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
+    }
     CK(cudaGetLastError());
     ++g_launches;
     s.h_status.resize(nq);
     CK(cudaMemcpyAsync(s.h_status.data(), d_status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
+    collect_timings();
     bool retry = false;
     for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
     if (!retry) break;
@@ -557,6 +763,27 @@ AEEResult load_sq(State& s, SqDevice& d, const RoverSqIndexDesc* desc, int l1_bi
 extern "C" const char* calculator_rover_last_error(void) { return g_last_error.c_str(); }
 
 extern "C" uint64_t calculator_rover_launch_count(void) { return g_launches.load(); }
+
+extern "C" void calculator_rover_kernel_timing(int32_t enable) {
+  KernelTimer& t = timer();
+  std::lock_guard<std::mutex> g(t.mu);
+  t.on = enable != 0;
+  for (int k = 0; k < ROVER_KERNEL_KINDS; ++k) {
+    t.launches[k] = 0;
+    t.ms[k] = 0.0;
+  }
+}
+
+extern "C" int32_t calculator_rover_kernel_times(int64_t* launches, double* ms, int32_t kinds) {
+  KernelTimer& t = timer();
+  std::lock_guard<std::mutex> g(t.mu);
+  const int32_t n = std::max(0, std::min<int32_t>(kinds, ROVER_KERNEL_KINDS));
+  for (int32_t k = 0; k < n; ++k) {
+    if (launches) launches[k] = t.launches[k];
+    if (ms) ms[k] = t.ms[k];
+  }
+  return n;
+}
 
 extern "C" AEEResult calculator_rover_pq_load(remote_handle64 h, const RoverPqIndexDesc* d) {
   (void)h;
@@ -652,12 +879,9 @@ extern "C" AEEResult calculator_rover_pq_search_device(remote_handle64 h, const 
   return pq_search_core(s, p, queries, nq, pool_sizes, top_ks, h_pool, o, strm);
 }
 
-extern "C" AEEResult calculator_rover_pq_search(remote_handle64 h, const RoverSearchParams* p,
-                                                const float* queries, int32_t nq, const int32_t* pool_sizes,
-                                                const int32_t* top_ks, const RoverSearchOutputs* out) {
-  (void)h;
-  State& s = st();
-  std::lock_guard<std::mutex> lock(s.mu);
+// Host-buffer PQ search (the lock is held by the caller).
+AEEResult pq_search_host(State& s, const RoverSearchParams* p, const float* queries, int32_t nq,
+                         const int32_t* pool_sizes, const int32_t* top_ks, const RoverSearchOutputs* out) {
   if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
   if (!valid_params(p) || nq < 0 || !out || !queries || !pool_sizes || (out->ids && !out->counts)) return AEE_EBADPARM;
   if (nq == 0) return AEE_SUCCESS;
@@ -718,6 +942,292 @@ extern "C" AEEResult calculator_rover_pq_search(remote_handle64 h, const RoverSe
   }
   if (out->stats && download(out->stats, d.stats, static_cast<size_t>(nq) * 4, strm)) return AEE_EFAILED;
   CK(cudaStreamSynchronize(strm));
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_pq_search(remote_handle64 h, const RoverSearchParams* p,
+                                                const float* queries, int32_t nq, const int32_t* pool_sizes,
+                                                const int32_t* top_ks, const RoverSearchOutputs* out) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  return pq_search_host(s, p, queries, nq, pool_sizes, top_ks, out);
+}
+
+static_assert(sizeof(RoverGateTraceRow) == sizeof(GateTraceRow), "trace row layout");
+
+extern "C" AEEResult calculator_rover_pq_trace(remote_handle64 h, const RoverSearchParams* p, const float* queries,
+                                               int32_t nq, const int32_t* pool_sizes, const RoverSearchOutputs* out,
+                                               RoverGateTraceRow* rows, int64_t capacity, int64_t* count) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!p || capacity < 0 || (capacity > 0 && !rows) || !count) return AEE_EBADPARM;
+  CK(s.trace_rows.ensure(static_cast<size_t>(std::max<int64_t>(capacity, 1)) * sizeof(GateTraceRow)));
+  CK(s.trace_count.ensure(sizeof(unsigned long long)));
+  s.trace_dev = s.trace_rows.as<GateTraceRow>();
+  s.trace_count_dev = s.trace_count.as<unsigned long long>();
+  s.trace_cap = capacity;
+  RoverSearchParams pp = *p;
+  pp.mode = ROVER_MODE_BATCHED;
+  pp.beam_width = 1;
+  AEEResult r = pq_search_host(s, &pp, queries, nq, pool_sizes, nullptr, out);
+  s.trace_dev = nullptr;
+  s.trace_count_dev = nullptr;
+  s.trace_cap = 0;
+  if (r != AEE_SUCCESS) return r;
+  unsigned long long n = 0;
+  CK(cudaMemcpy(&n, s.trace_count.p, sizeof(n), cudaMemcpyDeviceToHost));
+  *count = static_cast<int64_t>(n);
+  const int64_t keep = std::min<int64_t>(capacity, static_cast<int64_t>(n));
+  if (keep > 0) CK(cudaMemcpy(rows, s.trace_rows.p, static_cast<size_t>(keep) * sizeof(GateTraceRow),
+                              cudaMemcpyDeviceToHost));
+  return AEE_SUCCESS;
+}
+
+namespace {
+uint16_t to_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return static_cast<uint16_t>((u >> 16) | ((u & 0xffffu) ? 0x40u : 0u));
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return static_cast<uint16_t>(u >> 16);
+}
+}  // namespace
+
+extern "C" AEEResult calculator_rover_gate_load(remote_handle64 h, const float* params, const float* mu,
+                                                const float* sigma, const RoverGateThresholds* t) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!params || !mu || !sigma || !t) return AEE_EBADPARM;
+  for (int i = 0; i < ROVER_GATE_PARAMS; ++i)
+    if (!std::isfinite(params[i])) { set_error("gate parameter %d is not finite", i); return AEE_EBADPARM; }
+  for (int i = 0; i < kGateIn; ++i)
+    if (!std::isfinite(mu[i]) || !(sigma[i] > 0.0f) || !std::isfinite(sigma[i])) {
+      set_error("gate input %d: mean / deviation invalid", i);
+      return AEE_EBADPARM;
+    }
+  const float* w1 = params;                 // [5][64]
+  const float* b1 = w1 + kGateIn * kGateHidden;
+  const float* w2 = b1 + kGateHidden;       // [64][64]
+  const float* b2 = w2 + kGateHidden * kGateHidden;
+  const float* w3 = b2 + kGateHidden;       // [64][2]
+  const float* b3 = w3 + kGateHidden * kGateOut;
+  std::vector<uint16_t> w1t(kGateHidden * kGateW1Stride, 0), w2t(kGateHidden * kGateW2Stride, 0),
+      w3t(8 * kGateW2Stride, 0);
+  for (int o = 0; o < kGateHidden; ++o)
+    for (int i = 0; i < kGateIn; ++i) w1t[o * kGateW1Stride + i] = to_bf16(w1[i * kGateHidden + o]);
+  for (int o = 0; o < kGateHidden; ++o)
+    for (int i = 0; i < kGateHidden; ++i) w2t[o * kGateW2Stride + i] = to_bf16(w2[i * kGateHidden + o]);
+  for (int o = 0; o < kGateOut; ++o)
+    for (int i = 0; i < kGateHidden; ++i) w3t[o * kGateW2Stride + i] = to_bf16(w3[i * kGateOut + o]);
+  std::vector<float> bias(kGateHidden * 2 + 8, 0.0f);
+  std::copy(b1, b1 + kGateHidden, bias.begin());
+  std::copy(b2, b2 + kGateHidden, bias.begin() + kGateHidden);
+  std::copy(b3, b3 + kGateOut, bias.begin() + 2 * kGateHidden);
+  const size_t o1 = 0, o2 = o1 + w1t.size() * 2, o3 = o2 + w2t.size() * 2, ob = o3 + w3t.size() * 2;
+  const size_t total = ob + bias.size() * 4;
+  CK(s.gate_buf.ensure(total));
+  uint8_t* d = s.gate_buf.as<uint8_t>();
+  CK(cudaMemcpy(d + o1, w1t.data(), w1t.size() * 2, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + o2, w2t.data(), w2t.size() * 2, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + o3, w3t.data(), w3t.size() * 2, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + ob, bias.data(), bias.size() * 4, cudaMemcpyHostToDevice));
+  GateParams g{};
+  g.w1t = reinterpret_cast<const uint16_t*>(d + o1);
+  g.w2t = reinterpret_cast<const uint16_t*>(d + o2);
+  g.w3t = reinterpret_cast<const uint16_t*>(d + o3);
+  g.b1 = reinterpret_cast<const float*>(d + ob);
+  g.b2 = g.b1 + kGateHidden;
+  g.b3 = g.b2 + kGateHidden;
+  for (int i = 0; i < kGateIn; ++i) {
+    g.mu[i] = mu[i];
+    g.inv_sigma[i] = 1.0f / sigma[i];
+  }
+  g.band_lo = t->band_lo;
+  g.band_hi = t->band_hi;
+  g.refine_logit = t->refine_logit;
+  g.stop_logit = t->stop_logit;
+  g.enabled = 1;
+  s.gate = g;
+  return AEE_SUCCESS;
+}
+
+namespace {
+constexpr int kGateParamCount = ROVER_GATE_PARAMS;
+
+// Device copies of one training set.
+struct GateData {
+  DevBuf x, y, m, mu, sigma, stats;
+  AEEResult upload_rows(State& s, const float* hx, const float* hy, const float* hm, int64_t n) {
+    if (upload(x, hx, static_cast<size_t>(n) * kGateIn, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    if (upload(y, hy, static_cast<size_t>(n) * kGateOut, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    if (upload(m, hm, static_cast<size_t>(n) * kGateOut, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    return AEE_SUCCESS;
+  }
+  void release() { x.release(); y.release(); m.release(); mu.release(); sigma.release(); stats.release(); }
+};
+}  // namespace
+
+extern "C" AEEResult calculator_rover_gate_grad(remote_handle64 h, const float* x, const float* y, const float* m,
+                                                int64_t n, const float* params, const float* mu, const float* sigma,
+                                                const float* pos_weight, float* grad_out, float* loss_out) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!x || !y || !m || n <= 0 || !params || !mu || !sigma || !pos_weight || !grad_out || !loss_out)
+    return AEE_EBADPARM;
+  GateData d;
+  DevBuf p, g, l;
+  AEEResult r = d.upload_rows(s, x, y, m, n);
+  if (r == AEE_SUCCESS && (upload(p, params, kGateParamCount, s.stream) != AEE_SUCCESS ||
+                           upload(d.mu, mu, kGateIn, s.stream) != AEE_SUCCESS ||
+                           upload(d.sigma, sigma, kGateIn, s.stream) != AEE_SUCCESS))
+    r = AEE_ENOMEMORY;
+  if (r == AEE_SUCCESS) {
+    if (g.ensure(kGateParamCount * sizeof(float)) != cudaSuccess || l.ensure(sizeof(double)) != cudaSuccess) {
+      r = AEE_ENOMEMORY;
+    } else {
+      cudaMemsetAsync(g.p, 0, kGateParamCount * sizeof(float), s.stream);
+      cudaMemsetAsync(l.p, 0, sizeof(double), s.stream);
+      const cudaError_t e = launch_gate_fwd_bwd(p.as<float>(), d.mu.as<float>(), d.sigma.as<float>(), d.x.as<float>(),
+                                                d.y.as<float>(), d.m.as<float>(), nullptr, n, pos_weight[0],
+                                                pos_weight[1], static_cast<float>(n), g.as<float>(), l.as<double>(),
+                                                s.stream);
+      ++g_launches;
+      double loss = 0.0;
+      if (e != cudaSuccess ||
+          cudaMemcpyAsync(grad_out, g.p, kGateParamCount * sizeof(float), cudaMemcpyDeviceToHost, s.stream) !=
+              cudaSuccess ||
+          cudaMemcpyAsync(&loss, l.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
+          cudaStreamSynchronize(s.stream) != cudaSuccess) {
+        set_error("gate gradient: %s", cudaGetErrorString(cudaGetLastError()));
+        r = AEE_EFAILED;
+      } else {
+        *loss_out = static_cast<float>(loss / static_cast<double>(n));
+      }
+    }
+  }
+  d.release();
+  p.release();
+  g.release();
+  l.release();
+  return r;
+}
+
+extern "C" AEEResult calculator_rover_gate_train(remote_handle64 h, const float* x, const float* y, const float* m,
+                                                 int64_t n, const RoverGateTrainParams* tp, float* params_out,
+                                                 float* mu_out, float* sigma_out, float* epoch_loss) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!x || !y || !m || n <= 0 || !tp || tp->size < static_cast<int32_t>(offsetof(RoverGateTrainParams, reserved)) ||
+      tp->epochs <= 0 || tp->batch <= 0 || !(tp->lr > 0.0f) || !params_out || !mu_out || !sigma_out)
+    return AEE_EBADPARM;
+  GateData d;
+  DevBuf p, g, m1, m2, l, idx;
+  auto fail = [&](AEEResult r) {
+    d.release(); p.release(); g.release(); m1.release(); m2.release(); l.release(); idx.release();
+    return r;
+  };
+  if (d.upload_rows(s, x, y, m, n) != AEE_SUCCESS) return fail(AEE_ENOMEMORY);
+  // standardisation statistics
+  if (d.stats.ensure(2 * kGateIn * sizeof(double)) != cudaSuccess) return fail(AEE_ENOMEMORY);
+  cudaMemsetAsync(d.stats.p, 0, 2 * kGateIn * sizeof(double), s.stream);
+  launch_gate_stats(d.x.as<float>(), n, d.stats.as<double>(), s.stream);
+  ++g_launches;
+  double acc[2 * kGateIn];
+  if (cudaMemcpyAsync(acc, d.stats.p, sizeof(acc), cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
+      cudaStreamSynchronize(s.stream) != cudaSuccess) {
+    set_error("gate statistics: %s", cudaGetErrorString(cudaGetLastError()));
+    return fail(AEE_EFAILED);
+  }
+  float mu[kGateIn], sigma[kGateIn];
+  for (int i = 0; i < kGateIn; ++i) {
+    const double mean = acc[i] / static_cast<double>(n);
+    const double var = std::max(0.0, acc[kGateIn + i] / static_cast<double>(n) - mean * mean);
+    mu[i] = static_cast<float>(mean);
+    sigma[i] = static_cast<float>(std::max(std::sqrt(var), 1e-6));
+  }
+  if (upload(d.mu, mu, kGateIn, s.stream) != AEE_SUCCESS || upload(d.sigma, sigma, kGateIn, s.stream) != AEE_SUCCESS)
+    return fail(AEE_ENOMEMORY);
+  // He-uniform initialisation, zero biases
+  std::vector<float> init(kGateParamCount, 0.0f);
+  uint64_t rng = 0x9E3779B97F4A7C15ull ^ tp->seed;
+  auto uni = [&rng]() {
+    rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17;
+    return static_cast<float>((rng >> 11) * (1.0 / 9007199254740992.0));
+  };
+  auto fill = [&](int off, int fan_in, int count) {
+    const float lim = std::sqrt(6.0f / static_cast<float>(fan_in));
+    for (int i = 0; i < count; ++i) init[off + i] = (2.0f * uni() - 1.0f) * lim;
+  };
+  fill(0, kGateIn, kGateIn * kGateHidden);
+  fill(kGateIn * kGateHidden + kGateHidden, kGateHidden, kGateHidden * kGateHidden);
+  fill(kGateIn * kGateHidden + kGateHidden + kGateHidden * kGateHidden + kGateHidden, kGateHidden,
+       kGateHidden * kGateOut);
+  if (upload(p, init.data(), init.size(), s.stream) != AEE_SUCCESS) return fail(AEE_ENOMEMORY);
+  if (g.ensure(kGateParamCount * 4) != cudaSuccess || m1.ensure(kGateParamCount * 4) != cudaSuccess ||
+      m2.ensure(kGateParamCount * 4) != cudaSuccess || l.ensure(sizeof(double)) != cudaSuccess ||
+      idx.ensure(static_cast<size_t>(n) * sizeof(int64_t)) != cudaSuccess)
+    return fail(AEE_ENOMEMORY);
+  cudaMemsetAsync(m1.p, 0, kGateParamCount * 4, s.stream);
+  cudaMemsetAsync(m2.p, 0, kGateParamCount * 4, s.stream);
+  std::vector<int64_t> order(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) order[static_cast<size_t>(i)] = i;
+  const float b1 = tp->beta1 > 0.f ? tp->beta1 : 0.9f, b2 = tp->beta2 > 0.f ? tp->beta2 : 0.999f;
+  const float eps = tp->eps > 0.f ? tp->eps : 1e-8f;
+  int64_t step = 0;
+  for (int ep = 0; ep < tp->epochs; ++ep) {
+    for (int64_t i = n - 1; i > 0; --i) {   // Fisher-Yates on the host, one upload per epoch
+      const int64_t j = static_cast<int64_t>(uni() * static_cast<float>(i + 1)) % (i + 1);
+      std::swap(order[static_cast<size_t>(i)], order[static_cast<size_t>(j)]);
+    }
+    if (cudaMemcpyAsync(idx.p, order.data(), order.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s.stream) !=
+        cudaSuccess)
+      return fail(AEE_EFAILED);
+    cudaMemsetAsync(l.p, 0, sizeof(double), s.stream);
+    for (int64_t b0 = 0; b0 < n; b0 += tp->batch) {
+      const int64_t nb = std::min<int64_t>(tp->batch, n - b0);
+      cudaMemsetAsync(g.p, 0, kGateParamCount * 4, s.stream);
+      const cudaError_t e = launch_gate_fwd_bwd(p.as<float>(), d.mu.as<float>(), d.sigma.as<float>(), d.x.as<float>(),
+                                                d.y.as<float>(), d.m.as<float>(), idx.as<int64_t>() + b0, nb,
+                                                tp->pos_weight[0] > 0.f ? tp->pos_weight[0] : 1.0f,
+                                                tp->pos_weight[1] > 0.f ? tp->pos_weight[1] : 1.0f,
+                                                static_cast<float>(nb), g.as<float>(), l.as<double>(), s.stream);
+      if (e != cudaSuccess) { set_error("gate training: %s", cudaGetErrorString(e)); return fail(AEE_EFAILED); }
+      ++step;
+      const float bc1 = 1.0f - std::pow(b1, static_cast<float>(step));
+      const float bc2 = 1.0f - std::pow(b2, static_cast<float>(step));
+      launch_gate_adam(p.as<float>(), g.as<float>(), m1.as<float>(), m2.as<float>(), kGateParamCount, tp->lr, b1, b2,
+                       eps, tp->weight_decay, bc1, bc2, s.stream);
+      g_launches += 2;
+    }
+    double loss = 0.0;
+    if (cudaMemcpyAsync(&loss, l.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
+        cudaStreamSynchronize(s.stream) != cudaSuccess) {
+      set_error("gate training: %s", cudaGetErrorString(cudaGetLastError()));
+      return fail(AEE_EFAILED);
+    }
+    if (epoch_loss) epoch_loss[ep] = static_cast<float>(loss / static_cast<double>(n));
+  }
+  if (cudaMemcpy(params_out, p.p, kGateParamCount * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return fail(AEE_EFAILED);
+  std::copy(mu, mu + kGateIn, mu_out);
+  std::copy(sigma, sigma + kGateIn, sigma_out);
+  return fail(AEE_SUCCESS);
+}
+
+extern "C" AEEResult calculator_rover_gate_unload(remote_handle64 h) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  s.gate = GateParams{};
+  s.gate_buf.release();
   return AEE_SUCCESS;
 }
 

@@ -92,9 +92,85 @@ inline void pq_decoded_layout(PqSearchArgs* a, PqDecodedArgs* b, int refine_budg
   a->smem_per_warp = (off + vis_cap * 4 + 15) & ~15;
 }
 
+// ---- learned gate: 5 -> 64 -> 64 -> 2 MLP, BF16 weights, FP32 accumulation ----
+//
+// Inputs (standardised with mu / inv_sigma): log quantized distance, beam
+// rank / L, log worst-in-beam distance, hop count / L, query norm.
+// Outputs: refine-needed logit, stop-expanding logit.
+constexpr int kGateIn = 5;
+constexpr int kGateHidden = 64;
+constexpr int kGateOut = 2;
+constexpr int kGateW1Stride = 24;   // BF16 elements per transposed W1 row (16 used)
+constexpr int kGateW2Stride = 72;   // BF16 elements per transposed W2 / W3 row (64 used)
+constexpr int kMaxBeamWidth = 8;
+
+struct GateParams {
+  const uint16_t* w1t;   // [64][24] BF16, W1 transposed (out x in), inputs 0..4
+  const uint16_t* w2t;   // [64][72] BF16
+  const uint16_t* w3t;   // [8][72]  BF16, rows 0..1 used
+  const float* b1;       // [64]
+  const float* b2;       // [64]
+  const float* b3;       // [8]
+  float mu[kGateIn], inv_sigma[kGateIn];
+  float band_lo, band_hi;        // quantized / worst ratio: <= lo correct, >= hi keep, else MLP
+  float refine_logit, stop_logit;
+  int32_t enabled;               // 0: every candidate corrected, no early stop
+};
+
+// One trace row per scored candidate or expansion source (training data for
+// the gate).  Written by the batched kernel with beam width 1 and full
+// correction, i.e. along the reference's own expansion order.
+struct GateTraceRow {
+  int32_t query, hop, id, flags;   // flags: bit0 entered the pool, bit1 expansion source, bit2 seed
+  float quantized, rank, worst, qnorm;
+  float dist;                      // corrected distance
+  float pad[3];
+};
+
+struct PqBatchArgs {
+  int32_t beam_width;
+  GateParams gate;
+  GateTraceRow* trace;            // null = no trace
+  unsigned long long* trace_count;
+  int64_t trace_cap;
+  int32_t short_cap;              // gated seeds: ADC shortlist capacity
+  int32_t smem_short_offset, smem_lut_offset, smem_feat_offset, smem_logit_offset;
+};
+
+enum PqBatchKind : int { kBatchFull = 0, kBatchGated = 1 };
+using PqBatchFn = void (*)(PqSearchArgs, PqDecodedArgs, PqBatchArgs);
+PqBatchFn pq_batched_kernel_for(int dim, int kind);
+
+// Batched warp slice: the decoded slice, then (gated or traced) the seed
+// shortlist, the query's LUT, MLP features (BF16 [128][8]) and logits.
+inline void pq_batched_layout(PqSearchArgs* a, PqDecodedArgs* b, PqBatchArgs* c, int refine_budget, int vis_cap,
+                              bool lut) {
+  pq_decoded_layout(a, b, refine_budget, vis_cap);
+  int off = a->smem_per_warp;
+  if (lut) {
+    c->smem_short_offset = off;
+    off += c->short_cap * 8;
+    c->smem_lut_offset = off;
+    off += ((a->ix.m * a->ix.ks * 4) + 15) & ~15;
+    c->smem_feat_offset = off;
+    off += kMaxBatch * 8 * 2;
+    c->smem_logit_offset = off;
+    off += kMaxBatch * 2 * 4;
+  }
+  a->smem_per_warp = (off + 15) & ~15;
+}
+
 void launch_pq_decode(const PqIndexView& ix, float* decoded, cudaStream_t s);
 void launch_pq_seed_dists(const float* queries, int q_begin, int q_end, int dim, const float* decoded,
                           const int32_t* seed_ids, int n_seeds, float* out, cudaStream_t s);
+
+// ---- gate training (gate_train.cu) ------------------------------------------
+void launch_gate_stats(const float* x, int64_t n, double* acc, cudaStream_t s);
+cudaError_t launch_gate_fwd_bwd(const float* params, const float* mu, const float* sigma, const float* x,
+                                const float* y, const float* m, const int64_t* idx, int64_t n, float pw0, float pw1,
+                                float denom, float* grad, double* loss, cudaStream_t s);
+void launch_gate_adam(float* p, const float* g, float* m1, float* m2, int count, float lr, float b1, float b2,
+                      float eps, float wd, float bc1, float bc2, cudaStream_t s);
 
 // ---- SQ search (heap-exact) ----------------------------------------------
 
