@@ -32,7 +32,8 @@ extern "C" {
 /* Search modes. */
 #define ROVER_MODE_EXACT 0    /* reference expansion order, bit-exact results */
 #define ROVER_MODE_BATCHED 1  /* free-running: beam_width pool entries expanded per step,
-                                 every candidate corrected (PQ with correction only) */
+                                 every candidate corrected (PQ with correction only;
+                                 expand_count <= 64) */
 #define ROVER_MODE_GATED 2    /* batched, with the learned gate choosing which candidates
                                  are corrected and when a query stops expanding;
                                  without a loaded gate it runs as ROVER_MODE_BATCHED */
@@ -87,8 +88,8 @@ typedef struct RoverSearchParams {
     int32_t sq_mode;         /* SQ only: 0 = device search (calculator_retrieval_search),
                                 1 = SQMD session semantics */
     int32_t layout;          /* PQ with correction: ROVER_LAYOUT_* */
-    int32_t beam_width;      /* BATCHED / GATED: entries expanded per step (0 = largest
-                                that keeps beam_width * expand_count <= 128) */
+    int32_t beam_width;      /* BATCHED / GATED: entries expanded per step, 1..4 (0 = the
+                                largest with beam_width * expand_count <= 256) */
     int32_t reserved[4];
 } RoverSearchParams;
 
@@ -276,6 +277,7 @@ uint64_t calculator_rover_launch_count(void);
 #define ROVER_KERNEL_PQ_DECODED 2   /* PQ search, decoded rows */
 #define ROVER_KERNEL_PQ_BATCHED 3   /* PQ search, batched / gated modes */
 #define ROVER_KERNEL_SQ 4           /* SQ search */
+#define ROVER_KERNEL_PQ_SEED_RANK 5 /* all-queries x entry-seeds quantized distances, tensor cores */
 #define ROVER_KERNEL_KINDS 8
 void calculator_rover_kernel_timing(int32_t enable);
 int32_t calculator_rover_kernel_times(int64_t *launches, double *ms, int32_t kinds);

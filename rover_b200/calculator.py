@@ -156,7 +156,7 @@ class Calculator:
     def launch_count(self) -> int:
         return int(self.lib.calculator_rover_launch_count())
 
-    KERNEL_KINDS = ("pq_packed", "pq_seeds", "pq_decoded", "pq_batched", "sq")
+    KERNEL_KINDS = ("pq_packed", "pq_seeds", "pq_decoded", "pq_batched", "sq", "pq_seed_rank")
 
     # -- learned gate
     def gate_load(self, params, mu, sigma, band_lo=0.0, band_hi=0.0, refine_logit=0.0, stop_logit=1e30) -> None:

@@ -77,9 +77,12 @@ struct SeedSet {
   uint32_t seed = 0;
   int32_t count = 0, dups = 0;
   DevBuf ids, bits;
+  bool recon_ready = false;        // PQ reconstructions for ranking (gated search, traces)
+  DevBuf recon, recon_norms;
   void release() {
-    ids.release(); bits.release();
+    ids.release(); bits.release(); recon.release(); recon_norms.release();
     valid = false;
+    recon_ready = false;
   }
 };
 
@@ -123,7 +126,7 @@ struct State {
   SqDevice legacy;                // calculator_retrieval_load(_dma) index
   bool legacy_dma = false;
   // scratch
-  DevBuf visited, heaps, counter, status, stats, luts, seed_dists;
+  DevBuf visited, heaps, counter, status, stats, luts, seed_dists, seed_rank;
   DevBuf gate_buf;                // BF16 transposed weights + FP32 biases of the loaded gate
   GateParams gate{};              // enabled == 0: no gate loaded
   DevBuf trace_rows, trace_count; // calculator_rover_pq_trace
@@ -309,6 +312,22 @@ AEEResult ensure_seeds(State& s, PqDevice& pq, int32_t entry_points, uint32_t se
   ss.count = static_cast<int32_t>(ids.size());
   ss.dups = dups;
   ss.valid = true;
+  ss.recon_ready = false;
+  return AEE_SUCCESS;
+}
+
+// PQ reconstructions of the current seed set (for the tensor-core ranking).
+AEEResult ensure_seed_recon(State& s, PqDevice& pq) {
+  SeedSet& ss = pq.seeds;
+  if (ss.recon_ready) return AEE_SUCCESS;
+  CK(ss.recon.ensure(static_cast<size_t>(ss.count) * pq.view.dim * sizeof(float)));
+  CK(ss.recon_norms.ensure(static_cast<size_t>(ss.count) * sizeof(float)));
+  launch_pq_seed_recon(pq.view, ss.ids.as<int32_t>(), ss.count, ss.recon.as<float>(), ss.recon_norms.as<float>(),
+                       s.stream);
+  CK(cudaGetLastError());
+  ++g_launches;
+  CK(cudaStreamSynchronize(s.stream));
+  ss.recon_ready = true;
   return AEE_SUCCESS;
 }
 
@@ -539,9 +558,10 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
   const bool tracing = s.trace_dev != nullptr;
   const bool gated = p->mode == ROVER_MODE_GATED && s.gate.enabled && !tracing;
   int W = tracing ? 1 : p->beam_width;
-  if (W == 0) W = std::max(1, std::min(kMaxBeamWidth, kMaxBatch / std::max(1, expand)));
-  if (W < 1 || W > kMaxBeamWidth || W * expand > kMaxBatch) {
-    set_error("beam_width %d: need 1..%d with beam_width * expand_count <= %d", W, kMaxBeamWidth, kMaxBatch);
+  if (W == 0) W = std::max(1, std::min(kMaxBeamWidth, kMaxBatchIds / std::max(1, expand)));
+  if (expand > 2 * 32 || W < 1 || W > kMaxBeamWidth || W * expand > kMaxBatchIds) {
+    set_error("batched search: need expand_count <= 64 and beam_width 1..%d with beam_width * expand_count <= %d",
+              kMaxBeamWidth, kMaxBatchIds);
     return AEE_EBADPARM;
   }
   if (ensure_seeds(s, pq, p->entry_points, p->seed) != AEE_SUCCESS) return AEE_ENOMEMORY;
@@ -560,22 +580,23 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
   c.trace_count = s.trace_count_dev;
   c.trace_cap = s.trace_cap;
   c.short_cap = 2 * a.max_pool;
-  const bool lut = gated || tracing;
-  // the LUT takes 4 * m * ks bytes per warp: a smaller visited table keeps
-  // two CTAs per SM
-  pq_batched_layout(&a, &b, &c, p->refine_budget, lut ? kSharedVisitedSlots / 2 : kSharedVisitedSlots, lut);
+  const bool rows = gated || tracing;   // seed ADC rows, shortlist and MLP scratch
+  pq_batched_layout(&a, &b, &c, p->refine_budget, kSharedVisitedSlots, rows);
   const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, a.max_pool); return AEE_EBADPARM; }
-  const PqBatchFn kernel = pq_batched_kernel_for(pq.view.dim, gated ? kBatchGated : kBatchFull);
+  const PqBatchFn kernel = pq_batched_kernel_for(pq.view.dim, tracing ? kBatchTrace : gated ? kBatchGated : kBatchFull);
   CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
                           static_cast<int>(smem)));
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
-  const bool seed_pass = !gated;
-  const int chunk = seed_pass ? static_cast<int>(std::max<size_t>(
-                                    1, std::min<size_t>(nq, kSeedDistBudget / (static_cast<size_t>(ss.count) * sizeof(float)))))
-                              : nq;
+  const bool seed_pass = !gated;      // exact seed distances
+  const bool rank_pass = rows;        // quantized seed distances (tensor cores)
+  if (rank_pass && ensure_seed_recon(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
+  const size_t per_query = static_cast<size_t>(ss.count) * sizeof(float) * ((seed_pass ? 1 : 0) + (rank_pass ? 1 : 0));
+  const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(nq, kSeedDistBudget / per_query)));
   if (seed_pass) CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
+  if (rank_pass) CK(s.seed_rank.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
   b.seed_dists = seed_pass ? s.seed_dists.as<float>() : nullptr;
+  c.seed_rank = rank_pass ? s.seed_rank.as<float>() : nullptr;
   const int blocks_cap = std::max(1, std::min(max_blocks, (chunk + kSearchWarps - 1) / kSearchWarps));
   const size_t slots = static_cast<size_t>(blocks_cap) * kSearchWarps;
   uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * (2ull * a.max_pool + 64ull) * expand * W));
@@ -597,6 +618,15 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
           TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream);
           launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
                                s.seed_dists.as<float>(), stream);
+        }
+        CK(cudaGetLastError());
+        ++g_launches;
+      }
+      if (rank_pass) {
+        {
+          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
+          launch_pq_seed_rank(a.queries, q0, q1, pq.view.dim, pq.seeds.recon.as<float>(),
+                              pq.seeds.recon_norms.as<float>(), b.n_seeds, s.seed_rank.as<float>(), stream);
         }
         CK(cudaGetLastError());
         ++g_launches;
@@ -798,8 +828,11 @@ extern "C" AEEResult calculator_rover_pq_load(remote_handle64 h, const RoverPqIn
   }
   const size_t n = d->num_vectors;
   const size_t book = static_cast<size_t>(d->m) * d->ks * d->subdim;
-  for (size_t i = 0; i < book; ++i)
+  float absmax = 0.0f;
+  for (size_t i = 0; i < book; ++i) {
     if (!std::isfinite(d->codebook[i])) { set_error("codebook is not finite"); return AEE_EBADPARM; }
+    absmax = std::max(absmax, std::fabs(d->codebook[i]));
+  }
   PqDevice& pq = s.pq;
   pq.release();
   AEEResult r = AEE_SUCCESS;
@@ -844,6 +877,7 @@ extern "C" AEEResult calculator_rover_pq_load(remote_handle64 h, const RoverPqIn
   v.rcb = rcb;
   v.vpb = vpb;
   v.qparams = rcb ? pq.qparams.as<float>() : nullptr;
+  v.codebook_absmax = absmax;
   pq.graph_entry = d->graph_entry;
   pq.loaded = true;
   return AEE_SUCCESS;

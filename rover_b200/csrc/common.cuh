@@ -33,6 +33,7 @@ struct PqIndexView {
   const uint8_t* residual;  // 4096-byte blocks of vpb rows each
   int32_t residual_bits, rcb, vpb;
   const float* qparams;     // [n][2] {scale, zero}
+  float codebook_absmax;    // max |codebook entry| (bounds every LUT entry)
 };
 
 struct SqIndexView {

@@ -102,7 +102,8 @@ constexpr int kGateHidden = 64;
 constexpr int kGateOut = 2;
 constexpr int kGateW1Stride = 24;   // BF16 elements per transposed W1 row (16 used)
 constexpr int kGateW2Stride = 72;   // BF16 elements per transposed W2 / W3 row (64 used)
-constexpr int kMaxBeamWidth = 8;
+constexpr int kMaxBeamWidth = 4;
+constexpr int kMaxBatchIds = 256;  // fresh ids one batched step can claim (beam width x expand)
 
 struct GateParams {
   const uint16_t* w1t;   // [64][24] BF16, W1 transposed (out x in), inputs 0..4
@@ -133,29 +134,33 @@ struct PqBatchArgs {
   GateTraceRow* trace;            // null = no trace
   unsigned long long* trace_count;
   int64_t trace_cap;
+  const float* seed_rank;         // [q_end - q_begin][n_seeds] quantized seed distances (gated, traces)
   int32_t short_cap;              // gated seeds: ADC shortlist capacity
-  int32_t smem_short_offset, smem_lut_offset, smem_feat_offset, smem_logit_offset;
+  int32_t smem_ids_offset, smem_short_offset, smem_feat_offset, smem_logit_offset;
 };
 
-enum PqBatchKind : int { kBatchFull = 0, kBatchGated = 1 };
+enum PqBatchKind : int { kBatchFull = 0, kBatchGated = 1, kBatchTrace = 2 };
 using PqBatchFn = void (*)(PqSearchArgs, PqDecodedArgs, PqBatchArgs);
 PqBatchFn pq_batched_kernel_for(int dim, int kind);
 
-// Batched warp slice: the decoded slice, then (gated or traced) the seed
-// shortlist, the query's LUT, MLP features (BF16 [128][8]) and logits.
+constexpr int kGateRows = 32;    // MLP rows per warp pass (one per lane)
+
+// Batched warp slice: the decoded slice, the step's fresh ids, then (gated
+// or traced) the seed shortlist, MLP features (BF16 [32][8]) and logits
+// ([32][2]).
 inline void pq_batched_layout(PqSearchArgs* a, PqDecodedArgs* b, PqBatchArgs* c, int refine_budget, int vis_cap,
-                              bool lut) {
+                              bool gate_rows) {
   pq_decoded_layout(a, b, refine_budget, vis_cap);
   int off = a->smem_per_warp;
-  if (lut) {
+  c->smem_ids_offset = off;
+  off += kMaxBatchIds * 4;
+  if (gate_rows) {
     c->smem_short_offset = off;
     off += c->short_cap * 8;
-    c->smem_lut_offset = off;
-    off += ((a->ix.m * a->ix.ks * 4) + 15) & ~15;
     c->smem_feat_offset = off;
-    off += kMaxBatch * 8 * 2;
+    off += kGateRows * 8 * 2;
     c->smem_logit_offset = off;
-    off += kMaxBatch * 2 * 4;
+    off += kGateRows * 2 * 4;
   }
   a->smem_per_warp = (off + 15) & ~15;
 }
@@ -163,6 +168,13 @@ inline void pq_batched_layout(PqSearchArgs* a, PqDecodedArgs* b, PqBatchArgs* c,
 void launch_pq_decode(const PqIndexView& ix, float* decoded, cudaStream_t s);
 void launch_pq_seed_dists(const float* queries, int q_begin, int q_end, int dim, const float* decoded,
                           const int32_t* seed_ids, int n_seeds, float* out, cudaStream_t s);
+// Seed PQ reconstructions [n_seeds][dim] and their squared norms.
+void launch_pq_seed_recon(const PqIndexView& ix, const int32_t* seed_ids, int n_seeds, float* rows, float* norms,
+                          cudaStream_t s);
+// Quantized seed distances for ranking (TF32 tensor cores):
+// out[q - q_begin][u] = |q|^2 + |x~_u|^2 - 2 q . x~_u.  dim % 4 == 0.
+void launch_pq_seed_rank(const float* queries, int q_begin, int q_end, int dim, const float* rows, const float* norms,
+                         int n_seeds, float* out, cudaStream_t s);
 
 // ---- gate training (gate_train.cu) ------------------------------------------
 void launch_gate_stats(const float* x, int64_t n, double* acc, cudaStream_t s);

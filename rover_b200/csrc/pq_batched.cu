@@ -19,9 +19,11 @@
 //     evaluated: below the band they are corrected, above it they keep ADC.
 //   * stop head: per step, evaluated on the selected sources; when the mean
 //     stop logit passes its threshold the query stops expanding.
-// Entry seeds are ranked by ADC from the query's LUT (kept in shared memory)
-// and only a shortlist of twice the pool is gated and merged.  The final
-// refine (FP64, top refine_budget) runs as in every mode.
+// Entry seeds are ranked by their ADC distances (pq_seed_adc_kernel, one
+// LUT per query in shared memory) and only a shortlist of twice the pool is
+// gated and merged; expansion candidates are all corrected, since with
+// decoded rows a correction costs what the in-place ADC it would be gated on
+// costs.  The final refine (FP64, top refine_budget) runs as in every mode.
 //
 // The same kernel with beam width 1, full correction and a trace buffer
 // writes the gate's training rows: every scored candidate and every
@@ -66,26 +68,6 @@ __device__ __forceinline__ bool row_dist(const float* __restrict__ xrow, const f
   }
   *out = acc;
   return isfinite(acc);
-}
-
-// ADC distance from the query's LUT in shared memory (sequential sum over
-// subspaces as retrieval_pq_adc_scalar, pq_core.c:392).
-__device__ __forceinline__ float lut_adc(const PqIndexView& ix, const float* lut, int32_t id) {
-  const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
-  float adc = 0.0f;
-  if (ix.ks == 256 && (ix.m & 3) == 0) {
-    for (int m0 = 0; m0 < ix.m; m0 += 4) {
-      const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(code) + (m0 >> 2));
-#pragma unroll
-      for (int t = 0; t < 4; ++t) adc = fadd(adc, lut[(m0 + t) * 256 + ((w >> (8 * t)) & 255u)]);
-    }
-  } else {
-    for (int m = 0; m < ix.m; ++m) {
-      const int cc = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
-      adc = fadd(adc, lut[m * ix.ks + cc]);
-    }
-  }
-  return adc;
 }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -184,16 +166,20 @@ __device__ __forceinline__ void gate_rows(const GateParams& gp, const uint32_t* 
   __syncwarp();
 }
 
-__device__ __forceinline__ void trace_put(const PqBatchArgs& c, int lane, bool have, const GateTraceRow& row) {
+// Appends the rows of the lanes that have one; returns this lane's row
+// index, or ~0 when it wrote none (no row, or the buffer is full).
+__device__ __forceinline__ unsigned long long trace_put(const PqBatchArgs& c, int lane, bool have,
+                                                        const GateTraceRow& row) {
   const unsigned m = __ballot_sync(kFullMask, have);
-  if (!m) return;
+  if (!m) return ~0ull;
   unsigned long long start = 0;
   if (lane == 0) start = atomicAdd(c.trace_count, static_cast<unsigned long long>(__popc(m)));
   start = __shfl_sync(kFullMask, start, 0);
-  if (have) {
-    const unsigned long long idx = start + __popc(m & ((1u << lane) - 1u));
-    if (idx < static_cast<unsigned long long>(c.trace_cap)) c.trace[idx] = row;
-  }
+  if (!have) return ~0ull;
+  const unsigned long long idx = start + __popc(m & ((1u << lane) - 1u));
+  if (idx >= static_cast<unsigned long long>(c.trace_cap)) return ~0ull;
+  c.trace[idx] = row;
+  return idx;
 }
 
 // Position test after a merge: whether key (expanded bit clear) is in list.
@@ -202,12 +188,6 @@ __device__ __forceinline__ bool in_list(const uint64_t* list, int size, uint64_t
   return p < size && key_cmp(list[p]) == key_cmp(key);
 }
 
-__device__ __forceinline__ void sort_merge_any(uint64_t* list, int* size, int cap, uint64_t* stage, int nb,
-                                               int* cursor, int lane) {
-  if (nb <= 32) sort_and_merge<1>(list, size, cap, stage, nb, cursor, lane);
-  else if (nb <= 64) sort_and_merge<2>(list, size, cap, stage, nb, cursor, lane);
-  else sort_and_merge<4>(list, size, cap, stage, nb, cursor, lane);
-}
 
 }  // namespace
 
@@ -215,6 +195,7 @@ template <int D, int KIND>
 __global__ void __launch_bounds__(kSearchWarps * 32, 4)
 pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
   constexpr bool kGated = KIND == kBatchGated;
+  constexpr bool tracing = KIND == kBatchTrace;   // trace rows (full correction, beam width 1)
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -222,16 +203,13 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
   float* q = reinterpret_cast<float*>(base);
   uint64_t* list = reinterpret_cast<uint64_t*>(base + a.smem_query_bytes);
   uint64_t* stage = list + a.max_pool;
-  int32_t* batch = reinterpret_cast<int32_t*>(stage + kMaxBatch);
+  int32_t* batch = reinterpret_cast<int32_t*>(base + c.smem_ids_offset);   // kMaxBatchIds fresh ids per step
   uint32_t* vis = reinterpret_cast<uint32_t*>(base + b.smem_vis_offset);
   const uint32_t vmask = static_cast<uint32_t>(b.vis_cap - 1);
-  const bool tracing = c.trace != nullptr;
-  const bool use_lut = kGated || tracing;
-  uint64_t* shortl = use_lut ? reinterpret_cast<uint64_t*>(base + c.smem_short_offset) : nullptr;
-  float* lut = use_lut ? reinterpret_cast<float*>(base + c.smem_lut_offset) : nullptr;
+  constexpr bool adc_rows = kGated || tracing;     // quantized seed distances from pq_seed_rank_kernel
+  uint64_t* shortl = adc_rows ? reinterpret_cast<uint64_t*>(base + c.smem_short_offset) : nullptr;
   uint32_t* feat = kGated ? reinterpret_cast<uint32_t*>(base + c.smem_feat_offset) : nullptr;
   float* logits = kGated ? reinterpret_cast<float*>(base + c.smem_logit_offset) : nullptr;
-  const bool gate_on = kGated && c.gate.enabled;
   const int slot = blockIdx.x * kSearchWarps + warp;
   VisitedTable vt;
   vt.slots = a.visited + static_cast<size_t>(slot) * (a.visited_mask + 1ull);
@@ -250,7 +228,8 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
     const int cap = a.pool_sizes[qi];
     int32_t* status = a.status + qi;
     const int expand = min(a.expand_count, ix.degree);
-    if (cap <= 0 || cap > a.max_pool || expand <= 0 || W * expand > kMaxBatch || a.entry_points <= 0) {
+    if (cap <= 0 || cap > a.max_pool || expand <= 0 || expand > 2 * kWarp || W * expand > kMaxBatchIds ||
+        a.entry_points <= 0) {
       if (lane == 0) *status = kStatusBadParam;
       continue;
     }
@@ -268,92 +247,54 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
     const float qnorm = sqrtf(qsq);
     for (int i = lane; i < b.vis_cap; i += kWarp) vis[i] = kEmpty;
     __syncwarp();
-    // LUT (retrieval_pq_build_lut); kept in shared memory when ADC is needed
-    bool bad = false;
-    float lmax = 0.0f;
-    for (int e = lane; e < ix.m * ix.ks; e += kWarp) {
-      const int m = e / ix.ks;
-      const float* cen = ix.codebook + static_cast<size_t>(e) * ix.subdim;
-      float acc = 0.0f;
-      for (int j = 0; j < ix.subdim; ++j) {
-        const float diff = fsub(q[m * ix.subdim + j], __ldg(cen + j));
-        acc = fadd(acc, fmul(diff, diff));
+    bool check_adc = false;
+    if (!lut_provably_safe(ix, q, lane)) {
+      // retrieval_pq_build_lut fails the query on a non-finite LUT entry
+      bool bad = false;
+      float lmax = 0.0f;
+      for (int e = lane; e < ix.m * ix.ks; e += kWarp) {
+        const int m = e / ix.ks;
+        const float* cen = ix.codebook + static_cast<size_t>(e) * ix.subdim;
+        float acc = 0.0f;
+        for (int j = 0; j < ix.subdim; ++j) {
+          const float diff = fsub(q[m * ix.subdim + j], __ldg(cen + j));
+          acc = fadd(acc, fmul(diff, diff));
+        }
+        if (!isfinite(acc)) bad = true;
+        else lmax = fmaxf(lmax, acc);
       }
-      if (!isfinite(acc)) bad = true;
-      else lmax = fmaxf(lmax, acc);
-      if (use_lut) lut[e] = acc;
-    }
-    if (__any_sync(kFullMask, bad)) {
-      if (lane == 0) *status = kStatusNumeric;
-      continue;
-    }
+      if (__any_sync(kFullMask, bad)) {
+        if (lane == 0) *status = kStatusNumeric;
+        continue;
+      }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFullMask, lmax, off));
-    const bool check_adc = !(lmax <= adc_bound);
-    __syncwarp();
+      for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFullMask, lmax, off));
+      check_adc = !(lmax <= adc_bound);
+    }
     vt.gen = a.gen_base + static_cast<uint32_t>(qi);
     int size = 0, cursor = 0;
     unsigned long long scored = static_cast<unsigned long long>(b.n_seeds), corrected = 0, expanded = 0;
     unsigned long long dedup = lane == 0 ? static_cast<unsigned long long>(b.seed_dups) : 0ull;
     int32_t st = kStatusOk;
-    int scap = 0, ssize = 0;
+    int ssize = 0;
 
     // ---- ADC shortlist of the seeds (gated search, traces)
-    if (use_lut) {
-      scap = min(c.short_cap, 2 * cap);
+    if (adc_rows) {
+      const int scap = min(c.short_cap, 2 * cap);
+      const float* arow = c.seed_rank + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
       int dummy = 0;
-      for (int e0 = 0; e0 < b.n_seeds && st == kStatusOk; e0 += kMaxBatch) {
-        const uint64_t thr = ssize == scap ? key_cmp(shortl[scap - 1]) : kEmptyKey;
-        int cnt = 0;
-        bool nonfinite = false;
-#pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
-          const int e = e0 + r * kWarp + lane;
-          uint64_t k = kEmptyKey;
-          if (e < b.n_seeds) {
-            const int32_t id = __ldg(b.seed_ids + e);
-            const float adc = lut_adc(ix, lut, id);
-            if (!isfinite(adc)) nonfinite = true;
-            else k = make_key(adc, id);
-          }
-          const bool keep = k < thr;
-          const unsigned km = __ballot_sync(kFullMask, keep);
-          if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = k;
-          cnt += __popc(km);
-        }
-        if (__any_sync(kFullMask, nonfinite)) { st = kStatusNumeric; break; }
-        __syncwarp();
-        if (cnt) sort_merge_any(shortl, &ssize, scap, stage, cnt, &dummy, lane);
-      }
+      if (!select_top(shortl, &ssize, scap, stage, b.n_seeds, SeedRowKeys{arow, b.seed_ids}, &dummy, lane))
+        st = kStatusNumeric;
     }
 
-    if (!gate_on) {
+    if (!kGated) {
       // ---- exact seed pool from the all-seeds distance pass
       corrected = static_cast<unsigned long long>(b.n_seeds);
       const float* drow = b.seed_dists + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
-      for (int e0 = 0; e0 < b.n_seeds && st == kStatusOk; e0 += kMaxBatch) {
-        const uint64_t thr = size == cap ? key_cmp(list[cap - 1]) : kEmptyKey;
-        int cnt = 0;
-        bool nonfinite = false;
-#pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
-          const int e = e0 + r * kWarp + lane;
-          uint64_t k = kEmptyKey;
-          if (e < b.n_seeds) {
-            const float d = drow[e];
-            if (!isfinite(d)) nonfinite = true;
-            else k = make_key(d, __ldg(b.seed_ids + e));
-          }
-          const bool keep = k < thr;
-          const unsigned km = __ballot_sync(kFullMask, keep);
-          if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = k;
-          cnt += __popc(km);
-        }
-        if (__any_sync(kFullMask, nonfinite)) { st = kStatusNumeric; break; }
-        __syncwarp();
-        if (cnt) sort_merge_any(list, &size, cap, stage, cnt, &cursor, lane);
-      }
-      if (st == kStatusOk && check_adc && !use_lut) {
+      if (st == kStatusOk &&
+          !select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane))
+        st = kStatusNumeric;
+      if (st == kStatusOk && check_adc) {
         bool adc_bad = false;
         for (int e = lane; e < b.n_seeds; e += kWarp) {
           float adc, dist;
@@ -361,7 +302,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
         }
         if (__any_sync(kFullMask, adc_bad)) st = kStatusNumeric;
       }
-      if (st == kStatusOk && tracing) {
+      if constexpr (tracing) if (st == kStatusOk) {
         // seed rows: the ADC shortlist with ranks among the seeds; label =
         // the seed is in the exact seed pool
         const float worst = key_dist(shortl[min(ssize, cap) - 1]);
@@ -383,63 +324,41 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
         }
       }
     } else if (st == kStatusOk) {
-      // ---- gated seeds: the shortlist, gated, merged into the pool
+      // ---- gated seeds: the shortlist, 32 rows at a time (one per lane)
       const float worst = key_dist(shortl[min(ssize, cap) - 1]);
-      for (int i0 = 0; i0 < ssize && st == kStatusOk; i0 += kMaxBatch) {
-        const int nrow = min(kMaxBatch, ssize - i0);
-        // decide: 0 keep ADC, 1 correct, 2 ask the MLP (row index in feat)
-        int decision[kMaxBatch / kWarp];
-        int nmlp = 0;
-#pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
-          const int i = i0 + r * kWarp + lane;
-          int dcs = 0;
-          if (i < i0 + nrow) {
-            const float adc = key_dist(shortl[i]);
-            const float ratio = adc / worst;
-            dcs = ratio <= c.gate.band_lo ? 1 : (ratio >= c.gate.band_hi ? 0 : 2);
-          }
-          const unsigned mm = __ballot_sync(kFullMask, dcs == 2);
-          if (dcs == 2) {
-            const int row = nmlp + __popc(mm & ((1u << lane) - 1u));
-            gate_row(c.gate, key_dist(shortl[i]), static_cast<float>(i) / cap, worst, 0.0f, qnorm, feat + row * 4);
-            dcs = 2 + row;
-          }
-          nmlp += __popc(mm);
-          decision[r] = dcs;
+      for (int i0 = 0; i0 < ssize && st == kStatusOk; i0 += kGateRows) {
+        const int i = i0 + lane;
+        const bool have = i < ssize;
+        const uint64_t k = have ? shortl[i] : 0ull;
+        const float adc = key_dist(k);
+        const float ratio = adc / worst;
+        int dcs = have ? (ratio <= c.gate.band_lo ? 1 : (ratio >= c.gate.band_hi ? 0 : 2)) : 0;
+        const unsigned mm = __ballot_sync(kFullMask, dcs == 2);
+        int row = 0;
+        if (dcs == 2) {
+          row = __popc(mm & ((1u << lane) - 1u));
+          gate_row(c.gate, adc, static_cast<float>(i) / cap, worst, 0.0f, qnorm, feat + row * 4);
         }
-        if (nmlp) gate_rows(c.gate, feat, nmlp, logits, lane);
+        if (mm) gate_rows(c.gate, feat, __popc(mm), logits, lane);
+        if (dcs == 2) dcs = logits[row * 2] > c.gate.refine_logit ? 1 : 0;
+        float d = adc;
         bool sbad = false;
-        int ncorr = 0;
-#pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
-          const int i = i0 + r * kWarp + lane;
-          if (i < i0 + nrow) {
-            const uint64_t k = shortl[i];
-            const int32_t id = key_id(k);
-            int dcs = decision[r];
-            if (dcs >= 2) dcs = logits[(dcs - 2) * 2] > c.gate.refine_logit ? 1 : 0;
-            float d = key_dist(k);
-            if (dcs == 1) {
-              if (!row_dist<D>(b.decoded + static_cast<size_t>(id) * dim, q, dim, &d)) sbad = true;
-              ++ncorr;
-            }
-            stage[i - i0] = make_key(d, id);
-          }
-        }
+        if (dcs == 1 && !row_dist<D>(b.decoded + static_cast<size_t>(key_id(k)) * dim, q, dim, &d)) sbad = true;
         if (__any_sync(kFullMask, sbad)) { st = kStatusNumeric; break; }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) ncorr += __shfl_xor_sync(kFullMask, ncorr, off);
-        corrected += ncorr;
+        corrected += __popc(__ballot_sync(kFullMask, dcs == 1));
+        if (have) stage[lane] = make_key(d, key_id(k));
         __syncwarp();
-        sort_merge_any(list, &size, cap, stage, nrow, &cursor, lane);
+        const int nrow = min(kGateRows, ssize - i0);
+        merge_scored(list, &size, cap, stage, nrow, &cursor, lane);
       }
+      if (lane != 0) corrected = 0;   // counted warp-wide; reduced with the lanes below
     }
 
     // ---- expansion steps
     bool global_mode = false;
     int claimed = 0;
     const uint32_t load_limit = (a.visited_mask + 1u) >> 1;
+    unsigned long long ncorr_lane = 0;
     while (st == kStatusOk) {
       // the first W unexpanded entries
       int sel[kMaxBeamWidth];
@@ -459,33 +378,28 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       }
       if (nsel == 0) break;
       const float worst_now = key_dist(list[size - 1]);
-      if (gate_on) {
+      int my_pos = 0;
+#pragma unroll
+      for (int k = 0; k < kMaxBeamWidth; ++k)
+        if (k == lane && k < nsel) my_pos = sel[k];
+      if (kGated && c.gate.stop_logit < FLT_MAX) {
         // stop head on the selected sources
-        if (lane < nsel) {
-          int p = 0;
-#pragma unroll
-          for (int k = 0; k < kMaxBeamWidth; ++k)
-            if (k == lane) p = sel[k];
-          gate_row(c.gate, key_dist(list[p]), static_cast<float>(p) / cap, worst_now,
+        if (lane < nsel)
+          gate_row(c.gate, key_dist(list[my_pos]), static_cast<float>(my_pos) / cap, worst_now,
                    static_cast<float>(expanded) / cap, qnorm, feat + lane * 4);
-        }
         gate_rows(c.gate, feat, nsel, logits, lane);
-        float s = lane < nsel ? logits[lane * 2 + 1] : 0.0f;
+        float sl = lane < nsel ? logits[lane * 2 + 1] : 0.0f;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(kFullMask, s, off);
-        if (s / nsel > c.gate.stop_logit) break;
+        for (int off = 16; off > 0; off >>= 1) sl += __shfl_xor_sync(kFullMask, sl, off);
+        if (sl / nsel > c.gate.stop_logit) break;
       }
-      if (tracing) {
-        int p = 0;
-#pragma unroll
-        for (int k = 0; k < kMaxBeamWidth; ++k)
-          if (k == lane) p = sel[k];
+      if constexpr (tracing) {
         GateTraceRow row{};
         const bool have = lane < nsel;
         if (have) {
-          const uint64_t k = list[p];
+          const uint64_t k = list[my_pos];
           row.query = qi; row.hop = static_cast<int32_t>(expanded) + lane; row.id = key_id(k); row.flags = 2;
-          row.quantized = key_dist(k); row.rank = static_cast<float>(p) / cap; row.worst = worst_now;
+          row.quantized = key_dist(k); row.rank = static_cast<float>(my_pos) / cap; row.worst = worst_now;
           row.qnorm = qnorm; row.dist = key_dist(k);
         }
         trace_put(c, lane, have, row);
@@ -494,33 +408,37 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       if (lane == 0)
         for (int k = 0; k < nsel; ++k) list[sel[k]] |= kExpandedBit;
       cursor = sel[nsel - 1] + 1;
-      // rows in pool order: valid prefix, then first visits
+      // the W rows, loaded together, then checked and claimed in pool order
+      int32_t nid[kMaxBeamWidth][2];
+#pragma unroll
+      for (int k = 0; k < kMaxBeamWidth; ++k) {
+        const int32_t src = k < nsel ? key_id(list[sel[k]]) : 0;
+        const int32_t* row = ix.graph + static_cast<size_t>(src) * ix.degree;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int j = r * kWarp + lane;
+          nid[k][r] = (k < nsel && j < expand) ? __ldg(row + j) : -1;
+        }
+      }
       int nb = 0;
       bool full = false, row_bad = false;
+#pragma unroll 1
       for (int k = 0; k < nsel && !row_bad; ++k) {
-        const int32_t src = key_id(list[sel[k]]);
-        const int32_t* row = ix.graph + static_cast<size_t>(src) * ix.degree;
         int first_pad = expand;
-        int32_t nid_r[kMaxBatch / kWarp];
 #pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
+        for (int r = 0; r < 2; ++r) {
           const int j = r * kWarp + lane;
-          nid_r[r] = -1;
-          if (r * kWarp < expand) {
-            const int32_t nid = j < expand ? __ldg(row + j) : -1;
-            nid_r[r] = nid;
-            const unsigned pad = __ballot_sync(kFullMask, j < expand && nid == -1);
-            if (pad && first_pad == expand) first_pad = r * kWarp + __ffs(pad) - 1;
-          }
+          const unsigned pad = __ballot_sync(kFullMask, j < expand && nid[k][r] == -1);
+          if (pad && first_pad == expand) first_pad = r * kWarp + __ffs(pad) - 1;
         }
         bool rb = false;
 #pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
+        for (int r = 0; r < 2; ++r) {
           const int j = r * kWarp + lane;
           if (j < expand) {
-            const int32_t nid = nid_r[r];
-            if (j < first_pad) rb |= (nid < 0 || nid >= ix.n);
-            else rb |= (nid != -1);
+            const int32_t v = nid[k][r];
+            if (j < first_pad) rb |= (v < 0 || v >= ix.n);
+            else rb |= (v != -1);
           }
         }
         if (__any_sync(kFullMask, rb)) { row_bad = true; break; }
@@ -532,15 +450,14 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
           global_mode = true;
           __syncwarp();
         }
-        int fresh_here = 0;
 #pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
+        for (int r = 0; r < 2; ++r) {
           if (r * kWarp < first_pad) {
             const int j = r * kWarp + lane;
             int fresh = 0;
-            const int32_t nid = nid_r[r];
+            const int32_t v = nid[k][r];
             if (j < first_pad) {
-              const uint32_t u = static_cast<uint32_t>(nid);
+              const uint32_t u = static_cast<uint32_t>(v);
               if (__ldg(b.seed_bits + (u >> 5)) & (1u << (u & 31))) {
                 ++dedup;
               } else {
@@ -551,12 +468,11 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
               }
             }
             const unsigned fm = __ballot_sync(kFullMask, fresh);
-            if (fresh) batch[nb + __popc(fm & ((1u << lane) - 1u))] = nid;
+            if (fresh) batch[nb + __popc(fm & ((1u << lane) - 1u))] = v;
             nb += __popc(fm);
-            fresh_here += __popc(fm);
+            claimed += __popc(fm);
           }
         }
-        claimed += fresh_here;
       }
       if (row_bad) { st = kStatusBadRow; break; }
       expanded += nsel;
@@ -567,119 +483,67 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       __syncwarp();
       if (nb == 0) continue;
       scored += nb;
-      // prefetch the candidates' decoded rows
       for (int e = lane; e < nb; e += kWarp) {
         const float* xr = b.decoded + static_cast<size_t>(batch[e]) * dim;
         for (int off = 0; off < dim; off += 32) asm volatile("prefetch.global.L1 [%0];" ::"l"(xr + off));
       }
-      bool sbad = false;
-      int ncorr = 0;
-      if (!gate_on) {
-        float adc_r[kMaxBatch / kWarp];
-        for (int e = lane, r = 0; e < nb; e += kWarp, ++r) {
-          const int32_t id = batch[e];
+      // every candidate corrected, scored and merged 128 at a time
+      for (int c0 = 0; c0 < nb && st == kStatusOk; c0 += kMaxBatch) {
+        const int cnt = min(kMaxBatch, nb - c0);
+        bool sbad = false;
+        for (int e = lane; e < cnt; e += kWarp) {
+          const int32_t id = batch[c0 + e];
           float dist;
           if (!row_dist<D>(b.decoded + static_cast<size_t>(id) * dim, q, dim, &dist)) sbad = true;
-          if (use_lut) {
-            const float adc = lut_adc(ix, lut, id);
-            if (!isfinite(adc)) sbad = true;
-            adc_r[r] = adc;
-          } else if (check_adc) {
+          if (check_adc) {
             float adc, unused;
             if (!pq_score(ix, q, id, false, &adc, &unused)) sbad = true;
           }
           stage[e] = make_key(dist, id);
-          ++ncorr;
-        }
-        if (__any_sync(kFullMask, sbad)) { st = kStatusNumeric; break; }
-        if (tracing) {
-          // features against the pool before this merge, kept in the
-          // (otherwise unused) MLP scratch: ADC and rank per candidate
-          float* tq = reinterpret_cast<float*>(base + c.smem_feat_offset);
-          float* tr = tq + kMaxBatch;
-          uint64_t* tk = reinterpret_cast<uint64_t*>(base + c.smem_logit_offset);
-          for (int e = lane, r = 0; e < nb; e += kWarp, ++r) {
-            const uint64_t k = stage[e];
-            tq[e] = adc_r[r];
-            tr[e] = static_cast<float>(count_less(list, size, make_key(adc_r[r], key_id(k)))) / cap;
-            tk[e] = k;
-          }
-          __syncwarp();
-          sort_merge_any(list, &size, cap, stage, nb, &cursor, lane);
-          for (int e0 = 0; e0 < nb; e0 += kWarp) {
-            const int e = e0 + lane;
-            const bool have = e < nb;
-            GateTraceRow row{};
-            if (have) {
-              const uint64_t k = tk[e];
-              row.query = qi; row.hop = static_cast<int32_t>(expanded) - nsel; row.id = key_id(k);
-              row.flags = in_list(list, size, k) ? 1 : 0;
-              row.quantized = tq[e]; row.rank = tr[e]; row.worst = worst_now; row.qnorm = qnorm;
-              row.dist = key_dist(k);
-            }
-            trace_put(c, lane, have, row);
-          }
-        } else {
-          __syncwarp();
-          sort_merge_any(list, &size, cap, stage, nb, &cursor, lane);
-        }
-      } else {
-        // gated candidates: ADC, the band rule, the MLP inside the band
-        const bool full_pool = size == cap;
-        int decision[kMaxBatch / kWarp];
-        float adc_r[kMaxBatch / kWarp];
-        int nmlp = 0;
-#pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
-          const int e = lane + r * kWarp;
-          int dcs = 0;
-          float adc = 0.0f;
-          if (e < nb) {
-            const int32_t id = batch[e];
-            adc = lut_adc(ix, lut, id);
-            if (!isfinite(adc)) sbad = true;
-            const float ratio = full_pool ? adc / worst_now : 0.0f;
-            dcs = ratio <= c.gate.band_lo ? 1 : (ratio >= c.gate.band_hi ? 0 : 2);
-          }
-          adc_r[r] = adc;
-          const unsigned mm = __ballot_sync(kFullMask, dcs == 2);
-          if (dcs == 2) {
-            const int row = nmlp + __popc(mm & ((1u << lane) - 1u));
-            const float rank = static_cast<float>(count_less(list, size, make_key(adc, batch[e]))) / cap;
-            gate_row(c.gate, adc, rank, worst_now, static_cast<float>(expanded - nsel) / cap, qnorm, feat + row * 4);
-            dcs = 2 + row;
-          }
-          nmlp += __popc(mm);
-          decision[r] = dcs;
-        }
-        if (__any_sync(kFullMask, sbad)) { st = kStatusNumeric; break; }
-        if (nmlp) gate_rows(c.gate, feat, nmlp, logits, lane);
-#pragma unroll
-        for (int r = 0; r < kMaxBatch / kWarp; ++r) {
-          const int e = lane + r * kWarp;
-          if (e < nb) {
-            const int32_t id = batch[e];
-            int dcs = decision[r];
-            if (dcs >= 2) dcs = logits[(dcs - 2) * 2] > c.gate.refine_logit ? 1 : 0;
-            float d = adc_r[r];
-            if (dcs == 1) {
-              if (!row_dist<D>(b.decoded + static_cast<size_t>(id) * dim, q, dim, &d)) sbad = true;
-              ++ncorr;
-            }
-            stage[e] = make_key(d, id);
-          }
+          ++ncorr_lane;
         }
         if (__any_sync(kFullMask, sbad)) { st = kStatusNumeric; break; }
         __syncwarp();
-        sort_merge_any(list, &size, cap, stage, nb, &cursor, lane);
-      }
+        if constexpr (tracing) {
+          // rows before the merge (features against the current pool), the
+          // entered flag patched after it
+          unsigned long long tidx[kMaxBatch / kWarp];
+          uint64_t keys[kMaxBatch / kWarp];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) ncorr += __shfl_xor_sync(kFullMask, ncorr, off);
-      corrected += ncorr;
+          for (int r = 0; r < kMaxBatch / kWarp; ++r) {
+            const int e = lane + r * kWarp;
+            const bool have = e < cnt;
+            GateTraceRow row{};
+            keys[r] = have ? stage[e] : 0ull;
+            if (have) {
+              const int32_t id = key_id(keys[r]);
+              float adc = 0.0f, unused;
+              pq_score(ix, q, id, false, &adc, &unused);
+              row.query = qi; row.hop = static_cast<int32_t>(expanded) - nsel; row.id = id;
+              row.quantized = adc;
+              row.rank = static_cast<float>(count_less(list, size, make_key(adc, id))) / cap;
+              row.worst = worst_now; row.qnorm = qnorm; row.dist = key_dist(keys[r]);
+            }
+            tidx[r] = r * kWarp < cnt ? trace_put(c, lane, have, row) : ~0ull;
+          }
+          __syncwarp();
+          merge_scored(list, &size, cap, stage, cnt, &cursor, lane);
+#pragma unroll
+          for (int r = 0; r < kMaxBatch / kWarp; ++r)
+            if (tidx[r] != ~0ull && in_list(list, size, keys[r])) c.trace[tidx[r]].flags = 1;
+        } else {
+          merge_scored(list, &size, cap, stage, cnt, &cursor, lane);
+        }
+      }
     }
 
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) dedup += __shfl_xor_sync(kFullMask, dedup, off);
+    for (int off = 16; off > 0; off >>= 1) {
+      dedup += __shfl_xor_sync(kFullMask, dedup, off);
+      ncorr_lane += __shfl_xor_sync(kFullMask, ncorr_lane, off);
+    }
+    if (kGated) corrected = __shfl_sync(kFullMask, corrected, 0);
+    corrected += ncorr_lane;
     if (st != kStatusOk) {
       if (lane == 0) *status = st;
       continue;
@@ -692,6 +556,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
 
 PqBatchFn pq_batched_kernel_for(int dim, int kind) {
   if (dim % 4 != 0) return nullptr;
+  if (kind == kBatchTrace) return pq_batched_search_kernel<0, kBatchTrace>;
   if (kind == kBatchGated) {
     switch (dim) {
       case 128: return pq_batched_search_kernel<128, kBatchGated>;

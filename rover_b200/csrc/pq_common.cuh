@@ -157,6 +157,26 @@ __device__ __forceinline__ bool pq_score_fixed(const PqIndexView& ix, const floa
   return true;
 }
 
+// ADC distance from the query's LUT in shared memory (sequential sum over
+// subspaces as retrieval_pq_adc_scalar, pq_core.c:392).
+__device__ __forceinline__ float lut_adc(const PqIndexView& ix, const float* lut, int32_t id) {
+  const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
+  float adc = 0.0f;
+  if (ix.ks == 256 && (ix.m & 3) == 0) {
+    for (int m0 = 0; m0 < ix.m; m0 += 4) {
+      const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(code) + (m0 >> 2));
+#pragma unroll
+      for (int t = 0; t < 4; ++t) adc = fadd(adc, lut[(m0 + t) * 256 + ((w >> (8 * t)) & 255u)]);
+    }
+  } else {
+    for (int m = 0; m < ix.m; ++m) {
+      const int cc = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
+      adc = fadd(adc, lut[m * ix.ks + cc]);
+    }
+  }
+  return adc;
+}
+
 // ---------------------------------------------------------------------------
 // Final refine of the first `count` pool entries (refine_impl with the PQ
 // residual decode provider): FP32 decode ((c + code*s) + z), FP64 sum of
@@ -275,7 +295,9 @@ __device__ __forceinline__ bool score_one(const PqIndexView& ix, const float* __
   else return pq_score_fixed<M, SUB, RBITS>(ix, q, id, correction, adc, dist);
 }
 
-// Sort the scored batch (keys in `stage`) and merge it into the list.
+// Sort the scored batch (keys in `stage`) and merge it into the list.  The
+// caller may first drop keys that cannot enter (drop_non_entering): they
+// would land at or beyond the list's capacity and change nothing.
 template <int PER>
 __device__ __forceinline__ void sort_and_merge(uint64_t* list, int* size, int cap, uint64_t* stage, int nb,
                                                int* cursor, int lane) {
@@ -290,6 +312,109 @@ __device__ __forceinline__ void sort_and_merge(uint64_t* list, int* size, int ca
   const int min_ins = merge_batch<PER>(list, *size, cap, stage, v, nb, lane);
   *size = min(cap, *size + nb);
   *cursor = min(*cursor, min_ins);
+}
+
+__device__ __forceinline__ void sort_merge_any(uint64_t* list, int* size, int cap, uint64_t* stage, int nb,
+                                               int* cursor, int lane) {
+  if (nb <= 32) sort_and_merge<1>(list, size, cap, stage, nb, cursor, lane);
+  else if (nb <= 64) sort_and_merge<2>(list, size, cap, stage, nb, cursor, lane);
+  else sort_and_merge<4>(list, size, cap, stage, nb, cursor, lane);
+}
+
+// Forward declaration (defined below).
+__device__ __forceinline__ int drop_non_entering(const uint64_t* list, int size, int cap, uint64_t* stage, int nb,
+                                                 int lane);
+
+// Merges the scored keys stage[0..nb) (nb <= kMaxBatch) into the sorted
+// list of capacity cap: keys that cannot enter are dropped first, then the
+// rest are sorted and merged.  Same list, same cursor as merging them all.
+__device__ __forceinline__ void merge_scored(uint64_t* list, int* size, int cap, uint64_t* stage, int nb,
+                                             int* cursor, int lane) {
+  nb = drop_non_entering(list, *size, cap, stage, nb, lane);
+  if (nb > 0) sort_merge_any(list, size, cap, stage, nb, cursor, lane);
+}
+
+// Keys (distance, seed id) of one row of a queries x seeds distance matrix.
+struct SeedRowKeys {
+  const float* row;
+  const int32_t* ids;
+  __device__ __forceinline__ uint64_t operator()(int e, bool* nonfinite) const {
+    const float d = row[e];
+    if (!isfinite(d)) {
+      *nonfinite = true;
+      return kEmptyKey;
+    }
+    return make_key(d, __ldg(ids + e));
+  }
+};
+
+// Top-cap selection of n keys (key_at(e), e = 0..n-1) into the sorted list:
+// keys below the list's worst accumulate in stage and are merged once up to
+// kMaxBatch - 32 have gathered (or at the end), so the list is merged a few
+// times instead of once per chunk.  The result is the top-cap of all keys,
+// as inserting them one by one gives.  False if a distance is non-finite.
+template <class KeyAt>
+__device__ __forceinline__ bool select_top(uint64_t* list, int* size, int cap, uint64_t* stage, int n,
+                                           const KeyAt& key_at, int* cursor, int lane) {
+  int cnt = 0;
+  for (int e0 = 0; e0 < n; e0 += kWarp) {
+    const uint64_t thr = *size == cap ? key_cmp(list[cap - 1]) : kEmptyKey;
+    const int e = e0 + lane;
+    bool nonfinite = false;
+    const uint64_t k = e < n ? key_at(e, &nonfinite) : kEmptyKey;
+    if (__any_sync(kFullMask, nonfinite)) return false;
+    const bool keep = k != kEmptyKey && key_cmp(k) < thr;
+    const unsigned km = __ballot_sync(kFullMask, keep);
+    if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = k;
+    cnt += __popc(km);
+    if (cnt > kMaxBatch - kWarp || e0 + kWarp >= n) {
+      __syncwarp();
+      if (cnt) sort_merge_any(list, size, cap, stage, cnt, cursor, lane);
+      cnt = 0;
+    }
+  }
+  return true;
+}
+
+// Whether every LUT entry of this query is provably finite and no ADC sum
+// can overflow, without building the LUT.  With every q_j and codebook entry
+// finite, |fl(q - c)| <= (|q| + |c|)(1 + 2^-24), so an entry (a sequential
+// sum of subdim squares) is at most 1.0001 * subdim * (max|q| + max|c|)^2;
+// when that is at most FLT_MAX / (2 m) the reference's LUT and ADC checks
+// cannot fail.  Otherwise the caller builds the LUT and checks it.
+__device__ __forceinline__ bool lut_provably_safe(const PqIndexView& ix, const float* q, int lane) {
+  float qmax = 0.0f;
+  bool bad = false;
+  for (int d = lane; d < ix.dim; d += kWarp) {
+    const float v = q[d];
+    bad |= !isfinite(v);
+    qmax = fmaxf(qmax, fabsf(v));
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) qmax = fmaxf(qmax, __shfl_xor_sync(kFullMask, qmax, off));
+  if (__any_sync(kFullMask, bad)) return false;
+  const double t = static_cast<double>(qmax) + static_cast<double>(ix.codebook_absmax);
+  return 1.0001 * ix.subdim * t * t <= 3.4028234663852886e38 / (2.0 * ix.m);
+}
+
+// Drops from stage[0..nb) the keys that cannot enter a full list (not below
+// its worst key), compacting the rest in order.  Returns the new count.
+__device__ __forceinline__ int drop_non_entering(const uint64_t* list, int size, int cap, uint64_t* stage, int nb,
+                                                 int lane) {
+  if (size < cap) return nb;
+  const uint64_t thr = key_cmp(list[cap - 1]);
+  int cnt = 0;
+  for (int e0 = 0; e0 < nb; e0 += kWarp) {
+    const int e = e0 + lane;
+    const uint64_t k = e < nb ? stage[e] : kEmptyKey;
+    const bool keep = e < nb && key_cmp(k) < thr;
+    const unsigned km = __ballot_sync(kFullMask, keep);
+    __syncwarp();
+    if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = k;
+    cnt += __popc(km);
+    __syncwarp();
+  }
+  return cnt;
 }
 
 // Writes one finished query's outputs: the sorted pool (optional), the

@@ -155,6 +155,137 @@ void launch_pq_seed_dists(const float* queries, int q_begin, int q_end, int dim,
 }
 
 // ---------------------------------------------------------------------------
+// Seed reconstructions for ranking: x~[u] = the PQ reconstruction of seed u
+// (its centroids, no residual) and |x~[u]|^2.
+__global__ void pq_seed_recon_kernel(PqIndexView ix, const int32_t* __restrict__ seed_ids, int n_seeds,
+                                     float* __restrict__ rows, float* __restrict__ norms) {
+  const int u = blockIdx.x;
+  if (u >= n_seeds) return;
+  const int32_t id = seed_ids[u];
+  const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
+  float sq = 0.0f;
+  for (int d = threadIdx.x; d < ix.dim; d += blockDim.x) {
+    const int m = d / ix.subdim;
+    const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
+    const float v = __ldg(ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim + (d - m * ix.subdim));
+    rows[static_cast<size_t>(u) * ix.dim + d] = v;
+    sq += v * v;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) sq += __shfl_xor_sync(kFullMask, sq, off);
+  __shared__ float part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < static_cast<int>((blockDim.x + 31) / 32); ++w) t += part[w];
+    norms[u] = t;
+  }
+}
+
+void launch_pq_seed_recon(const PqIndexView& ix, const int32_t* seed_ids, int n_seeds, float* rows, float* norms,
+                          cudaStream_t s) {
+  pq_seed_recon_kernel<<<n_seeds, 128, 0, s>>>(ix, seed_ids, n_seeds, rows, norms);
+}
+
+// All queries x all seeds, quantized distance for ranking, on the tensor
+// cores: out[q][u] = |q|^2 + |x~_u|^2 - 2 q . x~_u with the dot products as
+// TF32 mma.sync m16n8k8 tiles (FP32 accumulation).  It is not the
+// reference's ADC sum (different order and TF32 operands); the gated search
+// only ranks seeds with it, and corrects the ones it keeps exactly.
+constexpr int kRkTile = 64;
+constexpr int kRkK = 32;
+
+__device__ __forceinline__ uint32_t to_tf32(float f) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
+  return r;
+}
+
+__global__ void __launch_bounds__(128) pq_seed_rank_kernel(const float* __restrict__ queries, int q_begin, int q_end,
+                                                           int dim, const float* __restrict__ rows,
+                                                           const float* __restrict__ norms, int n_seeds,
+                                                           float* __restrict__ out) {
+  __shared__ __align__(16) float qs[kRkTile][kRkK + 4];
+  __shared__ __align__(16) float xs[kRkTile][kRkK + 4];
+  __shared__ float qn[kRkTile];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;   // this warp's 32 x 32 sub-tile
+  const int q0 = q_begin + blockIdx.y * kRkTile, u0 = blockIdx.x * kRkTile;
+  float acc[2][4][4] = {};
+  float qsq = 0.0f;   // |q|^2 of row tid (tid < 64), FP32
+  for (int k0 = 0; k0 < dim; k0 += kRkK) {
+    const int kc = min(kRkK, dim - k0);
+    for (int i = tid; i < kRkTile * (kRkK / 4); i += 128) {
+      const int r = i / (kRkK / 4), c4 = (i % (kRkK / 4)) * 4;
+      float4 qv = make_float4(0.f, 0.f, 0.f, 0.f), xv = qv;
+      if (c4 < kc) {
+        if (q0 + r < q_end) qv = __ldg(reinterpret_cast<const float4*>(queries + static_cast<size_t>(q0 + r) * dim + k0 + c4));
+        if (u0 + r < n_seeds) xv = __ldg(reinterpret_cast<const float4*>(rows + static_cast<size_t>(u0 + r) * dim + k0 + c4));
+      }
+      *reinterpret_cast<float4*>(&qs[r][c4]) = qv;
+      *reinterpret_cast<float4*>(&xs[r][c4]) = xv;
+    }
+    __syncthreads();
+    if (tid < kRkTile)
+      for (int c = 0; c < kRkK; ++c) qsq += qs[tid][c] * qs[tid][c];
+#pragma unroll
+    for (int kk = 0; kk < kRkK; kk += 8) {
+      uint32_t a[2][4], b[4][2];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        const int r = wm + mi * 16 + g;
+        a[mi][0] = to_tf32(qs[r][kk + t]);
+        a[mi][1] = to_tf32(qs[r + 8][kk + t]);
+        a[mi][2] = to_tf32(qs[r][kk + t + 4]);
+        a[mi][3] = to_tf32(qs[r + 8][kk + t + 4]);
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const int n = wn + ni * 8 + g;
+        b[ni][0] = to_tf32(xs[n][kk + t]);
+        b[ni][1] = to_tf32(xs[n][kk + t + 4]);
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+          asm volatile(
+              "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+              "{%0,%1,%2,%3};\n"
+              : "+f"(acc[mi][ni][0]), "+f"(acc[mi][ni][1]), "+f"(acc[mi][ni][2]), "+f"(acc[mi][ni][3])
+              : "r"(a[mi][0]), "r"(a[mi][1]), "r"(a[mi][2]), "r"(a[mi][3]), "r"(b[ni][0]), "r"(b[ni][1]));
+    }
+    __syncthreads();
+  }
+  if (tid < kRkTile) qn[tid] = qsq;
+  __syncthreads();
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = wm + mi * 16 + g + 8 * h;
+      const int qq = q0 + r;
+      if (qq >= q_end) continue;
+      float* orow = out + static_cast<size_t>(qq - q_begin) * n_seeds;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int uu = u0 + wn + ni * 8 + 2 * t + e;
+          if (uu < n_seeds) orow[uu] = fmaxf(qn[r] + __ldg(norms + uu) - 2.0f * acc[mi][ni][2 * h + e], 0.0f);
+        }
+    }
+}
+
+void launch_pq_seed_rank(const float* queries, int q_begin, int q_end, int dim, const float* rows, const float* norms,
+                         int n_seeds, float* out, cudaStream_t s) {
+  const dim3 grid((n_seeds + kRkTile - 1) / kRkTile, (q_end - q_begin + kRkTile - 1) / kRkTile);
+  pq_seed_rank_kernel<<<grid, 128, 0, s>>>(queries, q_begin, q_end, dim, rows, norms, n_seeds, out);
+}
+
+// ---------------------------------------------------------------------------
 
 // Shared-memory visited insert: 1 = first visit, 0 = seen, -1 = no slot.
 __device__ __forceinline__ int smem_visit(uint32_t* tab, uint32_t mask, uint32_t id) {
@@ -233,27 +364,31 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
     for (int i = lane; i < b.vis_cap; i += kWarp) vis[i] = kEmptySlot;
     __syncwarp();
     // retrieval_pq_build_lut fails the query if any LUT entry is not finite;
-    // the largest entry decides whether ADC sums need checking at all.
-    bool bad = false;
-    float lmax = 0.0f;
-    for (int e = lane; e < ix.m * ix.ks; e += kWarp) {
-      const int m = e / ix.ks;
-      const float* cen = ix.codebook + static_cast<size_t>(e) * ix.subdim;
-      float acc = 0.0f;
-      for (int j = 0; j < ix.subdim; ++j) {
-        const float diff = fsub(q[m * ix.subdim + j], __ldg(cen + j));
-        acc = fadd(acc, fmul(diff, diff));
+    // the largest entry decides whether ADC sums need checking at all.  The
+    // LUT is only built when the bound cannot settle both.
+    bool check_adc = false;
+    if (!lut_provably_safe(ix, q, lane)) {
+      bool bad = false;
+      float lmax = 0.0f;
+      for (int e = lane; e < ix.m * ix.ks; e += kWarp) {
+        const int m = e / ix.ks;
+        const float* cen = ix.codebook + static_cast<size_t>(e) * ix.subdim;
+        float acc = 0.0f;
+        for (int j = 0; j < ix.subdim; ++j) {
+          const float diff = fsub(q[m * ix.subdim + j], __ldg(cen + j));
+          acc = fadd(acc, fmul(diff, diff));
+        }
+        if (!isfinite(acc)) bad = true;
+        else lmax = fmaxf(lmax, acc);
       }
-      if (!isfinite(acc)) bad = true;
-      else lmax = fmaxf(lmax, acc);
-    }
-    if (__any_sync(kFullMask, bad)) {
-      if (lane == 0) *status = kStatusNumeric;
-      continue;
-    }
+      if (__any_sync(kFullMask, bad)) {
+        if (lane == 0) *status = kStatusNumeric;
+        continue;
+      }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFullMask, lmax, off));
-    const bool check_adc = !(lmax <= adc_bound);
+      for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFullMask, lmax, off));
+      check_adc = !(lmax <= adc_bound);
+    }
     vt.gen = a.gen_base + static_cast<uint32_t>(qi);
     int size = 0, cursor = 0;
     unsigned long long scored = static_cast<unsigned long long>(b.n_seeds), expanded = 0;
@@ -262,31 +397,8 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
 
     // ---- initial pool: top-L of the seed row under (distance, id)
     const float* drow = b.seed_dists + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
-    for (int e0 = 0; e0 < b.n_seeds; e0 += kMaxBatch) {
-      const uint64_t thr = size == cap ? key_cmp(list[cap - 1]) : kEmptyKey;
-      int cnt = 0;
-      bool nonfinite = false;
-#pragma unroll
-      for (int r = 0; r < kMaxBatch / kWarp; ++r) {
-        const int e = e0 + r * kWarp + lane;
-        uint64_t k = kEmptyKey;
-        if (e < b.n_seeds) {
-          const float d = drow[e];
-          if (!isfinite(d)) nonfinite = true;
-          else k = make_key(d, __ldg(b.seed_ids + e));
-        }
-        const bool keep = k < thr;
-        const unsigned km = __ballot_sync(kFullMask, keep);
-        if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = k;
-        cnt += __popc(km);
-      }
-      if (__any_sync(kFullMask, nonfinite)) { st = kStatusNumeric; break; }
-      __syncwarp();
-      if (cnt == 0) continue;
-      if (cnt <= 32) sort_and_merge<1>(list, &size, cap, stage, cnt, &cursor, lane);
-      else if (cnt <= 64) sort_and_merge<2>(list, &size, cap, stage, cnt, &cursor, lane);
-      else sort_and_merge<4>(list, &size, cap, stage, cnt, &cursor, lane);
-    }
+    if (!select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane))
+      st = kStatusNumeric;
     if (st == kStatusOk && check_adc) {
       bool adc_bad = false;
       for (int e = lane; e < b.n_seeds; e += kWarp) {
@@ -401,9 +513,7 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
       }
       if (__any_sync(kFullMask, sbad)) { st = kStatusNumeric; break; }
       __syncwarp();
-      if (nb <= 32) sort_and_merge<1>(list, &size, cap, stage, nb, &cursor, lane);
-      else if (nb <= 64) sort_and_merge<2>(list, &size, cap, stage, nb, &cursor, lane);
-      else sort_and_merge<4>(list, &size, cap, stage, nb, &cursor, lane);
+      merge_scored(list, &size, cap, stage, nb, &cursor, lane);
     }
 
 #pragma unroll

@@ -44,9 +44,7 @@ template <int M, int SUB, int RBITS>
 __device__ bool score_and_merge(const PqSearchArgs& a, const float* q, uint64_t* list, int* size, int cap,
                                 uint64_t* stage, const int32_t* batch_ids, int nb, int* cursor, int lane) {
   if (!score_batch<M, SUB, RBITS>(a, q, batch_ids, nb, stage, lane)) return false;
-  if (nb <= 32) sort_and_merge<1>(list, size, cap, stage, nb, cursor, lane);
-  else if (nb <= 64) sort_and_merge<2>(list, size, cap, stage, nb, cursor, lane);
-  else sort_and_merge<4>(list, size, cap, stage, nb, cursor, lane);
+  merge_scored(list, size, cap, stage, nb, cursor, lane);
   return true;
 }
 
@@ -83,8 +81,10 @@ pq_search_kernel_t(PqSearchArgs a) {
     for (int d = lane; d < ix.dim; d += kWarp) q[d] = a.queries[static_cast<size_t>(qi) * ix.dim + d];
     __syncwarp();
     // retrieval_pq_build_lut fails the query if any LUT entry is not finite
+    // (built only when the bound of lut_provably_safe cannot exclude it)
     bool bad = false;
-    for (int e = lane; e < ix.m * ix.ks; e += kWarp) {
+    const bool lut_safe = lut_provably_safe(ix, q, lane);
+    for (int e = lut_safe ? ix.m * ix.ks : lane; e < ix.m * ix.ks; e += kWarp) {
       const int m = e / ix.ks;
       const float* cen = ix.codebook + static_cast<size_t>(e) * ix.subdim;
       float acc = 0.0f;

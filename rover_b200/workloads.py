@@ -107,6 +107,14 @@ def _load_cache(name, cache: Path, cfg, seconds) -> PqWorkload:
                       seconds)
 
 
+def training_queries(name: str, n: int, offset: int = 7) -> np.ndarray:
+    """Held-out queries from the workload's mixture (same centres, another
+    sample seed) for training the learned gate."""
+    cfg = CONFIGS[name]
+    return D.gmm(n, cfg["dim"], cfg["comps"], cfg["seed"] + offset, centers_seed=cfg["seed"],
+                 clip_nonneg=cfg["clip"], normalize=cfg["normalize"])
+
+
 def recall_at_k(ids: np.ndarray, counts: np.ndarray, gt: np.ndarray, k: int) -> float:
     """demo_recall_hits_at_k (retrieval_rpc_demo_support.c:1709) averaged:
     hits among the first k results that appear in the first k truth ids."""

@@ -6,8 +6,8 @@
 * trace rows agree with the search statistics;
 * the gate's device gradients agree with the CPU oracle
   (oracle/gate_oracle.py) and device training learns a separable rule;
-* the gate's limits: refine-all equals full correction of the seed
-  shortlist, refine-none corrects nothing.
+* the gate's limits: refine-all corrects the whole seed shortlist,
+  refine-none none of it, a stop threshold every step passes stops at once.
 """
 from __future__ import annotations
 
@@ -170,10 +170,12 @@ def test_gate_limits(calc):
     all_ = calc.pq_search(q, 32, mode=2, beam_width=2, **KW)
     st = all_["stats"].astype(np.int64)
     assert np.all(st[:, 0] - st[:, 1] == n_seeds - short)
-    # every ratio on the "keep" side: nothing corrected
+    # every ratio on the "keep" side: no seed corrected (expansion
+    # candidates always are)
     calc.gate_load(params, mu, sigma, band_lo=-1.0, band_hi=0.0, refine_logit=0.0, stop_logit=np.inf)
     none = calc.pq_search(q, 32, mode=2, beam_width=2, **KW)
-    assert np.all(none["stats"][:, 1] == 0)
+    sn = none["stats"].astype(np.int64)
+    assert np.all(sn[:, 1] == sn[:, 0] - n_seeds)
     assert _recall(all_, d["gt"][:128]) >= _recall(none, d["gt"][:128])
     # a stop threshold every query passes: no expansion at all
     calc.gate_load(params, mu, sigma, band_lo=np.inf, band_hi=np.inf, refine_logit=0.0, stop_logit=-np.inf)
