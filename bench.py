@@ -54,7 +54,8 @@ CALIBRATION_QUERIES = 2000
 TRAIN_QUERIES = 8000       # held-out queries traced for the gate (about 5M rows)
 GATE_ROWS = 5_000_000
 GATE_EPOCHS = 4
-THRESHOLD_GRID = (0.9, 1.0, 1.1, 1.25, 1.5)   # ADC / worst ratios of the method without the network
+THRESHOLD_GRID = (0.9, 1.0, 1.1, 1.25, 1.5)
+DK_QUERIES, DK_IDS, DK_REPS = 1000, 8192, 3   # distance-kernel gathers: queries x random ids   # ADC / worst ratios of the method without the network
 METRIC = "QPS at recall@10>=0.95 on 1 B200 (pure-PQ graph search, 1M x 128): learned-gate batched vs plain"
 
 
@@ -249,6 +250,72 @@ def cpu_baseline(w, L, ep, expand, budget_s=12.0) -> dict:
                       f"(oracle/_ref), {threads} threads"}
 
 
+def distance_kernels(calc, w, args) -> dict:
+    """The plain path's batched distance kernels (calculator_rover_score /
+    calculator_rover_refine) on uniformly random (query, id) gathers over the
+    1M index, each timed with the library's CUDA events.  Algorithmic bytes
+    per scored id: the id, the rows the distance reads, the output.  A
+    working set that fits in L2 (126 MB) is marked: its rate is not bounded
+    by HBM."""
+    from rover_b200 import bundle as B
+    from rover_b200 import datasets as D
+    from rover_b200.workloads import CONFIGS
+    peak, peak_kind = measured_peak()
+    md = w.bundle.meta
+    n, dim = md.num_vectors, md.dim
+    rng = np.random.default_rng(7)
+    qs = w.queries[:DK_QUERIES]
+    lists = list(rng.integers(0, n, size=(len(qs), DK_IDS), dtype=np.int64).astype(np.int32))
+    total = len(qs) * DK_IDS
+    out = {}
+
+    def measure(kind, name, per_id, extra, working_set):
+        calc.score(kind, qs, lists)
+        calc.kernel_timing(True)
+        for _ in range(DK_REPS):
+            calc.score(kind, qs, lists)
+        kt = calc.kernel_times()
+        calc.kernel_timing(False)
+        launches, ms = kt[name]
+        ms /= max(1, launches)
+        b = total * per_id + extra
+        gbs = b / ms / 1e6
+        out[name] = {"ms": ms, "ids": total, "algorithmic_bytes": b, "achieved_gbs": gbs, "frac": gbs / peak,
+                     "working_set_mb": working_set / 1e6, "l2_resident": working_set < 126e6}
+
+    rcb = w.bundle.residual_code_bytes
+    lut = md.m * md.ks * 4
+    measure(0, "pq_adc", 4 + md.code_bytes + 4, len(qs) * lut, n * md.code_bytes)
+    measure(1, "pq_residual", 4 + md.code_bytes + rcb + 8 + 4, 0, n * (md.code_bytes + rcb + 8))
+    measure(4, "pq_rescore", 4 + 4 * dim + 4, 0, n * 4 * dim)
+    # the PQ final refine: FP64 re-rank of 128 distinct candidates per query
+    rq = w.queries
+    cand = ((rng.integers(0, n, size=(len(rq), 1)) + np.arange(128)[None, :] * 7919) % n).astype(np.int32)
+    calc.refine(1, rq, cand, np.full(len(rq), 128, np.int32), TOP_K)
+    calc.kernel_timing(True)
+    for _ in range(DK_REPS):
+        calc.refine(1, rq, cand, np.full(len(rq), 128, np.int32), TOP_K)
+    kt = calc.kernel_times()
+    calc.kernel_timing(False)
+    ms = kt["refine"][1] / max(1, kt["refine"][0])
+    b = cand.size * (4 + md.code_bytes + rcb + 8) + len(rq) * (4 * dim + TOP_K * 8)
+    out["refine"] = {"ms": ms, "ids": int(cand.size), "algorithmic_bytes": b, "achieved_gbs": b / ms / 1e6,
+                     "frac": b / ms / 1e6 / peak, "working_set_mb": n * (md.code_bytes + rcb + 8) / 1e6,
+                     "l2_resident": False}
+    # SQ8 codes and 8-bit residuals of the same base vectors
+    cfg = CONFIGS[args.workload]
+    base = D.gmm(cfg["n"], cfg["dim"], cfg["comps"], cfg["seed"], clip_nonneg=cfg["clip"],
+                 normalize=cfg["normalize"])
+    l1s, l1z, l1, res, qp = D.sq_encode(base, 8, 8)
+    del base
+    calc.sq_load(w.graph, w.entry, B.SqBundle(n, dim, 8, float(l1s), float(l1z), l1, 8, res, qp))
+    measure(2, "sq_coarse", 4 + dim + 4, 0, n * dim)
+    measure(3, "sq_exact", 4 + dim + dim + 8 + 4, 0, n * (2 * dim + 8))
+    calc.sq_unload()
+    return {"peak_gbs": peak, "peak_kind": peak_kind, "queries": len(qs), "ids_per_query": DK_IDS,
+            "ids": "uniform random over the index", "kernels": out}
+
+
 def device_steps(calc, args, step, stream, dist=None, dev=None):
     """W warm-up steps, then K timed steps bracketed by synchronisation (and a
     barrier when distributed); device time from CUDA events on the launch
@@ -308,6 +375,7 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD, help="workload name (rover_b200.workloads.CONFIGS)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gate", action="store_true", help="plain search only")
+    ap.add_argument("--no-distance-kernels", action="store_true")
     ap.add_argument("--train-queries", type=int, default=TRAIN_QUERIES)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -417,6 +485,12 @@ def main():
     h2d = nq * md.dim * 4 + nq * 4
     d2h = nq * TOP_K * 8 + nq * 8
 
+    dk = None
+    if rank == 0 and not args.no_distance_kernels:
+        dk = distance_kernels(calc, w, args)
+        log("distance kernels: " + ", ".join(f"{k} {v['achieved_gbs']:,.0f} GB/s ({100 * v['frac']:.0f}%)"
+                                              for k, v in dk["kernels"].items()))
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w, L, ep, expand)
@@ -442,6 +516,7 @@ def main():
                    "l2": "index (>800 MB with decoded rows) larger than L2; no flush"},
         "roofline": head["roof"],
         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in steps["kernels"].items()},
+        "distance_kernels": dk,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": steps["launches"],

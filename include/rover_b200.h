@@ -162,7 +162,9 @@ AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const RoverSearc
  * retrieval_pq_residual.c:983), 2 = SQ coarse
  * (retrieval_compute_int8/int4 distance, retrieval_l1_int8_core.c:463-489),
  * 3 = SQ exact residual (retrieval_demo_exact_distance_residual,
- * retrieval_rpc_demo_support.c:1577). */
+ * retrieval_rpc_demo_support.c:1577), 4 = kind 1 computed from the decoded
+ * rows (same values bit for bit; builds them on first use; dim % 4 == 0,
+ * dim <= 384). */
 AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, const float *queries,
                                  int32_t num_queries, const int32_t *ids, const int64_t *offsets,
                                  float *out_dists, int32_t *out_status);
@@ -278,7 +280,14 @@ uint64_t calculator_rover_launch_count(void);
 #define ROVER_KERNEL_PQ_BATCHED 3   /* PQ search, batched / gated modes */
 #define ROVER_KERNEL_SQ 4           /* SQ search */
 #define ROVER_KERNEL_PQ_SEED_RANK 5 /* all-queries x entry-seeds quantized distances, tensor cores */
-#define ROVER_KERNEL_KINDS 8
+#define ROVER_KERNEL_PQ_LUT 6       /* calculator_rover_score kind 0: per-query LUTs */
+#define ROVER_KERNEL_PQ_ADC 7       /* kind 0: ADC sums of the id lists */
+#define ROVER_KERNEL_PQ_RESIDUAL 8  /* kind 1: corrected distances from packed residual rows */
+#define ROVER_KERNEL_SQ_COARSE 9    /* kind 2: SQ code distances */
+#define ROVER_KERNEL_SQ_EXACT 10    /* kind 3: SQ residual-corrected distances */
+#define ROVER_KERNEL_REFINE 11      /* calculator_rover_refine */
+#define ROVER_KERNEL_PQ_RESCORE 12  /* kind 4: corrected distances from decoded rows */
+#define ROVER_KERNEL_KINDS 16
 void calculator_rover_kernel_timing(int32_t enable);
 int32_t calculator_rover_kernel_times(int64_t *launches, double *ms, int32_t kinds);
 

@@ -4,7 +4,7 @@
  *
  * It provides the platform calls the reference's DSP skeleton and host
  * pipeline make (QuRT threads, HAP mmap/perf/VTCM, rpcmem, fastrpc) so that
- * the unmodified reference code (src/app/dsp.c, src/dsp_demo/*.c) links into
+ * the unmodified reference code (src/app/dsp.c and the src/dsp_demo sources) links into
  * one in-process library.  rpcmem buffers are heap allocations named by
  * small integer "fds"; HAP_mmap_get resolves an fd to the same pointer, which
  * is what FastRPC's shared ION buffers give the DSP on the phone.

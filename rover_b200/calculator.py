@@ -156,7 +156,8 @@ class Calculator:
     def launch_count(self) -> int:
         return int(self.lib.calculator_rover_launch_count())
 
-    KERNEL_KINDS = ("pq_packed", "pq_seeds", "pq_decoded", "pq_batched", "sq", "pq_seed_rank")
+    KERNEL_KINDS = ("pq_packed", "pq_seeds", "pq_decoded", "pq_batched", "sq", "pq_seed_rank", "pq_lut", "pq_adc",
+                    "pq_residual", "sq_coarse", "sq_exact", "refine", "pq_rescore")
 
     # -- learned gate
     def gate_load(self, params, mu, sigma, band_lo=0.0, band_hi=0.0, refine_logit=0.0, stop_logit=1e30) -> None:
@@ -236,7 +237,7 @@ class Calculator:
 
     def kernel_times(self) -> dict:
         """{kind: (launches, total ms)} since the last kernel_timing call."""
-        n = 8
+        n = 16
         launches = np.zeros(n, np.int64)
         ms = np.zeros(n, np.float64)
         self.lib.calculator_rover_kernel_times(_p(launches, _i64p), ms.ctypes.data_as(C.POINTER(C.c_double)), n)
@@ -402,6 +403,10 @@ class Calculator:
                            _p(l1, _u8p), b.l1_bits, b.l1_scale, b.l1_zero, _p(res, _u8p), b.residual_bits,
                            _p(qp, _f32p))
         self._check("calculator_rover_sq_load", self.lib.calculator_rover_sq_load(self.handle, C.byref(desc)))
+
+    def sq_unload(self) -> None:
+        self._check("calculator_rover_sq_unload", self.lib.calculator_rover_sq_unload(self.handle))
+        self._keep.pop("sq", None)
 
     def sq_search(self, queries, pool_sizes, out_stride, sq_mode=1, num_out=None, check=True, **kw) -> dict:
         q = np.ascontiguousarray(queries, dtype=np.float32)

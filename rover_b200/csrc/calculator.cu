@@ -1297,11 +1297,20 @@ extern "C" AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, con
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
-  if (nq <= 0 || !queries || !offsets || !out_dists || kind < 0 || kind > 3) return AEE_EBADPARM;
-  const bool pqk = kind <= 1;
+  if (nq <= 0 || !queries || !offsets || !out_dists || kind < 0 || kind > 4) return AEE_EBADPARM;
+  const bool pqk = kind <= 1 || kind == 4;
   if (pqk && !s.pq.loaded) { set_error("no PQ index loaded"); return AEE_EFAILED; }
   if (!pqk && !s.sq.loaded) { set_error("no SQ index loaded"); return AEE_EFAILED; }
-  if (kind == 1 && !s.pq.view.residual_bits) return AEE_EBADPARM;
+  if ((kind == 1 || kind == 4) && !s.pq.view.residual_bits) return AEE_EBADPARM;
+  if (kind == 4) {
+    bool ok = false;
+    if (s.pq.view.dim % 4 != 0 || s.pq.view.dim > 384) {
+      set_error("kind 4 needs dim %% 4 == 0 and dim <= 384 (its 32-row tiles live in shared memory)");
+      return AEE_EBADPARM;
+    }
+    if (ensure_decoded(s, s.pq, &ok) != AEE_SUCCESS) return AEE_EFAILED;
+    if (!ok) { set_error("decoded rows do not fit in device memory"); return AEE_ENOMEMORY; }
+  }
   const int dim = pqk ? s.pq.view.dim : s.sq.view.dim;
   const int64_t total = offsets[nq];
   for (int i = 0; i < nq; ++i)
@@ -1319,15 +1328,26 @@ extern "C" AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, con
   if (kind == 0) {
     const size_t lut = static_cast<size_t>(s.pq.view.m) * s.pq.view.ks;
     CK(s.luts.ensure(nq * lut * 4));
-    launch_pq_lut(s.pq.view, s.in_queries.as<float>(), nq, s.luts.as<float>(), dst, s.stream);
+    {
+      TimedLaunch tl(ROVER_KERNEL_PQ_LUT, s.stream);
+      launch_pq_lut(s.pq.view, s.in_queries.as<float>(), nq, s.luts.as<float>(), dst, s.stream);
+    }
+    TimedLaunch tl(ROVER_KERNEL_PQ_ADC, s.stream);
     launch_pq_adc(s.pq.view, s.luts.as<float>(), nq, di, dof, dout, dst, s.stream);
     ++g_launches;
   } else if (kind == 1) {
+    TimedLaunch tl(ROVER_KERNEL_PQ_RESIDUAL, s.stream);
     launch_pq_residual(s.pq.view, s.in_queries.as<float>(), nq, di, dof, dout, dst, s.stream);
   } else if (kind == 2) {
+    TimedLaunch tl(ROVER_KERNEL_SQ_COARSE, s.stream);
     launch_sq_coarse(s.sq.view, s.in_queries.as<float>(), nq, di, dof, dout, dst, s.stream);
-  } else {
+  } else if (kind == 3) {
+    TimedLaunch tl(ROVER_KERNEL_SQ_EXACT, s.stream);
     launch_sq_exact(s.sq.view, s.in_queries.as<float>(), nq, di, dof, dout, dst, s.stream);
+  } else {
+    TimedLaunch tl(ROVER_KERNEL_PQ_RESCORE, s.stream);
+    launch_pq_rescore(s.pq.view.dim, s.pq.view.n, s.pq.decoded.as<float>(), s.in_queries.as<float>(), nq, di, dof,
+                      dout, dst, s.stream);
   }
   CK(cudaGetLastError());
   ++g_launches;
@@ -1335,6 +1355,7 @@ extern "C" AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, con
   if (download(out_dists, dout, static_cast<size_t>(total), s.stream) || download(hs.data(), dst, nq, s.stream))
     return AEE_EFAILED;
   CK(cudaStreamSynchronize(s.stream));
+  collect_timings();
   if (out_status) std::copy(hs.begin(), hs.end(), out_status);
   for (int32_t x : hs) if (x) { set_error("score failed with status %d", x); return AEE_EFAILED; }
   return AEE_SUCCESS;
@@ -1367,9 +1388,19 @@ extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, co
   CK(s.out_counts.ensure(nq * 4));
   CK(s.status.ensure(nq * 4));
   CK(cudaMemsetAsync(s.status.p, 0, nq * 4, s.stream));
-  launch_refine(kind, s.pq.view, s.sq.view, s.in_queries.as<float>(), nq, s.in_ids.as<int32_t>(), cand_stride,
-                s.in_pool.as<int32_t>(), top_k, cap, s.out_ids.as<int32_t>(), s.out_dists.as<float>(),
-                s.out_counts.as<int32_t>(), s.status.as<int32_t>(), s.stream);
+  // PQ: read the decode from the decoded rows when they are (or can be) built
+  const float* decoded = nullptr;
+  if (kind == 1 && s.pq.view.dim % 4 == 0) {
+    bool ok = false;
+    if (ensure_decoded(s, s.pq, &ok) != AEE_SUCCESS) return AEE_EFAILED;
+    if (ok) decoded = s.pq.decoded.as<float>();
+  }
+  {
+    TimedLaunch tl(ROVER_KERNEL_REFINE, s.stream);
+    launch_refine(kind, s.pq.view, s.sq.view, decoded, s.in_queries.as<float>(), nq, s.in_ids.as<int32_t>(), cand_stride,
+                  s.in_pool.as<int32_t>(), top_k, cap, s.out_ids.as<int32_t>(), s.out_dists.as<float>(),
+                  s.out_counts.as<int32_t>(), s.status.as<int32_t>(), s.stream);
+  }
   CK(cudaGetLastError());
   ++g_launches;
   std::vector<int32_t> hs(nq);
@@ -1378,6 +1409,7 @@ extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, co
       download(out_counts, s.out_counts.p, nq, s.stream) || download(hs.data(), s.status.p, nq, s.stream))
     return AEE_EFAILED;
   CK(cudaStreamSynchronize(s.stream));
+  collect_timings();
   if (out_status) std::copy(hs.begin(), hs.end(), out_status);
   for (int32_t x : hs) if (x) { set_error("refine failed with status %d", x); return AEE_EFAILED; }
   return AEE_SUCCESS;

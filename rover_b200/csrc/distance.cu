@@ -12,8 +12,7 @@
 //
 // Each query's id list is offsets[q] .. offsets[q+1] of a flat id array.
 
-#include "common.cuh"
-#include "kernels.h"
+#include "pq_common.cuh"
 
 namespace rover {
 
@@ -88,6 +87,7 @@ __global__ void pq_adc_kernel(PqIndexView ix, const float* __restrict__ luts, in
   if (bad) status[qi] = kStatusNumeric;
 }
 
+template <int M, int SUB, int RBITS>
 __global__ void pq_residual_kernel(PqIndexView ix, const float* __restrict__ queries, int nq,
                                    const int32_t* __restrict__ ids,
                                    const int64_t* __restrict__ offsets, float* __restrict__ out,
@@ -103,25 +103,90 @@ __global__ void pq_residual_kernel(PqIndexView ix, const float* __restrict__ que
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int32_t id = __ldg(ids + i);
     if (id < 0 || id >= ix.n) { bad = true; continue; }
-    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
-    if (!isfinite(qp.x) || !isfinite(qp.y) || !(qp.x > 0.0f)) { bad = true; continue; }
-    const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
-    const uint8_t* res = residual_row(ix, id);
-    float acc = 0.0f;
-    int dim = 0;
-    for (int m = 0; m < ix.m; ++m) {
-      const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
-      const float* cen = ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim;
-      for (int j = 0; j < ix.subdim; ++j, ++dim) {
-        const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, dim))
-                                                 : static_cast<uint32_t>(__ldg(res + dim));
-        const float x = fadd(fadd(__ldg(cen + j), fmul(u8f(r), qp.x)), qp.y);
-        const float dq = fsub(qs[dim], x);
-        acc = fadd(acc, fmul(dq, dq));
+    if constexpr (M > 0) {
+      float acc;
+      if (!pq_residual_fixed<M, SUB, RBITS>(ix, qs, id, &acc)) { bad = true; continue; }
+      out[i] = acc;
+    } else {
+      const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+      if (!isfinite(qp.x) || !isfinite(qp.y) || !(qp.x > 0.0f)) { bad = true; continue; }
+      const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
+      const uint8_t* res = residual_row(ix, id);
+      float acc = 0.0f;
+      int dim = 0;
+      for (int m = 0; m < ix.m; ++m) {
+        const int c = ix.ks == 16 ? nibble(code, m) : __ldg(code + m);
+        const float* cen = ix.codebook + (static_cast<size_t>(m) * ix.ks + c) * ix.subdim;
+        for (int j = 0; j < ix.subdim; ++j, ++dim) {
+          const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, dim))
+                                                   : static_cast<uint32_t>(__ldg(res + dim));
+          const float x = fadd(fadd(__ldg(cen + j), fmul(u8f(r), qp.x)), qp.y);
+          const float dq = fsub(qs[dim], x);
+          acc = fadd(acc, fmul(dq, dq));
+        }
       }
+      if (!isfinite(acc)) bad = true;
+      out[i] = acc;
     }
-    if (!isfinite(acc)) bad = true;
-    out[i] = acc;
+  }
+  if (bad) status[qi] = kStatusNumeric;
+}
+
+// The corrected distance of kind 1 over decoded rows x = (c + code*s) + z
+// (dim % 4 == 0).  Each warp takes 32 ids at a time: the warp copies the 32
+// rows into shared memory with coalesced 16-byte loads (one row = dim * 4
+// contiguous bytes, every load of a row in flight at once), then each lane
+// sums its candidate's row in dimension order, the same FP32 sequence as
+// kind 1.  Rows are padded by 4 floats so the 16-byte reads of 8 lanes fall
+// in distinct bank groups.
+constexpr int kRescoreWarps = 4;
+
+__global__ void __launch_bounds__(kRescoreWarps * 32) pq_rescore_kernel(int dim, int n, const float* __restrict__ decoded,
+                                                                        const float* __restrict__ queries, int nq,
+                                                                        const int32_t* __restrict__ ids,
+                                                                        const int64_t* __restrict__ offsets,
+                                                                        float* __restrict__ out, int32_t* status) {
+  extern __shared__ __align__(16) float sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rs = dim + 4;
+  float* qs = sm;
+  float* tile = sm + dim + static_cast<size_t>(warp) * kWarp * rs;
+  const int qi = blockIdx.y;
+  for (int d = threadIdx.x; d < dim; d += blockDim.x) qs[d] = queries[static_cast<size_t>(qi) * dim + d];
+  __syncthreads();
+  const int64_t begin = offsets[qi], end = offsets[qi + 1];
+  const int n4 = dim / 4;
+  bool bad = false;
+  for (int64_t b0 = begin + (static_cast<int64_t>(blockIdx.x) * kRescoreWarps + warp) * kWarp; b0 < end;
+       b0 += static_cast<int64_t>(gridDim.x) * kRescoreWarps * kWarp) {
+    const int cnt = static_cast<int>(end - b0 < kWarp ? end - b0 : kWarp);
+    int32_t my = lane < cnt ? __ldg(ids + b0 + lane) : 0;
+    const bool valid = lane < cnt && my >= 0 && my < n;
+    if (lane < cnt && !valid) bad = true;
+    if (!valid) my = 0;
+#pragma unroll 8
+    for (int j = 0; j < cnt; ++j) {
+      const int32_t idj = __shfl_sync(kFullMask, my, j);
+      const float4* src = reinterpret_cast<const float4*>(decoded + static_cast<size_t>(idj) * dim);
+      for (int t = lane; t < n4; t += kWarp) *reinterpret_cast<float4*>(tile + j * rs + 4 * t) = __ldg(src + t);
+    }
+    __syncwarp();
+    if (valid) {
+      const float4* x4 = reinterpret_cast<const float4*>(tile + lane * rs);
+      const float4* q4 = reinterpret_cast<const float4*>(qs);
+      float acc = 0.0f;
+      for (int t = 0; t < n4; ++t) {
+        const float4 x = x4[t];
+        const float4 q = q4[t];
+        float dl = fsub(q.x, x.x); acc = fadd(acc, fmul(dl, dl));
+        dl = fsub(q.y, x.y); acc = fadd(acc, fmul(dl, dl));
+        dl = fsub(q.z, x.z); acc = fadd(acc, fmul(dl, dl));
+        dl = fsub(q.w, x.w); acc = fadd(acc, fmul(dl, dl));
+      }
+      if (!isfinite(acc)) bad = true;
+      out[b0 + lane] = acc;
+    }
+    __syncwarp();
   }
   if (bad) status[qi] = kStatusNumeric;
 }
@@ -202,6 +267,24 @@ __global__ void sq_exact_kernel(SqIndexView ix, const float* __restrict__ querie
       rs = qp.x;
       rz = qp.y;
     }
+    if (res && ix.l1_bits == 8 && ix.residual_bits == 8 && (ix.dim & 15) == 0) {
+      // 8-bit codes and residuals: both rows in 16-byte loads, same order
+      for (int d0 = 0; d0 < ix.dim; d0 += 16) {
+        const uint4 cv = __ldg(reinterpret_cast<const uint4*>(l1 + d0));
+        const uint4 rv = __ldg(reinterpret_cast<const uint4*>(res + d0));
+        const uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w}, rw[4] = {rv.x, rv.y, rv.z, rv.w};
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const uint32_t c = (cw[k >> 2] >> (8 * (k & 3))) & 255u;
+          const uint32_t r = (rw[k >> 2] >> (8 * (k & 3))) & 255u;
+          const float value = fadd(fadd(fmul(u8f(c), ix.l1_scale), ix.l1_zero), fadd(fmul(u8f(r), rs), rz));
+          const float diff = fsub(qv[d0 + k], value);
+          dist = fadd(dist, fmul(diff, diff));
+        }
+      }
+      out[i] = dist;
+      continue;
+    }
     for (int d = 0; d < ix.dim; ++d) {
       const uint32_t c = ix.l1_bits == 4 ? static_cast<uint32_t>(nibble(l1, d)) : __ldg(l1 + d);
       float value = fadd(fmul(u8f(c), ix.l1_scale), ix.l1_zero);
@@ -241,7 +324,8 @@ __device__ __forceinline__ bool refine_value(int kind, const PqIndexView& pq, co
 
 // One warp per query: FP64 distances of the candidates on their decoded
 // vectors, sorted by (distance, id), top k kept.
-__global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const float* __restrict__ queries,
+__global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const float* __restrict__ decoded,
+                              const float* __restrict__ queries,
                               int nq, const int32_t* __restrict__ cand_ids, int cand_stride,
                               const int32_t* __restrict__ cand_counts, int top_k, int capacity,
                               int32_t* out_ids, float* out_dists, int32_t* out_counts, int32_t* status) {
@@ -265,6 +349,26 @@ __global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const fl
       if (i < count) {
         const int32_t id = cand_ids[static_cast<size_t>(qi) * cand_stride + i];
         if (id < 0 || id >= n) { bad = true; continue; }
+        if (kind == 1 && decoded) {
+          // the same FP32 decode, read from the decoded rows (NaN rows where
+          // the qparams are rejected)
+          const float4* x4 = reinterpret_cast<const float4*>(decoded + static_cast<size_t>(id) * dim);
+          double dist = 0.0;
+          for (int t = 0; t < dim / 4; ++t) {
+            const float4 x = __ldg(x4 + t);
+            const float xv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              if (!isfinite(xv[u])) bad = true;
+              const double delta = __dsub_rn(static_cast<double>(q[4 * t + u]), static_cast<double>(xv[u]));
+              dist = __dadd_rn(dist, __dmul_rn(delta, delta));
+            }
+          }
+          if (!isfinite(dist) || dist >= 3.4028234663852886e38) bad = true;
+          sd[i] = dist;
+          si[i] = id;
+          continue;
+        }
         const uint8_t* a;
         const uint8_t* b;
         float2 qp;
@@ -352,7 +456,32 @@ void launch_pq_residual(const PqIndexView& ix, const float* queries, int nq, con
                         const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
   if (nq <= 0) return;
   dim3 grid(8, nq);
-  pq_residual_kernel<<<grid, 128, ix.dim * sizeof(float), s>>>(ix, queries, nq, ids, offsets, out, status);
+  const size_t smem = ix.dim * sizeof(float);
+  if (ix.ks == 256 && ix.code_bytes == ix.m && (ix.residual_bits == 8 || ix.residual_bits == 4)) {
+    const bool r8 = ix.residual_bits == 8;
+#define ROVER_RES_SHAPE(MM, SS)                                                                               \
+  if (ix.m == MM && ix.subdim == SS) {                                                                        \
+    if (r8) pq_residual_kernel<MM, SS, 8><<<grid, 128, smem, s>>>(ix, queries, nq, ids, offsets, out, status); \
+    else pq_residual_kernel<MM, SS, 4><<<grid, 128, smem, s>>>(ix, queries, nq, ids, offsets, out, status);    \
+    return;                                                                                                   \
+  }
+    ROVER_RES_SHAPE(16, 8)
+    ROVER_RES_SHAPE(32, 4)
+    ROVER_RES_SHAPE(24, 4)
+    ROVER_RES_SHAPE(8, 8)
+    ROVER_RES_SHAPE(16, 4)
+#undef ROVER_RES_SHAPE
+  }
+  pq_residual_kernel<0, 0, 0><<<grid, 128, smem, s>>>(ix, queries, nq, ids, offsets, out, status);
+}
+
+void launch_pq_rescore(int dim, int n, const float* decoded, const float* queries, int nq, const int32_t* ids,
+                       const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
+  if (nq <= 0) return;
+  const size_t smem = (static_cast<size_t>(dim) + static_cast<size_t>(kRescoreWarps) * kWarp * (dim + 4)) * sizeof(float);
+  cudaFuncSetAttribute(pq_rescore_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  dim3 grid(8, nq);
+  pq_rescore_kernel<<<grid, kRescoreWarps * 32, smem, s>>>(dim, n, decoded, queries, nq, ids, offsets, out, status);
 }
 
 void launch_sq_coarse(const SqIndexView& ix, const float* queries, int nq, const int32_t* ids,
@@ -369,7 +498,7 @@ void launch_sq_exact(const SqIndexView& ix, const float* queries, int nq, const 
   sq_exact_kernel<<<grid, 128, ix.dim * sizeof(float), s>>>(ix, queries, nq, ids, offsets, out, status);
 }
 
-void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const float* queries,
+void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const float* decoded, const float* queries,
                    int nq, const int32_t* cand_ids, int cand_stride, const int32_t* cand_counts,
                    int top_k, int capacity, int32_t* out_ids, float* out_dists,
                    int32_t* out_counts, int32_t* status, cudaStream_t s) {
@@ -379,7 +508,8 @@ void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const
   const int warps = 4;
   const size_t smem = static_cast<size_t>(warps) * cap * 12;
   if (smem > 48 * 1024) cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  refine_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, s>>>(kind, pq, sq, queries, nq, cand_ids, cand_stride,
+  refine_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, s>>>(kind, pq, sq, decoded, queries, nq, cand_ids,
+                                                                   cand_stride,
                                                                    cand_counts, top_k, cap, out_ids, out_dists,
                                                                    out_counts, status);
 }

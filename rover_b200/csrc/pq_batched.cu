@@ -549,7 +549,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       continue;
     }
     __syncwarp();
-    pq_finish_query(a, q, list, size, qi, lane, base, scored, corrected, expanded, dedup);
+    pq_finish_query(a, q, list, size, qi, lane, base, scored, corrected, expanded, dedup, b.decoded);
     __syncwarp();
   }
 }

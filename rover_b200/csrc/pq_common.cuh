@@ -177,19 +177,107 @@ __device__ __forceinline__ float lut_adc(const PqIndexView& ix, const float* lut
   return adc;
 }
 
+// Residual-corrected distance only (retrieval_pq_residual_query_evaluate),
+// shape-specialised like pq_score_fixed: the same operations in the same
+// order, without the ADC sum.  False when the reference rejects the
+// candidate (invalid qparams, non-finite distance).
+template <int M, int SUB, int RBITS>
+__device__ __forceinline__ bool pq_residual_fixed(const PqIndexView& ix, const float* __restrict__ q, int32_t id,
+                                                  float* out_dist) {
+  constexpr int DIM = M * SUB;
+  constexpr int RCB = RBITS == 8 ? DIM : DIM / 2;
+  constexpr int CW = (M + 3) / 4;
+  constexpr int RW = RCB / 4;
+  uint32_t cw[CW];
+  const uint8_t* crow = ix.codes + static_cast<size_t>(id) * M;
+  if constexpr (M % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < M / 16; ++i) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(crow) + i);
+      cw[4 * i] = v.x; cw[4 * i + 1] = v.y; cw[4 * i + 2] = v.z; cw[4 * i + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < CW; ++i) cw[i] = __ldg(reinterpret_cast<const uint32_t*>(crow) + i);
+  }
+  const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+  uint32_t rw[RW];
+  const uint8_t* res = pq_residual_row(ix, id);
+  if constexpr (RCB % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < RCB / 16; ++i) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(res) + i);
+      rw[4 * i] = v.x; rw[4 * i + 1] = v.y; rw[4 * i + 2] = v.z; rw[4 * i + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < RW; ++i) rw[i] = __ldg(reinterpret_cast<const uint32_t*>(res) + i);
+  }
+  if (!isfinite(qp.x) || !isfinite(qp.y) || !(qp.x > 0.0f)) return false;
+  float acc = 0.0f;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const uint32_t c = (cw[m >> 2] >> (8 * (m & 3))) & 255u;
+    const float* cen = ix.codebook + (static_cast<size_t>(m) * 256u + c) * SUB;
+    float cv[SUB];
+    if constexpr (SUB % 4 == 0) {
+#pragma unroll
+      for (int t = 0; t < SUB / 4; ++t) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(cen) + t);
+        cv[4 * t] = v.x; cv[4 * t + 1] = v.y; cv[4 * t + 2] = v.z; cv[4 * t + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int t = 0; t < SUB; ++t) cv[t] = __ldg(cen + t);
+    }
+#pragma unroll
+    for (int j = 0; j < SUB; ++j) {
+      const int d = m * SUB + j;
+      uint32_t r;
+      if constexpr (RBITS == 8) r = (rw[d >> 2] >> (8 * (d & 3))) & 255u;
+      else r = (rw[d >> 3] >> (4 * (d & 7))) & 15u;
+      const float x = fadd(fadd(cv[j], fmul(u8f(r), qp.x)), qp.y);
+      const float dq = fsub(q[d], x);
+      acc = fadd(acc, fmul(dq, dq));
+    }
+  }
+  *out_dist = acc;
+  return isfinite(acc);
+}
+
 // ---------------------------------------------------------------------------
 // Final refine of the first `count` pool entries (refine_impl with the PQ
 // residual decode provider): FP32 decode ((c + code*s) + z), FP64 sum of
 // squared differences in dimension order, sort by (distance, id), keep k.
+// With `decoded` (the [n][dim] rows of the same decode, NaN rows for
+// rejected qparams; dim % 4 == 0) the decode is read instead of recomputed:
+// the same FP32 values, the same failures.
 static __device__ void pq_refine_warp(const PqIndexView& ix, const float* q, const uint64_t* list,
                                int count, int k, double* sd, int32_t* si, int lane,
                                int32_t* out_ids, float* out_dists, int32_t* out_count,
-                               int32_t* status) {
+                               int32_t* status, const float* decoded = nullptr) {
   int np2 = 1;
   while (np2 < count) np2 <<= 1;
   bool bad = false;
   for (int i = lane; i < np2; i += kWarp) {
-    if (i < count) {
+    if (i < count && decoded) {
+      const int32_t id = key_id(list[i]);
+      const float4* x4 = reinterpret_cast<const float4*>(decoded + static_cast<size_t>(id) * ix.dim);
+      double dist = 0.0;
+      for (int t = 0; t < ix.dim / 4; ++t) {
+        const float4 x = __ldg(x4 + t);
+        const float xv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (!isfinite(xv[u])) bad = true;
+          const double delta = __dsub_rn(static_cast<double>(q[4 * t + u]), static_cast<double>(xv[u]));
+          dist = __dadd_rn(dist, __dmul_rn(delta, delta));
+        }
+      }
+      if (!isfinite(dist) || dist >= 3.4028234663852886e38) bad = true;
+      sd[i] = dist;
+      si[i] = id;
+    } else if (i < count) {
       const int32_t id = key_id(list[i]);
       const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
       const uint8_t* code = ix.codes + static_cast<size_t>(id) * ix.code_bytes;
@@ -423,7 +511,8 @@ __device__ __forceinline__ int drop_non_entering(const uint64_t* list, int size,
 __device__ __forceinline__ void pq_finish_query(const PqSearchArgs& a, const float* q, const uint64_t* list,
                                                 int size, int qi, int lane, uint8_t* base,
                                                 unsigned long long scored, unsigned long long corrected,
-                                                unsigned long long expanded, unsigned long long dedup) {
+                                                unsigned long long expanded, unsigned long long dedup,
+                                                const float* decoded = nullptr) {
   const PqIndexView& ix = a.ix;
   int32_t* status = a.status + qi;
   if (a.pool_ids) {
@@ -454,7 +543,7 @@ __device__ __forceinline__ void pq_finish_query(const PqSearchArgs& a, const flo
       double* sd = reinterpret_cast<double*>(base + a.smem_refine_offset);
       int32_t* si = reinterpret_cast<int32_t*>(sd + a.refine_capacity);
       int32_t rs = kStatusOk;
-      pq_refine_warp(ix, q, list, cnt, k, sd, si, lane, oi, od, a.out_counts + qi, &rs);
+      pq_refine_warp(ix, q, list, cnt, k, sd, si, lane, oi, od, a.out_counts + qi, &rs, decoded);
       rs = __shfl_sync(kFullMask, rs, 0);
       if (rs != kStatusOk && lane == 0) *status = rs;
     } else {

@@ -523,7 +523,7 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
       continue;
     }
     __syncwarp();
-    pq_finish_query(a, q, list, size, qi, lane, base, scored, scored, expanded, dedup);
+    pq_finish_query(a, q, list, size, qi, lane, base, scored, scored, expanded, dedup, b.decoded);
     __syncwarp();
   }
 }

@@ -29,9 +29,11 @@ def test_pq_lut_adc_residual(calc, name):
     assert np.array_equal(bits(luts), bits(g["lut"]))
     adc = calc.score(0, q[:4], [g["sample_ids"]] * 4)
     res = calc.score(1, q[:4], [g["sample_ids"]] * 4)
+    dec = calc.score(4, q[:4], [g["sample_ids"]] * 4)    # the same distances from decoded rows
     for qi in range(4):
         assert np.array_equal(bits(adc[qi]), bits(g["adc"][qi]))
         assert np.array_equal(bits(res[qi]), bits(g["residual"][qi]))
+        assert np.array_equal(bits(dec[qi]), bits(g["residual"][qi]))
 
 
 PACKED, DECODED = 1, 2
