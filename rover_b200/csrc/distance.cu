@@ -23,6 +23,41 @@ __device__ __forceinline__ const uint8_t* residual_row(const PqIndexView& ix, in
          (u - block * static_cast<uint32_t>(ix.vpb)) * static_cast<uint32_t>(ix.rcb);
 }
 
+// ---------------------------------------------------------------------------
+// Staged gathers: a warp takes 32 candidate ids at a time and streams their
+// rows into its shared-memory tile with cp.async (no register staging, all
+// of the tile's copies in flight at once), then each lane scores its
+// candidate from shared memory.  Row strides are odd multiples of 16 bytes
+// so that the 16-byte reads of 8 lanes fall in distinct bank groups.
+constexpr int kStageWarps = 4;
+
+__device__ __forceinline__ constexpr int stage_stride(int row_bytes) {
+  return ((((row_bytes + 15) / 16) | 1) * 16);
+}
+
+template <int CHUNK>
+__device__ __forceinline__ void cp_async_chunk(void* dst, const void* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  if constexpr (CHUNK == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else if constexpr (CHUNK == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void stage_wait() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Copies rows r = 0..cnt-1 of row_bytes (a multiple of CHUNK, sources
+// CHUNK-aligned) from src(r) to dst + r * stride.
+template <int CHUNK, class Src>
+__device__ __forceinline__ void stage_rows(uint8_t* dst, int stride, int row_bytes, int cnt, const Src& src, int lane) {
+  const int per = row_bytes / CHUNK;
+  for (int c = lane; c < cnt * per; c += kWarp) {
+    const int r = c / per, k = c - r * per;
+    cp_async_chunk<CHUNK>(dst + r * stride + k * CHUNK, src(r) + k * CHUNK);
+  }
+}
+
 __global__ void pq_lut_kernel(PqIndexView ix, const float* __restrict__ queries, int nq,
                               float* __restrict__ luts, int32_t* status) {
   const int qi = blockIdx.x;
@@ -133,13 +168,22 @@ __global__ void pq_residual_kernel(PqIndexView ix, const float* __restrict__ que
 }
 
 // The corrected distance of kind 1 over decoded rows x = (c + code*s) + z
-// (dim % 4 == 0).  Each warp takes 32 ids at a time: the warp copies the 32
-// rows into shared memory with coalesced 16-byte loads (one row = dim * 4
-// contiguous bytes, every load of a row in flight at once), then each lane
-// sums its candidate's row in dimension order, the same FP32 sequence as
-// kind 1.  Rows are padded by 4 floats so the 16-byte reads of 8 lanes fall
-// in distinct bank groups.
+// (dim % 4 == 0).  Each warp takes 32 ids at a time and streams their rows
+// into shared memory with cp.async (16 bytes per lane and instruction,
+// every row of the tile in flight at once, no register staging), then each
+// lane sums its candidate's row in dimension order, the same FP32 sequence
+// as kind 1.  Rows are padded by 4 floats so the 16-byte reads of 8 lanes
+// fall in distinct bank groups.
 constexpr int kRescoreWarps = 4;
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
 
 __global__ void __launch_bounds__(kRescoreWarps * 32) pq_rescore_kernel(int dim, int n, const float* __restrict__ decoded,
                                                                         const float* __restrict__ queries, int nq,
@@ -164,12 +208,12 @@ __global__ void __launch_bounds__(kRescoreWarps * 32) pq_rescore_kernel(int dim,
     const bool valid = lane < cnt && my >= 0 && my < n;
     if (lane < cnt && !valid) bad = true;
     if (!valid) my = 0;
-#pragma unroll 8
     for (int j = 0; j < cnt; ++j) {
       const int32_t idj = __shfl_sync(kFullMask, my, j);
-      const float4* src = reinterpret_cast<const float4*>(decoded + static_cast<size_t>(idj) * dim);
-      for (int t = lane; t < n4; t += kWarp) *reinterpret_cast<float4*>(tile + j * rs + 4 * t) = __ldg(src + t);
+      const float* src = decoded + static_cast<size_t>(idj) * dim;
+      for (int t = lane; t < n4; t += kWarp) cp_async16(tile + j * rs + 4 * t, src + 4 * t);
     }
+    cp_async_wait_all();
     __syncwarp();
     if (valid) {
       const float4* x4 = reinterpret_cast<const float4*>(tile + lane * rs);
@@ -344,31 +388,53 @@ __global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const fl
   while (np2 < count) np2 <<= 1;
   bool bad = count < 0 || count > capacity;
   for (int d = lane; d < dim; d += kWarp) bad |= !isfinite(q[d]);
-  if (!__any_sync(kFullMask, bad)) {
+  if (!__any_sync(kFullMask, bad) && kind == 1 && decoded) {
+    // the decode read from the decoded rows (NaN rows where the qparams are
+    // rejected), 32 candidates at a time staged in shared memory
+    const int rs = dim + 4;
+    float* tile = reinterpret_cast<float*>(si + static_cast<size_t>((blockDim.x >> 5) - warp) * capacity) +
+                  static_cast<size_t>(warp) * kWarp * rs;
+    for (int i0 = 0; i0 < np2; i0 += kWarp) {
+      const int i = i0 + lane;
+      const int cnt = max(0, min(kWarp, count - i0));
+      int32_t id = i < count ? cand_ids[static_cast<size_t>(qi) * cand_stride + i] : 0;
+      const bool valid = i < count && id >= 0 && id < n;
+      if (i < count && !valid) bad = true;
+      if (!valid) id = 0;
+      for (int j = 0; j < cnt; ++j) {
+        const int32_t idj = __shfl_sync(kFullMask, id, j);
+        const float* src = decoded + static_cast<size_t>(idj) * dim;
+        for (int t = lane; t < dim / 4; t += kWarp) cp_async_chunk<16>(tile + j * rs + 4 * t, src + 4 * t);
+      }
+      stage_wait();
+      __syncwarp();
+      if (i < count) {
+        double dist = 0.0;
+        const float4* x4 = reinterpret_cast<const float4*>(tile + lane * rs);
+        for (int t = 0; t < dim / 4; ++t) {
+          const float4 x = x4[t];
+          const float xv[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (!isfinite(xv[u])) bad = true;
+            const double delta = __dsub_rn(static_cast<double>(q[4 * t + u]), static_cast<double>(xv[u]));
+            dist = __dadd_rn(dist, __dmul_rn(delta, delta));
+          }
+        }
+        if (!isfinite(dist) || dist >= 3.4028234663852886e38) bad = true;
+        sd[i] = dist;
+        si[i] = id;
+      } else if (i < np2) {
+        sd[i] = __longlong_as_double(0x7ff0000000000000ll);
+        si[i] = 0x7fffffff;
+      }
+      __syncwarp();
+    }
+  } else if (!__any_sync(kFullMask, bad)) {
     for (int i = lane; i < np2; i += kWarp) {
       if (i < count) {
         const int32_t id = cand_ids[static_cast<size_t>(qi) * cand_stride + i];
         if (id < 0 || id >= n) { bad = true; continue; }
-        if (kind == 1 && decoded) {
-          // the same FP32 decode, read from the decoded rows (NaN rows where
-          // the qparams are rejected)
-          const float4* x4 = reinterpret_cast<const float4*>(decoded + static_cast<size_t>(id) * dim);
-          double dist = 0.0;
-          for (int t = 0; t < dim / 4; ++t) {
-            const float4 x = __ldg(x4 + t);
-            const float xv[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              if (!isfinite(xv[u])) bad = true;
-              const double delta = __dsub_rn(static_cast<double>(q[4 * t + u]), static_cast<double>(xv[u]));
-              dist = __dadd_rn(dist, __dmul_rn(delta, delta));
-            }
-          }
-          if (!isfinite(dist) || dist >= 3.4028234663852886e38) bad = true;
-          sd[i] = dist;
-          si[i] = id;
-          continue;
-        }
         const uint8_t* a;
         const uint8_t* b;
         float2 qp;
@@ -435,6 +501,97 @@ __global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const fl
   if (lane == 0) out_counts[qi] = outn;
 }
 
+// sq_coarse_kernel / sq_exact_kernel over staged rows (8-bit codes, and for
+// the exact distance 8-bit residuals; dim % 16 == 0).
+template <bool EXACT>
+__global__ void __launch_bounds__(kStageWarps * 32) sq_staged_kernel(SqIndexView ix, const float* __restrict__ queries,
+                                                                     int nq, const int32_t* __restrict__ ids,
+                                                                     const int64_t* __restrict__ offsets,
+                                                                     float* __restrict__ out, int32_t* status) {
+  extern __shared__ __align__(16) uint8_t smb[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int dim = ix.dim;
+  const int RS = stage_stride(dim);
+  const int warp_bytes = 128 + 32 * RS + (EXACT ? 32 * RS + 32 * 8 : 0);
+  float* qv = reinterpret_cast<float*>(smb);                       // exact: the query
+  uint8_t* qc = smb + dim * 4;                                     // coarse: its codes
+  uint8_t* wb = smb + dim * 5 + 16 - ((dim * 5) & 15) + warp * warp_bytes;
+  int32_t* sid = reinterpret_cast<int32_t*>(wb);
+  uint8_t* sl1 = wb + 128;
+  uint8_t* sres = sl1 + 32 * RS;
+  float2* sqp = reinterpret_cast<float2*>(sres + 32 * RS);
+  const int qi = blockIdx.y;
+  if (EXACT) {
+    for (int d = threadIdx.x; d < dim; d += blockDim.x) qv[d] = queries[static_cast<size_t>(qi) * dim + d];
+  } else {
+    quantize_query(ix, queries + static_cast<size_t>(qi) * dim, qc);
+  }
+  __syncthreads();
+  const int64_t begin = offsets[qi], end = offsets[qi + 1];
+  const float scale_sq = fmul(ix.l1_scale, ix.l1_scale);
+  bool bad = false;
+  for (int64_t b0 = begin + (static_cast<int64_t>(blockIdx.x) * kStageWarps + warp) * kWarp; b0 < end;
+       b0 += static_cast<int64_t>(gridDim.x) * kStageWarps * kWarp) {
+    const int cnt = static_cast<int>(end - b0 < kWarp ? end - b0 : kWarp);
+    const int32_t my = lane < cnt ? __ldg(ids + b0 + lane) : 0;
+    const bool valid = lane < cnt && my >= 0 && my < ix.n;
+    if (lane < cnt && !valid) bad = true;
+    sid[lane] = valid ? my : 0;
+    __syncwarp();
+    stage_rows<16>(sl1, RS, dim, cnt, [&](int r) { return ix.l1 + static_cast<size_t>(sid[r]) * dim; }, lane);
+    if (EXACT) {
+      stage_rows<16>(sres, RS, dim, cnt, [&](int r) { return ix.residual + static_cast<size_t>(sid[r]) * dim; }, lane);
+      stage_rows<8>(reinterpret_cast<uint8_t*>(sqp), 8, 8, cnt,
+                    [&](int r) { return reinterpret_cast<const uint8_t*>(ix.qparams + 2 * static_cast<size_t>(sid[r])); },
+                    lane);
+    }
+    stage_wait();
+    __syncwarp();
+    if (valid) {
+      const uint4* x = reinterpret_cast<const uint4*>(sl1 + lane * RS);
+      if (!EXACT) {
+        long long acc = 0;
+        int iacc = 0;
+        for (int t = 0; t < dim / 16; ++t) {
+          const uint4 v = x[t];
+          const uint4 w = *reinterpret_cast<const uint4*>(qc + 16 * t);
+          iacc += __dp4a(w.x, w.x, 0u) - 2 * static_cast<int>(__dp4a(w.x, v.x, 0u)) + __dp4a(v.x, v.x, 0u);
+          iacc += __dp4a(w.y, w.y, 0u) - 2 * static_cast<int>(__dp4a(w.y, v.y, 0u)) + __dp4a(v.y, v.y, 0u);
+          iacc += __dp4a(w.z, w.z, 0u) - 2 * static_cast<int>(__dp4a(w.z, v.z, 0u)) + __dp4a(v.z, v.z, 0u);
+          iacc += __dp4a(w.w, w.w, 0u) - 2 * static_cast<int>(__dp4a(w.w, v.w, 0u)) + __dp4a(v.w, v.w, 0u);
+          if ((t & 63) == 63) { acc += iacc; iacc = 0; }
+        }
+        acc += iacc;
+        out[b0 + lane] = fmul(__ll2float_rn(acc), scale_sq);
+      } else {
+        const uint4* rr = reinterpret_cast<const uint4*>(sres + lane * RS);
+        const float2 qp = sqp[lane];
+        float dist = 0.0f;
+        for (int t = 0; t < dim / 16; ++t) {
+          const uint4 cv = x[t], rv = rr[t];
+          const uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w}, rw[4] = {rv.x, rv.y, rv.z, rv.w};
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const uint32_t c = (cw[k >> 2] >> (8 * (k & 3))) & 255u;
+            const uint32_t r = (rw[k >> 2] >> (8 * (k & 3))) & 255u;
+            const float value = fadd(fadd(fmul(u8f(c), ix.l1_scale), ix.l1_zero), fadd(fmul(u8f(r), qp.x), qp.y));
+            const float diff = fsub(qv[16 * t + k], value);
+            dist = fadd(dist, fmul(diff, diff));
+          }
+        }
+        out[b0 + lane] = dist;
+      }
+    }
+    __syncwarp();
+  }
+  if (bad) status[qi] = kStatusBadParam;
+}
+
+size_t sq_staged_smem(int dim, bool exact) {
+  const int rs = ((((dim + 15) / 16) | 1) * 16);
+  return static_cast<size_t>(dim) * 5 + 16 + static_cast<size_t>(kStageWarps) * (128 + 32 * rs + (exact ? 32 * rs + 256 : 0));
+}
+
 // ---------------------------------------------------------------------------
 
 void launch_pq_lut(const PqIndexView& ix, const float* queries, int nq, float* luts,
@@ -488,6 +645,13 @@ void launch_sq_coarse(const SqIndexView& ix, const float* queries, int nq, const
                       const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
   if (nq <= 0) return;
   dim3 grid(8, nq);
+  if (ix.l1_bits == 8 && (ix.dim & 15) == 0 && sq_staged_smem(ix.dim, false) <= 227 * 1024) {
+    const size_t smem = sq_staged_smem(ix.dim, false);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(sq_staged_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    sq_staged_kernel<false><<<grid, kStageWarps * 32, smem, s>>>(ix, queries, nq, ids, offsets, out, status);
+    return;
+  }
   sq_coarse_kernel<<<grid, 128, (ix.dim + 15) & ~15, s>>>(ix, queries, nq, ids, offsets, out, status);
 }
 
@@ -495,6 +659,14 @@ void launch_sq_exact(const SqIndexView& ix, const float* queries, int nq, const 
                      const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
   if (nq <= 0) return;
   dim3 grid(8, nq);
+  if (ix.l1_bits == 8 && ix.residual && ix.residual_bits == 8 && ix.rcb == ix.dim && (ix.dim & 15) == 0 &&
+      sq_staged_smem(ix.dim, true) <= 227 * 1024) {
+    const size_t smem = sq_staged_smem(ix.dim, true);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(sq_staged_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    sq_staged_kernel<true><<<grid, kStageWarps * 32, smem, s>>>(ix, queries, nq, ids, offsets, out, status);
+    return;
+  }
   sq_exact_kernel<<<grid, 128, ix.dim * sizeof(float), s>>>(ix, queries, nq, ids, offsets, out, status);
 }
 
@@ -506,7 +678,13 @@ void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const
   int cap = 1;
   while (cap < capacity) cap <<= 1;
   const int warps = 4;
-  const size_t smem = static_cast<size_t>(warps) * cap * 12;
+  const int dim = kind == 1 ? pq.dim : sq.dim;
+  size_t smem = static_cast<size_t>(warps) * cap * 12;
+  if (kind == 1 && decoded) smem += static_cast<size_t>(warps) * kWarp * (dim + 4) * sizeof(float);
+  if (smem > 227 * 1024 && kind == 1 && decoded) {   // tile too large: decode per element instead
+    decoded = nullptr;
+    smem = static_cast<size_t>(warps) * cap * 12;
+  }
   if (smem > 48 * 1024) cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   refine_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, s>>>(kind, pq, sq, decoded, queries, nq, cand_ids,
                                                                    cand_stride,

@@ -177,42 +177,14 @@ __device__ __forceinline__ float lut_adc(const PqIndexView& ix, const float* lut
   return adc;
 }
 
-// Residual-corrected distance only (retrieval_pq_residual_query_evaluate),
-// shape-specialised like pq_score_fixed: the same operations in the same
-// order, without the ADC sum.  False when the reference rejects the
-// candidate (invalid qparams, non-finite distance).
+// Residual-corrected distance (retrieval_pq_residual_query_evaluate) of
+// one candidate whose code row and residual row are given as 32-bit words
+// (wherever they were loaded from): the operations and order of pq_score.
+// False when the reference rejects the candidate.
 template <int M, int SUB, int RBITS>
-__device__ __forceinline__ bool pq_residual_fixed(const PqIndexView& ix, const float* __restrict__ q, int32_t id,
+__device__ __forceinline__ bool pq_residual_words(const PqIndexView& ix, const float* __restrict__ q,
+                                                  const uint32_t* cw, const uint32_t* rw, float2 qp,
                                                   float* out_dist) {
-  constexpr int DIM = M * SUB;
-  constexpr int RCB = RBITS == 8 ? DIM : DIM / 2;
-  constexpr int CW = (M + 3) / 4;
-  constexpr int RW = RCB / 4;
-  uint32_t cw[CW];
-  const uint8_t* crow = ix.codes + static_cast<size_t>(id) * M;
-  if constexpr (M % 16 == 0) {
-#pragma unroll
-    for (int i = 0; i < M / 16; ++i) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(crow) + i);
-      cw[4 * i] = v.x; cw[4 * i + 1] = v.y; cw[4 * i + 2] = v.z; cw[4 * i + 3] = v.w;
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < CW; ++i) cw[i] = __ldg(reinterpret_cast<const uint32_t*>(crow) + i);
-  }
-  const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
-  uint32_t rw[RW];
-  const uint8_t* res = pq_residual_row(ix, id);
-  if constexpr (RCB % 16 == 0) {
-#pragma unroll
-    for (int i = 0; i < RCB / 16; ++i) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(res) + i);
-      rw[4 * i] = v.x; rw[4 * i + 1] = v.y; rw[4 * i + 2] = v.z; rw[4 * i + 3] = v.w;
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < RW; ++i) rw[i] = __ldg(reinterpret_cast<const uint32_t*>(res) + i);
-  }
   if (!isfinite(qp.x) || !isfinite(qp.y) || !(qp.x > 0.0f)) return false;
   float acc = 0.0f;
 #pragma unroll
@@ -243,6 +215,42 @@ __device__ __forceinline__ bool pq_residual_fixed(const PqIndexView& ix, const f
   }
   *out_dist = acc;
   return isfinite(acc);
+}
+
+// The same, loading the candidate's rows from global memory.
+template <int M, int SUB, int RBITS>
+__device__ __forceinline__ bool pq_residual_fixed(const PqIndexView& ix, const float* __restrict__ q, int32_t id,
+                                                  float* out_dist) {
+  constexpr int DIM = M * SUB;
+  constexpr int RCB = RBITS == 8 ? DIM : DIM / 2;
+  constexpr int CW = (M + 3) / 4;
+  constexpr int RW = RCB / 4;
+  uint32_t cw[CW];
+  const uint8_t* crow = ix.codes + static_cast<size_t>(id) * M;
+  if constexpr (M % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < M / 16; ++i) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(crow) + i);
+      cw[4 * i] = v.x; cw[4 * i + 1] = v.y; cw[4 * i + 2] = v.z; cw[4 * i + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < CW; ++i) cw[i] = __ldg(reinterpret_cast<const uint32_t*>(crow) + i);
+  }
+  uint32_t rw[RW];
+  const uint8_t* res = pq_residual_row(ix, id);
+  if constexpr (RCB % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < RCB / 16; ++i) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(res) + i);
+      rw[4 * i] = v.x; rw[4 * i + 1] = v.y; rw[4 * i + 2] = v.z; rw[4 * i + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < RW; ++i) rw[i] = __ldg(reinterpret_cast<const uint32_t*>(res) + i);
+  }
+  const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+  return pq_residual_words<M, SUB, RBITS>(ix, q, cw, rw, qp, out_dist);
 }
 
 // ---------------------------------------------------------------------------
