@@ -342,11 +342,9 @@ def device_steps(calc, args, step, stream, dist=None, dev=None):
     launches = calc.launch_count() - launches0
     ktimes = {k: v for k, v in calc.kernel_times().items() if v[0] > 0}
     calc.kernel_timing(False)
-    total_ms = t0.elapsed_time(t1)
+    from rover_b200 import replicas
+    total_ms = replicas.max_over_ranks(dist, t0.elapsed_time(t1), dev)
     if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     return dict(total_ms=total_ms, ms_per_step=total_ms / args.steps, launches=launches, kernels=ktimes,
                 clocks=clocks.summary())
@@ -388,10 +386,9 @@ def main():
         return 0
     dist = None
     if world > 1 and args.impl == "ours":
-        import datetime
-        import torch.distributed as dist
+        from rover_b200 import replicas
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = replicas.init("nccl", timeout_s=600)
     if torch.cuda.is_available():
         torch.cuda.set_device(local)
 
@@ -420,6 +417,8 @@ def main():
             return calc.pq_search(qs, L_, top_k=TOP_K, entry_points=ep_, expand_count=expand, correction=1,
                                   refine_budget=REFINE_BUDGET)
         ep, L, table = calibrate(search, w, CONFIGS[args.workload]["comps"])
+    from rover_b200 import replicas
+    ep, L = replicas.from_rank0(dist, (ep, L))     # every replica times rank 0's operating point
     kw = dict(entry_points=ep, expand_count=expand, correction=1, refine_budget=REFINE_BUDGET)
     final = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
     recall = workloads.recall_at_k(final["ids"], final["counts"], w.gt, TOP_K)
@@ -430,6 +429,11 @@ def main():
         if not wider:
             break
         L = wider[0]
+        final = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
+        recall = workloads.recall_at_k(final["ids"], final["counts"], w.gt, TOP_K)
+    L0 = replicas.from_rank0(dist, L)
+    if L0 != L:       # widened differently than rank 0: use rank 0's beam
+        L = L0
         final = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
         recall = workloads.recall_at_k(final["ids"], final["counts"], w.gt, TOP_K)
     log(f"plain operating point ep={ep} L={L} recall@10={recall:.4f}")
@@ -565,9 +569,9 @@ def gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world):
     # L values below the plain arm's are tried first since they are cheaper
     table = []
     # the tensor-core seed ranking makes larger seed sets cheap for this form
-    eps = sorted({max(1, ep // 2), ep, 2 * ep, 4 * ep})
+    eps = sorted({ep, 2 * ep})
     Ls = [x for x in L_SWEEP if x <= 2 * L]
-    for W in range(1, width_max + 1):
+    for W in range(min(2, width_max), width_max + 1):
         for ep_ in eps:
             for L_ in Ls:
                 for rl in (-np.inf, -1.0, 0.0):
@@ -597,12 +601,17 @@ def gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world):
         rec, _, r = run(t["L"], t["entry_points"], t["beam_width"], **thr)
         return t, thr, r, rec
 
-    chosen = settle("mlp")
-    ratio = settle("ratio")
-    if chosen is None:
+    from rover_b200 import replicas
+    ok = [t for t in table if t["kind"] == "mlp" and t["recall_at_10"] >= TARGET_RECALL]
+    pick = min(ok, key=lambda t: t["ms"]) if ok else None
+    pick = replicas.from_rank0(dist, pick)     # every replica times rank 0's point
+    if pick is None:
         log("gate: no calibrated point reaches the target")
         return None
-    t, thr, final, rec = chosen
+    thr = {k: pick[k] for k in ("band_lo", "band_hi", "refine_logit", "stop_logit") if k in pick}
+    rec, _, final = run(pick["L"], pick["entry_points"], pick["beam_width"], **thr)
+    t = pick
+    ratio = settle("ratio")
     model.load(calc, **thr)
     nq = len(w.queries)
     pool_d = torch.full((nq,), t["L"], dtype=torch.int32, device=dev)

@@ -283,7 +283,9 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       const int scap = min(c.short_cap, 2 * cap);
       const float* arow = c.seed_rank + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
       int dummy = 0;
-      if (!select_top(shortl, &ssize, scap, stage, b.n_seeds, SeedRowKeys{arow, b.seed_ids}, &dummy, lane))
+      const SeedRowKeys rk{arow, b.seed_ids};
+      if (!(scap <= kMaxBatch ? select_top_lanes(shortl, &ssize, scap, stage, b.n_seeds, rk, &dummy, lane)
+                              : select_top(shortl, &ssize, scap, stage, b.n_seeds, rk, &dummy, lane)))
         st = kStatusNumeric;
     }
 
@@ -292,7 +294,9 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       corrected = static_cast<unsigned long long>(b.n_seeds);
       const float* drow = b.seed_dists + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
       if (st == kStatusOk &&
-          !select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane))
+          !(cap <= kMaxBatch
+                ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)
+                : select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)))
         st = kStatusNumeric;
       if (st == kStatusOk && check_adc) {
         bool adc_bad = false;
@@ -408,6 +412,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       if (lane == 0)
         for (int k = 0; k < nsel; ++k) list[sel[k]] |= kExpandedBit;
       cursor = sel[nsel - 1] + 1;
+      prefetch_next_rows(ix, list, size, cursor, W, lane);
       // the W rows, loaded together, then checked and claimed in pool order
       int32_t nid[kMaxBeamWidth][2];
 #pragma unroll

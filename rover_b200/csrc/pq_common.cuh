@@ -447,29 +447,151 @@ struct SeedRowKeys {
 // Top-cap selection of n keys (key_at(e), e = 0..n-1) into the sorted list:
 // keys below the list's worst accumulate in stage and are merged once up to
 // kMaxBatch - 32 have gathered (or at the end), so the list is merged a few
-// times instead of once per chunk.  The result is the top-cap of all keys,
-// as inserting them one by one gives.  False if a distance is non-finite.
+// times instead of once per chunk.  Keys are read 8 chunks (256 keys) at a
+// time with every load in flight together, so a row costs n / 256 memory
+// round trips.  The result is the top-cap of all keys, as inserting them
+// one by one gives.  False if a distance is non-finite.
 template <class KeyAt>
 __device__ __forceinline__ bool select_top(uint64_t* list, int* size, int cap, uint64_t* stage, int n,
                                            const KeyAt& key_at, int* cursor, int lane) {
+  constexpr int kGroup = 8;
   int cnt = 0;
-  for (int e0 = 0; e0 < n; e0 += kWarp) {
-    const uint64_t thr = *size == cap ? key_cmp(list[cap - 1]) : kEmptyKey;
-    const int e = e0 + lane;
+  for (int g0 = 0; g0 < n; g0 += kGroup * kWarp) {
+    uint64_t k[kGroup];
     bool nonfinite = false;
-    const uint64_t k = e < n ? key_at(e, &nonfinite) : kEmptyKey;
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+      const int e = g0 + u * kWarp + lane;
+      k[u] = e < n ? key_at(e, &nonfinite) : kEmptyKey;
+    }
     if (__any_sync(kFullMask, nonfinite)) return false;
-    const bool keep = k != kEmptyKey && key_cmp(k) < thr;
-    const unsigned km = __ballot_sync(kFullMask, keep);
-    if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = k;
-    cnt += __popc(km);
-    if (cnt > kMaxBatch - kWarp || e0 + kWarp >= n) {
-      __syncwarp();
-      if (cnt) sort_merge_any(list, size, cap, stage, cnt, cursor, lane);
-      cnt = 0;
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+      const int e0 = g0 + u * kWarp;
+      if (e0 >= n) break;
+      const uint64_t thr = *size == cap ? key_cmp(list[cap - 1]) : kEmptyKey;
+      const bool keep = k[u] != kEmptyKey && key_cmp(k[u]) < thr;
+      const unsigned km = __ballot_sync(kFullMask, keep);
+      if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = k[u];
+      cnt += __popc(km);
+      if (cnt > kMaxBatch - kWarp || e0 + kWarp >= n) {
+        __syncwarp();
+        if (cnt) sort_merge_any(list, size, cap, stage, cnt, cursor, lane);
+        cnt = 0;
+      }
     }
   }
   return true;
+}
+
+// Top-cap selection (cap <= 128) of n keys in one pass: each lane keeps the
+// best 8 of its keys (e = lane, lane + 32, ...) in registers, the warp merges
+// those 256 candidates into the list, and T = the list's worst key decides
+// exactness: a lane whose 8th best is below T may hold more keys below T, so
+// it re-reads its keys and the ones in (8th best, T) are merged as well.
+// The list then holds the top-cap of all n keys, as select_top gives.
+template <class KeyAt>
+__device__ __forceinline__ bool select_top_lanes(uint64_t* list, int* size, int cap, uint64_t* stage, int n,
+                                                 const KeyAt& key_at, int* cursor, int lane) {
+  constexpr int K = 8, kGroup = 8;
+  uint64_t top[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) top[i] = kEmptyKey;
+  for (int g0 = 0; g0 < n; g0 += kGroup * kWarp) {
+    uint64_t k[kGroup];
+    bool nonfinite = false;
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+      const int e = g0 + u * kWarp + lane;
+      k[u] = e < n ? key_at(e, &nonfinite) : kEmptyKey;
+    }
+    if (__any_sync(kFullMask, nonfinite)) return false;
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+      if (k[u] < top[K - 1]) {
+        uint64_t v = k[u];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          const uint64_t lo = v < top[i] ? v : top[i];
+          v = v < top[i] ? top[i] : v;
+          top[i] = lo;
+        }
+      }
+    }
+  }
+  // the lanes' best 4, then their 5th..8th (filtered by the list's worst)
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint64_t thr = *size == cap ? key_cmp(list[cap - 1]) : kEmptyKey;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint64_t v = top[4 * h + i];
+      stage[i * kWarp + lane] = v < thr ? v : kEmptyKey;
+    }
+    __syncwarp();
+    int cnt = drop_non_entering(list, *size, cap, stage, 4 * kWarp, lane);
+    // empty slots sort last and never enter: count the real keys only
+    int real = 0;
+    for (int e = lane; e < cnt; e += kWarp) real += stage[e] != kEmptyKey;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) real += __shfl_xor_sync(kFullMask, real, off);
+    if (real) {
+      // compact the real keys to the front
+      int c2 = 0;
+      for (int e0 = 0; e0 < cnt; e0 += kWarp) {
+        const int e = e0 + lane;
+        const uint64_t v = e < cnt ? stage[e] : kEmptyKey;
+        const bool keep = v != kEmptyKey;
+        const unsigned km = __ballot_sync(kFullMask, keep);
+        __syncwarp();
+        if (keep) stage[c2 + __popc(km & ((1u << lane) - 1u))] = v;
+        c2 += __popc(km);
+        __syncwarp();
+      }
+      sort_merge_any(list, size, cap, stage, c2, cursor, lane);
+    }
+  }
+  // exactness: lanes whose 8th best is below the final worst key re-read
+  const uint64_t thr = *size == cap ? key_cmp(list[cap - 1]) : kEmptyKey;
+  const bool rescan = top[K - 1] != kEmptyKey && top[K - 1] < thr;
+  if (__any_sync(kFullMask, rescan)) {
+    int cnt = 0;
+    for (int e0 = 0; e0 < n; e0 += kWarp) {
+      const int e = e0 + lane;
+      bool nonfinite = false;
+      const uint64_t v = (rescan && e < n) ? key_at(e, &nonfinite) : kEmptyKey;
+      const bool keep = v > top[K - 1] && v < thr;
+      const unsigned km = __ballot_sync(kFullMask, keep);
+      if (keep) stage[cnt + __popc(km & ((1u << lane) - 1u))] = v;
+      cnt += __popc(km);
+      if (cnt > kMaxBatch - kWarp || e0 + kWarp >= n) {
+        __syncwarp();
+        if (cnt) sort_merge_any(list, size, cap, stage, cnt, cursor, lane);
+        cnt = 0;
+      }
+    }
+  }
+  return true;
+}
+
+// Prefetches into L2 the adjacency rows of the first `count` unexpanded
+// list entries at or after position `from`: the sources the next step will
+// most likely expand (a better candidate merged first only wastes the hint).
+__device__ __forceinline__ void prefetch_next_rows(const PqIndexView& ix, const uint64_t* list, int size, int from,
+                                                   int count, int lane) {
+  const int i = from + lane;
+  const bool cand = i < size && !(list[i] & kExpandedBit);
+  unsigned m = __ballot_sync(kFullMask, cand);
+  for (int k = 0; k < count && m; ++k) {
+    const int b = __ffs(m) - 1;
+    m &= m - 1;
+    if (lane == b) {
+      const char* row = reinterpret_cast<const char*>(ix.graph + static_cast<size_t>(key_id(list[i])) * ix.degree);
+      const int bytes = ix.degree * 4;
+      for (int off = 0; off < bytes + 127; off += 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(row + (off < bytes ? off : bytes - 1)));
+    }
+  }
 }
 
 // Whether every LUT entry of this query is provably finite and no ADC sum

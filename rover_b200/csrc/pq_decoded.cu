@@ -397,7 +397,9 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
 
     // ---- initial pool: top-L of the seed row under (distance, id)
     const float* drow = b.seed_dists + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
-    if (!select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane))
+    if (!(cap <= kMaxBatch
+              ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)
+              : select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)))
       st = kStatusNumeric;
     if (st == kStatusOk && check_adc) {
       bool adc_bad = false;
@@ -423,6 +425,7 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
       if (pos < 0) break;
       cursor = pos + 1;
       const int32_t src = key_id(list[pos]);
+      prefetch_next_rows(ix, list, size, pos + 1, 1, lane);
       __syncwarp();
       if (lane == 0) list[pos] |= kExpandedBit;
       const int32_t* row = ix.graph + static_cast<size_t>(src) * ix.degree;
