@@ -173,7 +173,12 @@ AEEResult calculator_rover_pq_lut(remote_handle64 h, const float *queries, int32
                                   float *out_luts, int32_t *out_status);
 
 /* Final refine of host-supplied candidate lists (refine_impl,
- * retrieval_final_refine.c:256): kind 0 = SQ decode, 1 = PQ residual decode. */
+ * retrieval_final_refine.c:256): kind 0 = SQ decode, 1 = PQ residual decode.
+ * kind 2 = the legacy SQ re-rank demo_rerank_candidates
+ * (retrieval_rpc_demo_support.c:1833): stable sort by id, exact residual
+ * distance (retrieval_demo_exact_distance_residual, :1397; FLT_MAX for an id
+ * outside the index), stable sort by distance, first top_k; no reorder map.
+ * At most 2048 candidates per query. */
 AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, const float *queries,
                                   int32_t num_queries, const int32_t *cand_ids, int32_t cand_stride,
                                   const int32_t *cand_counts, int32_t top_k, int32_t *out_ids,

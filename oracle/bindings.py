@@ -269,6 +269,7 @@ class Port:
         L.oracle_dsp_search.argtypes = [C.POINTER(_SqIndex), _f32p, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.c_int, _i32p, _f32p]
         L.oracle_refine.argtypes = [C.c_int, C.c_void_p, _f32p, _i32p, C.c_int, C.c_int, _i32p, _f32p]
+        L.oracle_sq_rerank.argtypes = [C.POINTER(_SqIndex), _f32p, _i32p, _f32p, C.c_int, C.c_int, _i32p, _f32p]
 
     def pq_index(self, graph, bundle):
         """(struct, keepalive) for a rover_b200.bundle.PqBundle + graph."""
@@ -381,6 +382,19 @@ class Port:
         if c < 0:
             raise RuntimeError("oracle_dsp_search failed")
         return ids[:c], d[:c]
+
+    def sq_rerank(self, ix, query, ids, top_k):
+        """demo_rerank_candidates restated (legacy SQ re-rank)."""
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        work = np.array(ids, dtype=np.int32)
+        wd = np.zeros(len(work), dtype=np.float32)
+        out_ids = np.full(max(top_k, 1), -1, dtype=np.int32)
+        out_d = np.zeros(max(top_k, 1), dtype=np.float32)
+        c = self.lib.oracle_sq_rerank(C.byref(ix[0]), _p(q, _f32p), _p(work, _i32p), _p(wd, _f32p), len(work), top_k,
+                                      _p(out_ids, _i32p), _p(out_d, _f32p))
+        if c < 0:
+            raise RuntimeError("oracle_sq_rerank failed")
+        return out_ids[:c], out_d[:c]
 
     def refine(self, kind, ix, query, ids, top_k):
         q = np.ascontiguousarray(query, dtype=np.float32)

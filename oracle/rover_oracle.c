@@ -401,6 +401,50 @@ float oracle_sq_exact(const OracleSqIndex *ix, const float *query, int id) {
     return dist;
 }
 
+/* demo_rerank_candidates (retrieval_rpc_demo_support.c:1833-1862) without a
+ * reorder map: stable insertion sort of the candidates by id
+ * (demo_sort_candidates_by_id :1776-1798), the exact residual distance of
+ * each (FLT_MAX for an id outside the index, :1565-1567), stable insertion
+ * sort by distance (demo_sort_candidates_by_distance :1800-1818), first
+ * min(top_k, count).  ids/dists are scratch of count entries. */
+int oracle_sq_rerank(const OracleSqIndex *ix, const float *query, int32_t *ids, float *dists, int count,
+                     int top_k, int32_t *out_ids, float *out_dists) {
+    int j, rc;
+    if (!ix || !query || !ids || !dists || count < 0) return -1;
+    for (j = 1; j < count; j++) {
+        int32_t tid = ids[j];
+        float tdt = dists[j];
+        int k = j - 1;
+        while (k >= 0 && !(ids[k] <= tid)) {
+            ids[k + 1] = ids[k];
+            dists[k + 1] = dists[k];
+            k--;
+        }
+        ids[k + 1] = tid;
+        dists[k + 1] = tdt;
+    }
+    for (j = 0; j < count; j++)
+        dists[j] = (ids[j] < 0 || ids[j] >= ix->n) ? FLT_MAX : oracle_sq_exact(ix, query, ids[j]);
+    for (j = 1; j < count; j++) {
+        int32_t tid = ids[j];
+        float tdt = dists[j];
+        int k = j - 1;
+        while (k >= 0 && dists[k] > tdt) {
+            ids[k + 1] = ids[k];
+            dists[k + 1] = dists[k];
+            k--;
+        }
+        ids[k + 1] = tid;
+        dists[k + 1] = tdt;
+    }
+    rc = top_k < count ? top_k : count;
+    for (j = 0; j < rc; j++) {
+        out_ids[j] = ids[j];
+        out_dists[j] = dists[j];
+    }
+    return rc;
+}
+
 /* retrieval_sqmd_make_seed_ids, retrieval_sqmd_seed.c:15-63 */
 int oracle_sq_seed_ids(int n, int entry_points, int graph_entry, uint32_t seed, int32_t *ids,
                        int capacity) {

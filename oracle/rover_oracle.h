@@ -57,6 +57,8 @@ int oracle_pq_search(const OraclePqIndex *ix, const float *query, const int32_t 
 int oracle_sq_quantize(const OracleSqIndex *ix, const float *query, uint8_t *out);
 float oracle_sq_coarse(const OracleSqIndex *ix, const uint8_t *query_code, int id);
 float oracle_sq_exact(const OracleSqIndex *ix, const float *query, int id);
+int oracle_sq_rerank(const OracleSqIndex *ix, const float *query, int32_t *ids, float *dists, int count,
+                     int top_k, int32_t *out_ids, float *out_dists);
 int oracle_sq_seed_ids(int n, int entry_points, int graph_entry, uint32_t seed, int32_t *ids,
                        int capacity);
 int oracle_sqmd_search(const OracleSqIndex *ix, const float *query, int entry_points,

@@ -1369,10 +1369,11 @@ extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, co
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
-  if (nq <= 0 || !queries || !cand_ids || !cand_counts || top_k <= 0 || cand_stride <= 0 || (kind != 0 && kind != 1))
+  if (nq <= 0 || !queries || !cand_ids || !cand_counts || top_k <= 0 || cand_stride <= 0 || kind < 0 || kind > 2)
     return AEE_EBADPARM;
   if (kind == 1 && (!s.pq.loaded || !s.pq.view.residual_bits)) { set_error("no PQ residual index"); return AEE_EFAILED; }
   if (kind == 0 && (!s.sq.loaded || !s.sq.view.residual)) { set_error("no SQ residual index"); return AEE_EFAILED; }
+  if (kind == 2 && !s.sq.loaded) { set_error("no SQ index loaded"); return AEE_EFAILED; }
   const int dim = kind == 1 ? s.pq.view.dim : s.sq.view.dim;
   int cap = 1;
   for (int i = 0; i < nq; ++i) {
@@ -1395,7 +1396,12 @@ extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, co
     if (ensure_decoded(s, s.pq, &ok) != AEE_SUCCESS) return AEE_EFAILED;
     if (ok) decoded = s.pq.decoded.as<float>();
   }
-  {
+  if (kind == 2) {
+    TimedLaunch tl(ROVER_KERNEL_REFINE, s.stream);
+    launch_rerank(s.sq.view, s.in_queries.as<float>(), nq, s.in_ids.as<int32_t>(), cand_stride,
+                  s.in_pool.as<int32_t>(), top_k, cap, s.out_ids.as<int32_t>(), s.out_dists.as<float>(),
+                  s.out_counts.as<int32_t>(), s.status.as<int32_t>(), s.stream);
+  } else {
     TimedLaunch tl(ROVER_KERNEL_REFINE, s.stream);
     launch_refine(kind, s.pq.view, s.sq.view, decoded, s.in_queries.as<float>(), nq, s.in_ids.as<int32_t>(), cand_stride,
                   s.in_pool.as<int32_t>(), top_k, cap, s.out_ids.as<int32_t>(), s.out_dists.as<float>(),

@@ -290,6 +290,30 @@ __global__ void sq_coarse_kernel(SqIndexView ix, const float* __restrict__ queri
   if (bad) status[qi] = kStatusBadParam;
 }
 
+// retrieval_demo_exact_distance_residual_scalar (support.c:1397) of one
+// vector: x = (l1*s + z) + (r*rs + rz) per dimension, sequential FP32 sum.
+__device__ __forceinline__ float sq_exact_one(const SqIndexView& ix, const float* q, int32_t id) {
+  const uint8_t* l1 = ix.l1 + static_cast<size_t>(id) * ix.l1_code_bytes;
+  const uint8_t* res = ix.residual ? ix.residual + static_cast<size_t>(id) * ix.rcb : nullptr;
+  float rs = 0.0f, rz = 0.0f, dist = 0.0f;
+  if (res) {
+    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+    rs = qp.x;
+    rz = qp.y;
+  }
+  for (int d = 0; d < ix.dim; ++d) {
+    const uint32_t c = ix.l1_bits == 4 ? static_cast<uint32_t>(nibble(l1, d)) : __ldg(l1 + d);
+    float value = fadd(fmul(u8f(c), ix.l1_scale), ix.l1_zero);
+    if (res) {
+      const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, d)) : __ldg(res + d);
+      value = fadd(value, fadd(fmul(u8f(r), rs), rz));
+    }
+    const float diff = fsub(q[d], value);
+    dist = fadd(dist, fmul(diff, diff));
+  }
+  return dist;
+}
+
 __global__ void sq_exact_kernel(SqIndexView ix, const float* __restrict__ queries, int nq,
                                 const int32_t* __restrict__ ids, const int64_t* __restrict__ offsets,
                                 float* __restrict__ out, int32_t* status) {
@@ -592,6 +616,107 @@ size_t sq_staged_smem(int dim, bool exact) {
   return static_cast<size_t>(dim) * 5 + 16 + static_cast<size_t>(kStageWarps) * (128 + 32 * rs + (exact ? 32 * rs + 256 : 0));
 }
 
+// demo_rerank_candidates (retrieval_rpc_demo_support.c:1833-1862), the
+// legacy SQ re-rank, one warp per query: a stable insertion sort by id, the
+// exact residual distance of every candidate (FLT_MAX for an id outside the
+// index), a stable insertion sort by distance, the first top_k.  Both stable
+// sorts are bitonic sorts of (key, position) pairs, which order exactly as
+// the insertion sorts do while every distance compares; when a distance is
+// NaN (the insertion sort then stops at it) lane 0 replays the insertion
+// sort itself.  No reorder map: the id is the sort key.
+__global__ void rerank_kernel(SqIndexView ix, const float* __restrict__ queries, int nq,
+                              const int32_t* __restrict__ cand_ids, int cand_stride,
+                              const int32_t* __restrict__ cand_counts, int top_k, int capacity, int32_t* out_ids,
+                              float* out_dists, int32_t* out_counts, int32_t* status) {
+  extern __shared__ __align__(16) uint8_t rsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (qi >= nq) return;
+  uint64_t* key = reinterpret_cast<uint64_t*>(rsm) + static_cast<size_t>(warp) * capacity;
+  float* dist = reinterpret_cast<float*>(reinterpret_cast<uint64_t*>(rsm) + static_cast<size_t>(blockDim.x >> 5) * capacity) +
+                static_cast<size_t>(warp) * capacity;
+  int32_t* ids = reinterpret_cast<int32_t*>(dist + static_cast<size_t>((blockDim.x >> 5) - warp) * capacity) +
+                 static_cast<size_t>(warp) * capacity;
+  const float* q = queries + static_cast<size_t>(qi) * ix.dim;
+  const int count = cand_counts[qi];
+  if (count < 0 || count > capacity) {
+    if (lane == 0) status[qi] = kStatusBadParam;
+    return;
+  }
+  int np2 = 1;
+  while (np2 < count) np2 <<= 1;
+  auto bitonic = [&]() {
+    for (int kk = 2; kk <= np2; kk <<= 1)
+      for (int j = kk >> 1; j > 0; j >>= 1) {
+        for (int i = lane; i < np2; i += kWarp) {
+          const int p = i ^ j;
+          if (p > i) {
+            const bool up = (i & kk) == 0;
+            const uint64_t a = key[i], b = key[p];
+            if (up == (a > b)) { key[i] = b; key[p] = a; }
+          }
+        }
+        __syncwarp();
+      }
+  };
+  // stable by id: (signed id, position)
+  for (int i = lane; i < np2; i += kWarp) {
+    if (i < count) {
+      const uint32_t id = static_cast<uint32_t>(cand_ids[static_cast<size_t>(qi) * cand_stride + i]) ^ 0x80000000u;
+      key[i] = (static_cast<uint64_t>(id) << 32) | static_cast<uint32_t>(i);
+    } else {
+      key[i] = ~0ull;
+    }
+  }
+  __syncwarp();
+  bitonic();
+  bool nan = false;
+  for (int i = lane; i < count; i += kWarp) {
+    const int32_t id = static_cast<int32_t>(static_cast<uint32_t>(key[i] >> 32) ^ 0x80000000u);
+    const float d = (id < 0 || id >= ix.n) ? 3.40282346638528859812e+38f : sq_exact_one(ix, q, id);
+    ids[i] = id;
+    dist[i] = d;
+    nan |= isnan(d);
+  }
+  __syncwarp();
+  if (!__any_sync(kFullMask, nan)) {
+    // stable by distance: (distance bits, rank after the id sort); the
+    // distances are sums of squares (>= +0) or FLT_MAX / inf
+    for (int i = lane; i < np2; i += kWarp)
+      key[i] = i < count ? (static_cast<uint64_t>(__float_as_uint(dist[i])) << 32) | static_cast<uint32_t>(i) : ~0ull;
+    __syncwarp();
+    bitonic();
+    const int outn = count < top_k ? count : top_k;
+    for (int i = lane; i < outn; i += kWarp) {
+      const int r = static_cast<int>(key[i] & 0xffffffffu);
+      out_ids[static_cast<size_t>(qi) * top_k + i] = ids[r];
+      out_dists[static_cast<size_t>(qi) * top_k + i] = dist[r];
+    }
+    if (lane == 0) out_counts[qi] = outn;
+    return;
+  }
+  if (lane == 0) {
+    for (int j = 1; j < count; ++j) {
+      const int32_t tid = ids[j];
+      const float tdt = dist[j];
+      int k = j - 1;
+      while (k >= 0 && dist[k] > tdt) {
+        ids[k + 1] = ids[k];
+        dist[k + 1] = dist[k];
+        --k;
+      }
+      ids[k + 1] = tid;
+      dist[k + 1] = tdt;
+    }
+    const int outn = count < top_k ? count : top_k;
+    for (int i = 0; i < outn; ++i) {
+      out_ids[static_cast<size_t>(qi) * top_k + i] = ids[i];
+      out_dists[static_cast<size_t>(qi) * top_k + i] = dist[i];
+    }
+    out_counts[qi] = outn;
+  }
+}
+
 // ---------------------------------------------------------------------------
 
 void launch_pq_lut(const PqIndexView& ix, const float* queries, int nq, float* luts,
@@ -668,6 +793,19 @@ void launch_sq_exact(const SqIndexView& ix, const float* queries, int nq, const 
     return;
   }
   sq_exact_kernel<<<grid, 128, ix.dim * sizeof(float), s>>>(ix, queries, nq, ids, offsets, out, status);
+}
+
+void launch_rerank(const SqIndexView& ix, const float* queries, int nq, const int32_t* cand_ids, int cand_stride,
+                   const int32_t* cand_counts, int top_k, int capacity, int32_t* out_ids, float* out_dists,
+                   int32_t* out_counts, int32_t* status, cudaStream_t s) {
+  if (nq <= 0) return;
+  int cap = 1;
+  while (cap < capacity) cap <<= 1;
+  const int warps = cap <= 1024 ? 4 : 1;
+  const size_t smem = static_cast<size_t>(warps) * cap * 16;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  rerank_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, s>>>(ix, queries, nq, cand_ids, cand_stride, cand_counts,
+                                                                   top_k, cap, out_ids, out_dists, out_counts, status);
 }
 
 void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const float* decoded, const float* queries,

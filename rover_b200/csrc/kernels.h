@@ -224,6 +224,10 @@ void launch_sq_coarse(const SqIndexView& ix, const float* queries, int nq, const
                       const int64_t* offsets, float* out, int32_t* status, cudaStream_t s);
 void launch_sq_exact(const SqIndexView& ix, const float* queries, int nq, const int32_t* ids,
                      const int64_t* offsets, float* out, int32_t* status, cudaStream_t s);
+// demo_rerank_candidates on the SQ index (capacity <= 4096 candidates).
+void launch_rerank(const SqIndexView& ix, const float* queries, int nq, const int32_t* cand_ids, int cand_stride,
+                   const int32_t* cand_counts, int top_k, int capacity, int32_t* out_ids, float* out_dists,
+                   int32_t* out_counts, int32_t* status, cudaStream_t s);
 // decoded: the PQ index's decoded rows (kind 1, dim % 4 == 0) or null.
 void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const float* decoded, const float* queries,
                    int nq, const int32_t* cand_ids, int cand_stride, const int32_t* cand_counts,

@@ -59,6 +59,32 @@ def test_pq_search_matches_reference(calc, name, tag, layout):
 
 
 @pytest.mark.parametrize("name", SQ_FIXTURES)
+def test_sq_rerank_matches_oracle(calc, port, name):
+    """Refine kind 2 (demo_rerank_candidates) against the oracle, bit for
+    bit: shuffled candidates with a repeated id and one outside the index,
+    then the legacy device search's own output lists."""
+    data, graph, b, g, q = load_fixture(name)
+    calc.sq_load(graph, data["graph_entry"], b)
+    ix = port.sq_index(graph, b)
+    rng = np.random.default_rng(5)
+    sample = np.asarray(g["sample_ids"], np.int32)
+    lists = [np.concatenate([rng.permutation(sample), sample[:2], [b.num_vectors + 3]]).astype(np.int32)
+             for _ in range(len(q))]
+    stride = max(len(x) for x in lists)
+    cand = np.full((len(q), stride), -1, np.int32)
+    counts = np.array([len(x) for x in lists], np.int32)
+    for i, x in enumerate(lists):
+        cand[i, :len(x)] = x
+    for top_k in (10, stride):
+        ids, d, c = calc.refine(2, q, cand, counts, top_k)
+        for qi in range(len(q)):
+            oi, od = port.sq_rerank(ix, q[qi], lists[qi], top_k)
+            assert c[qi] == len(oi)
+            assert np.array_equal(ids[qi, :c[qi]], oi)
+            assert np.array_equal(bits(d[qi, :c[qi]]), bits(od))
+
+
+@pytest.mark.parametrize("name", SQ_FIXTURES)
 def test_sq_distances(calc, name):
     data, graph, b, g, q = load_fixture(name)
     calc.sq_load(graph, data["graph_entry"], b)

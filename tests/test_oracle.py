@@ -59,6 +59,35 @@ def test_sq_codes_and_distances(port, name):
         assert np.array_equal(bits(port.sq_exact(ix, q[qi], g["sample_ids"])), bits(g["exact"][qi]))
 
 
+def _rerank_candidates(sample, n, seed=0):
+    """Candidates as a legacy search hands them to the re-rank: shuffled,
+    one id twice, one id outside the index."""
+    rng = np.random.default_rng(seed)
+    c = list(rng.permutation(np.asarray(sample, np.int32)))
+    return np.array(c[:3] + [c[1]] + c[3:] + [n + 5], np.int32)
+
+
+@pytest.mark.parametrize("name", SQ_FIXTURES)
+def test_sq_rerank_restatement(port, name):
+    """demo_rerank_candidates restated: its distances are the reference's
+    exact residual distances (pinned by the golden vectors), FLT_MAX for an
+    id outside the index; the order is stable by distance, ties in id order."""
+    data, graph, b, g, q = load_fixture(name)
+    ix = port.sq_index(graph, b)
+    sample = np.asarray(g["sample_ids"], np.int32)
+    for qi in range(4):
+        exact = dict(zip(sample.tolist(), bits(g["exact"][qi]).tolist()))
+        cand = _rerank_candidates(sample, b.num_vectors, qi)
+        ids, d = port.sq_rerank(ix, q[qi], cand, len(cand))
+        assert len(ids) == len(cand)
+        for i, di in zip(ids.tolist(), bits(d).tolist()):
+            assert di == (exact[i] if i in exact else bits(np.float32(3.4028235e38)))
+        keys = list(zip(d.tolist(), ids.tolist()))
+        assert keys == sorted(keys)          # (distance, id): ties kept in id order
+        top, _ = port.sq_rerank(ix, q[qi], cand, 5)
+        assert np.array_equal(top, ids[:5])
+
+
 @pytest.mark.parametrize("name", SQ_FIXTURES)
 @pytest.mark.parametrize("tag", ["on", "off", "on_ep8", "off_ep16_exp5"])
 def test_sqmd_search(port, name, tag):
