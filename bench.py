@@ -21,6 +21,12 @@ host->device query copy and the device->host result copy inside the timed
 region.  Multi-GPU runs are replicas (each rank searches its own 10,000
 queries; no collective on the data path) and report weak scaling.
 
+After the headline, the uneven-batch section (``config.uneven``, skipped
+with --no-uneven) times the 1M x 96 workload (M=24, degree 32, 20,000
+queries with per-query beam L log-uniform in [16, 512] and k in {1, 10,
+100}): a tuned search plan replayed from a captured CUDA graph against the
+direct device entry point on the same inputs, with their outputs compared.
+
 ``--impl reference`` times the reference's own CPU search code
 (oracle/_ref: retrieval_pure_pq_search_scalar_with_policy + residual
 correction + final refine, compiled from the reference sources) with all host
@@ -54,8 +60,13 @@ CALIBRATION_QUERIES = 2000
 TRAIN_QUERIES = 8000       # held-out queries traced for the gate (about 5M rows)
 GATE_ROWS = 5_000_000
 GATE_EPOCHS = 4
-THRESHOLD_GRID = (0.9, 1.0, 1.1, 1.25, 1.5)
-DK_QUERIES, DK_IDS, DK_REPS = 1000, 8192, 3   # distance-kernel gathers: queries x random ids   # ADC / worst ratios of the method without the network
+THRESHOLD_GRID = (0.9, 1.0, 1.1, 1.25, 1.5)   # ADC / worst ratios of the method without the network
+DK_QUERIES, DK_IDS, DK_REPS = 1000, 8192, 3   # distance-kernel gathers: queries x random ids
+UNEVEN_WORKLOAD = "pq_1m_d96"     # uneven batch: L log-uniform in [16, 512], k in {1, 10, 100}
+UNEVEN_L = (16, 512)
+UNEVEN_K = (1, 10, 100)
+UNEVEN_REFINE = 200               # refine_factor 2 x the largest k
+UNEVEN_EPS = (256, 1024, 4096)
 METRIC = "QPS at recall@10>=0.95 on 1 B200 (pure-PQ graph search, 1M x 128): learned-gate batched vs plain"
 
 
@@ -375,6 +386,7 @@ def main():
     ap.add_argument("--no-gate", action="store_true", help="plain search only")
     ap.add_argument("--no-distance-kernels", action="store_true")
     ap.add_argument("--train-queries", type=int, default=TRAIN_QUERIES)
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch plan section")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -499,6 +511,10 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w, L, ep, expand)
 
+    uneven = None
+    if not args.no_uneven:
+        uneven = uneven_section(calc, args, stream, dist, dev, world)
+
     steps = head["steps"]
     line = {
         "metric": METRIC,
@@ -516,6 +532,7 @@ def main():
                              "roofline": plain_roof, "calibration": table},
                    "gated_over_plain": head["qps"] / plain_qps if gated else 1.0,
                    "gate": gated["report"] if gated else None,
+                   "uneven": uneven,
                    "parallelism": f"replicas x{world}",
                    "l2": "index (>800 MB with decoded rows) larger than L2; no flush"},
         "roofline": head["roof"],
@@ -535,6 +552,126 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def uneven_recall(ids, counts, gt, ks):
+    """Mean over queries of recall@k_i (each query's own k), and recall@10
+    over the queries with k >= 10."""
+    per, per10 = [], []
+    for i in range(ids.shape[0]):
+        k = int(ks[i])
+        c = min(int(counts[i]), k)
+        per.append(len(np.intersect1d(ids[i, :c], gt[i, :k])) / k)
+        if k >= 10:
+            c10 = min(int(counts[i]), 10)
+            per10.append(len(np.intersect1d(ids[i, :c10], gt[i, :10])) / 10)
+    return float(np.mean(per)), float(np.mean(per10)) if per10 else None
+
+
+def uneven_section(calc, args, stream, dist, dev, world):
+    """20,000 queries with uneven beams and result counts on the 1M x 96
+    index, in one batch: a search plan (tuned on these queries, captured in a
+    CUDA graph, replayed each step) against calculator_rover_pq_search_device
+    with the same per-query arrays.  Both return the same ids and distances;
+    the section checks that on the last step's outputs."""
+    import torch
+    from rover_b200 import replicas, workloads
+    t0 = time.time()
+    w = workloads.build_pq(UNEVEN_WORKLOAD, cache_dir=args.cache_dir, verbose=False)
+    calc.pq_load(w.graph, w.entry, w.bundle)
+    nq = len(w.queries)
+    expand = int(w.graph.shape[1])
+    rng = np.random.default_rng(2025)
+    pools = np.exp(rng.uniform(np.log(UNEVEN_L[0]), np.log(UNEVEN_L[1]), nq)).astype(np.int32)
+    ks = rng.choice(UNEVEN_K, nq).astype(np.int32)
+    pools = np.maximum(pools, ks).astype(np.int32)
+    kmax = int(max(UNEVEN_K))
+    log(f"uneven workload ready in {time.time() - t0:.1f}s")
+
+    table = []
+    ep = UNEVEN_EPS[-1]
+    for ep_ in UNEVEN_EPS:
+        r = calc.pq_search(w.queries, pools, top_ks=ks, stats=False, entry_points=ep_, expand_count=expand,
+                           correction=1, refine_budget=UNEVEN_REFINE)
+        rk, r10 = uneven_recall(r["ids"], r["counts"], w.gt, ks)
+        table.append(dict(entry_points=ep_, recall_at_k=rk, recall_at_10=r10))
+        log(f"uneven calibration ep={ep_} recall@k={rk:.4f} recall@10={r10:.4f}")
+        if rk >= TARGET_RECALL:
+            ep = ep_
+            break
+    ep = replicas.from_rank0(dist, ep)
+    kw = dict(entry_points=ep, expand_count=expand, correction=1, refine_budget=UNEVEN_REFINE)
+
+    q_d = torch.from_numpy(np.ascontiguousarray(w.queries)).to(dev)
+    pool_d = torch.from_numpy(pools).to(dev)
+    topk_d = torch.from_numpy(ks).to(dev)
+
+    def outputs():
+        o = dict(ids=torch.empty((nq, kmax), dtype=torch.int32, device=dev),
+                 dists=torch.empty((nq, kmax), dtype=torch.float32, device=dev),
+                 counts=torch.empty(nq, dtype=torch.int32, device=dev),
+                 status=torch.empty(nq, dtype=torch.int32, device=dev))
+        p = {k: v.data_ptr() for k, v in o.items()}
+        p["stride"] = kmax
+        return o, p
+
+    d_out, d_ptrs = outputs()
+
+    def direct_step():
+        calc.pq_search_device(q_d.data_ptr(), nq, pool_d.data_ptr(), d_ptrs, topk_ptr=topk_d.data_ptr(),
+                              stream_ptr=stream.cuda_stream, **kw)
+
+    direct = device_steps(calc, args, direct_step, stream, dist, dev)
+
+    t_tune = time.time()
+    plan = calc.pq_plan(nq, pools, top_ks=ks, tune_queries_ptr=q_d.data_ptr(), **kw)
+    info = plan.describe()
+    tune_s = time.time() - t_tune
+    p_out, p_ptrs = outputs()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):         # one eager launch, per-kernel times from the library's events
+        calc.kernel_timing(True)
+        plan.launch(q_d.data_ptr(), p_ptrs, side.cuda_stream)
+        side.synchronize()
+        eager_kernels = {k: v[1] for k, v in calc.kernel_times().items() if v[0] > 0}
+        calc.kernel_timing(False)
+    stream.wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        plan.launch(q_d.data_ptr(), p_ptrs, torch.cuda.current_stream().cuda_stream)
+    replay = device_steps(calc, args, graph.replay, stream, dist, dev)
+    torch.cuda.synchronize()
+    identical = bool(torch.equal(p_out["status"], torch.zeros_like(p_out["status"])) and
+                     torch.equal(p_out["counts"], d_out["counts"]))
+    if identical:
+        mask = torch.arange(kmax, device=dev)[None, :] < d_out["counts"][:, None]
+        identical = bool(torch.equal(torch.where(mask, p_out["ids"], 0), torch.where(mask, d_out["ids"], 0)) and
+                         torch.equal(torch.where(mask, p_out["dists"], 0).view(torch.int32),
+                                     torch.where(mask, d_out["dists"], 0).view(torch.int32)))
+    ids = p_out["ids"].cpu().numpy()
+    counts = p_out["counts"].cpu().numpy()
+    rk, r10 = uneven_recall(ids, counts, w.gt, ks)
+    del graph
+    plan.destroy()
+    plan_qps = nq * args.steps * world / (replay["total_ms"] / 1e3)
+    direct_qps = nq * args.steps * world / (direct["total_ms"] / 1e3)
+    log(f"uneven: plan {plan_qps:,.0f} QPS ({replay['ms_per_step']:.3f} ms/step, {info['classes']} classes, "
+        f"{info['warps_per_cta']} warps, {info['shared_visited_slots']} slots, layout {info['layout']}), direct "
+        f"{direct_qps:,.0f} QPS, identical={identical}, recall@k={rk:.4f}")
+    return {"workload": UNEVEN_WORKLOAD, "n": int(w.bundle.meta.num_vectors), "dim": int(w.bundle.meta.dim),
+            "pq": f"M={w.bundle.meta.m}x{w.bundle.meta.ks}", "graph_degree": expand, "queries_per_step": nq,
+            "beam_L": f"log-uniform [{UNEVEN_L[0]}, {UNEVEN_L[1]}], L >= k", "top_k": list(UNEVEN_K),
+            "refine_budget": UNEVEN_REFINE, "entry_points": ep, "calibration": table,
+            "recall_at_k": rk, "recall_at_10": r10,
+            "plan": {"qps": plan_qps, "ms_per_step": replay["ms_per_step"], "replayed": "CUDA graph",
+                     "config": info, "tune_seconds": tune_s,
+                     "gpu_launches_per_step": info["launches"], "clocks": replay["clocks"],
+                     "eager_kernel_ms": eager_kernels},
+            "direct": {"qps": direct_qps, "ms_per_step": direct["ms_per_step"],
+                       "kernel_ms_per_step": {k: v[1] / args.steps for k, v in direct["kernels"].items()},
+                       "gpu_launches_per_step": direct["launches"] / args.steps},
+            "plan_over_direct": plan_qps / direct_qps, "identical_outputs": identical}
 
 
 def gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world):

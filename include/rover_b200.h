@@ -156,6 +156,86 @@ AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const RoverSearc
                                              const int32_t *top_ks, const RoverSearchOutputs *out,
                                              void *stream);
 
+/* ---- search plans: one set of searches replayed on new queries ----------
+ *
+ * The reference serves queries one at a time; a plan serves thousands with
+ * uneven beam widths and result counts (pool_sizes[i], top_ks[i], fixed when
+ * the plan is made) as a fixed sequence of kernels: a bookkeeping kernel,
+ * the all-queries entry-seed pass, one persistent search launch per
+ * beam-width class (queries sorted by width, widest first, so each class's
+ * shared-memory slices fit its widest query) and a second bookkeeping
+ * kernel.  A launch allocates nothing, never waits on the host and reads its
+ * per-launch state (visited-table generations, work counters) from device
+ * memory, so a CUDA graph captured from one launch can be replayed on new
+ * vectors written into the same query buffer.
+ *
+ * With tune_queries (device, [num_queries][dim]), creation times the
+ * configurations that leave results unchanged -- warps per CTA (2, 4, 8),
+ * shared-memory visited slots per warp (1024, 2048, 4096), beam-width
+ * classes (one, two, one per power of two), and for ROVER_MODE_EXACT the
+ * packed or decoded residual layout -- and keeps the fastest.  Every
+ * configuration returns the same ids and distances as
+ * calculator_rover_pq_search on the same inputs.
+ *
+ * A plan copies the entry seeds (and the loaded gate, for ROVER_MODE_GATED)
+ * when it is made and refers to the loaded PQ index: destroy plans, and the
+ * graphs captured from them, before unloading or replacing the index. */
+#define ROVER_PLAN_MAX_CLASSES 8
+
+typedef struct RoverPlanInfo {
+    int32_t num_queries;
+    int32_t mode;                    /* ROVER_MODE_* */
+    int32_t layout;                  /* ROVER_LAYOUT_PACKED or ROVER_LAYOUT_DECODED */
+    int32_t warps_per_cta;
+    int32_t shared_visited_slots;    /* per warp; 0 for the packed layout */
+    int32_t classes;                 /* beam-width classes = search launches */
+    int32_t launches;                /* kernels one plan launch enqueues */
+    int32_t candidates;              /* configurations timed at creation (0 = untuned) */
+    int32_t max_pool;
+    int32_t beam_width;              /* batched / gated modes */
+    int32_t class_pool[ROVER_PLAN_MAX_CLASSES];     /* widest beam of each class */
+    int32_t class_queries[ROVER_PLAN_MAX_CLASSES];
+    int32_t class_blocks[ROVER_PLAN_MAX_CLASSES];   /* CTAs of each class launch */
+    float tuned_ms;                  /* the kept configuration's launch time (0 = untuned) */
+    float default_ms;                /* the untuned default's launch time (0 = untuned) */
+    int64_t device_bytes;            /* device memory held by the plan */
+    int32_t class_split;             /* RoverPlanConfig.class_split of the kept configuration */
+    int32_t reserved[7];
+} RoverPlanInfo;
+
+/* One plan configuration (every one gives the same results). */
+typedef struct RoverPlanConfig {
+    int32_t layout;                  /* ROVER_LAYOUT_PACKED or ROVER_LAYOUT_DECODED */
+    int32_t warps_per_cta;           /* 1..8 (the packed layout runs 4) */
+    int32_t shared_visited_slots;    /* per warp, power of two 256..8192 (decoded layout) */
+    int32_t class_split;             /* 0: one class, 1: two, 2: one per power of two of the beam width */
+} RoverPlanConfig;
+
+typedef struct RoverPqPlan RoverPqPlan;   /* opaque */
+
+/* pool_sizes and top_ks (NULL = params->top_k) are host arrays of
+ * num_queries entries.  tune_queries may be NULL (no tuning: decoded layout
+ * when available, 4 warps, 2048 slots, one class). */
+AEEResult calculator_rover_pq_plan_create(remote_handle64 h, const RoverSearchParams *params,
+                                          int32_t num_queries, const int32_t *pool_sizes,
+                                          const int32_t *top_ks, const float *tune_queries,
+                                          RoverPqPlan **plan);
+/* A plan with a given configuration, e.g. one that an earlier tuned plan
+ * reported (calculator_rover_pq_plan_describe), without timing anything. */
+AEEResult calculator_rover_pq_plan_create_fixed(remote_handle64 h, const RoverSearchParams *params,
+                                                int32_t num_queries, const int32_t *pool_sizes,
+                                                const int32_t *top_ks, const RoverPlanConfig *config,
+                                                RoverPqPlan **plan);
+/* Enqueues the plan's searches on stream (a cudaStream_t, NULL = the
+ * library's stream) and returns without waiting.  queries and every output
+ * pointer are device pointers; out->status is required and is rewritten by
+ * every launch (ROVER_QUERY_TABLE_FULL marks a query whose visited table
+ * overflowed: rerun it through calculator_rover_pq_search). */
+AEEResult calculator_rover_pq_plan_launch(RoverPqPlan *plan, const float *queries,
+                                          const RoverSearchOutputs *out, void *stream);
+AEEResult calculator_rover_pq_plan_describe(const RoverPqPlan *plan, RoverPlanInfo *info);
+AEEResult calculator_rover_pq_plan_destroy(RoverPqPlan *plan);
+
 /* Distances for explicit (query, id) lists: ids[offsets[q] .. offsets[q+1]).
  * kind 0 = PQ ADC (retrieval_pq_adc_ids_batch, retrieval_pq_core.c:332),
  * 1 = PQ residual-corrected (retrieval_pq_residual_query_evaluate,
@@ -292,6 +372,7 @@ uint64_t calculator_rover_launch_count(void);
 #define ROVER_KERNEL_SQ_EXACT 10    /* kind 3: SQ residual-corrected distances */
 #define ROVER_KERNEL_REFINE 11      /* calculator_rover_refine */
 #define ROVER_KERNEL_PQ_RESCORE 12  /* kind 4: corrected distances from decoded rows */
+#define ROVER_KERNEL_PLAN 13        /* search plans: bookkeeping kernels */
 #define ROVER_KERNEL_KINDS 16
 void calculator_rover_kernel_timing(int32_t enable);
 int32_t calculator_rover_kernel_times(int64_t *launches, double *ms, int32_t kinds);

@@ -20,7 +20,7 @@ LIB_DIR = HERE / "lib"
 LIB = LIB_DIR / "libcalculator.so"
 HOST_DIR = HERE / "host"
 
-SOURCES = ["calculator.cu", "pq_search.cu", "pq_decoded.cu", "pq_batched.cu", "gate_train.cu", "sq_search.cu", "distance.cu", "rpcmem_compat.cpp"]
+SOURCES = ["calculator.cu", "pq_search.cu", "pq_decoded.cu", "pq_batched.cu", "gate_train.cu", "plan.cu", "sq_search.cu", "distance.cu", "rpcmem_compat.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

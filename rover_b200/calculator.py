@@ -83,6 +83,20 @@ class SearchOutputs(C.Structure):
                 ("status", _i32p)]
 
 
+class PlanInfo(C.Structure):
+    _fields_ = [("num_queries", C.c_int32), ("mode", C.c_int32), ("layout", C.c_int32),
+                ("warps_per_cta", C.c_int32), ("shared_visited_slots", C.c_int32), ("classes", C.c_int32),
+                ("launches", C.c_int32), ("candidates", C.c_int32), ("max_pool", C.c_int32),
+                ("beam_width", C.c_int32), ("class_pool", C.c_int32 * 8), ("class_queries", C.c_int32 * 8),
+                ("class_blocks", C.c_int32 * 8), ("tuned_ms", C.c_float), ("default_ms", C.c_float),
+                ("device_bytes", C.c_int64), ("class_split", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+class PlanConfig(C.Structure):
+    _fields_ = [("layout", C.c_int32), ("warps_per_cta", C.c_int32), ("shared_visited_slots", C.c_int32),
+                ("class_split", C.c_int32)]
+
+
 def _p(a, t):
     return None if a is None else a.ctypes.data_as(t)
 
@@ -132,6 +146,13 @@ class Calculator:
                                                  _i32p, C.POINTER(SearchOutputs)]
         L.calculator_rover_pq_search_device.argtypes = [C.c_uint64, C.POINTER(SearchParams), _f32p, C.c_int32,
                                                         _i32p, _i32p, C.POINTER(SearchOutputs), C.c_void_p]
+        L.calculator_rover_pq_plan_create.argtypes = [C.c_uint64, C.POINTER(SearchParams), C.c_int32, _i32p, _i32p,
+                                                      _f32p, C.POINTER(C.c_void_p)]
+        L.calculator_rover_pq_plan_create_fixed.argtypes = [C.c_uint64, C.POINTER(SearchParams), C.c_int32, _i32p,
+                                                            _i32p, C.POINTER(PlanConfig), C.POINTER(C.c_void_p)]
+        L.calculator_rover_pq_plan_launch.argtypes = [C.c_void_p, _f32p, C.POINTER(SearchOutputs), C.c_void_p]
+        L.calculator_rover_pq_plan_describe.argtypes = [C.c_void_p, C.POINTER(PlanInfo)]
+        L.calculator_rover_pq_plan_destroy.argtypes = [C.c_void_p]
         L.calculator_rover_score.argtypes = [C.c_uint64, C.c_int32, _f32p, C.c_int32, _i32p, _i64p, _f32p, _i32p]
         L.calculator_rover_pq_lut.argtypes = [C.c_uint64, _f32p, C.c_int32, _f32p, _i32p]
         L.calculator_rover_refine.argtypes = [C.c_uint64, C.c_int32, _f32p, C.c_int32, _i32p, C.c_int32, _i32p,
@@ -157,7 +178,7 @@ class Calculator:
         return int(self.lib.calculator_rover_launch_count())
 
     KERNEL_KINDS = ("pq_packed", "pq_seeds", "pq_decoded", "pq_batched", "sq", "pq_seed_rank", "pq_lut", "pq_adc",
-                    "pq_residual", "sq_coarse", "sq_exact", "refine", "pq_rescore")
+                    "pq_residual", "sq_coarse", "sq_exact", "refine", "pq_rescore", "plan")
 
     # -- learned gate
     def gate_load(self, params, mu, sigma, band_lo=0.0, band_hi=0.0, refine_logit=0.0, stop_logit=1e30) -> None:
@@ -355,6 +376,30 @@ class Calculator:
             self._check("calculator_rover_pq_search_device", rc)
         return rc
 
+    def pq_plan(self, nq: int, pool_sizes, top_ks=None, tune_queries_ptr: int = 0, top_k: int = 10,
+                config=None, **kw) -> "Plan":
+        """A search plan (calculator_rover_pq_plan_create) for nq queries with
+        these beam widths and result counts.  tune_queries_ptr: device address
+        of [nq][dim] FP32 queries to tune on (0 = no tuning).  config (a dict
+        with the keys of describe(), or a (layout, warps_per_cta,
+        shared_visited_slots, class_split) tuple) pins a configuration
+        instead (calculator_rover_pq_plan_create_fixed)."""
+        pools = np.ascontiguousarray(np.broadcast_to(np.asarray(pool_sizes, dtype=np.int32), (nq,)))
+        tks = None if top_ks is None else np.ascontiguousarray(np.broadcast_to(np.asarray(top_ks, dtype=np.int32), (nq,)))
+        p = self.params(top_k=top_k, **kw)
+        h = C.c_void_p()
+        if config is not None:
+            cfg = PlanConfig(*config) if not isinstance(config, dict) else PlanConfig(
+                config["layout"], config["warps_per_cta"], config["shared_visited_slots"], config["class_split"])
+            rc = self.lib.calculator_rover_pq_plan_create_fixed(self.handle, C.byref(p), nq, _p(pools, _i32p),
+                                                                _p(tks, _i32p), C.byref(cfg), C.byref(h))
+            self._check("calculator_rover_pq_plan_create_fixed", rc)
+        else:
+            rc = self.lib.calculator_rover_pq_plan_create(self.handle, C.byref(p), nq, _p(pools, _i32p),
+                                                          _p(tks, _i32p), _dp(_f32p, tune_queries_ptr), C.byref(h))
+            self._check("calculator_rover_pq_plan_create", rc)
+        return Plan(self, h, nq, int(tks.max()) if tks is not None else top_k)
+
     def pq_lut(self, queries, m, ks):
         q = np.ascontiguousarray(queries, dtype=np.float32)
         out = np.zeros((q.shape[0], m * ks), np.float32)
@@ -423,3 +468,49 @@ class Calculator:
         if check:
             self._check("calculator_rover_sq_search", rc)
         return r
+
+
+class Plan:
+    """A search plan: the same searches enqueued on new query vectors.  Every
+    pointer is a raw CUDA device address (e.g. torch tensor .data_ptr())."""
+
+    def __init__(self, calc: Calculator, handle: C.c_void_p, nq: int, max_k: int):
+        self.calc = calc
+        self.handle = handle
+        self.nq = nq
+        self.max_k = max_k
+
+    def launch(self, queries_ptr: int, out: dict, stream_ptr: int = 0) -> None:
+        """Enqueue (no wait).  out holds device pointers for ids, dists, counts,
+        stride, status (required) and optionally pool_*, stats."""
+        o = SearchOutputs(_dp(_i32p, out.get("ids")), _dp(_f32p, out.get("dists")), _dp(_i32p, out.get("counts")),
+                          out.get("stride", 0), _dp(_i32p, out.get("pool_ids")), _dp(_f32p, out.get("pool_dists")),
+                          _dp(_i32p, out.get("pool_counts")), _dp(_u64p, out.get("stats")),
+                          _dp(_i32p, out.get("status")))
+        rc = self.calc.lib.calculator_rover_pq_plan_launch(self.handle, _dp(_f32p, queries_ptr), C.byref(o),
+                                                           C.c_void_p(stream_ptr or None))
+        self.calc._check("calculator_rover_pq_plan_launch", rc)
+
+    def describe(self) -> dict:
+        info = PlanInfo()
+        self.calc._check("calculator_rover_pq_plan_describe",
+                         self.calc.lib.calculator_rover_pq_plan_describe(self.handle, C.byref(info)))
+        n = info.classes
+        return dict(num_queries=info.num_queries, mode=info.mode, layout=info.layout,
+                    warps_per_cta=info.warps_per_cta, shared_visited_slots=info.shared_visited_slots,
+                    classes=n, launches=info.launches, candidates=info.candidates, max_pool=info.max_pool,
+                    beam_width=info.beam_width, class_pool=list(info.class_pool[:n]),
+                    class_queries=list(info.class_queries[:n]), class_blocks=list(info.class_blocks[:n]),
+                    tuned_ms=info.tuned_ms, default_ms=info.default_ms, device_bytes=info.device_bytes,
+                    class_split=info.class_split)
+
+    def destroy(self) -> None:
+        if self.handle:
+            self.calc.lib.calculator_rover_pq_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -95,12 +96,14 @@ struct PqDevice {
   int32_t graph_entry = -1;
   bool loaded = false;
   bool has_graph = false;
+  uint64_t epoch = 0;             // bumped whenever the device copy is released (plans check it)
   void release() {
     graph.release(); codes.release(); codebook.release(); residual.release(); qparams.release();
     decoded.release(); seeds.release();
     decoded_ready = false;
     loaded = false;
     has_graph = false;
+    ++epoch;
   }
 };
 
@@ -178,7 +181,8 @@ KernelTimer& timer() {
 // Brackets one launch with events when timing is on.
 class TimedLaunch {
  public:
-  TimedLaunch(int kind, cudaStream_t s) : kind_(kind), s_(s) {
+  TimedLaunch(int kind, cudaStream_t s, bool enable = true) : kind_(kind), s_(s) {
+    if (!enable) return;
     KernelTimer& t = timer();
     std::lock_guard<std::mutex> g(t.mu);
     if (!t.on) return;
@@ -203,19 +207,27 @@ class TimedLaunch {
 };
 
 // Reads the events of finished launches (call after the stream synchronized).
+// Reads the events of finished launches; launches still in flight stay
+// pending for a later call.
 void collect_timings() {
   KernelTimer& t = timer();
   std::lock_guard<std::mutex> g(t.mu);
+  std::vector<KernelTimer::Pending> running;
   for (const auto& p : t.pending) {
+    if (cudaEventQuery(p.stop) == cudaErrorNotReady) {
+      running.push_back(p);
+      continue;
+    }
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
       t.launches[p.kind] += 1;
       t.ms[p.kind] += ms;
     }
+    cudaGetLastError();
     t.spare.push_back(p.start);
     t.spare.push_back(p.stop);
   }
-  t.pending.clear();
+  t.pending.swap(running);
 }
 
 AEEResult ensure_init(State& s) {
@@ -263,6 +275,24 @@ int resident_blocks(const void* kernel, int threads, size_t smem, int sms) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   return per_sm * sms;
+}
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` and never
+// lowers it: plans set the limit once when they are made, and their launches
+// (possibly replayed from a CUDA graph) must not find it lowered by a later
+// search with smaller slices.  Callers hold the state lock.
+AEEResult allow_smem(const void* fn, size_t bytes) {
+  static std::vector<std::pair<const void*, size_t>> limits;
+  for (auto& e : limits) {
+    if (e.first != fn) continue;
+    if (e.second >= bytes) return AEE_SUCCESS;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    e.second = bytes;
+    return AEE_SUCCESS;
+  }
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+  limits.emplace_back(fn, bytes);
+  return AEE_SUCCESS;
 }
 
 bool valid_params(const RoverSearchParams* p) {
@@ -373,8 +403,7 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
   const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, a.max_pool); return AEE_EBADPARM; }
   const PqDecodedFn kernel = pq_decoded_kernel_for(pq.view.dim);
-  CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          static_cast<int>(smem)));
+  if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
   const int chunk = static_cast<int>(std::max<size_t>(
       1, std::min<size_t>(nq, kSeedDistBudget / (static_cast<size_t>(ss.count) * sizeof(float)))));
@@ -501,8 +530,7 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
   const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, max_pool); return AEE_EBADPARM; }
   const PqSearchFn kernel = pq_search_kernel_for(pq.view, p->correction != 0);
-  CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          static_cast<int>(smem)));
+  if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
   const int blocks = std::max(1, std::min(max_blocks, (nq + kSearchWarps - 1) / kSearchWarps));
   const size_t slots = static_cast<size_t>(blocks) * kSearchWarps;
@@ -585,8 +613,7 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
   const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, a.max_pool); return AEE_EBADPARM; }
   const PqBatchFn kernel = pq_batched_kernel_for(pq.view.dim, tracing ? kBatchTrace : gated ? kBatchGated : kBatchFull);
-  CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          static_cast<int>(smem)));
+  if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
   const bool seed_pass = !gated;      // exact seed distances
   const bool rank_pass = rows;        // quantized seed distances (tensor cores)
@@ -702,7 +729,7 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
   a.status = d_status;
   const size_t per_warp = ((sq.view.dim * 4 + 15) & ~15) + ((sq.view.dim + 15) & ~15) + 64 * 8;
   const size_t smem = per_warp * kSearchWarps;
-  CK(cudaFuncSetAttribute(sq_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  if (allow_smem(reinterpret_cast<const void*>(sq_search_kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   int blocks = std::max(1, std::min(resident_blocks(reinterpret_cast<const void*>(sq_search_kernel), kSearchWarps * 32, smem, s.sms),
                                     (nq + kSearchWarps - 1) / kSearchWarps));
   // keep the heap scratch under 4 GiB
@@ -805,6 +832,7 @@ extern "C" void calculator_rover_kernel_timing(int32_t enable) {
 }
 
 extern "C" int32_t calculator_rover_kernel_times(int64_t* launches, double* ms, int32_t kinds) {
+  collect_timings();
   KernelTimer& t = timer();
   std::lock_guard<std::mutex> g(t.mu);
   const int32_t n = std::max(0, std::min<int32_t>(kinds, ROVER_KERNEL_KINDS));
@@ -986,6 +1014,706 @@ extern "C" AEEResult calculator_rover_pq_search(remote_handle64 h, const RoverSe
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   return pq_search_host(s, p, queries, nq, pool_sizes, top_ks, out);
+}
+
+// ---------------------------------------------------------------------------
+// Search plans (include/rover_b200.h): a fixed kernel sequence over a fixed
+// set of beam widths and result counts, enqueued without allocation or host
+// waits so that one launch can be captured into a CUDA graph and replayed.
+
+struct RoverPqPlan {};   // the opaque handle type of the C-ABI
+static_assert(ROVER_PLAN_MAX_CLASSES == rover::kMaxPlanClasses, "plan classes");
+
+namespace {
+
+constexpr uint32_t kPlanMagic = 0x4e414c50u;
+constexpr int32_t kPlanMaxQueries = 4000000;          // seed passes tile queries by 64 in grid.y
+constexpr size_t kPlanSeedBytes = 8ull << 30;          // query x seed distances held by one plan
+
+struct PlanConfig {
+  int layout = ROVER_LAYOUT_DECODED;
+  int warps = kSearchWarps;
+  int vis_cap = kSharedVisitedSlots;
+  int split = 0;            // 0: one class, 1: two classes, 2: one class per power of two of L
+};
+
+struct PlanClass {
+  int offset = 0, count = 0, max_pool = 0, blocks = 0;
+  uint32_t entries = 0;     // visited-table entries per warp slot
+  size_t smem = 0;
+};
+
+struct PqPlanImpl : RoverPqPlan {
+  uint32_t magic = kPlanMagic;
+  uint64_t epoch = 0;                   // PqDevice::epoch of the index the plan was made on
+  RoverSearchParams p{};
+  int nq = 0, expand = 0, max_pool = 0, max_k = 0, W = 1;
+  bool gated = false, has_topk = false;
+  bool decodable = false;               // decoded rows available for this request
+  bool allow_packed = false, allow_decoded = false;
+  PlanConfig cfg;
+  std::vector<PlanClass> classes;
+  std::vector<int32_t> h_pool, h_order;
+  uint32_t table_scale = 1;             // visited tables grown after an overflow while tuning
+  size_t visited_words = 0;
+  int candidates = 0;
+  float tuned_ms = 0.0f, default_ms = 0.0f;
+  int32_t n_seeds = 0, seed_dups = 0;
+  GateParams gate{};
+  DevBuf pool, topk, order, ctl, visited, seed_ids, seed_bits, recon, recon_norms, seed_dists, seed_rank, gate_buf;
+  size_t device_bytes() const {
+    return pool.bytes + topk.bytes + order.bytes + ctl.bytes + visited.bytes + seed_ids.bytes + seed_bits.bytes +
+           recon.bytes + recon_norms.bytes + seed_dists.bytes + seed_rank.bytes + gate_buf.bytes;
+  }
+  void release() {
+    for (DevBuf* b : {&pool, &topk, &order, &ctl, &visited, &seed_ids, &seed_bits, &recon, &recon_norms, &seed_dists,
+                      &seed_rank, &gate_buf})
+      b->release();
+  }
+};
+
+PqPlanImpl* plan_cast(const RoverPqPlan* p) {
+  auto* q = static_cast<PqPlanImpl*>(const_cast<RoverPqPlan*>(p));
+  return q && q->magic == kPlanMagic ? q : nullptr;
+}
+
+uint32_t ceil_pow2_log(int v) {
+  uint32_t l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+
+// Beam-width classes over the plan's order (widest first).  split 1 picks
+// the power-of-two boundary that minimises the shared memory the queries'
+// slices take (count x widest width of the class); split 2 gives each power
+// of two its own class (the narrowest merged down to kMaxPlanClasses).
+std::vector<PlanClass> plan_classes(const PqPlanImpl& P, int split) {
+  const int nq = P.nq;
+  std::vector<PlanClass> out;
+  auto add = [&](int off, int cnt) {
+    PlanClass c;
+    c.offset = off;
+    c.count = cnt;
+    c.max_pool = P.h_pool[P.h_order[off]];
+    out.push_back(c);
+  };
+  if (split == 0) {
+    add(0, nq);
+    return out;
+  }
+  std::vector<uint32_t> key(nq);
+  const uint32_t top = ceil_pow2_log(P.h_pool[P.h_order[0]]);
+  for (int j = 0; j < nq; ++j) {
+    const uint32_t k = ceil_pow2_log(P.h_pool[P.h_order[j]]);
+    key[j] = std::max(k, top >= kMaxPlanClasses - 1 ? top - (kMaxPlanClasses - 1) : 0u);
+  }
+  if (split == 2) {
+    int off = 0;
+    for (int j = 1; j <= nq; ++j)
+      if (j == nq || key[j] != key[off]) {
+        add(off, j - off);
+        off = j;
+      }
+    return out;
+  }
+  // split 1: one boundary between consecutive keys
+  int best_cut = nq;
+  double best_cost = static_cast<double>(nq) * P.h_pool[P.h_order[0]];
+  for (int j = 1; j < nq; ++j) {
+    if (key[j] == key[j - 1]) continue;
+    const double cost = static_cast<double>(j) * P.h_pool[P.h_order[0]] +
+                        static_cast<double>(nq - j) * P.h_pool[P.h_order[j]];
+    if (cost < best_cost) { best_cost = cost; best_cut = j; }
+  }
+  add(0, best_cut);
+  if (best_cut < nq) add(best_cut, nq - best_cut);
+  return out;
+}
+
+// Arguments shared by every search launch of a plan.
+PqSearchArgs plan_args(const State& s, const PqPlanImpl& P, const float* queries, const RoverSearchOutputs& o) {
+  const PqDevice& pq = s.pq;
+  PqSearchArgs a{};
+  a.ix = pq.view;
+  a.queries = queries;
+  a.nq = P.nq;
+  a.pool_sizes = P.pool.as<int32_t>();
+  a.top_ks = P.has_topk ? P.topk.as<int32_t>() : nullptr;
+  a.top_k = P.p.top_k;
+  a.entry_points = P.p.entry_points;
+  a.graph_entry = pq.graph_entry;
+  a.seed = P.p.seed;
+  a.expand_count = P.p.expand_count;
+  a.correction = P.p.correction;
+  a.refine_budget = P.p.refine_budget;
+  a.max_pool = P.max_pool;
+  a.pool_ids = o.pool_ids;
+  a.pool_dists = o.pool_dists;
+  a.pool_stride = o.pool_ids ? P.p.pool_stride : 0;
+  a.pool_counts = o.pool_counts;
+  a.out_ids = o.ids;
+  a.out_dists = o.dists;
+  a.out_stride = o.out_stride;
+  a.out_counts = o.counts;
+  a.stats = reinterpret_cast<unsigned long long*>(o.stats);
+  a.status = o.status;
+  a.visited = P.visited.as<unsigned long long>();
+  a.gen_dev = &P.ctl.as<PlanControl>()->gen;
+  a.order = P.order.as<int32_t>();
+  return a;
+}
+
+PqDecodedArgs plan_decoded_args(const State& s, const PqPlanImpl& P) {
+  PqDecodedArgs b{};
+  b.decoded = s.pq.decoded.as<float>();
+  b.seed_ids = P.seed_ids.as<int32_t>();
+  b.n_seeds = P.n_seeds;
+  b.seed_dups = P.seed_dups;
+  b.seed_bits = P.seed_bits.as<uint32_t>();
+  b.seed_dists = P.seed_dists.as<float>();
+  return b;
+}
+
+PqBatchArgs plan_batch_args(const PqPlanImpl& P) {
+  PqBatchArgs c{};
+  c.beam_width = P.W;
+  c.gate = P.gate;
+  c.gate.enabled = P.gated ? 1 : 0;
+  c.seed_rank = P.gated ? P.seed_rank.as<float>() : nullptr;
+  return c;
+}
+
+const void* plan_kernel(const State& s, const PqPlanImpl& P, int layout) {
+  const PqDevice& pq = s.pq;
+  if (layout == ROVER_LAYOUT_PACKED)
+    return reinterpret_cast<const void*>(pq_search_kernel_for(pq.view, P.p.correction != 0));
+  if (P.p.mode == ROVER_MODE_EXACT) return reinterpret_cast<const void*>(pq_decoded_kernel_for(pq.view.dim));
+  return reinterpret_cast<const void*>(pq_batched_kernel_for(pq.view.dim, P.gated ? kBatchGated : kBatchFull));
+}
+
+// Shared-memory slice layout of one class (a.max_pool set to its widest beam).
+void plan_layout(const PqPlanImpl& P, int layout, int vis_cap, PqSearchArgs* a, PqDecodedArgs* b, PqBatchArgs* c) {
+  if (layout == ROVER_LAYOUT_PACKED) {
+    pq_search_layout(a, P.p.refine_budget);
+  } else if (P.p.mode == ROVER_MODE_EXACT) {
+    pq_decoded_layout(a, b, P.p.refine_budget, vis_cap);
+  } else {
+    c->short_cap = 2 * a->max_pool;
+    pq_batched_layout(a, b, c, P.p.refine_budget, vis_cap, P.gated);
+  }
+}
+
+// Fixes the classes, launch shapes and visited tables of a configuration.
+// Returns AEE_EBADPARM (with nothing changed) when a slice does not fit.
+AEEResult plan_configure(State& s, PqPlanImpl& P, const PlanConfig& cfg) {
+  const PqDevice& pq = s.pq;
+  const int warps = cfg.layout == ROVER_LAYOUT_PACKED ? kSearchWarps : cfg.warps;
+  std::vector<PlanClass> cls = plan_classes(P, cfg.split);
+  const void* kernel = plan_kernel(s, P, cfg.layout);
+  size_t words = 0, smem_max = 0;
+  for (PlanClass& c : cls) {
+    PqSearchArgs a{};
+    a.ix = pq.view;
+    a.max_pool = c.max_pool;
+    PqDecodedArgs b{};
+    PqBatchArgs bc{};
+    bc.beam_width = P.W;
+    plan_layout(P, cfg.layout, cfg.vis_cap, &a, &b, &bc);
+    c.smem = static_cast<size_t>(a.smem_per_warp) * warps;
+    if (c.smem > 227 * 1024) return AEE_EBADPARM;
+    smem_max = std::max(smem_max, c.smem);
+  }
+  if (allow_smem(kernel, smem_max) != AEE_SUCCESS) return AEE_EFAILED;
+  for (PlanClass& c : cls) {
+    const int max_blocks = resident_blocks(kernel, warps * 32, c.smem, s.sms);
+    c.blocks = std::max(1, std::min(max_blocks, (c.count + warps - 1) / warps));
+    uint64_t est = (2ull * c.max_pool + 64ull) * static_cast<uint64_t>(P.expand);
+    if (cfg.layout == ROVER_LAYOUT_PACKED) est += static_cast<uint64_t>(std::min(P.p.entry_points, pq.view.n));
+    else est *= static_cast<uint64_t>(P.W);
+    c.entries = next_pow2(std::max<uint64_t>(4096, 2 * est) * P.table_scale);
+    words = std::max(words, static_cast<size_t>(c.blocks) * warps * c.entries);
+  }
+  if (words * 8 > P.visited.bytes) {
+    // fresh memory may hold anything a live tag could match: zero it
+    P.visited.release();
+    CK(P.visited.ensure(words * 8));
+    CK(cudaMemsetAsync(P.visited.p, 0, words * 8, s.stream));
+    CK(cudaStreamSynchronize(s.stream));
+  }
+  P.cfg = cfg;
+  P.cfg.warps = warps;
+  P.classes = cls;
+  P.visited_words = words;
+  return AEE_SUCCESS;
+}
+
+bool stream_capturing(cudaStream_t stream) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return cs != cudaStreamCaptureStatusNone;
+}
+
+// The kernels of one plan launch.  No allocation, no host synchronisation.
+AEEResult plan_enqueue(State& s, PqPlanImpl& P, const float* queries, const RoverSearchOutputs& o,
+                       cudaStream_t stream) {
+  const PqDevice& pq = s.pq;
+  const bool timed = !stream_capturing(stream);
+  PlanControl* ctl = P.ctl.as<PlanControl>();
+  const int nclass = static_cast<int>(P.classes.size());
+  {
+    TimedLaunch tl(ROVER_KERNEL_PLAN, stream, timed);
+    launch_plan_prepare(ctl, P.visited.as<unsigned long long>(), P.visited_words, o.status, P.nq, nclass, s.sms,
+                        stream);
+  }
+  CK(cudaGetLastError());
+  ++g_launches;
+  const bool decoded = P.cfg.layout != ROVER_LAYOUT_PACKED;
+  if (decoded && !P.gated) {
+    {
+      TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream, timed);
+      launch_pq_seed_dists(queries, 0, P.nq, pq.view.dim, pq.decoded.as<float>(), P.seed_ids.as<int32_t>(),
+                           P.n_seeds, P.seed_dists.as<float>(), stream);
+    }
+    CK(cudaGetLastError());
+    ++g_launches;
+  }
+  if (decoded && P.gated) {
+    {
+      TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream, timed);
+      launch_pq_seed_rank(queries, 0, P.nq, pq.view.dim, P.recon.as<float>(), P.recon_norms.as<float>(), P.n_seeds,
+                          P.seed_rank.as<float>(), stream);
+    }
+    CK(cudaGetLastError());
+    ++g_launches;
+  }
+  const void* kernel = plan_kernel(s, P, P.cfg.layout);
+  const int threads = P.cfg.warps * 32;
+  for (int ci = 0; ci < nclass; ++ci) {
+    const PlanClass& c = P.classes[ci];
+    PqSearchArgs a = plan_args(s, P, queries, o);
+    a.max_pool = c.max_pool;
+    a.visited_mask = c.entries - 1u;
+    a.next_query = &ctl->counters[ci];
+    PqDecodedArgs b = plan_decoded_args(s, P);
+    PqBatchArgs bc = plan_batch_args(P);
+    plan_layout(P, P.cfg.layout, P.cfg.vis_cap, &a, &b, &bc);
+    if (!decoded) {
+      a.order = P.order.as<int32_t>() + c.offset;
+      a.nq = c.count;
+      TimedLaunch tl(ROVER_KERNEL_PQ_PACKED, stream, timed);
+      reinterpret_cast<PqSearchFn>(const_cast<void*>(kernel))<<<c.blocks, threads, c.smem, stream>>>(a);
+    } else if (P.p.mode == ROVER_MODE_EXACT) {
+      b.q_begin = c.offset;
+      b.q_end = c.offset + c.count;
+      TimedLaunch tl(ROVER_KERNEL_PQ_DECODED, stream, timed);
+      reinterpret_cast<PqDecodedFn>(const_cast<void*>(kernel))<<<c.blocks, threads, c.smem, stream>>>(a, b);
+    } else {
+      b.q_begin = c.offset;
+      b.q_end = c.offset + c.count;
+      TimedLaunch tl(ROVER_KERNEL_PQ_BATCHED, stream, timed);
+      reinterpret_cast<PqBatchFn>(const_cast<void*>(kernel))<<<c.blocks, threads, c.smem, stream>>>(a, b, bc);
+    }
+    CK(cudaGetLastError());
+    ++g_launches;
+  }
+  {
+    TimedLaunch tl(ROVER_KERNEL_PLAN, stream, timed);
+    launch_plan_advance(ctl, P.nq, stream);
+  }
+  CK(cudaGetLastError());
+  ++g_launches;
+  return AEE_SUCCESS;
+}
+
+// Times one configuration on the tuning queries (best of `reps` launches
+// after one warm-up).  *overflow reports a visited-table overflow.
+AEEResult plan_time(State& s, PqPlanImpl& P, const float* queries, const RoverSearchOutputs& o, int reps,
+                    float* best_ms, bool* overflow) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    set_error("cudaEventCreate failed");
+    return AEE_EFAILED;
+  }
+  AEEResult r = AEE_SUCCESS;
+  float best = 0.0f;
+  for (int rep = 0; rep <= reps && r == AEE_SUCCESS; ++rep) {
+    cudaEventRecord(e0, s.stream);
+    r = plan_enqueue(s, P, queries, o, s.stream);
+    cudaEventRecord(e1, s.stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      set_error("plan launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+      r = AEE_EFAILED;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && (best == 0.0f || ms < best)) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  collect_timings();
+  if (r != AEE_SUCCESS) return r;
+  s.h_status.resize(P.nq);
+  CK(cudaMemcpy(s.h_status.data(), o.status, P.nq * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  *overflow = false;
+  for (int i = 0; i < P.nq; ++i) *overflow |= s.h_status[i] == kStatusTableFull;
+  *best_ms = best;
+  return AEE_SUCCESS;
+}
+
+// Copies the entry seeds (and for gated plans their reconstructions and the
+// loaded gate) into plan-owned buffers and sizes the seed-pass outputs.
+AEEResult plan_inputs(State& s, PqPlanImpl& P) {
+  PqDevice& pq = s.pq;
+  if (ensure_seeds(s, pq, P.p.entry_points, P.p.seed) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  const SeedSet& ss = pq.seeds;
+  P.n_seeds = ss.count;
+  P.seed_dups = ss.dups;
+  const size_t bits_bytes = (static_cast<size_t>(pq.view.n) + 31) / 32 * 4;
+  CK(P.seed_ids.ensure(static_cast<size_t>(ss.count) * 4));
+  CK(P.seed_bits.ensure(bits_bytes));
+  CK(cudaMemcpyAsync(P.seed_ids.p, ss.ids.p, static_cast<size_t>(ss.count) * 4, cudaMemcpyDeviceToDevice, s.stream));
+  CK(cudaMemcpyAsync(P.seed_bits.p, ss.bits.p, bits_bytes, cudaMemcpyDeviceToDevice, s.stream));
+  if (!P.allow_decoded) return AEE_SUCCESS;
+  const size_t seed_bytes = static_cast<size_t>(P.nq) * ss.count * sizeof(float);
+  if (seed_bytes > kPlanSeedBytes) {
+    set_error("a plan of %d queries x %d seeds needs %zu bytes of seed distances (limit %zu): use smaller plans",
+              P.nq, ss.count, seed_bytes, kPlanSeedBytes);
+    return AEE_EBADPARM;
+  }
+  if (P.gated) {
+    if (ensure_seed_recon(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
+    const size_t rb = static_cast<size_t>(ss.count) * pq.view.dim * sizeof(float);
+    CK(P.recon.ensure(rb));
+    CK(P.recon_norms.ensure(static_cast<size_t>(ss.count) * sizeof(float)));
+    CK(cudaMemcpyAsync(P.recon.p, ss.recon.p, rb, cudaMemcpyDeviceToDevice, s.stream));
+    CK(cudaMemcpyAsync(P.recon_norms.p, ss.recon_norms.p, static_cast<size_t>(ss.count) * sizeof(float),
+                       cudaMemcpyDeviceToDevice, s.stream));
+    CK(P.seed_rank.ensure(seed_bytes));
+    // the gate's weights move with the plan: rebase its pointers
+    CK(P.gate_buf.ensure(s.gate_buf.bytes));
+    CK(cudaMemcpyAsync(P.gate_buf.p, s.gate_buf.p, s.gate_buf.bytes, cudaMemcpyDeviceToDevice, s.stream));
+    auto rebase = [&](const void* q) {
+      return static_cast<const uint8_t*>(P.gate_buf.p) +
+             (static_cast<const uint8_t*>(q) - static_cast<const uint8_t*>(s.gate_buf.p));
+    };
+    P.gate = s.gate;
+    P.gate.w1t = reinterpret_cast<const uint16_t*>(rebase(s.gate.w1t));
+    P.gate.w2t = reinterpret_cast<const uint16_t*>(rebase(s.gate.w2t));
+    P.gate.w3t = reinterpret_cast<const uint16_t*>(rebase(s.gate.w3t));
+    P.gate.b1 = reinterpret_cast<const float*>(rebase(s.gate.b1));
+    P.gate.b2 = reinterpret_cast<const float*>(rebase(s.gate.b2));
+    P.gate.b3 = reinterpret_cast<const float*>(rebase(s.gate.b3));
+  } else {
+    CK(P.seed_dists.ensure(seed_bytes));
+  }
+  CK(cudaStreamSynchronize(s.stream));
+  return AEE_SUCCESS;
+}
+
+// Validates a plan request and fills everything but the configuration.
+AEEResult plan_setup(State& s, PqPlanImpl& P, const RoverSearchParams* p, int32_t nq, const int32_t* pool_sizes,
+                     const int32_t* top_ks) {
+  PqDevice& pq = s.pq;
+  if (!pq.loaded || !pq.has_graph) { set_error("no PQ index with a graph is loaded"); return AEE_EFAILED; }
+  if (!valid_params(p) || nq <= 0 || nq > kPlanMaxQueries || !pool_sizes) {
+    set_error("plan: invalid parameters or query count (1..%d)", kPlanMaxQueries);
+    return AEE_EBADPARM;
+  }
+  P.p = *p;
+  P.nq = nq;
+  P.epoch = pq.epoch;
+  P.h_pool.assign(pool_sizes, pool_sizes + nq);
+  P.max_pool = 0;
+  for (int32_t v : P.h_pool) {
+    if (v <= 0 || v > 4096) { set_error("pool sizes must be in 1..4096"); return AEE_EBADPARM; }
+    P.max_pool = std::max(P.max_pool, v);
+  }
+  P.has_topk = top_ks != nullptr;
+  P.max_k = p->top_k;
+  if (top_ks) {
+    P.max_k = 0;
+    for (int i = 0; i < nq; ++i) P.max_k = std::max(P.max_k, top_ks[i]);
+  }
+  if (p->correction && pq.view.residual_bits == 0) { set_error("correction needs residuals"); return AEE_EBADPARM; }
+  if (p->refine_budget > 0 && pq.view.residual_bits == 0) { set_error("refine needs residuals"); return AEE_EBADPARM; }
+  P.expand = std::min(p->expand_count, pq.view.degree);
+  if (P.expand > kMaxBatch) { set_error("expand_count above %d", kMaxBatch); return AEE_EBADPARM; }
+  P.decodable = p->correction != 0 && pq.view.dim % 4 == 0;
+  if (p->mode == ROVER_MODE_EXACT) {
+    P.allow_packed = p->layout != ROVER_LAYOUT_DECODED;
+    P.allow_decoded = P.decodable && p->layout != ROVER_LAYOUT_PACKED;
+    if (p->layout == ROVER_LAYOUT_DECODED && !P.decodable) {
+      set_error("the decoded layout needs correction on and dim %% 4 == 0");
+      return AEE_EBADPARM;
+    }
+  } else if (p->mode == ROVER_MODE_BATCHED || p->mode == ROVER_MODE_GATED) {
+    if (!P.decodable || p->layout == ROVER_LAYOUT_PACKED) {
+      set_error("batched and gated plans need correction on, decoded rows and dim %% 4 == 0");
+      return AEE_EBADPARM;
+    }
+    P.allow_decoded = true;
+    P.gated = p->mode == ROVER_MODE_GATED && s.gate.enabled;
+    P.W = p->beam_width;
+    if (P.W == 0) P.W = std::max(1, std::min(kMaxBeamWidth, kMaxBatchIds / std::max(1, P.expand)));
+    if (P.expand > 2 * 32 || P.W < 1 || P.W > kMaxBeamWidth || P.W * P.expand > kMaxBatchIds) {
+      set_error("batched plan: need expand_count <= 64 and beam_width 1..%d with beam_width * expand_count <= %d",
+                kMaxBeamWidth, kMaxBatchIds);
+      return AEE_EBADPARM;
+    }
+  } else {
+    set_error("unknown mode %d", p->mode);
+    return AEE_EBADPARM;
+  }
+  if (P.allow_decoded) {
+    bool ok = false;
+    if (ensure_decoded(s, pq, &ok) != AEE_SUCCESS) return AEE_EFAILED;
+    if (!ok) {
+      if (!P.allow_packed) { set_error("decoded rows do not fit in device memory"); return AEE_ENOMEMORY; }
+      P.allow_decoded = false;
+    }
+  }
+  // widest beams first: each class is a contiguous run, and inside a class
+  // the longest searches start first
+  P.h_order.resize(nq);
+  for (int i = 0; i < nq; ++i) P.h_order[i] = i;
+  std::stable_sort(P.h_order.begin(), P.h_order.end(),
+                   [&](int32_t x, int32_t y) { return P.h_pool[x] > P.h_pool[y]; });
+  if (upload(P.pool, P.h_pool.data(), nq, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  if (upload(P.order, P.h_order.data(), nq, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  if (top_ks && upload(P.topk, top_ks, nq, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  CK(P.ctl.ensure(sizeof(PlanControl)));
+  PlanControl c0{};
+  c0.gen = 1u;
+  CK(cudaMemcpyAsync(P.ctl.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+  return plan_inputs(s, P);
+}
+
+}  // namespace
+
+extern "C" AEEResult calculator_rover_pq_plan_create(remote_handle64 h, const RoverSearchParams* p, int32_t nq,
+                                                     const int32_t* pool_sizes, const int32_t* top_ks,
+                                                     const float* tune_queries, RoverPqPlan** plan) {
+  (void)h;
+  if (!plan) return AEE_EBADPARM;
+  *plan = nullptr;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  auto* P = new (std::nothrow) PqPlanImpl();
+  if (!P) return AEE_ENOMEMORY;
+  auto fail = [&](AEEResult r) {
+    P->release();
+    P->magic = 0;
+    delete P;
+    return r;
+  };
+  AEEResult r = plan_setup(s, *P, p, nq, pool_sizes, top_ks);
+  if (r != AEE_SUCCESS) return fail(r);
+  PlanConfig def;
+  def.layout = P->allow_decoded ? ROVER_LAYOUT_DECODED : ROVER_LAYOUT_PACKED;
+  if (!tune_queries) {
+    r = plan_configure(s, *P, def);
+    if (r == AEE_EBADPARM) set_error("shared memory slices too large for pool %d", P->max_pool);
+    if (r != AEE_SUCCESS) return fail(r);
+    *plan = P;
+    return AEE_SUCCESS;
+  }
+  if (P->allow_decoded && reinterpret_cast<uintptr_t>(tune_queries) % 16 != 0) {
+    set_error("queries must be 16-byte aligned");
+    return fail(AEE_EBADPARM);
+  }
+  // tuning outputs
+  DevBuf ids, dists, counts, status;
+  const int k = std::max(1, P->max_k);
+  auto free_out = [&]() { ids.release(); dists.release(); counts.release(); status.release(); };
+  if (ids.ensure(static_cast<size_t>(nq) * k * 4) != cudaSuccess ||
+      dists.ensure(static_cast<size_t>(nq) * k * 4) != cudaSuccess || counts.ensure(static_cast<size_t>(nq) * 4) ||
+      status.ensure(static_cast<size_t>(nq) * 4)) {
+    free_out();
+    set_error("out of device memory for the tuning outputs");
+    return fail(AEE_ENOMEMORY);
+  }
+  RoverSearchOutputs o{};
+  o.ids = ids.as<int32_t>();
+  o.dists = dists.as<float>();
+  o.counts = counts.as<int32_t>();
+  o.out_stride = k;
+  o.status = status.as<int32_t>();
+  std::vector<PlanConfig> space;
+  for (int layout : {ROVER_LAYOUT_DECODED, ROVER_LAYOUT_PACKED}) {
+    if (layout == ROVER_LAYOUT_DECODED && !P->allow_decoded) continue;
+    if (layout == ROVER_LAYOUT_PACKED && !P->allow_packed) continue;
+    for (int split : {0, 1, 2}) {
+      if (layout == ROVER_LAYOUT_PACKED) {
+        PlanConfig c;
+        c.layout = layout;
+        c.split = split;
+        space.push_back(c);
+        continue;
+      }
+      for (int warps : {2, 4, 8})
+        for (int vis : {1024, 2048, 4096}) {
+          PlanConfig c;
+          c.layout = layout;
+          c.warps = warps;
+          c.vis_cap = vis;
+          c.split = split;
+          space.push_back(c);
+        }
+    }
+  }
+  // the default first, so that its time is reported
+  std::stable_sort(space.begin(), space.end(), [&](const PlanConfig& x, const PlanConfig& y) {
+    const bool dx = x.layout == def.layout && x.warps == def.warps && x.vis_cap == def.vis_cap && x.split == 0;
+    const bool dy = y.layout == def.layout && y.warps == def.warps && y.vis_cap == def.vis_cap && y.split == 0;
+    return dx && !dy;
+  });
+  PlanConfig best;
+  float best_ms = 0.0f;
+  int tried = 0;
+  for (const PlanConfig& c : space) {
+    r = plan_configure(s, *P, c);
+    if (r == AEE_EBADPARM) continue;   // slices do not fit
+    if (r != AEE_SUCCESS) { free_out(); return fail(r); }
+    float ms = 0.0f;
+    bool overflow = false;
+    for (int grow = 0; grow < 3; ++grow) {
+      r = plan_time(s, *P, tune_queries, o, 2, &ms, &overflow);
+      if (r != AEE_SUCCESS) { free_out(); return fail(r); }
+      if (!overflow) break;
+      P->table_scale *= 4;
+      r = plan_configure(s, *P, c);
+      if (r != AEE_SUCCESS) { free_out(); return fail(r == AEE_EBADPARM ? AEE_ENOMEMORY : r); }
+    }
+    if (overflow) continue;
+    ++tried;
+    if (tried == 1) P->default_ms = ms;
+    if (best_ms == 0.0f || ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  free_out();
+  if (tried == 0) {
+    set_error("no plan configuration fits (pool %d)", P->max_pool);
+    return fail(AEE_EBADPARM);
+  }
+  // keep the winner's tables only
+  P->visited.release();
+  r = plan_configure(s, *P, best);
+  if (r != AEE_SUCCESS) return fail(r);
+  P->candidates = tried;
+  P->tuned_ms = best_ms;
+  *plan = P;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_pq_plan_create_fixed(remote_handle64 h, const RoverSearchParams* p,
+                                                           int32_t nq, const int32_t* pool_sizes,
+                                                           const int32_t* top_ks, const RoverPlanConfig* config,
+                                                           RoverPqPlan** plan) {
+  (void)h;
+  if (!plan || !config) return AEE_EBADPARM;
+  *plan = nullptr;
+  const RoverPlanConfig& k = *config;
+  const bool pow2 = k.shared_visited_slots >= 256 && k.shared_visited_slots <= 8192 &&
+                    (k.shared_visited_slots & (k.shared_visited_slots - 1)) == 0;
+  if ((k.layout != ROVER_LAYOUT_PACKED && k.layout != ROVER_LAYOUT_DECODED) || k.class_split < 0 ||
+      k.class_split > 2 || (k.layout == ROVER_LAYOUT_DECODED && (!pow2 || k.warps_per_cta < 1 ||
+                                                                 k.warps_per_cta > kMaxSearchWarps))) {
+    set_error("plan configuration out of range");
+    return AEE_EBADPARM;
+  }
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  auto* P = new (std::nothrow) PqPlanImpl();
+  if (!P) return AEE_ENOMEMORY;
+  auto fail = [&](AEEResult r) {
+    P->release();
+    P->magic = 0;
+    delete P;
+    return r;
+  };
+  AEEResult r = plan_setup(s, *P, p, nq, pool_sizes, top_ks);
+  if (r != AEE_SUCCESS) return fail(r);
+  if ((k.layout == ROVER_LAYOUT_PACKED && !P->allow_packed) || (k.layout == ROVER_LAYOUT_DECODED && !P->allow_decoded)) {
+    set_error("this request cannot run the %s layout", k.layout == ROVER_LAYOUT_PACKED ? "packed" : "decoded");
+    return fail(AEE_EBADPARM);
+  }
+  PlanConfig c;
+  c.layout = k.layout;
+  c.warps = k.layout == ROVER_LAYOUT_PACKED ? kSearchWarps : k.warps_per_cta;
+  c.vis_cap = k.layout == ROVER_LAYOUT_PACKED ? kSharedVisitedSlots : k.shared_visited_slots;
+  c.split = k.class_split;
+  r = plan_configure(s, *P, c);
+  if (r == AEE_EBADPARM) set_error("shared memory slices too large for pool %d", P->max_pool);
+  if (r != AEE_SUCCESS) return fail(r);
+  *plan = P;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_pq_plan_launch(RoverPqPlan* plan, const float* queries,
+                                                     const RoverSearchOutputs* out, void* stream) {
+  PqPlanImpl* P = plan_cast(plan);
+  if (!P || !queries || !out || !out->status || (out->ids && !out->counts)) return AEE_EBADPARM;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (!s.pq.loaded || s.pq.epoch != P->epoch) {
+    set_error("the index this plan was made on is no longer loaded");
+    return AEE_EFAILED;
+  }
+  if (P->cfg.layout != ROVER_LAYOUT_PACKED && reinterpret_cast<uintptr_t>(queries) % 16 != 0) {
+    set_error("queries must be 16-byte aligned");
+    return AEE_EBADPARM;
+  }
+  cudaStream_t strm = stream ? static_cast<cudaStream_t>(stream) : s.stream;
+  return plan_enqueue(s, *P, queries, *out, strm);
+}
+
+extern "C" AEEResult calculator_rover_pq_plan_describe(const RoverPqPlan* plan, RoverPlanInfo* info) {
+  const PqPlanImpl* P = plan_cast(plan);
+  if (!P || !info) return AEE_EBADPARM;
+  RoverPlanInfo r{};
+  r.num_queries = P->nq;
+  r.mode = P->p.mode;
+  r.layout = P->cfg.layout;
+  r.warps_per_cta = P->cfg.warps;
+  r.shared_visited_slots = P->cfg.layout == ROVER_LAYOUT_PACKED ? 0 : P->cfg.vis_cap;
+  r.classes = static_cast<int32_t>(P->classes.size());
+  const bool decoded = P->cfg.layout != ROVER_LAYOUT_PACKED;
+  r.launches = 2 + (decoded ? 1 : 0) + r.classes;
+  r.candidates = P->candidates;
+  r.max_pool = P->max_pool;
+  r.beam_width = P->p.mode == ROVER_MODE_EXACT ? 0 : P->W;
+  for (int i = 0; i < r.classes && i < ROVER_PLAN_MAX_CLASSES; ++i) {
+    r.class_pool[i] = P->classes[i].max_pool;
+    r.class_queries[i] = P->classes[i].count;
+    r.class_blocks[i] = P->classes[i].blocks;
+  }
+  r.tuned_ms = P->tuned_ms;
+  r.default_ms = P->default_ms;
+  r.device_bytes = static_cast<int64_t>(P->device_bytes());
+  r.class_split = P->cfg.split;
+  *info = r;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_pq_plan_destroy(RoverPqPlan* plan) {
+  PqPlanImpl* P = plan_cast(plan);
+  if (!P) return AEE_EBADPARM;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  P->release();
+  P->magic = 0;
+  delete P;
+  return AEE_SUCCESS;
 }
 
 static_assert(sizeof(RoverGateTraceRow) == sizeof(GateTraceRow), "trace row layout");
@@ -1889,8 +2617,7 @@ extern "C" AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const
   const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, max_pool); return AEE_EBADPARM; }
   const PqSearchFn kernel = pq_search_kernel_for(pq.view, p->correction != 0);
-  CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          static_cast<int>(smem)));
+  if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
 
   // Visited-table geometry: the same per-slot capacity rule as the
   // allocating path; the number of warp slots is what fits in the array.

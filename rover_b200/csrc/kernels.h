@@ -8,7 +8,8 @@
 
 namespace rover {
 
-constexpr int kSearchWarps = 4;   // query warps per CTA
+constexpr int kSearchWarps = 4;   // query warps per CTA (default)
+constexpr int kMaxSearchWarps = 8;  // decoded / batched kernels take 1..8 warps per CTA (blockDim.x / 32)
 constexpr int kMaxBatch = 128;    // max neighbours scored per expansion
 
 struct PqSearchArgs {
@@ -33,6 +34,8 @@ struct PqSearchArgs {
   unsigned long long* visited;   // per warp slot: visited_mask + 1 entries
   uint32_t visited_mask;
   uint32_t gen_base;             // generation of query 0 (queries use gen_base + qi)
+  const uint32_t* gen_dev;       // when set, the generation base is read here (plans: replays advance it)
+  const int32_t* order;          // when set, claimed work item j serves query order[j]
   unsigned int* next_query;      // work counter, zero at launch
   // shared-memory layout per warp
   int32_t smem_per_warp, smem_query_bytes, smem_refine_offset, refine_capacity;
@@ -175,6 +178,30 @@ void launch_pq_seed_recon(const PqIndexView& ix, const int32_t* seed_ids, int n_
 // out[q - q_begin][u] = |q|^2 + |x~_u|^2 - 2 q . x~_u.  dim % 4 == 0.
 void launch_pq_seed_rank(const float* queries, int q_begin, int q_end, int dim, const float* rows, const float* norms,
                          int n_seeds, float* out, cudaStream_t s);
+
+// ---- search plans (plan.cu) --------------------------------------------------
+//
+// A plan replays the same searches on new query vectors, possibly from a
+// captured CUDA graph, so the per-launch bookkeeping lives on the device: the
+// generation base of the launch's visited-table tags, a flag asking for the
+// tables to be cleared when the next launch's tags would wrap, and one work
+// counter per beam-width class.
+
+constexpr int kMaxPlanClasses = 8;
+
+struct PlanControl {
+  uint32_t gen;                          // generation of query 0 in the next launch
+  uint32_t clear;                        // 1: zero the visited tables before the next launch
+  uint32_t counters[kMaxPlanClasses];    // work counters of the class launches
+};
+
+// Zeroes the class counters and status[0, nq), and the visited tables when
+// ctl->clear is set.
+void launch_plan_prepare(PlanControl* ctl, unsigned long long* visited, size_t visited_words, int32_t* status, int nq,
+                         int classes, int sms, cudaStream_t s);
+// Moves ctl->gen past this launch's nq generations; asks for a clear when
+// the next launch's generations would pass 2^32 - 1.
+void launch_plan_advance(PlanControl* ctl, int nq, cudaStream_t s);
 
 // ---- gate training (gate_train.cu) ------------------------------------------
 void launch_gate_stats(const float* x, int64_t n, double* acc, cudaStream_t s);

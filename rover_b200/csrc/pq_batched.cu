@@ -192,7 +192,7 @@ __device__ __forceinline__ bool in_list(const uint64_t* list, int size, uint64_t
 }  // namespace
 
 template <int D, int KIND>
-__global__ void __launch_bounds__(kSearchWarps * 32, 4)
+__global__ void __launch_bounds__(kMaxSearchWarps * 32, 16 / kMaxSearchWarps)
 pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
   constexpr bool kGated = KIND == kBatchGated;
   constexpr bool tracing = KIND == kBatchTrace;   // trace rows (full correction, beam width 1)
@@ -210,7 +210,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
   uint64_t* shortl = adc_rows ? reinterpret_cast<uint64_t*>(base + c.smem_short_offset) : nullptr;
   uint32_t* feat = kGated ? reinterpret_cast<uint32_t*>(base + c.smem_feat_offset) : nullptr;
   float* logits = kGated ? reinterpret_cast<float*>(base + c.smem_logit_offset) : nullptr;
-  const int slot = blockIdx.x * kSearchWarps + warp;
+  const int slot = blockIdx.x * (blockDim.x >> 5) + warp;   // warps per CTA: set at launch
   VisitedTable vt;
   vt.slots = a.visited + static_cast<size_t>(slot) * (a.visited_mask + 1ull);
   vt.mask = a.visited_mask;
@@ -220,10 +220,13 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
   const int W = c.beam_width;
 
   for (;;) {
-    int qi = 0;
-    if (lane == 0) qi = b.q_begin + static_cast<int>(atomicAdd(a.next_query, 1u));
-    qi = __shfl_sync(kFullMask, qi, 0);
-    if (qi >= b.q_end) break;
+    int item = 0;
+    if (lane == 0) item = b.q_begin + static_cast<int>(atomicAdd(a.next_query, 1u));
+    item = __shfl_sync(kFullMask, item, 0);
+    if (item >= b.q_end) break;
+    // with an order, items index it and the seed rows cover every query
+    const int qi = a.order ? __ldg(a.order + item) : item;
+    const size_t seed_row = static_cast<size_t>(a.order ? qi : qi - b.q_begin) * b.n_seeds;
 
     const int cap = a.pool_sizes[qi];
     int32_t* status = a.status + qi;
@@ -271,7 +274,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFullMask, lmax, off));
       check_adc = !(lmax <= adc_bound);
     }
-    vt.gen = a.gen_base + static_cast<uint32_t>(qi);
+    vt.gen = (a.gen_dev ? *a.gen_dev : a.gen_base) + static_cast<uint32_t>(qi);
     int size = 0, cursor = 0;
     unsigned long long scored = static_cast<unsigned long long>(b.n_seeds), corrected = 0, expanded = 0;
     unsigned long long dedup = lane == 0 ? static_cast<unsigned long long>(b.seed_dups) : 0ull;
@@ -281,7 +284,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
     // ---- ADC shortlist of the seeds (gated search, traces)
     if (adc_rows) {
       const int scap = min(c.short_cap, 2 * cap);
-      const float* arow = c.seed_rank + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
+      const float* arow = c.seed_rank + seed_row;
       int dummy = 0;
       const SeedRowKeys rk{arow, b.seed_ids};
       if (!(scap <= kMaxBatch ? select_top_lanes(shortl, &ssize, scap, stage, b.n_seeds, rk, &dummy, lane)
@@ -292,7 +295,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
     if (!kGated) {
       // ---- exact seed pool from the all-seeds distance pass
       corrected = static_cast<unsigned long long>(b.n_seeds);
-      const float* drow = b.seed_dists + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
+      const float* drow = b.seed_dists + seed_row;
       if (st == kStatusOk &&
           !(cap <= kMaxBatch
                 ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)

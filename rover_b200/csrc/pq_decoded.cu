@@ -324,7 +324,7 @@ __device__ __forceinline__ bool decoded_dist(const float* __restrict__ xrow, con
 }
 
 template <int D>
-__global__ void __launch_bounds__(kSearchWarps * 32, 4)
+__global__ void __launch_bounds__(kMaxSearchWarps * 32, 16 / kMaxSearchWarps)
 pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5;
@@ -336,7 +336,7 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
   int32_t* batch = reinterpret_cast<int32_t*>(stage + kMaxBatch);
   uint32_t* vis = reinterpret_cast<uint32_t*>(base + b.smem_vis_offset);
   const uint32_t vmask = static_cast<uint32_t>(b.vis_cap - 1);
-  const int slot = blockIdx.x * kSearchWarps + warp;
+  const int slot = blockIdx.x * (blockDim.x >> 5) + warp;   // warps per CTA: set at launch
   VisitedTable vt;
   vt.slots = a.visited + static_cast<size_t>(slot) * (a.visited_mask + 1ull);
   vt.mask = a.visited_mask;
@@ -345,10 +345,13 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
   const float adc_bound = FLT_MAX / static_cast<float>(2 * ix.m);
 
   for (;;) {
-    int qi = 0;
-    if (lane == 0) qi = b.q_begin + static_cast<int>(atomicAdd(a.next_query, 1u));
-    qi = __shfl_sync(kFullMask, qi, 0);
-    if (qi >= b.q_end) break;
+    int item = 0;
+    if (lane == 0) item = b.q_begin + static_cast<int>(atomicAdd(a.next_query, 1u));
+    item = __shfl_sync(kFullMask, item, 0);
+    if (item >= b.q_end) break;
+    // with an order, items index it and the seed rows cover every query
+    const int qi = a.order ? __ldg(a.order + item) : item;
+    const size_t seed_row = static_cast<size_t>(a.order ? qi : qi - b.q_begin) * b.n_seeds;
 
     const int cap = a.pool_sizes[qi];
     int32_t* status = a.status + qi;
@@ -389,14 +392,14 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
       for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFullMask, lmax, off));
       check_adc = !(lmax <= adc_bound);
     }
-    vt.gen = a.gen_base + static_cast<uint32_t>(qi);
+    vt.gen = (a.gen_dev ? *a.gen_dev : a.gen_base) + static_cast<uint32_t>(qi);
     int size = 0, cursor = 0;
     unsigned long long scored = static_cast<unsigned long long>(b.n_seeds), expanded = 0;
     unsigned long long dedup = lane == 0 ? static_cast<unsigned long long>(b.seed_dups) : 0ull;
     int32_t st = kStatusOk;
 
     // ---- initial pool: top-L of the seed row under (distance, id)
-    const float* drow = b.seed_dists + static_cast<size_t>(qi - b.q_begin) * b.n_seeds;
+    const float* drow = b.seed_dists + seed_row;
     if (!(cap <= kMaxBatch
               ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)
               : select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)))

@@ -66,10 +66,11 @@ pq_search_kernel_t(PqSearchArgs a) {
   const PqIndexView& ix = a.ix;
 
   for (;;) {
-    int qi = 0;
-    if (lane == 0) qi = static_cast<int>(atomicAdd(a.next_query, 1u));
-    qi = __shfl_sync(kFullMask, qi, 0);
-    if (qi >= a.nq) break;
+    int item = 0;
+    if (lane == 0) item = static_cast<int>(atomicAdd(a.next_query, 1u));
+    item = __shfl_sync(kFullMask, item, 0);
+    if (item >= a.nq) break;
+    const int qi = a.order ? __ldg(a.order + item) : item;
 
     const int cap = a.pool_sizes[qi];
     int32_t* status = a.status + qi;
@@ -98,7 +99,7 @@ pq_search_kernel_t(PqSearchArgs a) {
       if (lane == 0) *status = kStatusNumeric;
       continue;
     }
-    vt.gen = a.gen_base + static_cast<uint32_t>(qi);
+    vt.gen = (a.gen_dev ? *a.gen_dev : a.gen_base) + static_cast<uint32_t>(qi);
     int size = 0, cursor = 0;
     unsigned long long scored = 0, expanded = 0, dedup = 0;
     int32_t st = kStatusOk;

@@ -1,0 +1,202 @@
+"""Search plans (calculator_rover_pq_plan_*): thousands of queries with uneven
+beam widths and result counts served by a fixed kernel sequence that a CUDA
+graph can capture.
+
+* every configuration the tuner chooses from (layout, warps per CTA,
+  shared-memory visited slots, beam-width classes) returns exactly what
+  calculator_rover_pq_search returns for the same queries;
+* a tuned plan times its candidates and keeps one of them;
+* a CUDA graph captured from one plan launch, replayed on new query vectors
+  written into the same buffer, returns each set's direct-search results
+  (the visited-table generations advance on the device between replays);
+* batched and gated plans match the direct batched and gated searches;
+* a plan refuses to launch once its index has been unloaded.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from test_gpu_parity import _random_pq_index, rows_equal
+
+pytestmark = pytest.mark.gpu
+
+PACKED, DECODED = 1, 2
+KW = dict(entry_points=64, expand_count=24, correction=1, refine_budget=200)
+
+
+def _uneven(nq, seed=3, lo=16, hi=512):
+    """Beam widths log-uniform in [lo, hi], k uniform in {1, 10, 100}, L >= k."""
+    rng = np.random.default_rng(seed)
+    L = np.exp(rng.uniform(np.log(lo), np.log(hi), nq)).astype(np.int32)
+    k = rng.choice([1, 10, 100], nq).astype(np.int32)
+    return np.maximum(L, k).astype(np.int32), k
+
+
+def _outputs(torch, nq, k, pool_stride):
+    dev = torch.device("cuda", 0)
+    return dict(ids=torch.full((nq, k), -1, dtype=torch.int32, device=dev),
+                dists=torch.zeros((nq, k), dtype=torch.float32, device=dev),
+                counts=torch.zeros(nq, dtype=torch.int32, device=dev),
+                pool_ids=torch.full((nq, pool_stride), -1, dtype=torch.int32, device=dev),
+                pool_dists=torch.zeros((nq, pool_stride), dtype=torch.float32, device=dev),
+                pool_counts=torch.zeros(nq, dtype=torch.int32, device=dev),
+                stats=torch.zeros((nq, 4), dtype=torch.int64, device=dev),
+                status=torch.full((nq,), 99, dtype=torch.int32, device=dev))
+
+
+def _ptrs(o, k):
+    d = {key: t.data_ptr() for key, t in o.items()}
+    d["stride"] = k
+    return d
+
+
+def _host(o):
+    r = {key: t.cpu().numpy() for key, t in o.items()}
+    r["stats"] = r["stats"].view(np.uint64)
+    return r
+
+
+def _same(r, ref):
+    assert np.all(r["status"] == 0)
+    rows_equal(r["ids"], r["dists"], r["counts"], ref["ids"], ref["dists"], ref["counts"])
+    rows_equal(r["pool_ids"], r["pool_dists"], r["pool_counts"], ref["pool_ids"], ref["pool_dists"],
+               ref["pool_counts"])
+    assert np.array_equal(r["stats"], ref["stats"])
+
+
+def _direct(calc, queries, pools, ks, stride, **kw):
+    return calc.pq_search(queries, pools, top_k=10, top_ks=ks, pool_stride=stride, **{**KW, **kw})
+
+
+def _run_plan(torch, plan, q_dev, nq, k, stride):
+    o = _outputs(torch, nq, k, stride)
+    plan.launch(q_dev.data_ptr(), _ptrs(o, k), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return _host(o)
+
+
+CONFIGS = [(PACKED, 4, 2048, s) for s in (0, 1, 2)] + \
+          [(DECODED, w, v, s) for w in (2, 4, 8) for v in (1024, 4096) for s in (0, 1, 2)]
+
+
+def test_every_plan_configuration_matches_direct_search(calc):
+    import torch
+    d = _random_pq_index()
+    calc.pq_load(d["graph"], d["entry"], d["bundle"])
+    queries = d["queries"]
+    nq = len(queries)
+    pools, ks = _uneven(nq)
+    stride = int(pools.max())
+    ref = _direct(calc, queries, pools, ks, stride)
+    q_dev = torch.from_numpy(np.ascontiguousarray(queries)).cuda()
+    for cfg in CONFIGS:
+        plan = calc.pq_plan(nq, pools, top_ks=ks, config=cfg, pool_stride=stride, **KW)
+        info = plan.describe()
+        assert (info["layout"], info["class_split"]) == (cfg[0], cfg[3])
+        assert sum(info["class_queries"]) == nq
+        assert info["class_pool"][0] == stride          # widest class first
+        r = _run_plan(torch, plan, q_dev, nq, int(ks.max()), stride)
+        _same(r, ref)
+        plan.destroy()
+
+
+def test_tuned_plan_keeps_a_timed_candidate(calc):
+    import torch
+    d = _random_pq_index()
+    calc.pq_load(d["graph"], d["entry"], d["bundle"])
+    queries = d["queries"]
+    nq = len(queries)
+    pools, ks = _uneven(nq, seed=4)
+    stride = int(pools.max())
+    q_dev = torch.from_numpy(np.ascontiguousarray(queries)).cuda()
+    plan = calc.pq_plan(nq, pools, top_ks=ks, tune_queries_ptr=q_dev.data_ptr(), pool_stride=stride, **KW)
+    info = plan.describe()
+    assert info["candidates"] >= 10
+    assert 0 < info["tuned_ms"] <= info["default_ms"]
+    assert info["launches"] == 2 + (info["layout"] == DECODED) + info["classes"]
+    _same(_run_plan(torch, plan, q_dev, nq, int(ks.max()), stride), _direct(calc, queries, pools, ks, stride))
+    plan.destroy()
+
+
+def test_graph_replays_serve_new_queries(calc):
+    import torch
+    d = _random_pq_index()
+    calc.pq_load(d["graph"], d["entry"], d["bundle"])
+    base_q = d["queries"]
+    nq = len(base_q)
+    pools, ks = _uneven(nq, seed=5)
+    stride, k = int(pools.max()), int(ks.max())
+    q_dev = torch.from_numpy(np.ascontiguousarray(base_q)).cuda()
+    plan = calc.pq_plan(nq, pools, top_ks=ks, tune_queries_ptr=q_dev.data_ptr(), pool_stride=stride, **KW)
+    o = _outputs(torch, nq, k, stride)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):          # one eager launch on the capture stream first
+        plan.launch(q_dev.data_ptr(), _ptrs(o, k), s.cuda_stream)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        plan.launch(q_dev.data_ptr(), _ptrs(o, k), torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(9)
+    sets = [base_q[rng.permutation(nq)], base_q + rng.normal(0, 0.05, base_q.shape).astype(np.float32), base_q]
+    for qs in sets:
+        qs = np.ascontiguousarray(qs, dtype=np.float32)
+        q_dev.copy_(torch.from_numpy(qs))
+        for t in o.values():
+            t.fill_(-7)
+        g.replay()
+        torch.cuda.synchronize()
+        _same(_host(o), _direct(calc, qs, pools, ks, stride))
+    del g
+    plan.destroy()
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_batched_and_gated_plans_match_direct_search(calc, mode):
+    import torch
+
+    from rover_b200.calculator import GATE_PARAMS
+    d = _random_pq_index()
+    calc.pq_load(d["graph"], d["entry"], d["bundle"])
+    queries = d["queries"]
+    nq = len(queries)
+    pools, ks = _uneven(nq, seed=6, hi=256)
+    stride, k = int(pools.max()), int(ks.max())
+    kw = dict(KW, mode=mode, beam_width=2)
+    if mode == 2:
+        # an untrained gate still decides deterministically; the band sends
+        # part of the shortlist through the network and the stop head acts
+        rng = np.random.default_rng(2)
+        params = rng.normal(0, 0.3, GATE_PARAMS).astype(np.float32)
+        calc.gate_load(params, np.zeros(5, np.float32), np.ones(5, np.float32), band_lo=0.9, band_hi=1.1,
+                       refine_logit=0.0, stop_logit=3.0)
+    try:
+        ref = _direct(calc, queries, pools, ks, stride, **kw)
+        q_dev = torch.from_numpy(np.ascontiguousarray(queries)).cuda()
+        plan = calc.pq_plan(nq, pools, top_ks=ks, tune_queries_ptr=q_dev.data_ptr(), pool_stride=stride, **kw)
+        info = plan.describe()
+        assert info["mode"] == mode and info["beam_width"] == 2
+        _same(_run_plan(torch, plan, q_dev, nq, k, stride), ref)
+        plan.destroy()
+    finally:
+        if mode == 2:
+            calc.gate_unload()
+
+
+def test_plan_refuses_a_replaced_index(calc):
+    import torch
+    from rover_b200.calculator import CalculatorError
+    d = _random_pq_index()
+    calc.pq_load(d["graph"], d["entry"], d["bundle"])
+    nq = 8
+    q_dev = torch.from_numpy(np.ascontiguousarray(d["queries"][:nq])).cuda()
+    plan = calc.pq_plan(nq, 32, pool_stride=32, **KW)
+    o = _outputs(torch, nq, 10, 32)
+    plan.launch(q_dev.data_ptr(), _ptrs(o, 10))
+    torch.cuda.synchronize()
+    calc.pq_load(d["graph"], d["entry"], d["bundle"])      # same data, new device copy
+    with pytest.raises(CalculatorError):
+        plan.launch(q_dev.data_ptr(), _ptrs(o, 10))
+    plan.destroy()
