@@ -296,6 +296,12 @@ typedef struct RoverGateThresholds {
 AEEResult calculator_rover_gate_load(remote_handle64 h, const float *params, const float *mu,
                                      const float *sigma, const RoverGateThresholds *thresholds);
 AEEResult calculator_rover_gate_unload(remote_handle64 h);
+/* The loaded gate's logits [n][2] (refine-needed, stop-expanding) for raw
+ * rows [n][5] = {quantized distance, pool rank / L, worst pool distance,
+ * hop count / L, query norm} (host buffers), computed by the same device
+ * code the gated search runs (log of the two distances, standardisation,
+ * BF16 tensor-core tiles). */
+AEEResult calculator_rover_gate_eval(remote_handle64 h, const float *rows, int64_t n, float *logits);
 
 /* One training row per scored candidate or expansion source. */
 typedef struct RoverGateTraceRow {

@@ -1,0 +1,107 @@
+/*
+ * rover_host.h -- the C host side of the B200 search path: Rover's index
+ * bundle loader and its checks, and the vector / graph file readers the
+ * `Rover search` command uses (librover_host.so, built with the `Rover`
+ * executable).
+ *
+ * The reference prepares and validates a bundle in Python
+ * (tools/index_bundle.py:187-226 validate, :229-345 prepare) and loads its
+ * members in C (src/dsp_demo/retrieval_pq_artifact.c:886-958 for .pqbook /
+ * .pqcodes, retrieval_pq_residual.c:716-835 for .pqresN / .qparams,
+ * retrieval_rpc_demo_support.c:1968 for l1.bin / qparams.bin / residual.bin,
+ * retrieval_rpc_demo_graph_index.c:1296 for graphs, support.c:2201/2234 for
+ * fvecs / ivecs).  This library does both in C: it reads index.json, checks
+ * every member's size and SHA-256, parses and cross-checks the binary
+ * headers, and hands back host buffers in the layout of RoverPqIndexDesc /
+ * RoverSqIndexDesc (rover_b200.h), ready for calculator_rover_pq_load /
+ * calculator_rover_sq_load.
+ *
+ * Every function returns 0 on success and -1 on failure with a message in
+ * rover_host_error().
+ */
+#ifndef ROVER_HOST_H
+#define ROVER_HOST_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "rover_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- SHA-256 (FIPS 180-4) ---- */
+typedef struct RoverSha256 {
+    uint32_t h[8];
+    uint64_t bytes;
+    uint8_t buf[64];
+    size_t fill;
+} RoverSha256;
+
+void rover_sha256_init(RoverSha256 *s);
+void rover_sha256_update(RoverSha256 *s, const void *data, size_t len);
+void rover_sha256_final(RoverSha256 *s, uint8_t out[32]);
+void rover_sha256(const void *data, size_t len, uint8_t out[32]);
+/* digest of the file's bytes from `offset` to the end */
+int rover_sha256_file(const char *path, long long offset, uint8_t out[32]);
+/* lower-case hex of `len` bytes into out[2 * len + 1] */
+void rover_hex(const uint8_t *bytes, size_t len, char *out);
+
+/* ---- vectors and graphs ---- */
+/* The first `count` vectors of an fvecs / ivecs file (each record: int32
+ * dimension, then `dim` values); every record must have dimension `dim`.
+ * *out is malloc'd [count][dim]. */
+int rover_read_fvecs(const char *path, int32_t count, int32_t dim, float **out);
+int rover_read_ivecs(const char *path, int32_t count, int32_t dim, int32_t **out);
+/* A dense INT32 adjacency [n][degree], -1 padded, in one of the reference's
+ * graph formats: "rover" (16-byte header 0x35314252, n, dim, degree),
+ * "dense" (raw rows), "nndescent" (int32 n, degree, pad; then per vector
+ * `degree` ids and `degree` float distances).  Ids must lie in [-1, n). */
+int rover_read_graph(const char *path, const char *format, int32_t n, int32_t dim, int32_t degree,
+                     int32_t **out);
+/* index_bundle.py's graph checks: no self edges, no duplicate edges. */
+int rover_check_graph(const int32_t *graph, int32_t n, int32_t degree);
+
+/* ---- index bundles ---- */
+typedef struct RoverBundle {
+    int32_t method;                 /* 0 = SQ, 1 = PQ */
+    int32_t n, dim, degree, graph_entry, residual_bits;
+    int32_t *graph;                 /* [n][degree] */
+    /* PQ members (method 1) */
+    RoverPqIndexDesc pq;            /* points into the buffers below */
+    float *pq_codebook;
+    uint8_t *pq_codes;
+    uint8_t *pq_residual_blocks;
+    float *pq_qparams;
+    uint8_t index_uuid[16];
+    /* SQ members (method 0) */
+    RoverSqIndexDesc sq;
+    uint8_t *sq_l1;
+    uint8_t *sq_residual_rows;      /* unpacked [n][residual code bytes] */
+    float *sq_qparams;
+} RoverBundle;
+
+/* A rover.index.v1 directory: validate index.json (schema, method, sizes,
+ * required members, paths inside the directory, sizes and -- with verify --
+ * SHA-256 of every member, PQ member names), read the graph and the method's
+ * members, check their headers against each other and the manifest. */
+int rover_bundle_open_dir(const char *dir, int verify, RoverBundle **out);
+/* The same members named one by one (the CLI's --graph / --pq-* options).
+ * residual_bits 0 = no residuals. */
+int rover_bundle_open_pq(const char *graph_path, const char *graph_format, int32_t n, int32_t dim,
+                         int32_t degree, int32_t graph_entry, const char *pq_book, const char *pq_codes,
+                         const char *pq_residual, const char *pq_qparams, int32_t residual_bits, int verify,
+                         RoverBundle **out);
+int rover_bundle_open_sq(const char *graph_path, const char *graph_format, int32_t n, int32_t dim,
+                         int32_t degree, int32_t graph_entry, const char *l1, const char *residual,
+                         const char *qparams, RoverBundle **out);
+void rover_bundle_close(RoverBundle *b);
+
+const char *rover_host_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ROVER_HOST_H */

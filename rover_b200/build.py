@@ -1,6 +1,9 @@
-"""Build libcalculator.so (the C-ABI + sm_100a kernels) in-tree with nvcc.
+"""Build libcalculator.so (the C-ABI + sm_100a kernels) in-tree with nvcc,
+and the C host: librover_host.so (bundle loader) and the `Rover` executable.
 
-    python -m rover_b200.build          # -> rover_b200/lib/libcalculator.so
+    python -m rover_b200.build          # -> rover_b200/lib/libcalculator.so,
+                                        #    rover_b200/lib/librover_host.so,
+                                        #    rover_b200/bin/Rover
 
 Compiled for sm_100a only.  -fmad=false keeps every floating-point multiply
 and add separately rounded, as the reference's host build does; the kernels
@@ -19,6 +22,10 @@ CSRC = HERE / "csrc"
 LIB_DIR = HERE / "lib"
 LIB = LIB_DIR / "libcalculator.so"
 HOST_DIR = HERE / "host"
+HOST_LIB = LIB_DIR / "librover_host.so"
+BIN_DIR = HERE / "bin"
+ROVER = BIN_DIR / "Rover"
+HOST_SOURCES = ["sha256.c", "json.c", "bundle.c"]
 
 SOURCES = ["calculator.cu", "pq_search.cu", "pq_decoded.cu", "pq_batched.cu", "gate_train.cu", "plan.cu", "sq_search.cu", "distance.cu", "rpcmem_compat.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -60,7 +67,32 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-Xlinker", "-Bsymbolic",
                "-lcudart_static", "-lpthread", "-ldl", "-lrt"]
         subprocess.run(cmd, check=True)
+    build_host(force)
     return LIB
+
+
+def cc() -> str:
+    for cand in (os.environ.get("CC"), shutil.which("gcc"), shutil.which("cc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("no C compiler found")
+
+
+def build_host(force: bool = False) -> Path:
+    """librover_host.so and bin/Rover (gcc; no CUDA needed to build them)."""
+    LIB_DIR.mkdir(exist_ok=True)
+    BIN_DIR.mkdir(exist_ok=True)
+    include = HERE.parent / "include"
+    headers = list(HOST_DIR.glob("*.h")) + list(include.glob("*.h"))
+    srcs = [HOST_DIR / s for s in HOST_SOURCES]
+    flags = ["-std=c11", "-O2", "-Wall", "-Wextra", "-Wno-unused-parameter", "-I", str(include), "-I", str(HOST_DIR)]
+    if force or _stale(HOST_LIB, [*srcs, *headers]):
+        subprocess.run([cc(), *flags, "-fPIC", "-shared", "-o", str(HOST_LIB), *map(str, srcs), "-lm"], check=True)
+    cli = HOST_DIR / "rover_cli.c"
+    if force or _stale(ROVER, [cli, HOST_LIB, LIB, *headers]):
+        subprocess.run([cc(), *flags, "-o", str(ROVER), str(cli), "-L", str(LIB_DIR), "-lrover_host", "-lcalculator",
+                        "-lm", "-Wl,-rpath,$ORIGIN/../lib"], check=True)
+    return ROVER
 
 
 if __name__ == "__main__":

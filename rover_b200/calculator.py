@@ -131,6 +131,7 @@ class Calculator:
         L.calculator_rover_launch_count.restype = C.c_uint64
         L.calculator_rover_gate_load.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.POINTER(GateThresholds)]
         L.calculator_rover_gate_unload.argtypes = [C.c_uint64]
+        L.calculator_rover_gate_eval.argtypes = [C.c_uint64, _f32p, C.c_int64, _f32p]
         L.calculator_rover_gate_train.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.c_int64,
                                                   C.POINTER(GateTrainParams), _f32p, _f32p, _f32p, _f32p]
         L.calculator_rover_gate_grad.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.c_int64, _f32p, _f32p, _f32p,
@@ -192,6 +193,15 @@ class Calculator:
 
     def gate_unload(self) -> None:
         self._check("calculator_rover_gate_unload", self.lib.calculator_rover_gate_unload(self.handle))
+
+    def gate_eval(self, rows) -> np.ndarray:
+        """The loaded gate's logits [n][2] for raw rows [n][5] (quantized
+        distance, rank / L, worst distance, hop / L, query norm)."""
+        x = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1, 5)
+        out = np.zeros((len(x), 2), np.float32)
+        self._check("calculator_rover_gate_eval",
+                    self.lib.calculator_rover_gate_eval(self.handle, _p(x, _f32p), len(x), _p(out, _f32p)))
+        return out
 
     def gate_train(self, x, y, m, epochs=4, batch=4096, lr=2e-3, weight_decay=0.0, seed=1,
                    pos_weight=(1.0, 1.0)) -> dict:

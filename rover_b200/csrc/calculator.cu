@@ -1993,6 +1993,36 @@ extern "C" AEEResult calculator_rover_gate_unload(remote_handle64 h) {
   return AEE_SUCCESS;
 }
 
+extern "C" AEEResult calculator_rover_gate_eval(remote_handle64 h, const float* rows, int64_t n, float* logits) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (n < 0 || (n > 0 && (!rows || !logits))) return AEE_EBADPARM;
+  if (!s.gate.enabled) { set_error("no gate loaded"); return AEE_EFAILED; }
+  if (n == 0) return AEE_SUCCESS;
+  DevBuf in, out;
+  auto done = [&](AEEResult r) { in.release(); out.release(); return r; };
+  if (in.ensure(static_cast<size_t>(n) * 5 * sizeof(float)) != cudaSuccess ||
+      out.ensure(static_cast<size_t>(n) * 2 * sizeof(float)) != cudaSuccess) {
+    set_error("out of device memory for %lld gate rows", static_cast<long long>(n));
+    return done(AEE_ENOMEMORY);
+  }
+  if (cudaMemcpyAsync(in.p, rows, static_cast<size_t>(n) * 5 * sizeof(float), cudaMemcpyHostToDevice, s.stream) !=
+      cudaSuccess)
+    return done(AEE_EFAILED);
+  launch_gate_eval(s.gate, in.as<float>(), n, out.as<float>(), s.stream);
+  ++g_launches;
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(logits, out.p, static_cast<size_t>(n) * 2 * sizeof(float), cudaMemcpyDeviceToHost,
+                      s.stream) != cudaSuccess ||
+      cudaStreamSynchronize(s.stream) != cudaSuccess) {
+    set_error("gate evaluation failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return done(AEE_EFAILED);
+  }
+  return done(AEE_SUCCESS);
+}
+
 extern "C" AEEResult calculator_rover_pq_lut(remote_handle64 h, const float* queries, int32_t nq, float* out_luts,
                                              int32_t* out_status) {
   (void)h;

@@ -203,6 +203,10 @@ void launch_plan_prepare(PlanControl* ctl, unsigned long long* visited, size_t v
 // the next launch's generations would pass 2^32 - 1.
 void launch_plan_advance(PlanControl* ctl, int nq, cudaStream_t s);
 
+// The gate's logits [n][2] of raw rows [n][5] (quantized distance, rank / L,
+// worst distance, hop / L, query norm), as the batched search evaluates them.
+void launch_gate_eval(const GateParams& g, const float* rows, int64_t n, float* logits, cudaStream_t s);
+
 // ---- gate training (gate_train.cu) ------------------------------------------
 void launch_gate_stats(const float* x, int64_t n, double* acc, cudaStream_t s);
 cudaError_t launch_gate_fwd_bwd(const float* params, const float* mu, const float* sigma, const float* x,

@@ -562,6 +562,34 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
   }
 }
 
+// The loaded gate on explicit rows, through the same feature packing and
+// tensor-core tiles as the search: one warp per 32 rows.
+__global__ void __launch_bounds__(128) gate_eval_kernel(GateParams g, const float* __restrict__ rows, int64_t n,
+                                                        float* __restrict__ logits) {
+  __shared__ uint32_t feat[4][32 * 4];
+  __shared__ float out[4][32 * 2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t base = (static_cast<int64_t>(blockIdx.x) * 4 + warp) * 32;
+  if (base >= n) return;
+  const int64_t r = base + lane;
+  if (r < n) {
+    const float* x = rows + r * 5;
+    gate_row(g, x[0], x[1], x[2], x[3], x[4], feat[warp] + lane * 4);
+  } else {
+    for (int k = 0; k < 4; ++k) feat[warp][lane * 4 + k] = 0u;
+  }
+  gate_rows(g, feat[warp], 32, out[warp], lane);
+  if (r < n) {
+    logits[r * 2] = out[warp][lane * 2];
+    logits[r * 2 + 1] = out[warp][lane * 2 + 1];
+  }
+}
+
+void launch_gate_eval(const GateParams& g, const float* rows, int64_t n, float* logits, cudaStream_t s) {
+  const int64_t blocks = (n + 127) / 128;
+  if (blocks > 0) gate_eval_kernel<<<static_cast<unsigned>(blocks), 128, 0, s>>>(g, rows, n, logits);
+}
+
 PqBatchFn pq_batched_kernel_for(int dim, int kind) {
   if (dim % 4 != 0) return nullptr;
   if (kind == kBatchTrace) return pq_batched_search_kernel<0, kBatchTrace>;

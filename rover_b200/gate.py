@@ -151,3 +151,75 @@ def train(calc: Calculator, rows: np.ndarray, ids: np.ndarray, counts: np.ndarra
                 stop_rows=int(m[:, 1].sum()), stop_positive=float(y[m[:, 1] > 0, 1].mean()),
                 epoch_loss=[float(v) for v in out["losses"]])
     return GateModel(out["params"], out["mu"], out["sigma"], band_lo=lo, band_hi=hi, info=info)
+
+
+# ---------------------------------------------------------------- stop head
+
+STOP_RULES = ("hop", "rank", "ratio")
+
+
+def stop_scores(calc: Calculator, model: GateModel, rows: np.ndarray, pool: int) -> tuple[np.ndarray, dict]:
+    """Per expansion source row: the trained stop head's logit (evaluated by
+    the device code the search runs, calculator_rover_gate_eval) and the
+    single-feature scores of the method without the network -- hop count,
+    pool rank of the source, source distance / worst pool distance (higher
+    = stop sooner).  Returns (source rows, {name: score})."""
+    src = rows[(rows["flags"] & SOURCE) != 0]
+    raw = np.stack([src["quantized"], src["rank"], src["worst"], src["hop"].astype(np.float32) / np.float32(pool),
+                    src["qnorm"]], 1).astype(np.float32)
+    model.load(calc)
+    logits = calc.gate_eval(raw)
+    scores = {"network": logits[:, 1].astype(np.float64), "hop": src["hop"].astype(np.float64),
+              "rank": src["rank"].astype(np.float64),
+              "ratio": (src["quantized"] / np.maximum(src["worst"], 1e-30)).astype(np.float64)}
+    return src, scores
+
+
+def stop_savings(rows: np.ndarray, ids: np.ndarray, counts: np.ndarray, scores: dict, top_k: int = 10,
+                 budgets=(0.002, 0.005, 0.01, 0.02), thresholds: int = 200) -> dict:
+    """For each stop score: the largest share of a trace's expansions that a
+    threshold on it saves (each query stops before its first source whose
+    score passes the threshold) while losing at most `budget` of the final
+    top-k results (a result is lost when it was first scored at or after the
+    stopping hop -- the stop label of `labels`).  `rows` are the full trace
+    rows of the queries `ids` / `counts` (the search's final results); the
+    scores are aligned with the source rows in trace order."""
+    nq = ids.shape[0]
+    src_mask = (rows["flags"] & SOURCE) != 0
+    src = rows[src_mask]
+    q = src["query"].astype(np.int64)
+    hop = src["hop"].astype(np.int64)
+    order = np.lexsort((hop, q))
+    q, hop = q[order], hop[order]
+    total = np.bincount(q, minlength=nq)
+    starts = np.concatenate([[0], np.cumsum(total)[:-1]])
+    # hop at which each final result was first scored (seeds: -1)
+    k = np.minimum(counts, top_k)
+    span = np.int64(1) << 32
+    res = np.concatenate([np.int64(i) * span + ids[i, :k[i]].astype(np.int64) for i in range(nq)]) if nq else \
+        np.zeros(0, np.int64)
+    cand = rows[~src_mask]
+    key = cand["query"].astype(np.int64) * span + cand["id"].astype(np.int64)
+    hit = np.isin(key, res)
+    found_hop = np.where((cand["flags"][hit] & SEED) != 0, -1, cand["hop"][hit]).astype(np.int64)
+    found_q = cand["query"][hit].astype(np.int64)
+    out = {}
+    n = len(q)
+    has = total > 0
+    for name, s in scores.items():
+        s = np.asarray(s, np.float64)[order]
+        best = {str(b): 0.0 for b in budgets}
+        for t in np.unique(np.quantile(s, np.linspace(0.0, 1.0, thresholds))):
+            idx = np.where(s > t, np.arange(n), n)
+            first = np.full(nq, n, np.int64)
+            if n:
+                first[has] = np.minimum.reduceat(idx, starts[has])
+            stops = first < n
+            stop_hop = np.where(stops, hop[np.minimum(first, n - 1)], np.iinfo(np.int64).max)
+            saved = float(np.where(stops, total - (first - starts), 0).sum()) / max(1, int(total.sum()))
+            lost = float((found_hop >= stop_hop[found_q]).sum()) / max(1, nq * top_k)
+            for b in budgets:
+                if lost <= b and saved > best[str(b)]:
+                    best[str(b)] = saved
+        out[name] = best
+    return out

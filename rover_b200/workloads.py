@@ -19,6 +19,7 @@ from __future__ import annotations
 import hashlib
 import json
 import os
+import sys
 import time
 from dataclasses import dataclass
 from pathlib import Path
@@ -66,7 +67,8 @@ def build_pq(name: str, cache_dir: str | Path | None = None, device=None, gt_k: 
         cache = Path(cache_dir) / f"{name}-{_key(cfg)}"
         if (cache / "done").exists():
             return _load_cache(name, cache, cfg, time.time() - t0)
-    log = (lambda *a: print(f"[workload {name} {time.time() - t0:6.1f}s]", *a, flush=True)) if verbose else (lambda *a: None)
+    log = (lambda *a: print(f"[workload {name} {time.time() - t0:6.1f}s]", *a, file=sys.stderr, flush=True)) \
+        if verbose else (lambda *a: None)
     base = D.gmm(cfg["n"], cfg["dim"], cfg["comps"], cfg["seed"], clip_nonneg=cfg["clip"],
                  normalize=cfg["normalize"])
     queries = D.gmm(cfg["nq"], cfg["dim"], cfg["comps"], cfg["seed"] + 1, centers_seed=cfg["seed"],
