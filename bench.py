@@ -60,6 +60,7 @@ CALIBRATION_QUERIES = 2000
 TRAIN_QUERIES = 8000       # held-out queries traced for the gate (about 5M rows)
 GATE_ROWS = 5_000_000
 GATE_EPOCHS = 4
+STUDY_QUERIES = 2000       # held-out traces for the stop head's trace-level comparison
 THRESHOLD_GRID = (0.9, 1.0, 1.1, 1.25, 1.5)   # ADC / worst ratios of the method without the network
 DK_QUERIES, DK_IDS, DK_REPS = 1000, 8192, 3   # distance-kernel gathers: queries x random ids
 UNEVEN_WORKLOAD = "pq_1m_d96"     # uneven batch: L log-uniform in [16, 512], k in {1, 10, 100}
@@ -140,7 +141,7 @@ def measured_peak():
 
 
 def algorithmic_bytes(stats: np.ndarray, counts: np.ndarray, md, rcb: int, expand: int, dim: int) -> int:
-    """Per launch: E*4*expand (adjacency rows read) + S*c (codes of scored
+    """Per call: E*4*expand (adjacency rows read) + S*c (codes of scored
     candidates) + C*(r + 8) (residual row + qparams of corrected candidates)
     + F*(c + r + 8) (refined candidates) + 4*d per query."""
     s = stats.astype(np.int64)
@@ -148,6 +149,13 @@ def algorithmic_bytes(stats: np.ndarray, counts: np.ndarray, md, rcb: int, expan
     b = (s[:, 2] * 4 * expand + s[:, 0] * md.code_bytes + s[:, 1] * (rcb + 8)
          + refined * (md.code_bytes + rcb + 8) + 4 * dim)
     return int(b.sum())
+
+
+def seed_pass_bytes(nq: int, seeds: int, md, rcb: int, corrected: bool) -> int:
+    """The seed pass's share of algorithmic_bytes: every entry seed's code,
+    plus its residual row and qparams when the pass corrects them (the exact
+    form; the gated form ranks seeds by quantized distance)."""
+    return int(nq * seeds * (md.code_bytes + ((rcb + 8) if corrected else 0)))
 
 
 def calibrate(search, w, comps, log_prefix=""):
@@ -361,15 +369,35 @@ def device_steps(calc, args, step, stream, dist=None, dev=None):
                 clocks=clocks.summary())
 
 
-def roofline(bytes_per_call, kernels, steps, label):
+SEED_KERNELS = ("pq_seeds", "pq_seed_rank")
+# DRAM bytes per query of the search kernels, read from one ncu capture each
+# (dram__bytes_read.sum + dram__bytes_write.sum over the queries of a
+# 2,000-query launch at the headline operating points); scaled to a launch by
+# its query count.
+PROFILED_TRAFFIC = {
+    "pq_batched": (226.0e3, "profiles/pq_batched_gated_pq1m_2000q.md (W=2, L=32, 4,096 entry points)"),
+    "pq_decoded": (None, None),
+}
+
+
+def roofline(bytes_per_call, seed_bytes_per_call, kernels, steps, nq, label):
+    """The search kernel's roofline: its algorithmic bytes per launch (the
+    call's bytes minus the seed pass's share) over its own mean launch
+    duration; traffic = its measured DRAM bytes per query x nq."""
     peak, peak_kind = measured_peak()
-    call_s = sum(v[1] for v in kernels.values()) / steps / 1e3
-    achieved = bytes_per_call / call_s / 1e9
-    top = max(kernels, key=lambda k: kernels[k][1]) if kernels else None
+    search = [k for k in kernels if k not in SEED_KERNELS] or list(kernels)
+    top = max(search, key=lambda k: kernels[k][1])
+    launches, total_ms = kernels[top]
+    launch_s = total_ms / max(1, launches) / 1e3
+    per_launch = (bytes_per_call - seed_bytes_per_call) * steps / max(1, launches)
+    achieved = per_launch / launch_s / 1e9
+    per_query, source = PROFILED_TRAFFIC.get(top, (None, None))
+    traffic = per_query * nq * steps / max(1, launches) if per_query else None
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_kind": peak_kind, "kernel": top,
-            "timed": "+".join(sorted(kernels)) + f" per {label} search call",
-            "algorithmic_bytes_per_launch": bytes_per_call}
+            "traffic": traffic, "traffic_source": source, "peak_kind": peak_kind, "kernel": top,
+            "launch_ms": launch_s * 1e3, "algorithmic_bytes_per_launch": per_launch,
+            "call_algorithmic_bytes": bytes_per_call, "seed_pass_bytes": seed_bytes_per_call,
+            "timed": f"{top} per {label} search call (seed pass: " + "+".join(k for k in kernels if k in SEED_KERNELS) + ")"}
 
 
 def main():
@@ -470,7 +498,8 @@ def main():
 
     plain = device_steps(calc, args, plain_step, stream, dist, dev)
     plain_qps = nq * args.steps * world / (plain["total_ms"] / 1e3)
-    plain_roof = roofline(plain_bytes, plain["kernels"], args.steps, "plain")
+    plain_seed = seed_pass_bytes(nq, min(ep, md.num_vectors), md, rcb, True)
+    plain_roof = roofline(plain_bytes, plain_seed, plain["kernels"], args.steps, nq, "plain")
     log(f"plain {plain_qps:,.0f} QPS ({plain['ms_per_step']:.3f} ms/step)")
 
     # ---- learned-gate batched form
@@ -690,6 +719,16 @@ def gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world):
     log(f"gate: {len(rows):,} trace rows from {len(train_q)} queries, trained on {model.info['rows']:,} "
         f"in {time.time() - t0:.1f}s, loss {model.info['epoch_loss']}, band [{model.band_lo:.3f}, {model.band_hi:.3f}]")
     width_max = max(1, min(4, 256 // expand))
+    # trace-level view of the trained stop head against the single-feature
+    # rules of the method without the network, on held-out queries; its
+    # thresholds for a few loss budgets seed the calibration grid below
+    er, eids, ecounts = gate_mod.collect(calc, w.queries[:STUDY_QUERIES], L, top_k=TOP_K, **tkw)
+    _, scores = gate_mod.stop_scores(calc, model, er, L)
+    stop_study = gate_mod.stop_savings(er, eids, ecounts, scores, top_k=TOP_K)
+    stop_grid = sorted({round(v["threshold"], 3) for v in stop_study["network"].values()
+                        if np.isfinite(v["threshold"])}, reverse=True)
+    log("stop head (share of expansions saved at a loss budget of final top-10 results): " +
+        "; ".join(f"{k} " + " ".join(f"{b}:{v['saved']:.3f}" for b, v in d.items()) for k, d in stop_study.items()))
 
     def run(L_, ep_, W, **thr):
         """Full query set: recall and the summed device time of the call's
@@ -707,12 +746,12 @@ def gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world):
     table = []
     # the tensor-core seed ranking makes larger seed sets cheap for this form
     eps = sorted({ep, 2 * ep})
-    Ls = [x for x in L_SWEEP if x <= 2 * L]
+    Ls = [x for x in (16, 24) + L_SWEEP if x <= 2 * L]
     for W in range(min(2, width_max), width_max + 1):
         for ep_ in eps:
             for L_ in Ls:
                 for rl in (-np.inf, -1.0, 0.0):
-                    for sl in (np.inf, 3.0, 2.0, 1.0):
+                    for sl in (np.inf, *stop_grid):
                         thr = dict(refine_logit=rl, stop_logit=sl)
                         if rl == -np.inf:
                             thr.update(band_lo=np.inf, band_hi=np.inf)
@@ -778,11 +817,14 @@ def gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world):
                   band=[model.band_lo, model.band_hi], refine_logit=thr.get("refine_logit"),
                   stop_logit=thr.get("stop_logit"), beam_width=t["beam_width"], entry_points=t["entry_points"],
                   L=t["L"], calibration_ms=t["ms"], without_network=ratio_qps,
+                  stop_head_trace_savings=dict(queries=STUDY_QUERIES, L=L, budgets=stop_study),
                   calibration=sorted((r for r in table if r["recall_at_10"] >= TARGET_RECALL),
                                      key=lambda r: r["ms"])[:30])
     log(f"gated {qps:,.0f} QPS recall@10={rec:.4f} at W={t['beam_width']} ep={t['entry_points']} L={t['L']} {thr}")
     return dict(qps=qps, steps=steps, recall=rec, stats=final["stats"], kw=gkw, L=t["L"], report=report,
-                roof=roofline(gbytes, steps["kernels"], args.steps, "gated"))
+                roof=roofline(gbytes, seed_pass_bytes(nq, min(t["entry_points"], md.num_vectors), md,
+                                                      w.bundle.residual_code_bytes, False),
+                              steps["kernels"], args.steps, nq, "gated"))
 
 
 if __name__ == "__main__":

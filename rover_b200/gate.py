@@ -177,8 +177,8 @@ def stop_scores(calc: Calculator, model: GateModel, rows: np.ndarray, pool: int)
 
 def stop_savings(rows: np.ndarray, ids: np.ndarray, counts: np.ndarray, scores: dict, top_k: int = 10,
                  budgets=(0.002, 0.005, 0.01, 0.02), thresholds: int = 200) -> dict:
-    """For each stop score: the largest share of a trace's expansions that a
-    threshold on it saves (each query stops before its first source whose
+    """For each stop score and loss budget: the largest share of a trace's
+    expansions that a threshold on the score saves (and that threshold) (each query stops before its first source whose
     score passes the threshold) while losing at most `budget` of the final
     top-k results (a result is lost when it was first scored at or after the
     stopping hop -- the stop label of `labels`).  `rows` are the full trace
@@ -208,8 +208,8 @@ def stop_savings(rows: np.ndarray, ids: np.ndarray, counts: np.ndarray, scores: 
     has = total > 0
     for name, s in scores.items():
         s = np.asarray(s, np.float64)[order]
-        best = {str(b): 0.0 for b in budgets}
-        for t in np.unique(np.quantile(s, np.linspace(0.0, 1.0, thresholds))):
+        best = {str(b): {"saved": 0.0, "threshold": float("inf")} for b in budgets}
+        for t in np.unique(np.quantile(s, np.linspace(0.0, 1.0, thresholds))) if n else []:
             idx = np.where(s > t, np.arange(n), n)
             first = np.full(nq, n, np.int64)
             if n:
@@ -219,7 +219,7 @@ def stop_savings(rows: np.ndarray, ids: np.ndarray, counts: np.ndarray, scores: 
             saved = float(np.where(stops, total - (first - starts), 0).sum()) / max(1, int(total.sum()))
             lost = float((found_hop >= stop_hop[found_q]).sum()) / max(1, nq * top_k)
             for b in budgets:
-                if lost <= b and saved > best[str(b)]:
-                    best[str(b)] = saved
+                if lost <= b and saved > best[str(b)]["saved"]:
+                    best[str(b)] = {"saved": saved, "threshold": float(t)}
         out[name] = best
     return out

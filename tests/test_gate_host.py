@@ -41,12 +41,14 @@ def test_stop_savings_by_hand():
     scores = {"hop": src["hop"].astype(np.float64), "never": np.zeros(len(src))}
     res = G.stop_savings(rows, ids, counts, scores, top_k=3, budgets=(0.0, 0.2, 0.5))
     # lossless: only query 0's last expansion (hop 3) can go -> 1 of 6
-    assert abs(res["hop"]["0.0"] - 1 / 6) < 1e-12
+    assert abs(res["hop"]["0.0"]["saved"] - 1 / 6) < 1e-12
+    assert 2 <= res["hop"]["0.0"]["threshold"] < 3
     # losing result 7 of query 0 (1 of 6 results) allows stopping both
     # queries before hop 1 -> 4 of 6
-    assert abs(res["hop"]["0.2"] - 4 / 6) < 1e-12
-    assert abs(res["hop"]["0.5"] - 4 / 6) < 1e-12      # a threshold never fires at hop 0 (s > t)
-    assert res["never"] == {"0.0": 0.0, "0.2": 0.0, "0.5": 0.0}
+    assert abs(res["hop"]["0.2"]["saved"] - 4 / 6) < 1e-12
+    assert 0 <= res["hop"]["0.2"]["threshold"] < 1
+    assert abs(res["hop"]["0.5"]["saved"] - 4 / 6) < 1e-12      # a threshold never fires at hop 0 (s > t)
+    assert all(v["saved"] == 0.0 for v in res["never"].values())
 
 
 def test_labels_agree_with_savings():
