@@ -21,7 +21,10 @@ host->device query copy and the device->host result copy inside the timed
 region.  Multi-GPU runs are replicas (each rank searches its own 10,000
 queries; no collective on the data path) and report weak scaling.
 
-After the headline, the uneven-batch section (``config.uneven``, skipped
+After the headline, the SQ section (``config.sq``, skipped with --no-sq)
+runs the small SQ workload (20,000 x 128, SQ8 + 8-bit residuals, exact
+32-NN graph, 1,000 queries, L=64, refine 20 -> 10) against the reference's
+own SQMD search + refine on the host threads, and the uneven-batch section (``config.uneven``, skipped
 with --no-uneven) times the 1M x 96 workload (M=24, degree 32, 20,000
 queries with per-query beam L log-uniform in [16, 512] and k in {1, 10,
 100}): a tuned search plan replayed from a captured CUDA graph against the
@@ -415,6 +418,7 @@ def main():
     ap.add_argument("--no-distance-kernels", action="store_true")
     ap.add_argument("--train-queries", type=int, default=TRAIN_QUERIES)
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch plan section")
+    ap.add_argument("--no-sq", action="store_true", help="skip the SQ section")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -540,6 +544,10 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w, L, ep, expand)
 
+    sq = None
+    if not args.no_sq:
+        sq = sq_section(calc, args, rank)
+
     uneven = None
     if not args.no_uneven:
         uneven = uneven_section(calc, args, stream, dist, dev, world)
@@ -562,6 +570,7 @@ def main():
                    "gated_over_plain": head["qps"] / plain_qps if gated else 1.0,
                    "gate": gated["report"] if gated else None,
                    "uneven": uneven,
+                   "sq": sq,
                    "parallelism": f"replicas x{world}",
                    "l2": "index (>800 MB with decoded rows) larger than L2; no flush"},
         "roofline": head["roof"],
@@ -581,6 +590,86 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+SQ_WORKLOAD = "sq_20k_d128"
+SQ_L, SQ_REFINE, SQ_EXPAND = 64, 20, 32
+SQ_EPS = (1, 64, 128, 256, 512)     # the medoid alone, then multiples of the mixture's 64 clusters
+
+
+def sq_section(calc, args, rank) -> dict:
+    """The SQ drop-in on the small SQ workload: SQMD search from the medoid
+    and the calibrated entry points, L=64, expand 32, exact residual correction, the
+    top-20 refined (FP64 over reconstructions) to the top-10; all 1,000
+    queries in one batch through the host-buffer entry points, against the
+    reference's own SQMD search + refine on all host threads."""
+    import torch
+    from rover_b200 import workloads
+    w = workloads.build_sq(SQ_WORKLOAD)
+    calc.sq_load(w.graph, w.entry, w.bundle)
+    nq = len(w.queries)
+    from rover_b200.workloads import recall_at_k
+    # an exact 32-NN graph of this mixture has one component per cluster, so
+    # the medoid alone reaches one cluster: entry points (the medoid, then
+    # the reference's LCG draws) are calibrated as for the PQ workload
+    table, ep = [], SQ_EPS[-1]
+    for ep_ in SQ_EPS:
+        r = calc.sq_search(w.queries, SQ_L, SQ_REFINE, sq_mode=1, num_out=SQ_REFINE, entry_points=ep_,
+                           expand_count=SQ_EXPAND, correction=1)
+        ids_, _, counts_ = calc.refine(0, w.queries, r["ids"], np.minimum(r["counts"], SQ_REFINE), TOP_K)
+        rec = recall_at_k(ids_, counts_, w.gt, TOP_K)
+        table.append({"entry_points": ep_, "recall_at_10": rec})
+        if rec >= TARGET_RECALL:
+            ep = ep_
+            break
+    kw = dict(sq_mode=1, num_out=SQ_REFINE, entry_points=ep, expand_count=SQ_EXPAND, correction=1)
+
+    def step():
+        r = calc.sq_search(w.queries, SQ_L, SQ_REFINE, **kw)
+        return calc.refine(0, w.queries, r["ids"], np.minimum(r["counts"], SQ_REFINE), TOP_K), r
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    calc.kernel_timing(True)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        (ids, dists, counts), r = step()
+        times.append(time.perf_counter() - t0)
+    kt = {k: v[1] / args.steps for k, v in calc.kernel_times().items() if v[0] > 0}
+    calc.kernel_timing(False)
+    calc.sq_unload()
+    out = {"workload": SQ_WORKLOAD, "n": w.bundle.num_vectors, "dim": w.bundle.dim, "sq_bits": w.bundle.l1_bits,
+           "residual_bits": w.bundle.residual_bits, "graph_degree": int(w.graph.shape[1]), "queries_per_step": nq,
+           "beam_L": SQ_L, "entry_points": ep, "calibration": table, "expand_count": SQ_EXPAND,
+           "refine": f"top {SQ_REFINE} -> {TOP_K}",
+           "recall_at_10": recall_at_k(ids, counts, w.gt, TOP_K),
+           "e2e_qps": nq * len(times) / sum(times), "kernel_ms_per_step": kt,
+           "kernel_qps": nq / (sum(kt.values()) / 1e3) if kt else None}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import bindings
+        if bindings.reference_available():
+            ref = bindings.Reference()
+            threads = os.cpu_count() or 1
+            hs = ref.sq_open(w.bundle)
+            t0 = time.perf_counter()
+            rr = ref.sqmd_search(hs, w.graph, w.entry, w.queries, SQ_L, ep, SQ_EXPAND, correction=1, lanes=4,
+                                 threads=threads, out_cap=SQ_REFINE)
+            oi, od, oc = ref.refine(0, hs, w.queries, rr["ids"], rr["dists"], np.minimum(rr["counts"], SQ_REFINE),
+                                    TOP_K)
+            elapsed = time.perf_counter() - t0
+            ref.sq_close(hs)
+            same = bool(np.array_equal(oc, counts) and all(
+                np.array_equal(oi[i, :oc[i]], ids[i, :oc[i]]) and
+                np.array_equal(od[i, :oc[i]].view(np.uint32), dists[i, :oc[i]].view(np.uint32)) for i in range(nq)))
+            out["cpu_reference"] = {"qps": nq / elapsed, "cores": threads, "identical_results": same,
+                                    "sample": f"all {nq} queries, reference SQMD search + retrieval_final_refine"}
+    log(f"sq: e2e {out['e2e_qps']:,.0f} QPS, kernels {out['kernel_qps'] or 0:,.0f} QPS, "
+        f"recall@10={out['recall_at_10']:.4f}" +
+        (f", reference CPU {out['cpu_reference']['qps']:,.0f} QPS identical={out['cpu_reference']['identical_results']}"
+         if "cpu_reference" in out else ""))
+    return out
 
 
 def uneven_recall(ids, counts, gt, ks):

@@ -52,6 +52,39 @@ CONFIGS = {
 }
 
 
+# SQ: base n=20,000 d=128 from a 64-component mixture (centres N(0, 4I),
+# sigma 0.5), 1,000 queries, exact 32-NN graph (ties by lower id), entry =
+# medoid, 8-bit global SQ codec with 8-bit residuals (the reference's codec
+# is one scale / zero for the whole index), exact top-100 ground truth.
+SQ_CONFIGS = {
+    "sq_20k_d128": dict(n=20_000, dim=128, comps=64, nq=1_000, degree=32, l1_bits=8, rbits=8, seed=2023),
+}
+
+
+@dataclass
+class SqWorkload:
+    name: str
+    queries: np.ndarray
+    gt: np.ndarray
+    graph: np.ndarray
+    entry: int
+    bundle: B.SqBundle
+    build_seconds: float = 0.0
+
+
+def build_sq(name: str, device=None, gt_k: int = 100) -> SqWorkload:
+    cfg = SQ_CONFIGS[name]
+    t0 = time.time()
+    base = D.gmm(cfg["n"], cfg["dim"], cfg["comps"], cfg["seed"])
+    queries = D.gmm(cfg["nq"], cfg["dim"], cfg["comps"], cfg["seed"] + 1, centers_seed=cfg["seed"])
+    gt = D.exact_knn(queries, base, gt_k, device=device)
+    graph = D.knn_graph(base, cfg["degree"], device=device)
+    entry = D.medoid(base, device=device)
+    scale, zero, l1, res, qp = D.sq_encode(base, cfg["l1_bits"], cfg["rbits"])
+    bundle = B.SqBundle(cfg["n"], cfg["dim"], cfg["l1_bits"], scale, zero, l1, cfg["rbits"], res, qp)
+    return SqWorkload(name, queries, gt, graph, entry, bundle, time.time() - t0)
+
+
 def _key(cfg: dict) -> str:
     return hashlib.sha256(json.dumps(cfg, sort_keys=True).encode()).hexdigest()[:16]
 

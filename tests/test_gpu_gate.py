@@ -182,3 +182,50 @@ def test_gate_limits(calc):
     stop = calc.pq_search(q, 32, mode=2, beam_width=2, **KW)
     assert np.all(stop["stats"][:, 2] == 0)
     calc.gate_unload()
+
+
+RULES = ("hop", "rank", "ratio")
+
+
+def test_trained_stop_head_beats_the_method_without_it(calc):
+    """What the trained network gains over the method without it.  On the
+    100K x 128 workload (256 entry seeds, L = 48), the gate is trained on the
+    traces of 4,000 held-out queries; on the traces of the workload's 2,000
+    queries its stop head saves more expansions than a threshold on any one
+    of its inputs (hop count, source rank, source / worst distance) at every
+    loss budget of final top-10 results, and at least twice as many at the
+    tight budgets.  In the gated search kernel, the network's threshold for
+    a 0.5 % budget cuts expansions while the top-10 stay within that budget
+    of the same search without stopping."""
+    from rover_b200 import gate as gate_mod
+    from rover_b200 import workloads
+    w = workloads.build_pq("pq_100k_d128", verbose=False)
+    calc.pq_load(w.graph, w.entry, w.bundle)
+    kw = dict(entry_points=256, expand_count=48, correction=1, refine_budget=20)
+    L = 48
+    train_q = workloads.training_queries("pq_100k_d128", 4000, offset=8)
+    rows, ids, counts = gate_mod.collect(calc, train_q, L, top_k=10, **kw)
+    model = gate_mod.train(calc, rows, ids, counts, L, top_k=10, epochs=6, seed=1)
+    er, eids, ecounts = gate_mod.collect(calc, w.queries, L, top_k=10, **kw)
+    _, scores = gate_mod.stop_scores(calc, model, er, L)
+    budgets = ("0.002", "0.005", "0.01", "0.02")
+    res = gate_mod.stop_savings(er, eids, ecounts, scores, top_k=10, budgets=tuple(float(b) for b in budgets))
+    table = {k: [round(v[b]["saved"], 3) for b in budgets] for k, v in res.items()}
+    for b in budgets:
+        best_rule = max(res[r][b]["saved"] for r in RULES)
+        assert res["network"][b]["saved"] >= best_rule, table
+    for b in ("0.002", "0.005"):
+        assert res["network"][b]["saved"] >= 2 * max(res[r][b]["saved"] for r in RULES), table
+    # the same threshold inside the gated kernel (beam width 1, every
+    # shortlisted seed corrected)
+    thr = res["network"]["0.005"]["threshold"]
+    model.load(calc, band_lo=np.inf, band_hi=np.inf, refine_logit=-np.inf, stop_logit=np.inf)
+    full = calc.pq_search(w.queries, L, top_k=10, mode=2, beam_width=1, **kw)
+    model.load(calc, band_lo=np.inf, band_hi=np.inf, refine_logit=-np.inf, stop_logit=thr)
+    stop = calc.pq_search(w.queries, L, top_k=10, mode=2, beam_width=1, **kw)
+    calc.gate_unload()
+    exp_full = full["stats"][:, 2].astype(np.int64).sum()
+    exp_stop = stop["stats"][:, 2].astype(np.int64).sum()
+    kept = np.mean([len(np.intersect1d(stop["ids"][i, :10], full["ids"][i, :10])) / 10 for i in range(len(w.queries))])
+    assert exp_stop <= 0.85 * exp_full, (exp_stop, exp_full)
+    assert kept >= 1.0 - 0.005 - 0.01, kept
