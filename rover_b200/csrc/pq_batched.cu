@@ -508,7 +508,6 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
             if (!pq_score(ix, q, id, false, &adc, &unused)) sbad = true;
           }
           stage[e] = make_key(dist, id);
-          prefetch_source_row(ix, stage[e], list, size, cap);
           ++ncorr_lane;
         }
         if (__any_sync(kFullMask, sbad)) { st = kStatusNumeric; break; }

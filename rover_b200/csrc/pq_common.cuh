@@ -594,18 +594,6 @@ __device__ __forceinline__ void prefetch_next_rows(const PqIndexView& ix, const 
   }
 }
 
-// Candidates about to enter the pool will be expansion sources within a few
-// steps: their graph rows are prefetched into L2 as they are scored, so the
-// expansion that reads one finds it on chip.
-__device__ __forceinline__ void prefetch_source_row(const PqIndexView& ix, uint64_t key, const uint64_t* list,
-                                                    int size, int cap) {
-  if (size == cap && key_cmp(key) >= key_cmp(list[cap - 1])) return;
-  const char* row = reinterpret_cast<const char*>(ix.graph + static_cast<size_t>(key_id(key)) * ix.degree);
-  const int bytes = ix.degree * 4;
-  for (int off = 0; off < bytes + 127; off += 128)
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(row + (off < bytes ? off : bytes - 1)));
-}
-
 // Whether every LUT entry of this query is provably finite and no ADC sum
 // can overflow, without building the LUT.  With every q_j and codebook entry
 // finite, |fl(q - c)| <= (|q| + |c|)(1 + 2^-24), so an entry (a sequential

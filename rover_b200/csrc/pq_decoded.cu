@@ -516,7 +516,6 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
           if (!pq_score(ix, q, id, false, &adc, &unused)) sbad = true;
         }
         stage[e] = make_key(dist, id);
-        prefetch_source_row(ix, stage[e], list, size, cap);
       }
       if (__any_sync(kFullMask, sbad)) { st = kStatusNumeric; break; }
       __syncwarp();
