@@ -295,6 +295,29 @@ AEEResult allow_smem(const void* fn, size_t bytes) {
   return AEE_SUCCESS;
 }
 
+// The largest seed filter (in bits: 64 Ki down to 8 Ki) that leaves the
+// kernel's resident CTAs per SM unchanged next to warp slices of `slices`
+// bytes per CTA; 0 when even the smallest would cost a CTA.
+int seed_filter_bits(const void* kernel, int threads, size_t slices) {
+  if (allow_smem(kernel, std::min<size_t>(slices + 8192, 227 * 1024)) != AEE_SUCCESS) return 0;
+  int base = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&base, kernel, threads, slices) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  for (int bits = 65536; bits >= 8192; bits >>= 1) {
+    const size_t total = slices + bits / 8;
+    if (total > 227 * 1024) continue;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, total) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (occ >= base) return bits;
+  }
+  return 0;
+}
+
 bool valid_params(const RoverSearchParams* p) {
   return p && p->size >= static_cast<int32_t>(offsetof(RoverSearchParams, reserved)) && p->entry_points > 0 &&
          p->expand_count > 0 && p->refine_budget >= 0 && p->refine_budget <= 2000 &&
@@ -400,9 +423,11 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
   b.seed_dups = ss.dups;
   b.seed_bits = ss.bits.as<uint32_t>();
   pq_decoded_layout(&a, &b, p->refine_budget, kSharedVisitedSlots);
-  const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
-  if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, a.max_pool); return AEE_EBADPARM; }
+  const size_t slices = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
+  if (slices > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", slices, a.max_pool); return AEE_EBADPARM; }
   const PqDecodedFn kernel = pq_decoded_kernel_for(pq.view.dim);
+  b.filter_bits = seed_filter_bits(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, slices);
+  const size_t smem = slices + static_cast<size_t>(b.filter_bits) / 8;
   if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
   const int chunk = static_cast<int>(std::max<size_t>(
@@ -610,9 +635,11 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
   c.short_cap = 2 * a.max_pool;
   const bool rows = gated || tracing;   // seed ADC rows, shortlist and MLP scratch
   pq_batched_layout(&a, &b, &c, p->refine_budget, kSharedVisitedSlots, rows);
-  const size_t smem = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
-  if (smem > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", smem, a.max_pool); return AEE_EBADPARM; }
+  const size_t slices = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
+  if (slices > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", slices, a.max_pool); return AEE_EBADPARM; }
   const PqBatchFn kernel = pq_batched_kernel_for(pq.view.dim, tracing ? kBatchTrace : gated ? kBatchGated : kBatchFull);
+  b.filter_bits = seed_filter_bits(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, slices);
+  const size_t smem = slices + static_cast<size_t>(b.filter_bits) / 8;
   if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
   const bool seed_pass = !gated;      // exact seed distances
@@ -1040,7 +1067,8 @@ struct PlanConfig {
 struct PlanClass {
   int offset = 0, count = 0, max_pool = 0, blocks = 0;
   uint32_t entries = 0;     // visited-table entries per warp slot
-  size_t smem = 0;
+  size_t smem = 0;          // per CTA: seed filter + warp slices
+  int filter_bits = 0;      // seed filter (decoded and batched kernels)
 };
 
 struct PqPlanImpl : RoverPqPlan {
@@ -1219,8 +1247,10 @@ AEEResult plan_configure(State& s, PqPlanImpl& P, const PlanConfig& cfg) {
     PqBatchArgs bc{};
     bc.beam_width = P.W;
     plan_layout(P, cfg.layout, cfg.vis_cap, &a, &b, &bc);
-    c.smem = static_cast<size_t>(a.smem_per_warp) * warps;
-    if (c.smem > 227 * 1024) return AEE_EBADPARM;
+    const size_t slices = static_cast<size_t>(a.smem_per_warp) * warps;
+    if (slices > 227 * 1024) return AEE_EBADPARM;
+    c.filter_bits = cfg.layout == ROVER_LAYOUT_PACKED ? 0 : seed_filter_bits(kernel, warps * 32, slices);
+    c.smem = slices + static_cast<size_t>(c.filter_bits) / 8;
     smem_max = std::max(smem_max, c.smem);
   }
   if (allow_smem(kernel, smem_max) != AEE_SUCCESS) return AEE_EFAILED;
@@ -1300,6 +1330,7 @@ AEEResult plan_enqueue(State& s, PqPlanImpl& P, const float* queries, const Rove
     PqDecodedArgs b = plan_decoded_args(s, P);
     PqBatchArgs bc = plan_batch_args(P);
     plan_layout(P, P.cfg.layout, P.cfg.vis_cap, &a, &b, &bc);
+    b.filter_bits = c.filter_bits;
     if (!decoded) {
       a.order = P.order.as<int32_t>() + c.offset;
       a.nq = c.count;

@@ -80,6 +80,8 @@ struct PqDecodedArgs {
   int32_t q_begin, q_end;      // queries served by this launch
   int32_t vis_cap;             // shared-memory visited slots per warp (power of two)
   int32_t smem_vis_offset;     // byte offset of that table in the warp slice
+  int32_t filter_bits;         // seed filter at the start of the CTA's shared memory (power of two, 0 = none);
+                               // the warp slices follow it
 };
 
 using PqDecodedFn = void (*)(PqSearchArgs, PqDecodedArgs);

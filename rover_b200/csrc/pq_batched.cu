@@ -199,7 +199,8 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  uint8_t* base = smem + static_cast<size_t>(warp) * a.smem_per_warp;
+  uint32_t* seed_filter = reinterpret_cast<uint32_t*>(smem);
+  uint8_t* base = smem + b.filter_bits / 8 + static_cast<size_t>(warp) * a.smem_per_warp;
   float* q = reinterpret_cast<float*>(base);
   uint64_t* list = reinterpret_cast<uint64_t*>(base + a.smem_query_bytes);
   uint64_t* stage = list + a.max_pool;
@@ -219,6 +220,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
   const float adc_bound = FLT_MAX / static_cast<float>(2 * ix.m);
   const int W = c.beam_width;
 
+  if (b.filter_bits) seed_filter_build(seed_filter, b.filter_bits, b.seed_ids, b.n_seeds);
   for (;;) {
     int item = 0;
     if (lane == 0) item = b.q_begin + static_cast<int>(atomicAdd(a.next_query, 1u));
@@ -466,7 +468,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
             const int32_t v = nid[k][r];
             if (j < first_pad) {
               const uint32_t u = static_cast<uint32_t>(v);
-              if (__ldg(b.seed_bits + (u >> 5)) & (1u << (u & 31))) {
+              if (seed_filter_maybe(seed_filter, b.filter_bits, u) && (__ldg(b.seed_bits + (u >> 5)) & (1u << (u & 31)))) {
                 ++dedup;
               } else {
                 const int rr = global_mode ? visited_insert(vt, u) : smem_claim(vis, vmask, u);

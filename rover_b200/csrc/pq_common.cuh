@@ -594,6 +594,32 @@ __device__ __forceinline__ void prefetch_next_rows(const PqIndexView& ix, const 
   }
 }
 
+// Per-CTA Bloom filter of the entry seeds in shared memory (two hashes).  It
+// has no false negatives, so a miss proves an id is not a seed and skips the
+// dependent global read of the seed bitmap on the claim path; a hit is
+// settled by the bitmap.  Built by every thread of the CTA before any warp
+// starts a query.
+__device__ __forceinline__ int filter_shift(int bits) { return 33 - __ffs(bits); }   // 32 - log2(bits)
+
+__device__ __forceinline__ void seed_filter_build(uint32_t* f, int bits, const int32_t* __restrict__ seeds, int n) {
+  for (int i = threadIdx.x; i < (bits >> 5); i += blockDim.x) f[i] = 0u;
+  __syncthreads();
+  const int shift = filter_shift(bits);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t u = static_cast<uint32_t>(__ldg(seeds + i));
+    const uint32_t h1 = (u * 0x9E3779B1u) >> shift, h2 = hash_id(u) & static_cast<uint32_t>(bits - 1);
+    atomicOr(f + (h1 >> 5), 1u << (h1 & 31));
+    atomicOr(f + (h2 >> 5), 1u << (h2 & 31));
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool seed_filter_maybe(const uint32_t* f, int bits, uint32_t u) {
+  if (!bits) return true;
+  const uint32_t h1 = (u * 0x9E3779B1u) >> filter_shift(bits), h2 = hash_id(u) & static_cast<uint32_t>(bits - 1);
+  return ((f[h1 >> 5] >> (h1 & 31)) & (f[h2 >> 5] >> (h2 & 31)) & 1u) != 0u;
+}
+
 // Whether every LUT entry of this query is provably finite and no ADC sum
 // can overflow, without building the LUT.  With every q_j and codebook entry
 // finite, |fl(q - c)| <= (|q| + |c|)(1 + 2^-24), so an entry (a sequential
