@@ -80,10 +80,14 @@ struct SeedSet {
   DevBuf ids, bits;
   bool recon_ready = false;        // PQ reconstructions for ranking (gated search, traces)
   DevBuf recon, recon_norms;
+  bool drows_ready = false;        // decoded rows for the verified exact seed pool
+  DevBuf drows, drow_norms;
+  float drow_norm_max = 0.0f;      // largest of drow_norms (+inf if one is not finite)
   void release() {
-    ids.release(); bits.release(); recon.release(); recon_norms.release();
+    ids.release(); bits.release(); recon.release(); recon_norms.release(); drows.release(); drow_norms.release();
     valid = false;
     recon_ready = false;
+    drows_ready = false;
   }
 };
 
@@ -366,6 +370,7 @@ AEEResult ensure_seeds(State& s, PqDevice& pq, int32_t entry_points, uint32_t se
   ss.dups = dups;
   ss.valid = true;
   ss.recon_ready = false;
+  ss.drows_ready = false;
   return AEE_SUCCESS;
 }
 
@@ -381,6 +386,27 @@ AEEResult ensure_seed_recon(State& s, PqDevice& pq) {
   ++g_launches;
   CK(cudaStreamSynchronize(s.stream));
   ss.recon_ready = true;
+  return AEE_SUCCESS;
+}
+
+// The current seed set's decoded rows and their norms (the TF32 ranking of
+// the verified exact seed pool).  Needs the decoded rows.
+AEEResult ensure_seed_drows(State& s, PqDevice& pq) {
+  SeedSet& ss = pq.seeds;
+  if (ss.drows_ready) return AEE_SUCCESS;
+  CK(ss.drows.ensure(static_cast<size_t>(ss.count) * pq.view.dim * sizeof(float)));
+  CK(ss.drow_norms.ensure(static_cast<size_t>(ss.count) * sizeof(float)));
+  launch_pq_seed_gather(pq.decoded.as<float>(), pq.view.dim, ss.ids.as<int32_t>(), ss.count, ss.drows.as<float>(),
+                        ss.drow_norms.as<float>(), s.stream);
+  CK(cudaGetLastError());
+  ++g_launches;
+  std::vector<float> norms(ss.count);
+  CK(cudaMemcpyAsync(norms.data(), ss.drow_norms.p, norms.size() * sizeof(float), cudaMemcpyDeviceToHost, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+  float mx = 0.0f;
+  for (float v : norms) mx = std::isfinite(v) ? std::max(mx, v) : INFINITY;
+  ss.drow_norm_max = mx;
+  ss.drows_ready = true;
   return AEE_SUCCESS;
 }
 
@@ -415,6 +441,10 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
                             cudaStream_t stream) {
   PqDevice& pq = s.pq;
   if (ensure_seeds(s, pq, p->entry_points, p->seed) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  // pools up to kMaxBatch: TF32-ranked seeds verified exactly in the kernel;
+  // wider pools: every seed's exact distance up front
+  const bool verify = a.max_pool <= kMaxBatch;
+  if (verify && ensure_seed_drows(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
   const SeedSet& ss = pq.seeds;
   PqDecodedArgs b{};
   b.decoded = pq.decoded.as<float>();
@@ -422,6 +452,10 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
   b.n_seeds = ss.count;
   b.seed_dups = ss.dups;
   b.seed_bits = ss.bits.as<uint32_t>();
+  b.seed_verify = verify ? 1 : 0;
+  b.seed_norms = ss.drow_norms.as<float>();
+  b.seed_norm_max = ss.drow_norm_max;
+  b.seed_stride = verify ? (ss.count + 3) / 4 * 4 : ss.count;   // rank rows are read as float4
   pq_decoded_layout(&a, &b, p->refine_budget, kSharedVisitedSlots);
   const size_t slices = static_cast<size_t>(a.smem_per_warp) * kSearchWarps;
   if (slices > 227 * 1024) { set_error("shared memory %zu too large (pool %d)", slices, a.max_pool); return AEE_EBADPARM; }
@@ -431,8 +465,8 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
   if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
   const int chunk = static_cast<int>(std::max<size_t>(
-      1, std::min<size_t>(nq, kSeedDistBudget / (static_cast<size_t>(ss.count) * sizeof(float)))));
-  CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
+      1, std::min<size_t>(nq, kSeedDistBudget / (static_cast<size_t>(b.seed_stride) * sizeof(float)))));
+  CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * b.seed_stride * sizeof(float)));
   b.seed_dists = s.seed_dists.as<float>();
   const int blocks_cap = std::max(1, std::min(max_blocks, (chunk + kSearchWarps - 1) / kSearchWarps));
   const size_t slots = static_cast<size_t>(blocks_cap) * kSearchWarps;
@@ -449,7 +483,11 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
     a.next_query = s.counter.as<unsigned int>();
     for (int q0 = 0; q0 < nq; q0 += chunk) {
       const int q1 = std::min(nq, q0 + chunk);
-      {
+      if (verify) {
+        TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
+        launch_pq_seed_rank(a.queries, q0, q1, pq.view.dim, ss.drows.as<float>(), ss.drow_norms.as<float>(),
+                            b.n_seeds, s.seed_dists.as<float>(), stream, b.seed_stride);
+      } else {
         TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream);
         launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
                              s.seed_dists.as<float>(), stream);
@@ -1089,13 +1127,18 @@ struct PqPlanImpl : RoverPqPlan {
   int32_t n_seeds = 0, seed_dups = 0;
   GateParams gate{};
   DevBuf pool, topk, order, ctl, visited, seed_ids, seed_bits, recon, recon_norms, seed_dists, seed_rank, gate_buf;
+  DevBuf drows, drow_norms;             // exact plans: the seeds' decoded rows for the verified seed pool
+  bool verify_seeds = false;            // exact decoded plan with every pool <= kMaxBatch
+  int32_t seed_stride = 0;              // floats per query row of seed_dists
+  float drow_norm_max = 0.0f;
   size_t device_bytes() const {
     return pool.bytes + topk.bytes + order.bytes + ctl.bytes + visited.bytes + seed_ids.bytes + seed_bits.bytes +
-           recon.bytes + recon_norms.bytes + seed_dists.bytes + seed_rank.bytes + gate_buf.bytes;
+           recon.bytes + recon_norms.bytes + seed_dists.bytes + seed_rank.bytes + gate_buf.bytes + drows.bytes +
+           drow_norms.bytes;
   }
   void release() {
     for (DevBuf* b : {&pool, &topk, &order, &ctl, &visited, &seed_ids, &seed_bits, &recon, &recon_norms, &seed_dists,
-                      &seed_rank, &gate_buf})
+                      &seed_rank, &gate_buf, &drows, &drow_norms})
       b->release();
   }
 };
@@ -1199,6 +1242,10 @@ PqDecodedArgs plan_decoded_args(const State& s, const PqPlanImpl& P) {
   b.seed_dups = P.seed_dups;
   b.seed_bits = P.seed_bits.as<uint32_t>();
   b.seed_dists = P.seed_dists.as<float>();
+  b.seed_verify = P.verify_seeds ? 1 : 0;
+  b.seed_norms = P.drow_norms.as<float>();
+  b.seed_norm_max = P.drow_norm_max;
+  b.seed_stride = P.seed_stride;
   return b;
 }
 
@@ -1301,7 +1348,15 @@ AEEResult plan_enqueue(State& s, PqPlanImpl& P, const float* queries, const Rove
   CK(cudaGetLastError());
   ++g_launches;
   const bool decoded = P.cfg.layout != ROVER_LAYOUT_PACKED;
-  if (decoded && !P.gated) {
+  if (decoded && P.verify_seeds) {
+    {
+      TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream, timed);
+      launch_pq_seed_rank(queries, 0, P.nq, pq.view.dim, P.drows.as<float>(), P.drow_norms.as<float>(), P.n_seeds,
+                          P.seed_dists.as<float>(), stream, P.seed_stride);
+    }
+    CK(cudaGetLastError());
+    ++g_launches;
+  } else if (decoded && !P.gated) {
     {
       TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream, timed);
       launch_pq_seed_dists(queries, 0, P.nq, pq.view.dim, pq.decoded.as<float>(), P.seed_ids.as<int32_t>(),
@@ -1410,7 +1465,9 @@ AEEResult plan_inputs(State& s, PqPlanImpl& P) {
   CK(cudaMemcpyAsync(P.seed_ids.p, ss.ids.p, static_cast<size_t>(ss.count) * 4, cudaMemcpyDeviceToDevice, s.stream));
   CK(cudaMemcpyAsync(P.seed_bits.p, ss.bits.p, bits_bytes, cudaMemcpyDeviceToDevice, s.stream));
   if (!P.allow_decoded) return AEE_SUCCESS;
-  const size_t seed_bytes = static_cast<size_t>(P.nq) * ss.count * sizeof(float);
+  P.verify_seeds = P.p.mode == ROVER_MODE_EXACT && P.max_pool <= kMaxBatch && !P.gated;
+  P.seed_stride = P.verify_seeds ? (ss.count + 3) / 4 * 4 : ss.count;
+  const size_t seed_bytes = static_cast<size_t>(P.nq) * P.seed_stride * sizeof(float);
   if (seed_bytes > kPlanSeedBytes) {
     set_error("a plan of %d queries x %d seeds needs %zu bytes of seed distances (limit %zu): use smaller plans",
               P.nq, ss.count, seed_bytes, kPlanSeedBytes);
@@ -1441,6 +1498,16 @@ AEEResult plan_inputs(State& s, PqPlanImpl& P) {
     P.gate.b3 = reinterpret_cast<const float*>(rebase(s.gate.b3));
   } else {
     CK(P.seed_dists.ensure(seed_bytes));
+    if (P.verify_seeds) {
+      if (ensure_seed_drows(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
+      const size_t rb = static_cast<size_t>(ss.count) * pq.view.dim * sizeof(float);
+      CK(P.drows.ensure(rb));
+      CK(P.drow_norms.ensure(static_cast<size_t>(ss.count) * sizeof(float)));
+      CK(cudaMemcpyAsync(P.drows.p, ss.drows.p, rb, cudaMemcpyDeviceToDevice, s.stream));
+      CK(cudaMemcpyAsync(P.drow_norms.p, ss.drow_norms.p, static_cast<size_t>(ss.count) * sizeof(float),
+                         cudaMemcpyDeviceToDevice, s.stream));
+      P.drow_norm_max = ss.drow_norm_max;
+    }
   }
   CK(cudaStreamSynchronize(s.stream));
   return AEE_SUCCESS;

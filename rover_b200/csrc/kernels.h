@@ -82,6 +82,12 @@ struct PqDecodedArgs {
   int32_t smem_vis_offset;     // byte offset of that table in the warp slice
   int32_t filter_bits;         // seed filter at the start of the CTA's shared memory (power of two, 0 = none);
                                // the warp slices follow it
+  int32_t seed_verify;         // 1: seed_dists holds TF32 ranks of the seeds' decoded rows (launch_pq_seed_rank
+                               // over launch_pq_seed_gather's rows), verified exactly in the kernel; only
+                               // with every pool size <= kMaxBatch
+  const float* seed_norms;     // [n_seeds] |x_s|^2 of those rows (seed_verify)
+  float seed_norm_max;         // their maximum (+inf if one is not finite)
+  int32_t seed_stride;         // floats between seed_dists rows (0 = n_seeds); a multiple of 4 with seed_verify
 };
 
 using PqDecodedFn = void (*)(PqSearchArgs, PqDecodedArgs);
@@ -174,12 +180,15 @@ void launch_pq_decode(const PqIndexView& ix, float* decoded, cudaStream_t s);
 void launch_pq_seed_dists(const float* queries, int q_begin, int q_end, int dim, const float* decoded,
                           const int32_t* seed_ids, int n_seeds, float* out, cudaStream_t s);
 // Seed PQ reconstructions [n_seeds][dim] and their squared norms.
+// rows[u] = decoded[seed_ids[u]], norms[u] = |rows[u]|^2 (FP32).
+void launch_pq_seed_gather(const float* decoded, int dim, const int32_t* seed_ids, int n_seeds, float* rows,
+                           float* norms, cudaStream_t s);
 void launch_pq_seed_recon(const PqIndexView& ix, const int32_t* seed_ids, int n_seeds, float* rows, float* norms,
                           cudaStream_t s);
 // Quantized seed distances for ranking (TF32 tensor cores):
 // out[q - q_begin][u] = |q|^2 + |x~_u|^2 - 2 q . x~_u.  dim % 4 == 0.
 void launch_pq_seed_rank(const float* queries, int q_begin, int q_end, int dim, const float* rows, const float* norms,
-                         int n_seeds, float* out, cudaStream_t s);
+                         int n_seeds, float* out, cudaStream_t s, int out_stride = 0);   // 0: rows of n_seeds
 
 // ---- search plans (plan.cu) --------------------------------------------------
 //

@@ -183,6 +183,34 @@ __global__ void pq_seed_recon_kernel(PqIndexView ix, const int32_t* __restrict__
   }
 }
 
+__global__ void pq_seed_gather_kernel(const float* __restrict__ decoded, int dim, const int32_t* __restrict__ seed_ids,
+                                      int n_seeds, float* __restrict__ rows, float* __restrict__ norms) {
+  const int u = blockIdx.x;
+  if (u >= n_seeds) return;
+  const float* src = decoded + static_cast<size_t>(seed_ids[u]) * dim;
+  float sq = 0.0f;
+  for (int d = threadIdx.x; d < dim; d += blockDim.x) {
+    const float v = __ldg(src + d);
+    rows[static_cast<size_t>(u) * dim + d] = v;
+    sq += v * v;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) sq += __shfl_xor_sync(kFullMask, sq, off);
+  __shared__ float part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < static_cast<int>((blockDim.x + 31) / 32); ++w) t += part[w];
+    norms[u] = t;
+  }
+}
+
+void launch_pq_seed_gather(const float* decoded, int dim, const int32_t* seed_ids, int n_seeds, float* rows,
+                           float* norms, cudaStream_t s) {
+  pq_seed_gather_kernel<<<n_seeds, 128, 0, s>>>(decoded, dim, seed_ids, n_seeds, rows, norms);
+}
+
 void launch_pq_seed_recon(const PqIndexView& ix, const int32_t* seed_ids, int n_seeds, float* rows, float* norms,
                           cudaStream_t s) {
   pq_seed_recon_kernel<<<n_seeds, 128, 0, s>>>(ix, seed_ids, n_seeds, rows, norms);
@@ -205,7 +233,7 @@ __device__ __forceinline__ uint32_t to_tf32(float f) {
 __global__ void __launch_bounds__(128) pq_seed_rank_kernel(const float* __restrict__ queries, int q_begin, int q_end,
                                                            int dim, const float* __restrict__ rows,
                                                            const float* __restrict__ norms, int n_seeds,
-                                                           float* __restrict__ out) {
+                                                           float* __restrict__ out, int out_stride) {
   __shared__ __align__(16) float qs[kRkTile][kRkK + 4];
   __shared__ __align__(16) float xs[kRkTile][kRkK + 4];
   __shared__ float qn[kRkTile];
@@ -268,7 +296,7 @@ __global__ void __launch_bounds__(128) pq_seed_rank_kernel(const float* __restri
       const int r = wm + mi * 16 + g + 8 * h;
       const int qq = q0 + r;
       if (qq >= q_end) continue;
-      float* orow = out + static_cast<size_t>(qq - q_begin) * n_seeds;
+      float* orow = out + static_cast<size_t>(qq - q_begin) * out_stride;
 #pragma unroll
       for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
@@ -280,9 +308,10 @@ __global__ void __launch_bounds__(128) pq_seed_rank_kernel(const float* __restri
 }
 
 void launch_pq_seed_rank(const float* queries, int q_begin, int q_end, int dim, const float* rows, const float* norms,
-                         int n_seeds, float* out, cudaStream_t s) {
+                         int n_seeds, float* out, cudaStream_t s, int out_stride) {
   const dim3 grid((n_seeds + kRkTile - 1) / kRkTile, (q_end - q_begin + kRkTile - 1) / kRkTile);
-  pq_seed_rank_kernel<<<grid, 128, 0, s>>>(queries, q_begin, q_end, dim, rows, norms, n_seeds, out);
+  pq_seed_rank_kernel<<<grid, 128, 0, s>>>(queries, q_begin, q_end, dim, rows, norms, n_seeds, out,
+                                           out_stride ? out_stride : n_seeds);
 }
 
 // ---------------------------------------------------------------------------
@@ -323,6 +352,136 @@ __device__ __forceinline__ bool decoded_dist(const float* __restrict__ xrow, con
   return isfinite(acc);
 }
 
+// ---- verified seed pool --------------------------------------------------
+//
+// The exact pool after the seeds is the top-L of every seed's sequential FP32
+// distance d.  Instead of computing all of them, the seeds are ranked by
+// A = |q|^2 + |x|^2 - 2 q.x with TF32 tensor-core dot products
+// (pq_seed_rank_kernel over the seeds' decoded rows), whose error obeys
+//   |A - d| <= eps = 3 * 2^-9 sqrt(|q|^2 |x|^2) + 2^-13 (|q|^2 + |x|^2 + A):
+// rounding both operands to TF32 (relative 2^-11 each) moves each product by
+// at most 2^-10 of its size, an FP32 accumulation of 128 products adds well
+// under 2^-13, so the dot product is within 2^-9.8 |q||x| and A within twice
+// that; the FP32 norms, the final combination and the sequential sum d add
+// relative errors below 2^-16 of |q|^2 + |x|^2 + d.  Both terms of eps are
+// 2.6x and 8x those bounds.
+//
+// The L seeds of smallest A are computed exactly first; the largest of those
+// L distances, U, is at least the exact L-th distance, so every seed of the
+// exact top-L has A - eps <= d <= U.  The remaining seeds with A - eps <= U
+// are computed too, and the top-L of everything computed is the exact top-L.
+// A NaN row has A = 0 (the rank clamps at zero), ranks first and fails the
+// query when its exact distance is computed, as the all-seeds pass does; a
+// non-finite norm or bound sends every seed to the exact computation.
+__device__ __forceinline__ float seed_eps(float qn, float xn, float a) {
+  return 0.005859375f * sqrtf(qn * xn) + 1.220703125e-4f * (qn + xn + a);
+}
+
+// Exact distances of cand[0..cnt) into stage, then merged into the list;
+// false if one is non-finite.
+template <int D>
+__device__ __forceinline__ bool exact_batch(uint64_t* list, int* size, int cap, uint64_t* stage, const int32_t* cand,
+                                            int cnt, const float* decoded, const float* q, int dim, int* cursor,
+                                            float* umax, int lane) {
+  bool bad = false;
+  float mx = 0.0f;
+  for (int k = lane; k < cnt; k += kWarp) {
+    const int32_t id = cand[k];
+    float d;
+    if (!decoded_dist<D>(decoded + static_cast<size_t>(id) * dim, q, dim, &d)) bad = true;
+    mx = fmaxf(mx, d);
+    stage[k] = make_key(d, id);
+  }
+  if (__any_sync(kFullMask, bad)) return false;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFullMask, mx, off));
+  *umax = mx;
+  __syncwarp();
+  merge_scored(list, size, cap, stage, cnt, cursor, lane);
+  return true;
+}
+
+// The exact top-cap (cap <= kMaxBatch) of the seeds into list; false if an
+// exact distance is non-finite (the query then fails as in the all-seeds pass).
+template <int D>
+__device__ bool verified_seed_pool(uint64_t* list, int* size, int cap, uint64_t* stage, int32_t* cand,
+                                   const PqDecodedArgs& b, const float* arow, const float* q, int dim, int* cursor,
+                                   int lane) {
+  const int n = b.n_seeds;
+  float qn = 0.0f;
+  for (int t = lane; t < dim; t += kWarp) qn += q[t] * q[t];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) qn += __shfl_xor_sync(kFullMask, qn, off);
+  // the cap seeds of smallest A (ties by id), computed exactly
+  if (!select_top_lanes(list, size, cap, stage, n, SeedRowKeys{arow, b.seed_ids}, cursor, lane)) return false;
+  const int s1 = *size;
+  const uint64_t last = key_cmp(list[s1 - 1]);
+  for (int k = lane; k < s1; k += kWarp) cand[k] = key_id(list[k]);
+  __syncwarp();
+  *size = 0;
+  *cursor = 0;
+  float U = 0.0f;
+  if (!exact_batch<D>(list, size, cap, stage, cand, s1, b.decoded, q, dim, cursor, &U, lane)) return false;
+  if (s1 < cap) return true;   // every seed is in
+  // the rest: seeds outside the first set that the bound cannot rule out.
+  // With xmax the largest seed norm, A - eps <= U implies A <= T below, so a
+  // single comparison rules out almost every seed; the few that pass take
+  // the exact test.  A non-finite T (a NaN or huge norm, query or bound)
+  // makes every seed a candidate.
+  const float a_last = key_dist(last);
+  const int32_t id_last = key_id(last);
+  const float xmax = b.seed_norm_max;
+  float T = (U + 0.005859375f * sqrtf(qn * xmax) + 1.220703125e-4f * (qn + xmax)) / (1.0f - 1.220703125e-4f);
+  T = T * 1.0000005f;
+  const bool all = !(qn < 1e37f) || !(T < 1e37f);
+  // the row is read as float4 (its stride is a multiple of 4 seeds), four
+  // loads per lane in flight: 512 seeds per load round
+  constexpr int kGroup = 4;
+  const float4* arow4 = reinterpret_cast<const float4*>(arow);
+  int cnt = 0;
+  float unused;
+  for (int g0 = 0; g0 < n; g0 += kGroup * kWarp * 4) {
+    float4 av4[kGroup];
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+      const int v = g0 / 4 + u * kWarp + lane;
+      av4[u] = 4 * v < n ? arow4[v] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < kGroup; ++u) {
+      const float aj[4] = {av4[u].x, av4[u].y, av4[u].z, av4[u].w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int e = g0 + (u * kWarp + lane) * 4 + j;
+      bool c = false;
+      int32_t id = 0;
+      const float a = aj[j];
+      // outside the first set: A above its last key's A, or equal with a larger id
+      if (e < n && (all || a <= T) && a >= a_last) {
+        id = __ldg(b.seed_ids + e);
+        if (a > a_last || id > id_last) {
+          const float xn = __ldg(b.seed_norms + e);
+          const float lo = a - seed_eps(qn, xn, a);
+          c = all || !(lo < 1e37f && xn < 1e37f) || lo <= U;
+        }
+      }
+      const unsigned m = __ballot_sync(kFullMask, c);
+      if (c) cand[cnt + __popc(m & ((1u << lane) - 1u))] = id;
+      cnt += __popc(m);
+      if (cnt > kMaxBatch - kWarp) {
+        __syncwarp();
+        if (!exact_batch<D>(list, size, cap, stage, cand, cnt, b.decoded, q, dim, cursor, &unused, lane)) return false;
+        cnt = 0;
+      }
+    }
+    }
+  }
+  __syncwarp();
+  if (cnt > 0 && !exact_batch<D>(list, size, cap, stage, cand, cnt, b.decoded, q, dim, cursor, &unused, lane))
+    return false;
+  return true;
+}
+
 template <int D>
 __global__ void __launch_bounds__(kMaxSearchWarps * 32, 16 / kMaxSearchWarps)
 pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
@@ -353,7 +512,7 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
     if (item >= b.q_end) break;
     // with an order, items index it and the seed rows cover every query
     const int qi = a.order ? __ldg(a.order + item) : item;
-    const size_t seed_row = static_cast<size_t>(a.order ? qi : qi - b.q_begin) * b.n_seeds;
+    const size_t seed_row = static_cast<size_t>(a.order ? qi : qi - b.q_begin) * (b.seed_stride ? b.seed_stride : b.n_seeds);
 
     const int cap = a.pool_sizes[qi];
     int32_t* status = a.status + qi;
@@ -402,10 +561,16 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
 
     // ---- initial pool: top-L of the seed row under (distance, id)
     const float* drow = b.seed_dists + seed_row;
-    if (!(cap <= kMaxBatch
-              ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)
-              : select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)))
+    if (b.seed_verify) {
+      // the host sets seed_verify only when every pool fits kMaxBatch
+      if (cap > kMaxBatch) st = kStatusBadParam;
+      else if (!verified_seed_pool<D>(list, &size, cap, stage, batch, b, drow, q, dim, &cursor, lane))
+        st = kStatusNumeric;
+    } else if (!(cap <= kMaxBatch
+                     ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)
+                     : select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane))) {
       st = kStatusNumeric;
+    }
     if (st == kStatusOk && check_adc) {
       bool adc_bad = false;
       for (int e = lane; e < b.n_seeds; e += kWarp) {
