@@ -134,6 +134,7 @@ struct State {
   bool legacy_dma = false;
   // scratch
   DevBuf visited, heaps, counter, status, stats, luts, seed_dists, seed_rank;
+  DevBuf seed_top, seed_top_next;  // per query: top-M seed ranks (pq_seed_topm_kernel)
   DevBuf gate_buf;                // BF16 transposed weights + FP32 biases of the loaded gate
   GateParams gate{};              // enabled == 0: no gate loaded
   DevBuf trace_rows, trace_count; // calculator_rover_pq_trace
@@ -468,6 +469,13 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
       1, std::min<size_t>(nq, kSeedDistBudget / (static_cast<size_t>(b.seed_stride) * sizeof(float)))));
   CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * b.seed_stride * sizeof(float)));
   b.seed_dists = s.seed_dists.as<float>();
+  if (verify) {
+    b.top_m = seed_top_m(ss.count, a.max_pool);
+    CK(s.seed_top.ensure(static_cast<size_t>(chunk) * b.top_m * sizeof(uint64_t)));
+    CK(s.seed_top_next.ensure(static_cast<size_t>(chunk) * sizeof(float)));
+    b.seed_top = s.seed_top.as<uint64_t>();
+    b.seed_top_next = s.seed_top_next.as<float>();
+  }
   const int blocks_cap = std::max(1, std::min(max_blocks, (chunk + kSearchWarps - 1) / kSearchWarps));
   const size_t slots = static_cast<size_t>(blocks_cap) * kSearchWarps;
   uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * (2ull * a.max_pool + 64ull) * expand));
@@ -487,6 +495,9 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
         TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
         launch_pq_seed_rank(a.queries, q0, q1, pq.view.dim, ss.drows.as<float>(), ss.drow_norms.as<float>(),
                             b.n_seeds, s.seed_dists.as<float>(), stream, b.seed_stride);
+        launch_pq_seed_topm(s.seed_dists.as<float>(), b.seed_stride, b.n_seeds, q1 - q0, b.top_m,
+                            s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
+        ++g_launches;
       } else {
         TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream);
         launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
@@ -686,7 +697,14 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
   const size_t per_query = static_cast<size_t>(ss.count) * sizeof(float) * ((seed_pass ? 1 : 0) + (rank_pass ? 1 : 0));
   const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(nq, kSeedDistBudget / per_query)));
   if (seed_pass) CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
-  if (rank_pass) CK(s.seed_rank.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
+  if (rank_pass) {
+    CK(s.seed_rank.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
+    b.top_m = seed_top_m(ss.count, a.max_pool);
+    CK(s.seed_top.ensure(static_cast<size_t>(chunk) * b.top_m * sizeof(uint64_t)));
+    CK(s.seed_top_next.ensure(static_cast<size_t>(chunk) * sizeof(float)));
+    b.seed_top = s.seed_top.as<uint64_t>();
+    b.seed_top_next = s.seed_top_next.as<float>();
+  }
   b.seed_dists = seed_pass ? s.seed_dists.as<float>() : nullptr;
   c.seed_rank = rank_pass ? s.seed_rank.as<float>() : nullptr;
   const int blocks_cap = std::max(1, std::min(max_blocks, (chunk + kSearchWarps - 1) / kSearchWarps));
@@ -719,9 +737,11 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
           TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
           launch_pq_seed_rank(a.queries, q0, q1, pq.view.dim, pq.seeds.recon.as<float>(),
                               pq.seeds.recon_norms.as<float>(), b.n_seeds, s.seed_rank.as<float>(), stream);
+          launch_pq_seed_topm(s.seed_rank.as<float>(), b.n_seeds, b.n_seeds, q1 - q0, b.top_m,
+                              s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
         }
         CK(cudaGetLastError());
-        ++g_launches;
+        g_launches += 2;
       }
       b.q_begin = q0;
       b.q_end = q1;
@@ -1128,17 +1148,19 @@ struct PqPlanImpl : RoverPqPlan {
   GateParams gate{};
   DevBuf pool, topk, order, ctl, visited, seed_ids, seed_bits, recon, recon_norms, seed_dists, seed_rank, gate_buf;
   DevBuf drows, drow_norms;             // exact plans: the seeds' decoded rows for the verified seed pool
+  DevBuf seed_top, seed_top_next;       // per query: top-M seed ranks (verified and gated plans)
+  int32_t top_m = 0;
   bool verify_seeds = false;            // exact decoded plan with every pool <= kMaxBatch
   int32_t seed_stride = 0;              // floats per query row of seed_dists
   float drow_norm_max = 0.0f;
   size_t device_bytes() const {
     return pool.bytes + topk.bytes + order.bytes + ctl.bytes + visited.bytes + seed_ids.bytes + seed_bits.bytes +
            recon.bytes + recon_norms.bytes + seed_dists.bytes + seed_rank.bytes + gate_buf.bytes + drows.bytes +
-           drow_norms.bytes;
+           drow_norms.bytes + seed_top.bytes + seed_top_next.bytes;
   }
   void release() {
     for (DevBuf* b : {&pool, &topk, &order, &ctl, &visited, &seed_ids, &seed_bits, &recon, &recon_norms, &seed_dists,
-                      &seed_rank, &gate_buf, &drows, &drow_norms})
+                      &seed_rank, &gate_buf, &drows, &drow_norms, &seed_top, &seed_top_next})
       b->release();
   }
 };
@@ -1246,6 +1268,11 @@ PqDecodedArgs plan_decoded_args(const State& s, const PqPlanImpl& P) {
   b.seed_norms = P.drow_norms.as<float>();
   b.seed_norm_max = P.drow_norm_max;
   b.seed_stride = P.seed_stride;
+  if (P.top_m) {
+    b.seed_top = P.seed_top.as<uint64_t>();
+    b.seed_top_next = P.seed_top_next.as<float>();
+    b.top_m = P.top_m;
+  }
   return b;
 }
 
@@ -1353,9 +1380,11 @@ AEEResult plan_enqueue(State& s, PqPlanImpl& P, const float* queries, const Rove
       TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream, timed);
       launch_pq_seed_rank(queries, 0, P.nq, pq.view.dim, P.drows.as<float>(), P.drow_norms.as<float>(), P.n_seeds,
                           P.seed_dists.as<float>(), stream, P.seed_stride);
+      launch_pq_seed_topm(P.seed_dists.as<float>(), P.seed_stride, P.n_seeds, P.nq, P.top_m,
+                          P.seed_top.as<uint64_t>(), P.seed_top_next.as<float>(), stream);
     }
     CK(cudaGetLastError());
-    ++g_launches;
+    g_launches += 2;
   } else if (decoded && !P.gated) {
     {
       TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream, timed);
@@ -1370,6 +1399,8 @@ AEEResult plan_enqueue(State& s, PqPlanImpl& P, const float* queries, const Rove
       TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream, timed);
       launch_pq_seed_rank(queries, 0, P.nq, pq.view.dim, P.recon.as<float>(), P.recon_norms.as<float>(), P.n_seeds,
                           P.seed_rank.as<float>(), stream);
+      launch_pq_seed_topm(P.seed_rank.as<float>(), P.n_seeds, P.n_seeds, P.nq, P.top_m, P.seed_top.as<uint64_t>(),
+                          P.seed_top_next.as<float>(), stream);
     }
     CK(cudaGetLastError());
     ++g_launches;
@@ -1472,6 +1503,11 @@ AEEResult plan_inputs(State& s, PqPlanImpl& P) {
     set_error("a plan of %d queries x %d seeds needs %zu bytes of seed distances (limit %zu): use smaller plans",
               P.nq, ss.count, seed_bytes, kPlanSeedBytes);
     return AEE_EBADPARM;
+  }
+  if (P.gated || P.verify_seeds) {
+    P.top_m = seed_top_m(ss.count, P.max_pool);
+    CK(P.seed_top.ensure(static_cast<size_t>(P.nq) * P.top_m * sizeof(uint64_t)));
+    CK(P.seed_top_next.ensure(static_cast<size_t>(P.nq) * sizeof(float)));
   }
   if (P.gated) {
     if (ensure_seed_recon(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
@@ -1786,7 +1822,7 @@ extern "C" AEEResult calculator_rover_pq_plan_describe(const RoverPqPlan* plan, 
   r.shared_visited_slots = P->cfg.layout == ROVER_LAYOUT_PACKED ? 0 : P->cfg.vis_cap;
   r.classes = static_cast<int32_t>(P->classes.size());
   const bool decoded = P->cfg.layout != ROVER_LAYOUT_PACKED;
-  r.launches = 2 + (decoded ? 1 : 0) + r.classes;
+  r.launches = 2 + (decoded ? 1 : 0) + ((decoded && (P->verify_seeds || P->gated)) ? 1 : 0) + r.classes;
   r.candidates = P->candidates;
   r.max_pool = P->max_pool;
   r.beam_width = P->p.mode == ROVER_MODE_EXACT ? 0 : P->W;

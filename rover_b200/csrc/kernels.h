@@ -1,6 +1,7 @@
 // kernels.h -- launch-side view of the search and distance kernels.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -88,6 +89,12 @@ struct PqDecodedArgs {
   const float* seed_norms;     // [n_seeds] |x_s|^2 of those rows (seed_verify)
   float seed_norm_max;         // their maximum (+inf if one is not finite)
   int32_t seed_stride;         // floats between seed_dists rows (0 = n_seeds); a multiple of 4 with seed_verify
+  // per query row of the rank matrix (seed_verify, gated, traces): its top_m smallest keys (rank, seed index),
+  // ascending, and the (top_m + 1)-th smallest rank (+inf when n_seeds <= top_m, NaN when the row held a
+  // non-finite rank); null = select from the rank row in the search kernel
+  const uint64_t* seed_top;
+  const float* seed_top_next;
+  int32_t top_m;
 };
 
 using PqDecodedFn = void (*)(PqSearchArgs, PqDecodedArgs);
@@ -180,6 +187,17 @@ void launch_pq_decode(const PqIndexView& ix, float* decoded, cudaStream_t s);
 void launch_pq_seed_dists(const float* queries, int q_begin, int q_end, int dim, const float* decoded,
                           const int32_t* seed_ids, int n_seeds, float* out, cudaStream_t s);
 // Seed PQ reconstructions [n_seeds][dim] and their squared norms.
+// Per row of a queries x seeds rank matrix (row stride `stride`): the m
+// smallest keys (rank, seed index) ascending into keys[row][m] and the
+// (m + 1)-th smallest rank into next[row] (+inf if n_seeds <= m, NaN if the
+// row holds a non-finite rank).  One warp per row.
+void launch_pq_seed_topm(const float* rank, int stride, int n_seeds, int rows, int m, uint64_t* keys, float* next,
+                         cudaStream_t s);
+inline int seed_top_m(int n_seeds, int max_pool) {
+  const int m = std::max(2 * max_pool, max_pool + 64);
+  return std::min(n_seeds, std::min(1024, (m + 31) / 32 * 32));
+}
+
 // rows[u] = decoded[seed_ids[u]], norms[u] = |rows[u]|^2 (FP32).
 void launch_pq_seed_gather(const float* decoded, int dim, const int32_t* seed_ids, int n_seeds, float* rows,
                            float* norms, cudaStream_t s);

@@ -228,7 +228,8 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
     if (item >= b.q_end) break;
     // with an order, items index it and the seed rows cover every query
     const int qi = a.order ? __ldg(a.order + item) : item;
-    const size_t seed_row = static_cast<size_t>(a.order ? qi : qi - b.q_begin) * b.n_seeds;
+    const size_t seed_row_index = static_cast<size_t>(a.order ? qi : qi - b.q_begin);
+    const size_t seed_row = seed_row_index * b.n_seeds;
 
     const int cap = a.pool_sizes[qi];
     int32_t* status = a.status + qi;
@@ -287,11 +288,23 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
     if (adc_rows) {
       const int scap = min(c.short_cap, 2 * cap);
       const float* arow = c.seed_rank + seed_row;
-      int dummy = 0;
-      const SeedRowKeys rk{arow, b.seed_ids};
-      if (!(scap <= kMaxBatch ? select_top_lanes(shortl, &ssize, scap, stage, b.n_seeds, rk, &dummy, lane)
-                              : select_top(shortl, &ssize, scap, stage, b.n_seeds, rk, &dummy, lane)))
-        st = kStatusNumeric;
+      const float next = b.seed_top ? b.seed_top_next[seed_row_index] : 0.0f;
+      if (b.seed_top && next == next && scap <= b.top_m) {
+        // the row's top ranks, selected by pq_seed_topm_kernel: (rank, seed index) -> (rank, id)
+        const uint64_t* top = b.seed_top + seed_row_index * b.top_m;
+        ssize = min(scap, b.n_seeds);
+        for (int i = lane; i < ssize; i += kWarp) {
+          const uint64_t k = top[i];
+          shortl[i] = make_key(key_dist(k), __ldg(b.seed_ids + key_id(k)));
+        }
+        __syncwarp();
+      } else {
+        int dummy = 0;
+        const SeedRowKeys rk{arow, b.seed_ids};
+        if (!(scap <= kMaxBatch ? select_top_lanes(shortl, &ssize, scap, stage, b.n_seeds, rk, &dummy, lane)
+                                : select_top(shortl, &ssize, scap, stage, b.n_seeds, rk, &dummy, lane)))
+          st = kStatusNumeric;
+      }
     }
 
     if (!kGated) {

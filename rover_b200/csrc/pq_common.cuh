@@ -444,6 +444,20 @@ struct SeedRowKeys {
   }
 };
 
+// Keys (rank, seed index) of one row of a queries x seeds rank matrix: the
+// index, not the id, so the seed's per-seed data (norms) stays reachable.
+struct SeedIndexKeys {
+  const float* row;
+  __device__ __forceinline__ uint64_t operator()(int e, bool* nonfinite) const {
+    const float d = row[e];
+    if (!isfinite(d)) {
+      *nonfinite = true;
+      return kEmptyKey;
+    }
+    return make_key(d, e);
+  }
+};
+
 // Top-cap selection of n keys (key_at(e), e = 0..n-1) into the sorted list:
 // keys below the list's worst accumulate in stage and are merged once up to
 // kMaxBatch - 32 have gathered (or at the end), so the list is merged a few

@@ -206,6 +206,134 @@ __global__ void pq_seed_gather_kernel(const float* __restrict__ decoded, int dim
   }
 }
 
+// One CTA per row: a radix select (8 bits per pass, MSB first) finds the
+// (m+1)-th smallest rank t; the ranks below t and the ones equal to it are
+// gathered as keys (rank, seed index), sorted, and the first m written.
+// Ranks are non-negative floats (the rank kernel clamps at zero), so their
+// bit patterns order as unsigned integers; a non-finite rank marks the row.
+constexpr int kTopThreads = 128;
+constexpr int kTopGather = 2048;   // gathered keys held in shared memory
+
+__global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* __restrict__ rank, int stride,
+                                                                   int n_seeds, int rows, int m,
+                                                                   uint64_t* __restrict__ keys,
+                                                                   float* __restrict__ next) {
+  __shared__ unsigned hist[256];
+  __shared__ unsigned s_prefix, s_mask, s_remaining, s_count;
+  __shared__ uint64_t gathered[kTopGather];
+  const int row = blockIdx.x;
+  if (row >= rows) return;
+  const float* r = rank + static_cast<size_t>(row) * stride;
+  const int tid = threadIdx.x;
+  auto bits_at = [&](int e) -> uint32_t { return __float_as_uint(__ldg(r + e) + 0.0f); };
+  bool bad = false;
+  for (int e = tid; e < n_seeds; e += kTopThreads) bad |= !(__ldg(r + e) < 3.0e38f);
+  uint64_t* out = keys + static_cast<size_t>(row) * m;
+  if (__syncthreads_or(bad)) {
+    for (int i = tid; i < m; i += kTopThreads) out[i] = kEmptyKey;
+    if (tid == 0) next[row] = __int_as_float(0x7fc00000);
+    return;
+  }
+  const int target = min(m + 1, n_seeds);   // rank (1-based) of the value to find
+  if (tid == 0) { s_prefix = 0u; s_mask = 0u; s_remaining = static_cast<unsigned>(target); }
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = tid; i < 256; i += kTopThreads) hist[i] = 0u;
+    __syncthreads();
+    const unsigned prefix = s_prefix, mask = s_mask;
+    for (int e = tid; e < n_seeds; e += kTopThreads) {
+      const uint32_t v = bits_at(e);
+      if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (tid < kWarp) {
+      // the bin holding the remaining-th element: lane l owns bins 8l..8l+7
+      const int lane = tid;
+      unsigned own[8], sum = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { own[k] = hist[8 * lane + k]; sum += own[k]; }
+      unsigned incl = sum;
+#pragma unroll
+      for (int off = 1; off < kWarp; off <<= 1) {
+        const unsigned v = __shfl_up_sync(kFullMask, incl, off);
+        if (lane >= off) incl += v;
+      }
+      const unsigned rem0 = s_remaining;
+      const unsigned hit = __ballot_sync(kFullMask, incl >= rem0);
+      const int owner = hit ? __ffs(hit) - 1 : kWarp - 1;
+      if (lane == owner) {
+        unsigned rem = rem0 - (incl - sum), bin = 8u * lane;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+          if (own[k] >= rem) break;
+          rem -= own[k];
+          ++bin;
+        }
+        s_remaining = rem;
+        s_prefix = prefix | (bin << shift);
+        s_mask = mask | (255u << shift);
+      }
+    }
+    __syncthreads();
+  }
+  const uint32_t t = s_prefix;   // the target-th smallest rank's bits
+  if (tid == 0) s_count = 0u;
+  __syncthreads();
+  for (int e = tid; e < n_seeds; e += kTopThreads) {
+    const uint32_t v = bits_at(e);
+    if (v <= t) {
+      const unsigned slot = atomicAdd(&s_count, 1u);
+      if (slot < kTopGather) gathered[slot] = (static_cast<uint64_t>(v) << 32) | static_cast<uint32_t>(e);
+    }
+  }
+  __syncthreads();
+  const int cnt = static_cast<int>(s_count);
+  if (cnt > kTopGather) {   // a flood of equal ranks: let the search kernel scan the row
+    for (int i = tid; i < m; i += kTopThreads) out[i] = kEmptyKey;
+    if (tid == 0) next[row] = __int_as_float(0x7fc00000);
+    return;
+  }
+  if (cnt <= 8 * kWarp) {
+    // one warp sorts in registers
+    if (tid < kWarp) {
+      uint64_t v[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = tid + kWarp * r < cnt ? gathered[tid + kWarp * r] : kEmptyKey;
+      warp_bitonic_sort<8>(v, tid);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int i = tid + kWarp * r;
+        if (i < m) out[i] = i < cnt ? v[r] : kEmptyKey;
+        if (i == m && n_seeds > m) next[row] = __uint_as_float(static_cast<uint32_t>(v[r] >> 32));
+      }
+      for (int i = 8 * kWarp + tid; i < m; i += kWarp) out[i] = kEmptyKey;
+      if (tid == 0 && n_seeds <= m) next[row] = __int_as_float(0x7f800000);
+    }
+    return;
+  }
+  int np2 = 1;
+  while (np2 < cnt) np2 <<= 1;
+  for (int i = cnt + tid; i < np2; i += kTopThreads) gathered[i] = kEmptyKey;
+  __syncthreads();
+  for (int k = 2; k <= np2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < np2; i += kTopThreads) {
+        const int p = i ^ j;
+        if (p > i) {
+          const uint64_t x = gathered[i], y = gathered[p];
+          if (((i & k) == 0) == (x > y)) { gathered[i] = y; gathered[p] = x; }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = tid; i < m; i += kTopThreads) out[i] = i < cnt ? gathered[i] : kEmptyKey;
+  if (tid == 0) next[row] = n_seeds > m ? __uint_as_float(static_cast<uint32_t>(gathered[m] >> 32)) : __int_as_float(0x7f800000);
+}
+
+void launch_pq_seed_topm(const float* rank, int stride, int n_seeds, int rows, int m, uint64_t* keys, float* next,
+                         cudaStream_t s) {
+  pq_seed_topm_kernel<<<rows, kTopThreads, 0, s>>>(rank, stride, n_seeds, rows, m, keys, next);
+}
+
 void launch_pq_seed_gather(const float* decoded, int dim, const int32_t* seed_ids, int n_seeds, float* rows,
                            float* norms, cudaStream_t s) {
   pq_seed_gather_kernel<<<n_seeds, 128, 0, s>>>(decoded, dim, seed_ids, n_seeds, rows, norms);
@@ -402,44 +530,99 @@ __device__ __forceinline__ bool exact_batch(uint64_t* list, int* size, int cap, 
 }
 
 // The exact top-cap (cap <= kMaxBatch) of the seeds into list; false if an
-// exact distance is non-finite (the query then fails as in the all-seeds pass).
+// exact distance is non-finite (the query then fails as in the all-seeds
+// pass).  Keys of the first set and of the scans are (rank, seed index).
+// top / next: this query's top-M ranks from pq_seed_topm_kernel (null, or a
+// NaN next, when the row must be scanned here).
 template <int D>
 __device__ bool verified_seed_pool(uint64_t* list, int* size, int cap, uint64_t* stage, int32_t* cand,
-                                   const PqDecodedArgs& b, const float* arow, const float* q, int dim, int* cursor,
-                                   int lane) {
+                                   const PqDecodedArgs& b, const float* arow, const uint64_t* top, float next,
+                                   const float* q, int dim, int* cursor, int lane) {
   const int n = b.n_seeds;
   float qn = 0.0f;
   for (int t = lane; t < dim; t += kWarp) qn += q[t] * q[t];
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) qn += __shfl_xor_sync(kFullMask, qn, off);
-  // the cap seeds of smallest A (ties by id), computed exactly
-  if (!select_top_lanes(list, size, cap, stage, n, SeedRowKeys{arow, b.seed_ids}, cursor, lane)) return false;
-  const int s1 = *size;
-  const uint64_t last = key_cmp(list[s1 - 1]);
-  for (int k = lane; k < s1; k += kWarp) cand[k] = key_id(list[k]);
+  float unused;
+  // the cap seeds of smallest rank, computed exactly: their largest distance U
+  bool have_top = top != nullptr && next == next;
+  int s1 = 0;
+  uint64_t last = 0;
+  bool all = !(qn < 1e37f);
+  if (have_top) {
+    s1 = min(cap, n);
+    last = key_cmp(top[s1 - 1]);
+    for (int k = lane; k < s1; k += kWarp) cand[k] = __ldg(b.seed_ids + key_id(top[k]));
+  } else if (!all) {
+    if (select_top_lanes(list, size, cap, stage, n, SeedIndexKeys{arow}, cursor, lane)) {
+      s1 = *size;
+      last = key_cmp(list[s1 - 1]);
+      for (int k = lane; k < s1; k += kWarp) cand[k] = __ldg(b.seed_ids + key_id(list[k]));
+    } else {
+      all = true;   // a non-finite rank: compute every seed
+    }
+  }
   __syncwarp();
   *size = 0;
   *cursor = 0;
   float U = 0.0f;
-  if (!exact_batch<D>(list, size, cap, stage, cand, s1, b.decoded, q, dim, cursor, &U, lane)) return false;
-  if (s1 < cap) return true;   // every seed is in
-  // the rest: seeds outside the first set that the bound cannot rule out.
-  // With xmax the largest seed norm, A - eps <= U implies A <= T below, so a
-  // single comparison rules out almost every seed; the few that pass take
-  // the exact test.  A non-finite T (a NaN or huge norm, query or bound)
-  // makes every seed a candidate.
-  const float a_last = key_dist(last);
-  const int32_t id_last = key_id(last);
+  if (s1 > 0 && !exact_batch<D>(list, size, cap, stage, cand, s1, b.decoded, q, dim, cursor, &U, lane)) return false;
+  if (!all && s1 < cap) return true;   // every seed is in
+  // With xmax the largest seed norm, A - eps <= U implies A <= T: one
+  // comparison rules out almost every other seed; the few that pass take the
+  // exact test.  A non-finite T computes every seed.
   const float xmax = b.seed_norm_max;
-  float T = (U + 0.005859375f * sqrtf(qn * xmax) + 1.220703125e-4f * (qn + xmax)) / (1.0f - 1.220703125e-4f);
+  const float K = 0.005859375f * sqrtf(qn * xmax) + 1.220703125e-4f * (qn + xmax);
+  float T = (U + K) / (1.0f - 1.220703125e-4f);
   T = T * 1.0000005f;
-  const bool all = !(qn < 1e37f) || !(T < 1e37f);
-  // the row is read as float4 (its stride is a multiple of 4 seeds), four
-  // loads per lane in flight: 512 seeds per load round
+  all = all || !(T < 1e37f);
+  const float a_last = key_dist(last);
+  const int e_last = key_id(last);
+  int cnt = 0;
+  if (have_top && !all) {
+    const int m = b.top_m;
+    // the listed seeds past the first set; every unlisted seed has rank >=
+    // next, which rules all of them out when next (1 - 2^-13) - K > U
+    const bool listed_only = n <= m || next * (1.0f - 1.220703125e-4f) * 0.9999995f - K > U;
+    if (listed_only) {
+      const int lim = min(m, n);
+      for (int i0 = s1; i0 < lim; i0 += kWarp) {
+        const int i = i0 + lane;
+        bool c = false;
+        int32_t id = 0;
+        float a = 0.0f;
+        if (i < lim) {
+          const uint64_t k = top[i];
+          a = key_dist(k);
+          if (a <= T) {
+            const int e = key_id(k);
+            const float xn = __ldg(b.seed_norms + e);
+            const float lo = a - seed_eps(qn, xn, a);
+            c = !(lo < 1e37f && xn < 1e37f) || lo <= U;
+            id = __ldg(b.seed_ids + e);
+          }
+        }
+        const unsigned m_ = __ballot_sync(kFullMask, c);
+        if (c) cand[cnt + __popc(m_ & ((1u << lane) - 1u))] = id;
+        cnt += __popc(m_);
+        if (cnt > kMaxBatch - kWarp) {
+          __syncwarp();
+          if (!exact_batch<D>(list, size, cap, stage, cand, cnt, b.decoded, q, dim, cursor, &unused, lane)) return false;
+          cnt = 0;
+        }
+        if (!__any_sync(kFullMask, i < lim && a <= T)) break;   // ascending: the rest exceed T
+      }
+      __syncwarp();
+      if (cnt > 0 && !exact_batch<D>(list, size, cap, stage, cand, cnt, b.decoded, q, dim, cursor, &unused, lane))
+        return false;
+      return true;
+    }
+  }
+  // the row scan: every seed outside the first set ((rank, index) > last)
+  // that the bound cannot rule out (every one of them when `all`); the row
+  // is read as float4 (its stride is a multiple of 4), 512 seeds per round
   constexpr int kGroup = 4;
   const float4* arow4 = reinterpret_cast<const float4*>(arow);
-  int cnt = 0;
-  float unused;
   for (int g0 = 0; g0 < n; g0 += kGroup * kWarp * 4) {
     float4 av4[kGroup];
 #pragma unroll
@@ -451,29 +634,30 @@ __device__ bool verified_seed_pool(uint64_t* list, int* size, int cap, uint64_t*
     for (int u = 0; u < kGroup; ++u) {
       const float aj[4] = {av4[u].x, av4[u].y, av4[u].z, av4[u].w};
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int e = g0 + (u * kWarp + lane) * 4 + j;
-      bool c = false;
-      int32_t id = 0;
-      const float a = aj[j];
-      // outside the first set: A above its last key's A, or equal with a larger id
-      if (e < n && (all || a <= T) && a >= a_last) {
-        id = __ldg(b.seed_ids + e);
-        if (a > a_last || id > id_last) {
-          const float xn = __ldg(b.seed_norms + e);
-          const float lo = a - seed_eps(qn, xn, a);
-          c = all || !(lo < 1e37f && xn < 1e37f) || lo <= U;
+      for (int j = 0; j < 4; ++j) {
+        const int e = g0 + (u * kWarp + lane) * 4 + j;
+        bool c = false;
+        int32_t id = 0;
+        const float a = aj[j];
+        if (e < n) {
+          if (all) {
+            c = s1 == 0 || a > a_last || (a == a_last && e > e_last) || !(a == a);
+          } else if (a <= T && (a > a_last || (a == a_last && e > e_last))) {
+            const float xn = __ldg(b.seed_norms + e);
+            const float lo = a - seed_eps(qn, xn, a);
+            c = !(lo < 1e37f && xn < 1e37f) || lo <= U;
+          }
+          if (c) id = __ldg(b.seed_ids + e);
+        }
+        const unsigned m_ = __ballot_sync(kFullMask, c);
+        if (c) cand[cnt + __popc(m_ & ((1u << lane) - 1u))] = id;
+        cnt += __popc(m_);
+        if (cnt > kMaxBatch - kWarp) {
+          __syncwarp();
+          if (!exact_batch<D>(list, size, cap, stage, cand, cnt, b.decoded, q, dim, cursor, &unused, lane)) return false;
+          cnt = 0;
         }
       }
-      const unsigned m = __ballot_sync(kFullMask, c);
-      if (c) cand[cnt + __popc(m & ((1u << lane) - 1u))] = id;
-      cnt += __popc(m);
-      if (cnt > kMaxBatch - kWarp) {
-        __syncwarp();
-        if (!exact_batch<D>(list, size, cap, stage, cand, cnt, b.decoded, q, dim, cursor, &unused, lane)) return false;
-        cnt = 0;
-      }
-    }
     }
   }
   __syncwarp();
@@ -512,7 +696,8 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
     if (item >= b.q_end) break;
     // with an order, items index it and the seed rows cover every query
     const int qi = a.order ? __ldg(a.order + item) : item;
-    const size_t seed_row = static_cast<size_t>(a.order ? qi : qi - b.q_begin) * (b.seed_stride ? b.seed_stride : b.n_seeds);
+    const size_t seed_row_index = static_cast<size_t>(a.order ? qi : qi - b.q_begin);
+    const size_t seed_row = seed_row_index * (b.seed_stride ? b.seed_stride : b.n_seeds);
 
     const int cap = a.pool_sizes[qi];
     int32_t* status = a.status + qi;
@@ -564,7 +749,10 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
     if (b.seed_verify) {
       // the host sets seed_verify only when every pool fits kMaxBatch
       if (cap > kMaxBatch) st = kStatusBadParam;
-      else if (!verified_seed_pool<D>(list, &size, cap, stage, batch, b, drow, q, dim, &cursor, lane))
+      else if (!verified_seed_pool<D>(list, &size, cap, stage, batch, b, drow,
+                                      b.seed_top ? b.seed_top + seed_row_index * b.top_m : nullptr,
+                                      b.seed_top ? b.seed_top_next[seed_row_index] : 0.0f,
+                                      q, dim, &cursor, lane))
         st = kStatusNumeric;
     } else if (!(cap <= kMaxBatch
                      ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)
