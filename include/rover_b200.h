@@ -303,6 +303,17 @@ AEEResult calculator_rover_gate_unload(remote_handle64 h);
  * BF16 tensor-core tiles). */
 AEEResult calculator_rover_gate_eval(remote_handle64 h, const float *rows, int64_t n, float *logits);
 
+/* Seed selection of the verified exact seed pool, on host buffers: for each
+ * row of rank[rows][n_seeds] (non-negative floats) the m smallest keys
+ * (rank bits << 32 | seed index) ascending into keys[rows][m] (all ones past
+ * the row's end) and the (m + 1)-th smallest rank into next[rows] (+inf when
+ * n_seeds <= m; NaN, with every key all ones, when the row holds a rank of
+ * 3e38 or more or more than 2,048 ranks tie with the (m + 1)-th, which the
+ * search answers by scanning the row).  Runs the device code the searches
+ * run. */
+AEEResult calculator_rover_seed_topm(remote_handle64 h, const float *rank, int32_t rows, int32_t n_seeds, int32_t m,
+                                     uint64_t *keys, float *next);
+
 /* One training row per scored candidate or expansion source. */
 typedef struct RoverGateTraceRow {
     int32_t query, hop, id;

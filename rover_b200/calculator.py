@@ -132,6 +132,7 @@ class Calculator:
         L.calculator_rover_gate_load.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.POINTER(GateThresholds)]
         L.calculator_rover_gate_unload.argtypes = [C.c_uint64]
         L.calculator_rover_gate_eval.argtypes = [C.c_uint64, _f32p, C.c_int64, _f32p]
+        L.calculator_rover_seed_topm.argtypes = [C.c_uint64, _f32p, C.c_int32, C.c_int32, C.c_int32, _u64p, _f32p]
         L.calculator_rover_gate_train.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.c_int64,
                                                   C.POINTER(GateTrainParams), _f32p, _f32p, _f32p, _f32p]
         L.calculator_rover_gate_grad.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.c_int64, _f32p, _f32p, _f32p,
@@ -202,6 +203,19 @@ class Calculator:
         self._check("calculator_rover_gate_eval",
                     self.lib.calculator_rover_gate_eval(self.handle, _p(x, _f32p), len(x), _p(out, _f32p)))
         return out
+
+    def seed_topm(self, rank, m: int):
+        """The m smallest (rank bits << 32 | seed index) keys of each row of
+        rank [rows][n_seeds] ascending, and each row's (m+1)-th rank, as the
+        verified seed pool selects them on the device."""
+        r = np.ascontiguousarray(rank, dtype=np.float32)
+        rows, n = r.shape
+        keys = np.zeros((rows, m), np.uint64)
+        nxt = np.zeros(rows, np.float32)
+        self._check("calculator_rover_seed_topm",
+                    self.lib.calculator_rover_seed_topm(self.handle, _p(r, _f32p), rows, n, m, _p(keys, _u64p),
+                                                        _p(nxt, _f32p)))
+        return keys, nxt
 
     def gate_train(self, x, y, m, epochs=4, batch=4096, lr=2e-3, weight_decay=0.0, seed=1,
                    pos_weight=(1.0, 1.0)) -> dict:

@@ -2157,6 +2157,39 @@ extern "C" AEEResult calculator_rover_gate_eval(remote_handle64 h, const float* 
   return done(AEE_SUCCESS);
 }
 
+extern "C" AEEResult calculator_rover_seed_topm(remote_handle64 h, const float* rank, int32_t rows, int32_t n_seeds,
+                                                int32_t m, uint64_t* keys, float* next) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (rows < 0 || n_seeds < 0 || m < 0 || (rows > 0 && (!rank || !next || (m > 0 && !keys)))) return AEE_EBADPARM;
+  if (rows == 0 || m == 0) return AEE_SUCCESS;
+  const size_t nr = static_cast<size_t>(rows) * n_seeds, nk = static_cast<size_t>(rows) * m;
+  DevBuf in, out_keys, out_next;
+  auto done = [&](AEEResult r) { in.release(); out_keys.release(); out_next.release(); return r; };
+  if (in.ensure(std::max<size_t>(nr, 1) * sizeof(float)) != cudaSuccess ||
+      out_keys.ensure(nk * sizeof(uint64_t)) != cudaSuccess ||
+      out_next.ensure(static_cast<size_t>(rows) * sizeof(float)) != cudaSuccess) {
+    set_error("out of device memory for %d x %d ranks", rows, n_seeds);
+    return done(AEE_ENOMEMORY);
+  }
+  if (nr && cudaMemcpyAsync(in.p, rank, nr * sizeof(float), cudaMemcpyHostToDevice, s.stream) != cudaSuccess)
+    return done(AEE_EFAILED);
+  launch_pq_seed_topm(in.as<float>(), n_seeds, n_seeds, rows, m, out_keys.as<uint64_t>(), out_next.as<float>(),
+                      s.stream);
+  ++g_launches;
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(keys, out_keys.p, nk * sizeof(uint64_t), cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
+      cudaMemcpyAsync(next, out_next.p, static_cast<size_t>(rows) * sizeof(float), cudaMemcpyDeviceToHost,
+                      s.stream) != cudaSuccess ||
+      cudaStreamSynchronize(s.stream) != cudaSuccess) {
+    set_error("seed selection failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return done(AEE_EFAILED);
+  }
+  return done(AEE_SUCCESS);
+}
+
 extern "C" AEEResult calculator_rover_pq_lut(remote_handle64 h, const float* queries, int32_t nq, float* out_luts,
                                              int32_t* out_status) {
   (void)h;

@@ -190,7 +190,8 @@ void launch_pq_seed_dists(const float* queries, int q_begin, int q_end, int dim,
 // Per row of a queries x seeds rank matrix (row stride `stride`): the m
 // smallest keys (rank, seed index) ascending into keys[row][m] and the
 // (m + 1)-th smallest rank into next[row] (+inf if n_seeds <= m, NaN if the
-// row holds a non-finite rank).  One warp per row.
+// row holds a rank of 3e38 or more, or more than 2,048 ranks tie with the
+// (m + 1)-th).  One CTA per row.
 void launch_pq_seed_topm(const float* rank, int stride, int n_seeds, int rows, int m, uint64_t* keys, float* next,
                          cudaStream_t s);
 inline int seed_top_m(int n_seeds, int max_pool) {
