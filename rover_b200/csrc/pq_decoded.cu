@@ -206,26 +206,94 @@ __global__ void pq_seed_gather_kernel(const float* __restrict__ decoded, int dim
   }
 }
 
-// Per row of a queries x seeds rank matrix: the m smallest keys (rank bits,
-// seed index) ascending and the (m+1)-th smallest rank.  Ranks are
-// non-negative floats (the rank kernel clamps at zero, + 0.0f folds -0), so
-// their bit patterns order as unsigned integers; a rank that is not below
-// 3e38 marks the row (empty keys, NaN next) and the search kernel scans it.
-constexpr int kTopThreads = 128;           // wide kernel; the register kernel runs 128 or 256
-constexpr int kTopPer = 32;                // ranks per thread held in registers
-constexpr int kTopSort = 8 * kWarp;        // keys one warp sorts in registers
-constexpr int kTopGather = 2048;           // keys held in shared memory
+// One CTA per row: a radix select (8 bits per pass, MSB first) finds the
+// (m+1)-th smallest rank t; the ranks below t and the ones equal to it are
+// gathered as keys (rank, seed index), sorted, and the first m written.
+// Ranks are non-negative floats (the rank kernel clamps at zero), so their
+// bit patterns order as unsigned integers; a non-finite rank marks the row.
+constexpr int kTopThreads = 128;
+constexpr int kTopGather = 2048;   // gathered keys held in shared memory
 
-__device__ __forceinline__ void topm_mark(uint64_t* out, float* next, int row, int m, int tid) {
-  for (int i = tid; i < m; i += blockDim.x) out[i] = kEmptyKey;
-  if (tid == 0) next[row] = __int_as_float(0x7fc00000);
-}
-
-// Sorts the cnt (<= kTopGather) gathered keys, which are the row's cnt
-// smallest, and writes the first m and the (m+1)-th rank.
-__device__ void topm_sort_write(uint64_t* gathered, int cnt, int n_seeds, int m, uint64_t* out, float* next, int row,
-                                int tid) {
-  if (cnt <= kTopSort) {
+__global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* __restrict__ rank, int stride,
+                                                                   int n_seeds, int rows, int m,
+                                                                   uint64_t* __restrict__ keys,
+                                                                   float* __restrict__ next) {
+  __shared__ unsigned hist[256];
+  __shared__ unsigned s_prefix, s_mask, s_remaining, s_count;
+  __shared__ uint64_t gathered[kTopGather];
+  const int row = blockIdx.x;
+  if (row >= rows) return;
+  const float* r = rank + static_cast<size_t>(row) * stride;
+  const int tid = threadIdx.x;
+  auto bits_at = [&](int e) -> uint32_t { return __float_as_uint(__ldg(r + e) + 0.0f); };
+  bool bad = false;
+  for (int e = tid; e < n_seeds; e += kTopThreads) bad |= !(__ldg(r + e) < 3.0e38f);
+  uint64_t* out = keys + static_cast<size_t>(row) * m;
+  if (__syncthreads_or(bad)) {
+    for (int i = tid; i < m; i += kTopThreads) out[i] = kEmptyKey;
+    if (tid == 0) next[row] = __int_as_float(0x7fc00000);
+    return;
+  }
+  const int target = min(m + 1, n_seeds);   // rank (1-based) of the value to find
+  if (tid == 0) { s_prefix = 0u; s_mask = 0u; s_remaining = static_cast<unsigned>(target); }
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = tid; i < 256; i += kTopThreads) hist[i] = 0u;
+    __syncthreads();
+    const unsigned prefix = s_prefix, mask = s_mask;
+    for (int e = tid; e < n_seeds; e += kTopThreads) {
+      const uint32_t v = bits_at(e);
+      if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (tid < kWarp) {
+      // the bin holding the remaining-th element: lane l owns bins 8l..8l+7
+      const int lane = tid;
+      unsigned own[8], sum = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { own[k] = hist[8 * lane + k]; sum += own[k]; }
+      unsigned incl = sum;
+#pragma unroll
+      for (int off = 1; off < kWarp; off <<= 1) {
+        const unsigned v = __shfl_up_sync(kFullMask, incl, off);
+        if (lane >= off) incl += v;
+      }
+      const unsigned rem0 = s_remaining;
+      const unsigned hit = __ballot_sync(kFullMask, incl >= rem0);
+      const int owner = hit ? __ffs(hit) - 1 : kWarp - 1;
+      if (lane == owner) {
+        unsigned rem = rem0 - (incl - sum), bin = 8u * lane;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+          if (own[k] >= rem) break;
+          rem -= own[k];
+          ++bin;
+        }
+        s_remaining = rem;
+        s_prefix = prefix | (bin << shift);
+        s_mask = mask | (255u << shift);
+      }
+    }
+    __syncthreads();
+  }
+  const uint32_t t = s_prefix;   // the target-th smallest rank's bits
+  if (tid == 0) s_count = 0u;
+  __syncthreads();
+  for (int e = tid; e < n_seeds; e += kTopThreads) {
+    const uint32_t v = bits_at(e);
+    if (v <= t) {
+      const unsigned slot = atomicAdd(&s_count, 1u);
+      if (slot < kTopGather) gathered[slot] = (static_cast<uint64_t>(v) << 32) | static_cast<uint32_t>(e);
+    }
+  }
+  __syncthreads();
+  const int cnt = static_cast<int>(s_count);
+  if (cnt > kTopGather) {   // a flood of equal ranks: let the search kernel scan the row
+    for (int i = tid; i < m; i += kTopThreads) out[i] = kEmptyKey;
+    if (tid == 0) next[row] = __int_as_float(0x7fc00000);
+    return;
+  }
+  if (cnt <= 8 * kWarp) {
+    // one warp sorts in registers
     if (tid < kWarp) {
       uint64_t v[8];
 #pragma unroll
@@ -244,11 +312,11 @@ __device__ void topm_sort_write(uint64_t* gathered, int cnt, int n_seeds, int m,
   }
   int np2 = 1;
   while (np2 < cnt) np2 <<= 1;
-  for (int i = cnt + tid; i < np2; i += blockDim.x) gathered[i] = kEmptyKey;
+  for (int i = cnt + tid; i < np2; i += kTopThreads) gathered[i] = kEmptyKey;
   __syncthreads();
   for (int k = 2; k <= np2; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = tid; i < np2; i += blockDim.x) {
+      for (int i = tid; i < np2; i += kTopThreads) {
         const int p = i ^ j;
         if (p > i) {
           const uint64_t x = gathered[i], y = gathered[p];
@@ -257,218 +325,14 @@ __device__ void topm_sort_write(uint64_t* gathered, int cnt, int n_seeds, int m,
       }
       __syncthreads();
     }
-  for (int i = tid; i < m; i += blockDim.x) out[i] = i < cnt ? gathered[i] : kEmptyKey;
+  for (int i = tid; i < m; i += kTopThreads) out[i] = i < cnt ? gathered[i] : kEmptyKey;
   if (tid == 0) next[row] = n_seeds > m ? __uint_as_float(static_cast<uint32_t>(gathered[m] >> 32)) : __int_as_float(0x7f800000);
-}
-
-// One CTA per row of up to kThreads * kTopPer seeds, the row in registers
-// (element j * kThreads + tid in v[j]).  A 256-bin histogram over the bit
-// range still in play (bin width a power of two, the range starting at the
-// row's smallest value) finds the bin holding the target-th smallest value,
-// target = min(m + 1, n_seeds).  Every value in a lower bin is below every
-// value in that bin, so the values up to the end of that bin are the row's
-// smallest, ties included; when they are few enough to sort (kTopSort keys,
-// or kTopGather when target itself is above kTopSort) they are gathered and
-// sorted, otherwise the histogram is taken again over that bin alone.  A bin
-// of width one holds equal values only: if it still overflows kTopGather the
-// row is marked for a scan.
-template <int kThreads>
-__global__ void __launch_bounds__(kThreads) pq_seed_topm_kernel(const float* __restrict__ rank, int stride,
-                                                                int n_seeds, int rows, int m,
-                                                                uint64_t* __restrict__ keys,
-                                                                float* __restrict__ next) {
-  constexpr int kWarps = kThreads / kWarp;
-  __shared__ unsigned hist[kWarps][256];
-  __shared__ uint32_t red_lo[kWarps], red_hi[kWarps];
-  __shared__ unsigned s_below, s_total, s_fill;
-  __shared__ int s_bin;
-  __shared__ uint64_t gathered[kTopGather];
-  const int row = blockIdx.x;
-  if (row >= rows) return;
-  const float* r = rank + static_cast<size_t>(row) * stride;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  uint64_t* out = keys + static_cast<size_t>(row) * m;
-  uint32_t v[kTopPer];
-  uint32_t lo = 0xffffffffu, hi = 0u;
-  bool bad = false;
-#pragma unroll
-  for (int j = 0; j < kTopPer; ++j) {
-    const int e = j * kThreads + tid;
-    v[j] = 0xffffffffu;   // above every finite rank: never counted or gathered
-    if (e < n_seeds) {
-      const float x = __ldg(r + e);
-      bad |= !(x < 3.0e38f);
-      v[j] = __float_as_uint(x + 0.0f);
-      lo = min(lo, v[j]);
-      hi = max(hi, v[j]);
-    }
-  }
-  if (__syncthreads_or(bad)) {
-    topm_mark(out, next, row, m, tid);
-    return;
-  }
-  lo = __reduce_min_sync(kFullMask, lo);
-  hi = __reduce_max_sync(kFullMask, hi);
-  if (lane == 0) { red_lo[warp] = lo; red_hi[warp] = hi; }
-  __syncthreads();
-#pragma unroll
-  for (int w = 0; w < kWarps; ++w) { lo = min(lo, red_lo[w]); hi = max(hi, red_hi[w]); }
-  const unsigned target = static_cast<unsigned>(min(m + 1, n_seeds));
-  const unsigned cap = target <= static_cast<unsigned>(kTopSort) ? kTopSort : kTopGather;
-  uint32_t wlo = lo, whi = hi;       // the bit range still in play
-  unsigned below = 0, total = static_cast<unsigned>(n_seeds);   // values < wlo, values <= whi
-  while (total > cap) {
-    const int sh = max(0, 24 - __clz(whi - wlo));   // (whi - wlo) >> sh < 256
-    for (int i = tid; i < kWarps * 256; i += kThreads) (&hist[0][0])[i] = 0u;
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kTopPer; ++j)
-      if (v[j] >= wlo && v[j] <= whi) atomicAdd(&hist[warp][(v[j] - wlo) >> sh], 1u);
-    __syncthreads();
-    for (int b = tid; b < 256; b += kThreads) {
-      unsigned c = 0;
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) c += hist[w][b];
-      hist[0][b] = c;
-    }
-    __syncthreads();
-    if (warp == 0) {
-      // lane l owns bins 8l .. 8l+7; the first bin whose inclusive count
-      // reaches need = target - below
-      unsigned own[8], sum = 0;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) { own[k] = hist[0][8 * lane + k]; sum += own[k]; }
-      unsigned incl = sum;
-#pragma unroll
-      for (int off = 1; off < kWarp; off <<= 1) {
-        const unsigned x = __shfl_up_sync(kFullMask, incl, off);
-        if (lane >= off) incl += x;
-      }
-      const unsigned need = target - below;
-      const unsigned hit = __ballot_sync(kFullMask, incl >= need);
-      if (hit == 0u) {
-        if (lane == 0) s_bin = -1;
-      } else if (lane == __ffs(hit) - 1) {
-        unsigned before = incl - sum, inbin = 0;
-        int bin = -1;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          if (bin < 0 && before + own[k] >= need) { bin = 8 * lane + k; inbin = own[k]; }
-          if (bin < 0) before += own[k];
-        }
-        s_bin = bin;
-        s_below = below + before;
-        s_total = below + before + inbin;
-      }
-    }
-    __syncthreads();
-    const int bin = s_bin;
-    if (bin < 0) {   // the counts contradict the range: never expected
-      topm_mark(out, next, row, m, tid);
-      return;
-    }
-    below = s_below;
-    total = s_total;
-    const uint64_t nlo = static_cast<uint64_t>(wlo) + (static_cast<uint64_t>(bin) << sh);
-    const uint64_t bin_hi = nlo + (1ull << sh) - 1ull;
-    wlo = static_cast<uint32_t>(nlo);
-    if (bin_hi < whi) whi = static_cast<uint32_t>(bin_hi);
-    if (sh == 0) break;
-  }
-  if (total > static_cast<unsigned>(kTopGather)) {   // a flood of equal ranks
-    topm_mark(out, next, row, m, tid);
-    return;
-  }
-  if (tid == 0) s_fill = 0u;
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < kTopPer; ++j) {
-    const bool take = v[j] <= whi;
-    const unsigned ballot = __ballot_sync(kFullMask, take);
-    if (ballot == 0u) continue;
-    unsigned base = 0;
-    if (lane == __ffs(ballot) - 1) base = atomicAdd(&s_fill, static_cast<unsigned>(__popc(ballot)));
-    base = __shfl_sync(kFullMask, base, __ffs(ballot) - 1);
-    if (take) {
-      const unsigned slot = base + __popc(ballot & ((1u << lane) - 1u));
-      if (slot < static_cast<unsigned>(kTopGather))
-        gathered[slot] = (static_cast<uint64_t>(v[j]) << 32) | static_cast<uint32_t>(j * kThreads + tid);
-    }
-  }
-  __syncthreads();
-  topm_sort_write(gathered, static_cast<int>(total), n_seeds, m, out, next, row, tid);
-}
-
-// Rows longer than 256 * kTopPer: the same result by a radix select over the
-// row in global memory (8 bits per pass, MSB first) for the target-th
-// smallest value t, then a gather of every value <= t.
-__global__ void __launch_bounds__(kTopThreads) pq_seed_topm_wide_kernel(const float* __restrict__ rank, int stride,
-                                                                        int n_seeds, int rows, int m,
-                                                                        uint64_t* __restrict__ keys,
-                                                                        float* __restrict__ next) {
-  __shared__ unsigned hist[256];
-  __shared__ unsigned s_prefix, s_mask, s_remaining, s_count;
-  __shared__ uint64_t gathered[kTopGather];
-  const int row = blockIdx.x;
-  if (row >= rows) return;
-  const float* r = rank + static_cast<size_t>(row) * stride;
-  const int tid = threadIdx.x;
-  auto bits_at = [&](int e) -> uint32_t { return __float_as_uint(__ldg(r + e) + 0.0f); };
-  bool bad = false;
-  for (int e = tid; e < n_seeds; e += kTopThreads) bad |= !(__ldg(r + e) < 3.0e38f);
-  uint64_t* out = keys + static_cast<size_t>(row) * m;
-  if (__syncthreads_or(bad)) {
-    topm_mark(out, next, row, m, tid);
-    return;
-  }
-  const int target = min(m + 1, n_seeds);
-  if (tid == 0) { s_prefix = 0u; s_mask = 0u; s_remaining = static_cast<unsigned>(target); }
-  for (int shift = 24; shift >= 0; shift -= 8) {
-    for (int i = tid; i < 256; i += kTopThreads) hist[i] = 0u;
-    __syncthreads();
-    const unsigned prefix = s_prefix, mask = s_mask;
-    for (int e = tid; e < n_seeds; e += kTopThreads) {
-      const uint32_t v = bits_at(e);
-      if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & 255u], 1u);
-    }
-    __syncthreads();
-    if (tid == 0) {
-      unsigned rem = s_remaining, bin = 0;
-      while (bin < 255u && hist[bin] < rem) rem -= hist[bin++];
-      s_remaining = rem;
-      s_prefix = prefix | (bin << shift);
-      s_mask = mask | (255u << shift);
-    }
-    __syncthreads();
-  }
-  const uint32_t t = s_prefix;
-  if (tid == 0) s_count = 0u;
-  __syncthreads();
-  for (int e = tid; e < n_seeds; e += kTopThreads) {
-    const uint32_t v = bits_at(e);
-    if (v <= t) {
-      const unsigned slot = atomicAdd(&s_count, 1u);
-      if (slot < kTopGather) gathered[slot] = (static_cast<uint64_t>(v) << 32) | static_cast<uint32_t>(e);
-    }
-  }
-  __syncthreads();
-  const int cnt = static_cast<int>(s_count);
-  if (cnt > kTopGather) {
-    topm_mark(out, next, row, m, tid);
-    return;
-  }
-  topm_sort_write(gathered, cnt, n_seeds, m, out, next, row, tid);
 }
 
 void launch_pq_seed_topm(const float* rank, int stride, int n_seeds, int rows, int m, uint64_t* keys, float* next,
                          cudaStream_t s) {
   if (rows <= 0 || m <= 0) return;
-  if (n_seeds <= 128 * kTopPer)
-    pq_seed_topm_kernel<128><<<rows, 128, 0, s>>>(rank, stride, n_seeds, rows, m, keys, next);
-  else if (n_seeds <= 256 * kTopPer)
-    pq_seed_topm_kernel<256><<<rows, 256, 0, s>>>(rank, stride, n_seeds, rows, m, keys, next);
-  else
-    pq_seed_topm_wide_kernel<<<rows, kTopThreads, 0, s>>>(rank, stride, n_seeds, rows, m, keys, next);
+  pq_seed_topm_kernel<<<rows, kTopThreads, 0, s>>>(rank, stride, n_seeds, rows, m, keys, next);
 }
 
 void launch_pq_seed_gather(const float* decoded, int dim, const int32_t* seed_ids, int n_seeds, float* rows,

@@ -3,12 +3,11 @@ per row of a queries x seeds rank matrix, the m smallest keys
 (rank bits << 32 | seed index) in ascending order and the (m+1)-th smallest
 rank, bit for bit against a numpy sort of the same row.
 
-Covers the register-histogram kernel (rows of up to 8,192 seeds, 128 or 256
-threads: spread, clustered and narrow value ranges that take one to four
-histogram passes, results the register sort and the shared-memory sort
-finish), the wide kernel (longer rows), rows shorter than m, signed zeros,
-ties across the cut, a flood of equal ranks and rows with an infinite, huge
-or NaN rank (all marked for a scan: NaN next, empty keys).
+Covers rows of 50 to 9,000 seeds with spread, clustered, narrow (a few ulps
+apart) and many-exponent values, results the register sort and the
+shared-memory sort finish, rows shorter than m, signed zeros, ties across
+the cut, a flood of equal ranks and rows with an infinite, huge or NaN rank
+(all marked for a scan: NaN next, empty keys).
 """
 from __future__ import annotations
 
