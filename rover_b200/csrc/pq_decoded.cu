@@ -359,6 +359,13 @@ __device__ __forceinline__ uint32_t to_tf32(float f) {
   return r;
 }
 
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const uint32_t* p) {
+  const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+
 // Operands are staged in shared memory already rounded to TF32, two K
 // chunks deep: the next chunk's global loads are in flight while the tensor
 // cores work on the current one.  Thread tid stages rows tid / 8 + 16 j
@@ -412,20 +419,23 @@ __global__ void __launch_bounds__(128) pq_seed_rank_kernel(const float* __restri
     if (more) load(k0 + kRkK);
 #pragma unroll
     for (int kk = 0; kk < kRkK; kk += 8) {
+      // ldmatrix x4: lanes 8i .. 8i+7 address the rows of 8 x 4-word matrix
+      // i, and register i of lane l receives word l % 4 of row l / 4 of it.
+      // A (rows q, words k): matrices (rows 0-7, k 0-3), (8-15, 0-3),
+      // (0-7, 4-7), (8-15, 4-7) are a0..a3 of m16n8k8.  B (rows seed,
+      // words k): (ni, k 0-3), (ni, 4-7) are b0, b1; two ni per load.
       uint32_t a[2][4], b[4][2];
 #pragma unroll
-      for (int mi = 0; mi < 2; ++mi) {
-        const int r = wm + mi * 16 + g;
-        a[mi][0] = qs[buf][r][kk + t];
-        a[mi][1] = qs[buf][r + 8][kk + t];
-        a[mi][2] = qs[buf][r][kk + t + 4];
-        a[mi][3] = qs[buf][r + 8][kk + t + 4];
-      }
+      for (int mi = 0; mi < 2; ++mi)
+        ldsm_x4(a[mi], &qs[buf][wm + mi * 16 + (lane & 7) + 8 * ((lane >> 3) & 1)][kk + 4 * (lane >> 4)]);
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-        const int n = wn + ni * 8 + g;
-        b[ni][0] = xs[buf][n][kk + t];
-        b[ni][1] = xs[buf][n][kk + t + 4];
+      for (int p = 0; p < 2; ++p) {
+        uint32_t r4[4];
+        ldsm_x4(r4, &xs[buf][wn + (2 * p + (lane >> 4)) * 8 + (lane & 7)][kk + 4 * ((lane >> 3) & 1)]);
+        b[2 * p][0] = r4[0];
+        b[2 * p][1] = r4[1];
+        b[2 * p + 1][0] = r4[2];
+        b[2 * p + 1][1] = r4[3];
       }
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
