@@ -138,7 +138,10 @@ AEEResult calculator_rover_pq_search_device(remote_handle64 h, const RoverSearch
  * counterpart in the reference: it exists for callers that cannot allocate
  * device memory while they search -- a server whose memory pool already owns
  * the GPU, or a latency-bound loop that must not take cudaMalloc/cudaFree's
- * implicit synchronization.  Nothing is allocated per call: the kernel's
+ * implicit synchronization.  It runs the exact search (params->mode
+ * ROVER_MODE_EXACT) over the packed residual rows (params->layout AUTO or
+ * PACKED) and refuses other modes and layouts with AEE_EBADPARM.  Nothing is
+ * allocated per call: the kernel's
  * visited tables, work counter and error flag live in a fixed 64 MiB device
  * array inside the library (held by every GPU that loads the library until
  * the process exits).  All pointers are device pointers; out->status is

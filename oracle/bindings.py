@@ -31,11 +31,13 @@ def _p(a, t):
 
 
 def build(reference_dir: str | None = None) -> None:
-    """Compile the port always, and the reference when its sources exist."""
-    ref = Path(reference_dir or os.environ.get("ROVER_REFERENCE", "/root/reference"))
+    """Compile the port always, and the reference when its sources exist:
+    at ``reference_dir``, else $ROVER_REFERENCE, else the checkout location
+    the Makefile names (its ``ref-if-present`` target skips a missing one)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "port"], check=True)
-    if (ref / "src" / "app" / "dsp.c").is_file():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
+    ref = reference_dir or os.environ.get("ROVER_REFERENCE")
+    extra = [f"REF={Path(ref).resolve()}"] if ref else []
+    subprocess.run(["make", "-s", "-C", str(HERE), "ref-if-present", *extra], check=True)
 
 
 def reference_available() -> bool:

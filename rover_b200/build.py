@@ -15,6 +15,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -50,7 +51,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     obj_dir = HERE / "_build"
     obj_dir.mkdir(exist_ok=True)
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list((HERE.parent / "include").glob("*.h"))
-    objs = []
+    objs, jobs = [], []
     for src in SOURCES:
         s = CSRC / src
         o = obj_dir / (s.stem + ".o")
@@ -62,7 +63,11 @@ def build(force: bool = False, verbose: bool = False) -> Path:
                "-o", str(o)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        jobs.append(cmd)
+    # translation units compile independently: run them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(subprocess.run, cmd, check=True) for cmd in jobs]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-Xlinker", "-Bsymbolic",
                "-lcudart_static", "-lpthread", "-ldl", "-lrt"]

@@ -125,6 +125,7 @@ struct SqDevice {
 struct State {
   std::mutex mu;
   bool init = false;
+  int device = -1;                // the device current at the first call: index copies, stream, scratch
   int sms = 0;
   cudaStream_t stream = nullptr;
   int32_t l1_bits = 4;           // calculator_rover_configure
@@ -236,11 +237,21 @@ void collect_timings() {
 }
 
 AEEResult ensure_init(State& s) {
-  if (s.init) return AEE_SUCCESS;
   int dev = 0;
   CK(cudaGetDevice(&dev));
+  if (s.init) {
+    // the index copies, the stream and the scratch live on s.device: a call
+    // made with another device current would hand that device's kernels
+    // pointers it cannot use, so it is refused before anything is launched
+    if (dev != s.device) {
+      set_error("device %d is current, but this library's state lives on device %d", dev, s.device);
+      return AEE_EFAILED;
+    }
+    return AEE_SUCCESS;
+  }
   CK(cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+  s.device = dev;
   s.init = true;
   return AEE_SUCCESS;
 }
@@ -1098,6 +1109,7 @@ extern "C" AEEResult calculator_rover_pq_search(remote_handle64 h, const RoverSe
   (void)h;
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
   return pq_search_host(s, p, queries, nq, pool_sizes, top_ks, out);
 }
 
@@ -1799,6 +1811,7 @@ extern "C" AEEResult calculator_rover_pq_plan_launch(RoverPqPlan* plan, const fl
   if (!P || !queries || !out || !out->status || (out->ids && !out->counts)) return AEE_EBADPARM;
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
   if (!s.pq.loaded || s.pq.epoch != P->epoch) {
     set_error("the index this plan was made on is no longer loaded");
     return AEE_EFAILED;
@@ -2753,12 +2766,18 @@ extern "C" AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const
               "and each requested output needs its arrays and a positive stride");
     return AEE_EBADPARM;
   }
+  // this entry runs the exact search over packed residual rows only
+  if (p->mode != ROVER_MODE_EXACT || p->layout == ROVER_LAYOUT_DECODED) {
+    set_error("the no-alloc search runs mode ROVER_MODE_EXACT with the packed (or auto) layout only");
+    return AEE_EBADPARM;
+  }
   if (nq == 0) return AEE_SUCCESS;
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   std::lock_guard<std::mutex> nlock(g_noalloc_mu);
   const PqDevice& pq = s.pq;
   if (!pq.loaded || !pq.has_graph) { set_error("no PQ index with a graph is loaded"); return AEE_EFAILED; }
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;   // refuses a device other than the index's
   if (max_pool <= 0 || max_pool > 4096) { set_error("max_pool must be in 1..4096"); return AEE_EBADPARM; }
   if (p->correction && pq.view.residual_bits == 0) { set_error("correction needs residuals"); return AEE_EBADPARM; }
   if (p->refine_budget > 0 && pq.view.residual_bits == 0) { set_error("refine needs residuals"); return AEE_EBADPARM; }

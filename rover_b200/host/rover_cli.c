@@ -20,9 +20,11 @@
  * Index construction (build-index / insert / resume) is not part of this
  * search path. */
 #define _GNU_SOURCE
+#include <ctype.h>
 #include <errno.h>
 #include <limits.h>
 #include <math.h>
+#include <stdarg.h>
 #include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -35,173 +37,299 @@
 #include "rover_b200.h"
 #include "rover_host.h"
 
+/* ---- configuration ------------------------------------------------------
+ *
+ * The option names, their defaults and the wording of every refusal are the
+ * reference CLI's interface (src/app/config.c:12-116) and stay identical, so
+ * scripts written for `Rover search` drive this binary unchanged.  The
+ * parser itself is a table of typed option specs bound to the fields they
+ * set, and the checks are an ordered list of rules; the first failing rule's
+ * message is printed, as the reference does. */
 typedef struct {
     const char* command;
+    /* integers */
     int parent_n, expand_count, rnn_s, rnn_t1, gt_k, n, dim, nq, degree, sq_bits, residual_bits, pq_bits, pq_m,
-        pq_compression, top_k, pool, entry_points, lanes, source_window, first_factor, cache_pages,
+        pq_compression, pq_subdim, top_k, pool, entry_points, lanes, source_window, first_factor, cache_pages,
         refine_cache_pages, refine_factor, train_samples, train_iters, seed, domain, unsigned_pd, build_pool,
         build_candidates, build_iterations, build_threads, build_refine_candidates, backlink_threads,
-        checkpoint_every, reverse_candidates, cooldown_every, cooldown_ms;
-    int graph_entry, third_residual, correction, disk, split_distance, refine_all, refine_mode;
+        checkpoint_every, reverse_candidates, cooldown_every, cooldown_ms, graph_entry;
+    /* two-way switches (0 = first spelling) */
+    int third_residual, refine, correction, disk, split_distance, refine_all;
+    int refine_mode;   /* derived: 0 none, 1 residual refine, 2 with the third residual */
+    /* text */
     const char *parent_graph, *build_distance, *method, *search_mode, *build_method, *graph_format, *index_dir, *base,
         *query, *gt, *graph, *order_map, *output, *l1, *residual, *qparams, *residual_map, *error4, *bias, *pq_prefix,
         *pq_book, *pq_codes, *pq_residual, *pq_qparams, *result_dir, *metrics, *checkpoint, *identity, *layout,
         *layout_hash, *dataset;
 } Config;
 
-/* config.c:11-25 defaults */
-static Config cfg = {
-    .graph_entry = -1, .expand_count = 32, .rnn_s = 16, .rnn_t1 = 4, .build_distance = "cpu", .gt_k = 100,
-    .sq_bits = 4, .residual_bits = 4, .pq_bits = 8, .disk = 1, .top_k = 10, .pool = 128, .entry_points = 32,
-    .lanes = 4, .source_window = 1, .first_factor = 3, .cache_pages = 2048, .refine_cache_pages = 2048,
-    .refine_factor = 2, .correction = 1, .train_samples = 100000, .train_iters = 20, .seed = 42, .domain = 3,
-    .unsigned_pd = 1, .degree = 16, .build_pool = 128, .build_candidates = 16, .build_iterations = 1,
-    .build_threads = 1, .backlink_threads = 1, .checkpoint_every = 1000000, .cooldown_ms = 10000,
-    .parent_graph = "", .method = "sq", .search_mode = "sqmd", .build_method = "stream-insert",
-    .graph_format = "nndescent", .base = "", .query = "", .gt = "", .graph = "", .order_map = "", .index_dir = "",
-    .residual_map = "", .l1 = "", .residual = "", .qparams = "", .error4 = "", .bias = "", .output = "results.jsonl",
-    .pq_prefix = "", .pq_book = "", .pq_codes = "", .pq_residual = "", .pq_qparams = "", .result_dir = ".",
-    .metrics = "metrics.csv", .checkpoint = "", .identity = "", .layout = "original",
-    .layout_hash = "0000000000000000000000000000000000000000000000000000000000000000", .dataset = "dataset",
-};
+static Config cfg;
 
-typedef struct { const char* name; size_t offset; int integer; } Option;
-#define INT(name, field) {name, offsetof(Config, field), 1}
-#define STR(name, field) {name, offsetof(Config, field), 0}
-static const Option options[] = {
-    INT("parent-n", parent_n), STR("parent-graph", parent_graph), STR("build-distance", build_distance),
-    INT("expand-count", expand_count), INT("rnn-s", rnn_s), INT("rnn-t1", rnn_t1), INT("gt-k", gt_k), INT("n", n),
-    INT("dim", dim), INT("nq", nq), INT("graph-degree", degree), INT("sq-bits", sq_bits),
-    INT("residual-bits", residual_bits), INT("pq-bits", pq_bits), INT("pq-m", pq_m),
-    INT("pq-compression", pq_compression), INT("top-k", top_k), INT("pool", pool), INT("entry-points", entry_points),
-    INT("lanes", lanes), INT("source-window", source_window), INT("first-stage-factor", first_factor),
-    INT("cache-pages", cache_pages), INT("refine-cache-pages", refine_cache_pages), INT("refine-factor", refine_factor),
-    INT("pq-train-samples", train_samples), INT("pq-train-iters", train_iters), INT("seed", seed),
-    INT("domain", domain), INT("unsigned-pd", unsigned_pd), INT("build-pool", build_pool),
-    INT("build-candidates", build_candidates), INT("build-iterations", build_iterations),
-    INT("build-threads", build_threads), INT("build-refine-candidates", build_refine_candidates),
-    INT("backlink-threads", backlink_threads), INT("checkpoint-every", checkpoint_every),
-    INT("reverse-candidates", reverse_candidates), INT("cooldown-every", cooldown_every),
-    INT("cooldown-ms", cooldown_ms), STR("method", method), STR("search-mode", search_mode),
-    STR("build-method", build_method), STR("graph-format", graph_format), STR("index-dir", index_dir),
-    STR("base", base), STR("query", query), STR("gt", gt), STR("graph", graph), STR("order-map", order_map),
-    STR("output", output), STR("l1", l1), STR("residual", residual), STR("qparams", qparams),
-    STR("residual-map", residual_map), STR("error4", error4), STR("bias", bias), STR("pq-prefix", pq_prefix),
-    STR("pq-book", pq_book), STR("pq-codes", pq_codes), STR("pq-residual", pq_residual),
-    STR("pq-qparams", pq_qparams), STR("result-dir", result_dir), STR("metrics", metrics),
-    STR("checkpoint", checkpoint), STR("identity", identity), STR("layout", layout), STR("layout-hash", layout_hash),
-    STR("dataset", dataset),
-};
+static void config_defaults(Config* c) {
+    memset(c, 0, sizeof(*c));
+    c->graph_entry = -1;
+    c->expand_count = 32; c->rnn_s = 16; c->rnn_t1 = 4; c->gt_k = 100;
+    c->sq_bits = 4; c->residual_bits = 4; c->pq_bits = 8; c->disk = 1;
+    c->top_k = 10; c->pool = 128; c->entry_points = 32; c->lanes = 4; c->source_window = 1;
+    c->first_factor = 3; c->refine_factor = 2; c->cache_pages = 2048; c->refine_cache_pages = 2048;
+    c->correction = 1; c->train_samples = 100000; c->train_iters = 20; c->seed = 42;
+    c->domain = 3; c->unsigned_pd = 1; c->degree = 16;
+    c->build_pool = 128; c->build_candidates = 16; c->build_iterations = 1; c->build_threads = 1;
+    c->backlink_threads = 1; c->checkpoint_every = 1000000; c->cooldown_ms = 10000;
+    const char* empty = "";
+    c->parent_graph = c->base = c->query = c->gt = c->graph = c->order_map = c->index_dir = empty;
+    c->residual_map = c->l1 = c->residual = c->qparams = c->error4 = c->bias = empty;
+    c->pq_prefix = c->pq_book = c->pq_codes = c->pq_residual = c->pq_qparams = empty;
+    c->checkpoint = c->identity = empty;
+    c->build_distance = "cpu"; c->method = "sq"; c->search_mode = "sqmd"; c->build_method = "stream-insert";
+    c->graph_format = "nndescent"; c->output = "results.jsonl"; c->result_dir = "."; c->metrics = "metrics.csv";
+    c->layout = "original"; c->dataset = "dataset";
+    c->layout_hash = "0000000000000000000000000000000000000000000000000000000000000000";
+}
 
-static int number(const char* s, int* out) {
-    char* end;
-    errno = 0;
-    long n = strtol(s, &end, 10);
-    if (errno || !*s || *end || n < 0 || n > INT_MAX) return -1;
-    *out = (int)n;
+enum OptKind { OPT_COUNT, OPT_ENTRY, OPT_TEXT, OPT_SWITCH };
+
+typedef struct {
+    const char* name;
+    enum OptKind kind;
+    void* field;
+    const char* spellings;   /* OPT_SWITCH: "first|second" */
+} OptSpec;
+
+static const OptSpec kOptions[] = {
+    {"parent-n", OPT_COUNT, &cfg.parent_n, 0},             {"parent-graph", OPT_TEXT, &cfg.parent_graph, 0},
+    {"build-distance", OPT_TEXT, &cfg.build_distance, 0},  {"expand-count", OPT_COUNT, &cfg.expand_count, 0},
+    {"rnn-s", OPT_COUNT, &cfg.rnn_s, 0},                   {"rnn-t1", OPT_COUNT, &cfg.rnn_t1, 0},
+    {"gt-k", OPT_COUNT, &cfg.gt_k, 0},                     {"n", OPT_COUNT, &cfg.n, 0},
+    {"dim", OPT_COUNT, &cfg.dim, 0},                       {"nq", OPT_COUNT, &cfg.nq, 0},
+    {"graph-degree", OPT_COUNT, &cfg.degree, 0},           {"sq-bits", OPT_COUNT, &cfg.sq_bits, 0},
+    {"residual-bits", OPT_COUNT, &cfg.residual_bits, 0},   {"pq-bits", OPT_COUNT, &cfg.pq_bits, 0},
+    {"pq-m", OPT_COUNT, &cfg.pq_m, 0},                     {"pq-compression", OPT_COUNT, &cfg.pq_compression, 0},
+    {"top-k", OPT_COUNT, &cfg.top_k, 0},                   {"pool", OPT_COUNT, &cfg.pool, 0},
+    {"entry-points", OPT_COUNT, &cfg.entry_points, 0},     {"lanes", OPT_COUNT, &cfg.lanes, 0},
+    {"source-window", OPT_COUNT, &cfg.source_window, 0},   {"first-stage-factor", OPT_COUNT, &cfg.first_factor, 0},
+    {"cache-pages", OPT_COUNT, &cfg.cache_pages, 0},       {"refine-cache-pages", OPT_COUNT, &cfg.refine_cache_pages, 0},
+    {"refine-factor", OPT_COUNT, &cfg.refine_factor, 0},   {"pq-train-samples", OPT_COUNT, &cfg.train_samples, 0},
+    {"pq-train-iters", OPT_COUNT, &cfg.train_iters, 0},    {"seed", OPT_COUNT, &cfg.seed, 0},
+    {"domain", OPT_COUNT, &cfg.domain, 0},                 {"unsigned-pd", OPT_COUNT, &cfg.unsigned_pd, 0},
+    {"build-pool", OPT_COUNT, &cfg.build_pool, 0},         {"build-candidates", OPT_COUNT, &cfg.build_candidates, 0},
+    {"build-iterations", OPT_COUNT, &cfg.build_iterations, 0},
+    {"build-threads", OPT_COUNT, &cfg.build_threads, 0},
+    {"build-refine-candidates", OPT_COUNT, &cfg.build_refine_candidates, 0},
+    {"backlink-threads", OPT_COUNT, &cfg.backlink_threads, 0},
+    {"checkpoint-every", OPT_COUNT, &cfg.checkpoint_every, 0},
+    {"reverse-candidates", OPT_COUNT, &cfg.reverse_candidates, 0},
+    {"cooldown-every", OPT_COUNT, &cfg.cooldown_every, 0}, {"cooldown-ms", OPT_COUNT, &cfg.cooldown_ms, 0},
+    {"method", OPT_TEXT, &cfg.method, 0},                  {"search-mode", OPT_TEXT, &cfg.search_mode, 0},
+    {"build-method", OPT_TEXT, &cfg.build_method, 0},      {"graph-format", OPT_TEXT, &cfg.graph_format, 0},
+    {"index-dir", OPT_TEXT, &cfg.index_dir, 0},            {"base", OPT_TEXT, &cfg.base, 0},
+    {"query", OPT_TEXT, &cfg.query, 0},                    {"gt", OPT_TEXT, &cfg.gt, 0},
+    {"graph", OPT_TEXT, &cfg.graph, 0},                    {"order-map", OPT_TEXT, &cfg.order_map, 0},
+    {"output", OPT_TEXT, &cfg.output, 0},                  {"l1", OPT_TEXT, &cfg.l1, 0},
+    {"residual", OPT_TEXT, &cfg.residual, 0},              {"qparams", OPT_TEXT, &cfg.qparams, 0},
+    {"residual-map", OPT_TEXT, &cfg.residual_map, 0},      {"error4", OPT_TEXT, &cfg.error4, 0},
+    {"bias", OPT_TEXT, &cfg.bias, 0},                      {"pq-prefix", OPT_TEXT, &cfg.pq_prefix, 0},
+    {"pq-book", OPT_TEXT, &cfg.pq_book, 0},                {"pq-codes", OPT_TEXT, &cfg.pq_codes, 0},
+    {"pq-residual", OPT_TEXT, &cfg.pq_residual, 0},        {"pq-qparams", OPT_TEXT, &cfg.pq_qparams, 0},
+    {"result-dir", OPT_TEXT, &cfg.result_dir, 0},          {"metrics", OPT_TEXT, &cfg.metrics, 0},
+    {"checkpoint", OPT_TEXT, &cfg.checkpoint, 0},          {"identity", OPT_TEXT, &cfg.identity, 0},
+    {"layout", OPT_TEXT, &cfg.layout, 0},                  {"layout-hash", OPT_TEXT, &cfg.layout_hash, 0},
+    {"dataset", OPT_TEXT, &cfg.dataset, 0},
+    /* options the reference lists on a separate help line */
+    {"third-residual", OPT_SWITCH, &cfg.third_residual, "off|on"},
+    {"refine", OPT_SWITCH, &cfg.refine, "off|on"},
+    {"correction", OPT_SWITCH, &cfg.correction, "off|online"},
+    {"storage", OPT_SWITCH, &cfg.disk, "memory|disk"},
+    {"split-distance", OPT_SWITCH, &cfg.split_distance, "off|on"},
+    {"pq-subdim", OPT_COUNT, &cfg.pq_subdim, 0},
+    {"graph-entry", OPT_ENTRY, &cfg.graph_entry, 0},
+};
+#define OPTION_COUNT (sizeof(kOptions) / sizeof(kOptions[0]))
+
+/* A decimal count in [0, INT_MAX]; nothing else may follow the digits. */
+static int read_count(const char* text, int* out) {
+    if (!*text) return -1;
+    long long v = 0;
+    for (const char* p = text; *p; ++p) {
+        if (*p < '0' || *p > '9') return -1;
+        v = v * 10 + (*p - '0');
+        if (v > INT_MAX) return -1;
+    }
+    *out = (int)v;
     return 0;
 }
 
-static int choice(const char* s, const char* a, const char* b, int* v) {
-    if (!strcmp(s, a)) { *v = 0; return 0; }
-    if (!strcmp(s, b)) { *v = 1; return 0; }
+/* Index of `word` among the '|'-separated spellings, or -1. */
+static int spelling_index(const char* spellings, const char* word) {
+    const size_t len = strlen(word);
+    int index = 0;
+    for (const char* s = spellings;; ++index) {
+        const char* bar = strchr(s, '|');
+        const size_t n = bar ? (size_t)(bar - s) : strlen(s);
+        if (n == len && !strncmp(s, word, n)) return index;
+        if (!bar) return -1;
+        s = bar + 1;
+    }
+}
+
+static const OptSpec* find_option(const char* name) {
+    for (size_t i = 0; i < OPTION_COUNT; ++i)
+        if (!strcmp(kOptions[i].name, name)) return &kOptions[i];
+    return NULL;
+}
+
+/* 0 = stored, -1 = the value does not parse for this option. */
+static int store_option(const OptSpec* o, const char* value) {
+    switch (o->kind) {
+    case OPT_TEXT: *(const char**)o->field = value; return 0;
+    case OPT_COUNT: return read_count(value, (int*)o->field);
+    case OPT_ENTRY:
+        if (!strcmp(value, "-1")) { *(int*)o->field = -1; return 0; }
+        return read_count(value, (int*)o->field);
+    case OPT_SWITCH: {
+        const int k = spelling_index(o->spellings, value);
+        if (k < 0) return -1;
+        *(int*)o->field = k;
+        return 0;
+    }
+    }
     return -1;
 }
 
-/* config.c:61-118: 1 = help printed, -1 = invalid, 0 = run */
+static void print_help(void) {
+    puts("Rover search|build-index|insert|resume [options]\n"
+         "B200 build: `search` runs every query on the GPU through libcalculator.so.");
+    for (size_t i = 0; i < OPTION_COUNT; ++i)
+        if (kOptions[i].kind == OPT_COUNT || kOptions[i].kind == OPT_TEXT)
+            if (strcmp(kOptions[i].name, "pq-subdim")) printf("  --%s VALUE\n", kOptions[i].name);
+    fputs(" ", stdout);
+    for (size_t i = 0; i < OPTION_COUNT; ++i)
+        if (kOptions[i].kind == OPT_SWITCH) printf(" --%s %s", kOptions[i].name, kOptions[i].spellings);
+    puts("  --refine-all  --pq-subdim N  --graph-entry ID|-1");
+}
+
+/* ---- checks, in the reference's order (config.c:82-116) ---------------- */
+static int is(const char* a, const char* b) { return !strcmp(a, b); }
+static int pow2_upto(int v, int cap) { return v <= cap && !(v & (v - 1)); }
+
+static int rule_shape(const Config* c) { return c->n > 0 && c->dim > 0 && c->dim <= 1024; }
+static int rule_domain(const Config* c) { return c->domain <= 3 && c->unsigned_pd <= 1; }
+static int rule_degree(const Config* c) { return c->degree > 0 && c->degree < c->n; }
+static int rule_bits(const Config* c) {
+    return (c->sq_bits == 4 || c->sq_bits == 8) && (c->pq_bits == 4 || c->pq_bits == 8) &&
+           (c->residual_bits == 4 || c->residual_bits == 8);
+}
+static int rule_method(const Config* c) { return is(c->method, "sq") || is(c->method, "pq"); }
+static int rule_topk(const Config* c) {
+    return c->top_k > 0 && c->top_k <= 100 && c->pool >= c->top_k && c->pool <= 2000;
+}
+static int rule_expand(const Config* c) {
+    return c->expand_count >= 1 && c->expand_count <= 32 && c->graph_entry < c->n && c->rnn_s > 0 && c->rnn_t1 > 0;
+}
+static int rule_capacity(const Config* c) {
+    return c->entry_points > 0 && c->entry_points <= c->n && c->lanes > 0 && c->lanes <= 8 &&
+           c->source_window >= 1 && c->source_window <= 2;
+}
+static int rule_factors(const Config* c) {
+    const int cap = 2000 / c->top_k;
+    return c->first_factor > 0 && c->first_factor <= cap && c->refine_factor > 0 && c->refine_factor <= cap;
+}
+static int rule_cache_shape(const Config* c) {
+    return pow2_upto(c->cache_pages, 65536) && pow2_upto(c->refine_cache_pages, 65536);
+}
+static int rule_gt(const Config* c) { return c->gt_k > 0 && c->gt_k <= 1000000; }
+static int rule_cache_size(const Config* c) {
+    return c->cache_pages > 0 && (!c->third_residual || c->refine_cache_pages > 0);
+}
+static int rule_refine(const Config* c) { return !c->refine || c->correction; }
+static int rule_split(const Config* c) {
+    return !c->split_distance || (is(c->method, "sq") && c->sq_bits == 4 && c->correction && *c->bias);
+}
+static int rule_mode(const Config* c) { return is(c->search_mode, "sqmd") || is(c->search_mode, "db-pair"); }
+
+typedef struct { int (*holds)(const Config*); const char* message; } Rule;
+static const Rule kRules[] = {
+    {rule_shape, "n > 0 and dim in 1..1024 required"},
+    {rule_domain, "domain 0..3 and unsigned-pd 0/1 required"},
+    {rule_degree, "graph-degree must be in 1..n-1"},
+    {rule_bits, "code and residual bits must be 4 or 8"},
+    {rule_method, "method must be sq or pq"},
+    {rule_topk, "top-k 1..100; pool top-k..2000"},
+    {rule_expand, "invalid expand-count/graph-entry/RNN parameters"},
+    {rule_capacity, "invalid entry/lane/source-window capacity"},
+    {rule_factors, "candidate factor exceeds capacity"},
+    {rule_cache_shape, "cache pages must be powers of two up to 65536"},
+    {rule_gt, "invalid GT width"},
+    {rule_cache_size, "positive cache size required"},
+    {rule_refine, "coarse-only search with final residual refinement is outside this release"},
+    {rule_split, "split distance requires SQ4 online correction and a verified bias file"},
+    {rule_mode, "search-mode must be sqmd or db-pair"},
+};
+
+static int refuse(const char* message) {
+    fprintf(stderr, "Rover: %s\n", message);
+    return -1;
+}
+
+/* PQ grouping: at most one of --pq-subdim / --pq-m / --pq-compression picks
+ * M; without one, M = dim / 16.  Then the compression figure follows from M
+ * (config.c:99-105). */
+static int settle_pq_grouping(Config* c) {
+    const int chosen = (c->pq_subdim != 0) + (c->pq_m != 0) + (c->pq_compression != 0);
+    if (chosen > 1) return refuse("choose only one PQ grouping parameter");
+    if (c->pq_subdim) {
+        if (c->dim % c->pq_subdim) return refuse("PQ subdim must divide dim");
+        c->pq_m = c->dim / c->pq_subdim;
+    } else if (c->pq_compression) {
+        const int64_t bits_per_code = (int64_t)c->pq_compression * c->pq_bits;
+        const int64_t total_bits = (int64_t)c->dim * 32;
+        if (total_bits % bits_per_code) return refuse("non-integral PQ M");
+        c->pq_m = (int)(total_bits / bits_per_code);
+    } else if (!c->pq_m) {
+        if (c->dim % 16) return refuse("set pq-m or pq-subdim explicitly for this dimension");
+        c->pq_m = c->dim / 16;
+    }
+    if (!(c->pq_m > 0 && c->pq_m <= c->dim && c->dim % c->pq_m == 0)) return refuse("PQ M must divide dim");
+    c->pq_compression = c->dim * 4 / ((c->pq_m * c->pq_bits + 7) / 8);
+    return 0;
+}
+
+/* 1 = help printed, -1 = invalid, 0 = run */
 static int parse(int argc, char** argv) {
+    static const char* const commands[] = {"search", "build-index", "insert", "resume"};
     Config* c = &cfg;
-    int refine = 0, subdim = 0;
-    if (argc < 2 || !strcmp(argv[1], "--help")) {
-        puts("Rover search|build-index|insert|resume [options]\n"
-             "B200 build: `search` runs every query on the GPU through libcalculator.so.");
-        for (size_t i = 0; i < sizeof(options) / sizeof(*options); i++) printf("  --%s VALUE\n", options[i].name);
-        puts("  --third-residual off|on  --refine off|on  --refine-all\n  --correction off|online  "
-             "--storage memory|disk  --split-distance off|on  --pq-subdim N  --graph-entry ID|-1");
-        return 1;
-    }
+    config_defaults(c);
+    if (argc < 2 || is(argv[1], "--help")) { print_help(); return 1; }
     c->command = argv[1];
-    if (strcmp(c->command, "search") && strcmp(c->command, "build-index") && strcmp(c->command, "insert") &&
-        strcmp(c->command, "resume"))
-        return -1;
-    for (int i = 2; i < argc; i++) {
-        const char* key = argv[i];
-        int found = 0;
-        if (!strcmp(key, "--refine-all")) { c->refine_all = 1; continue; }
-        if (strncmp(key, "--", 2) || ++i >= argc) { fprintf(stderr, "Missing option value: %s\n", key); return -1; }
-        key += 2;
-        const char* v = argv[i];
-        if (!strcmp(key, "graph-entry")) {
-            if (!strcmp(v, "-1")) c->graph_entry = -1;
-            else if (number(v, &c->graph_entry)) return -1;
-            continue;
-        }
-        if (!strcmp(key, "third-residual")) { if (choice(v, "off", "on", &c->third_residual)) return -1; continue; }
-        if (!strcmp(key, "refine")) { if (choice(v, "off", "on", &refine)) return -1; continue; }
-        if (!strcmp(key, "correction")) { if (choice(v, "off", "online", &c->correction)) return -1; continue; }
-        if (!strcmp(key, "storage")) { if (choice(v, "memory", "disk", &c->disk)) return -1; continue; }
-        if (!strcmp(key, "split-distance")) { if (choice(v, "off", "on", &c->split_distance)) return -1; continue; }
-        if (!strcmp(key, "pq-subdim")) { if (number(v, &subdim)) return -1; continue; }
-        for (size_t j = 0; j < sizeof(options) / sizeof(*options); j++)
-            if (!strcmp(key, options[j].name)) {
-                char* field = (char*)c + options[j].offset;
-                if (options[j].integer) { if (number(v, (int*)field)) return -1; }
-                else *(const char**)field = v;
-                found = 1;
-                break;
-            }
-        if (!found) { fprintf(stderr, "Unknown option: --%s\n", key); return -1; }
+    int known = 0;
+    for (size_t i = 0; i < sizeof(commands) / sizeof(commands[0]); ++i) known |= is(c->command, commands[i]);
+    if (!known) return -1;
+    for (int i = 2; i < argc; ++i) {
+        const char* arg = argv[i];
+        if (is(arg, "--refine-all")) { c->refine_all = 1; continue; }
+        if (strncmp(arg, "--", 2) || i + 1 >= argc) { fprintf(stderr, "Missing option value: %s\n", arg); return -1; }
+        const OptSpec* o = find_option(arg + 2);
+        const char* value = argv[++i];
+        if (!o) { fprintf(stderr, "Unknown option: %s\n", arg); return -1; }
+        if (store_option(o, value)) return -1;
     }
-#define REQUIRE(test, message) do { if (!(test)) { fprintf(stderr, "Rover: %s\n", message); return -1; } } while (0)
-    REQUIRE(c->n > 0 && c->dim > 0 && c->dim <= 1024, "n > 0 and dim in 1..1024 required");
-    REQUIRE(c->domain <= 3 && c->unsigned_pd <= 1, "domain 0..3 and unsigned-pd 0/1 required");
-    REQUIRE(c->degree > 0 && c->degree < c->n, "graph-degree must be in 1..n-1");
-    REQUIRE((c->sq_bits == 4 || c->sq_bits == 8) && (c->pq_bits == 4 || c->pq_bits == 8) &&
-                (c->residual_bits == 4 || c->residual_bits == 8),
-            "code and residual bits must be 4 or 8");
-    REQUIRE(!strcmp(c->method, "sq") || !strcmp(c->method, "pq"), "method must be sq or pq");
-    REQUIRE(c->top_k > 0 && c->top_k <= 100 && c->pool >= c->top_k && c->pool <= 2000, "top-k 1..100; pool top-k..2000");
-    REQUIRE(c->expand_count >= 1 && c->expand_count <= 32 && c->graph_entry < c->n && c->rnn_s > 0 && c->rnn_t1 > 0,
-            "invalid expand-count/graph-entry/RNN parameters");
-    REQUIRE(c->entry_points > 0 && c->entry_points <= c->n && c->lanes > 0 && c->lanes <= 8 && c->source_window >= 1 &&
-                c->source_window <= 2,
-            "invalid entry/lane/source-window capacity");
-    REQUIRE(c->first_factor > 0 && c->first_factor <= 2000 / c->top_k && c->refine_factor > 0 &&
-                c->refine_factor <= 2000 / c->top_k,
-            "candidate factor exceeds capacity");
-    REQUIRE(c->cache_pages <= 65536 && !(c->cache_pages & (c->cache_pages - 1)) && c->refine_cache_pages <= 65536 &&
-                !(c->refine_cache_pages & (c->refine_cache_pages - 1)),
-            "cache pages must be powers of two up to 65536");
-    REQUIRE(c->gt_k > 0 && c->gt_k <= 1000000, "invalid GT width");
-    REQUIRE(c->cache_pages > 0 && (!c->third_residual || c->refine_cache_pages > 0), "positive cache size required");
-    REQUIRE(!refine || c->correction, "coarse-only search with final residual refinement is outside this release");
-    REQUIRE(!c->split_distance || (!strcmp(c->method, "sq") && c->sq_bits == 4 && c->correction && *c->bias),
-            "split distance requires SQ4 online correction and a verified bias file");
-    REQUIRE(!strcmp(c->search_mode, "sqmd") || !strcmp(c->search_mode, "db-pair"), "search-mode must be sqmd or db-pair");
-    if (!strcmp(c->method, "pq")) {
-        REQUIRE(strcmp(c->search_mode, "db-pair"), "PQ supports SQMD; DB Pair is an SQ path");
-        REQUIRE((!!subdim + !!c->pq_m + !!c->pq_compression) <= 1, "choose only one PQ grouping parameter");
-        if (subdim) { REQUIRE(c->dim % subdim == 0, "PQ subdim must divide dim"); c->pq_m = c->dim / subdim; }
-        if (c->pq_compression) {
-            int64_t divisor = (int64_t)c->pq_compression * c->pq_bits;
-            REQUIRE((c->dim * 32) % divisor == 0, "non-integral PQ M");
-            c->pq_m = (int)((c->dim * 32) / divisor);
-        }
-        if (!c->pq_m) { REQUIRE(c->dim % 16 == 0, "set pq-m or pq-subdim explicitly for this dimension"); c->pq_m = c->dim / 16; }
-        REQUIRE(c->pq_m > 0 && c->pq_m <= c->dim && c->dim % c->pq_m == 0, "PQ M must divide dim");
-        c->pq_compression = c->dim * 4 / ((c->pq_m * c->pq_bits + 7) / 8);
+    for (size_t r = 0; r < sizeof(kRules) / sizeof(kRules[0]); ++r)
+        if (!kRules[r].holds(c)) return refuse(kRules[r].message);
+    if (is(c->method, "pq")) {
+        if (is(c->search_mode, "db-pair")) return refuse("PQ supports SQMD; DB Pair is an SQ path");
+        if (settle_pq_grouping(c)) return -1;
         c->search_mode = "pure_pq";
-    } else if (!strcmp(c->search_mode, "db-pair")) {
+    } else if (is(c->search_mode, "db-pair")) {
         c->search_mode = "db_pair";
     }
-    c->refine_mode = refine ? (c->third_residual ? 2 : 1) : 0;
-    REQUIRE(!c->third_residual, "the third-level (ERROR4) refine is not part of this build");
-    REQUIRE(!c->split_distance, "the SQ4 split-distance correction is not part of this build");
-    REQUIRE(strcmp(c->search_mode, "db_pair"), "the DB-pair search mode is not part of this build");
-    if (!strcmp(c->command, "search"))
-        REQUIRE(c->nq > 0 && c->top_k <= c->n && *c->query && (*c->graph || *c->index_dir),
-                "search requires query, graph, nq and top-k <= n");
-    REQUIRE(c->train_iters > 0 && c->train_samples > 0, "positive PQ training settings required");
+    c->refine_mode = c->refine ? 1 + (c->third_residual != 0) : 0;
+    if (c->third_residual) return refuse("the third-level (ERROR4) refine is not part of this build");
+    if (c->split_distance) return refuse("the SQ4 split-distance correction is not part of this build");
+    if (is(c->search_mode, "db_pair")) return refuse("the DB-pair search mode is not part of this build");
+    if (is(c->command, "search") &&
+        !(c->nq > 0 && c->top_k <= c->n && *c->query && (*c->graph || *c->index_dir)))
+        return refuse("search requires query, graph, nq and top-k <= n");
+    if (!(c->train_iters > 0 && c->train_samples > 0)) return refuse("positive PQ training settings required");
     return 0;
 }
 
@@ -211,52 +339,100 @@ static unsigned long long now_us(void) {
     return (unsigned long long)ts.tv_sec * 1000000ull + (unsigned long long)ts.tv_nsec / 1000ull;
 }
 
-/* results.jsonl and the order map (config.c:121-156) */
-static FILE* results;
-static int *original_ids, *index_ids;
+/* ---- results ------------------------------------------------------------
+ *
+ * --order-map lists, for each index row, the original id of the vector
+ * stored there: a permutation of 0..n-1 as whitespace-separated decimals.
+ * Results are written in original ids; ground truth (original ids) is
+ * translated to index ids.  Each results.jsonl line is
+ * {"query":Q,"ids":[...],"distances":[...]} with distances in %.9g, the
+ * reference's format (config.c:145-156), built in memory and written once. */
+typedef struct {
+    FILE* out;
+    int* to_original;   /* index row -> original id, NULL without a map */
+    int* to_index;      /* original id -> index row */
+    char* line;
+    size_t cap;
+} ResultSink;
+
+static ResultSink sink;
+
+static int load_order_map(const char* path, int n) {
+    FILE* f = fopen(path, "rb");
+    if (!f) return -1;
+    fseek(f, 0, SEEK_END);
+    const long size = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    char* text = size >= 0 ? (char*)malloc((size_t)size + 1) : NULL;
+    const int ok_read = text && fread(text, 1, (size_t)size, f) == (size_t)size;
+    fclose(f);
+    sink.to_original = (int*)malloc((size_t)n * sizeof(int));
+    sink.to_index = (int*)malloc((size_t)n * sizeof(int));
+    if (!ok_read || !sink.to_original || !sink.to_index) { free(text); return -1; }
+    text[size] = 0;
+    for (int i = 0; i < n; ++i) sink.to_index[i] = -1;
+    const char* p = text;
+    int rows = 0, bad = 0;
+    for (;;) {
+        while (*p && isspace((unsigned char)*p)) ++p;
+        if (!*p) break;
+        char* end;
+        errno = 0;
+        const long id = strtol(p, &end, 10);
+        if (end == p || errno || rows >= n || id < 0 || id >= n || sink.to_index[id] != -1) { bad = 1; break; }
+        sink.to_original[rows] = (int)id;
+        sink.to_index[id] = rows++;
+        p = end;
+    }
+    free(text);
+    return bad || rows != n ? -1 : 0;
+}
 
 static int results_open(void) {
-    if (*cfg.order_map) {
-        FILE* map = fopen(cfg.order_map, "r");
-        original_ids = (int*)malloc((size_t)cfg.n * sizeof(int));
-        index_ids = (int*)malloc((size_t)cfg.n * sizeof(int));
-        if (!map || !original_ids || !index_ids) { if (map) fclose(map); return -1; }
-        for (int i = 0; i < cfg.n; i++) index_ids[i] = -1;
-        for (int i = 0; i < cfg.n; i++) {
-            int id;
-            if (fscanf(map, "%d", &id) != 1 || id < 0 || id >= cfg.n || index_ids[id] != -1) { fclose(map); return -1; }
-            original_ids[i] = id;
-            index_ids[id] = i;
-        }
-        int extra;
-        if (fscanf(map, "%d", &extra) != EOF) { fclose(map); return -1; }
-        fclose(map);
+    if (*cfg.order_map && load_order_map(cfg.order_map, cfg.n)) return -1;
+    sink.out = fopen(cfg.output, "wx");
+    return sink.out ? 0 : -1;
+}
+
+static int append(size_t* len, const char* fmt, ...) {
+    for (;;) {
+        va_list ap;
+        va_start(ap, fmt);
+        const int n = vsnprintf(sink.line + *len, sink.cap - *len, fmt, ap);
+        va_end(ap);
+        if (n < 0) return -1;
+        if (*len + (size_t)n < sink.cap) { *len += (size_t)n; return 0; }
+        const size_t cap = sink.cap ? 2 * sink.cap + (size_t)n : 4096;
+        char* grown = (char*)realloc(sink.line, cap);
+        if (!grown) return -1;
+        sink.line = grown;
+        sink.cap = cap;
     }
-    results = fopen(cfg.output, "wx");
-    return results ? 0 : -1;
 }
 
 static int write_result(int query, const int* ids, const float* distances, int count) {
+    if (!sink.out) return -1;
     for (int i = 0; i < count; i++)
         if (ids[i] < 0 || ids[i] >= cfg.n || (distances && !isfinite(distances[i]))) return -1;
-    if (!results) return -1;
-    fprintf(results, "{\"query\":%d,\"ids\":[", query);
-    for (int i = 0; i < count; i++) fprintf(results, "%s%d", i ? "," : "", original_ids ? original_ids[ids[i]] : ids[i]);
-    fprintf(results, "],\"distances\":[");
-    for (int i = 0; i < count; i++) fprintf(results, "%s%.9g", i ? "," : "", distances ? distances[i] : 0.0);
-    fprintf(results, "]}\n");
-    return ferror(results) ? -1 : 0;
+    size_t len = 0;
+    int rc = append(&len, "{\"query\":%d,\"ids\":[", query);
+    for (int i = 0; !rc && i < count; i++)
+        rc = append(&len, i ? ",%d" : "%d", sink.to_original ? sink.to_original[ids[i]] : ids[i]);
+    if (!rc) rc = append(&len, "],\"distances\":[");
+    for (int i = 0; !rc && i < count; i++) rc = append(&len, i ? ",%.9g" : "%.9g", distances ? distances[i] : 0.0);
+    if (!rc) rc = append(&len, "]}\n");
+    if (rc || fwrite(sink.line, 1, len, sink.out) != len) return -1;
+    return 0;
 }
 
 static int results_close(void) {
-    const int rc = results ? fclose(results) : 0;
-    results = NULL;
-    free(original_ids);
-    free(index_ids);
-    original_ids = index_ids = NULL;
+    const int rc = sink.out ? fclose(sink.out) : 0;
+    free(sink.to_original);
+    free(sink.to_index);
+    free(sink.line);
+    memset(&sink, 0, sizeof(sink));
     return rc;
 }
-
 static int recall_hits(const int* ids, int count, const int32_t* gt_row, int gt_k, int k) {
     int hits = 0;
     for (int i = 0; i < k && i < count; i++)
@@ -491,9 +667,9 @@ static int search(remote_handle64 h) {
         free(queries);
         return -1;
     }
-    if (gt && index_ids)   /* ground truth in original ids -> index ids (support.c:2273) */
+    if (gt && sink.to_index)   /* ground truth in original ids -> index ids (support.c:2273) */
         for (size_t j = 0; j < (size_t)cfg.nq * cfg.gt_k; j++)
-            if (gt[j] >= 0 && gt[j] < cfg.n) gt[j] = index_ids[gt[j]];
+            if (gt[j] >= 0 && gt[j] < cfg.n) gt[j] = sink.to_index[gt[j]];
     if (pq) {
         printf("RETRIEVAL_DB_MODE=pure_pq\n\n=== Pure-PQ SQMD Search (B200) ===\n");
         printf("dataset=%s N=%d dim=%d bits=%d M=%d Ks=%d compression=%dx correction=%s residual_bits=%d result=%s\n",

@@ -13,7 +13,7 @@ fixture directory written as {dir}.  The ground-truth file the runs evaluate
 against (cli_gt.ivecs) holds, per query, the reference's own top-10 of the fixture's
 first golden search padded with -1 to 100 columns.
 
-Usage: python tests/golden/make_cli_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_cli_golden.py --reference REFERENCE_CHECKOUT (or $ROVER_REFERENCE)
 """
 from __future__ import annotations
 
@@ -78,7 +78,9 @@ def relative(args: list[str], d: Path) -> list[str]:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("ROVER_REFERENCE"),
+                    required="ROVER_REFERENCE" not in os.environ,
+                    help="reference checkout (default: $ROVER_REFERENCE)")
     args = ap.parse_args()
     bindings.build(args.reference)
     rover_ref = ROOT / "oracle" / "_ref" / "rover_ref"

@@ -16,11 +16,12 @@ For each fixture it
   4. stores the reference's independent NumPy ADC known-answer values
      (build_pure_pq_index.reference_adc) next to them.
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py --reference REFERENCE_CHECKOUT (or $ROVER_REFERENCE)
 """
 from __future__ import annotations
 
 import argparse
+import os
 import hashlib
 import json
 import shutil
@@ -194,7 +195,9 @@ def make_sq(ref_tools, ref, name, n, dim, comps, sq_bits, rbits, degree, prune, 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("ROVER_REFERENCE"),
+                    required="ROVER_REFERENCE" not in os.environ,
+                    help="reference checkout (default: $ROVER_REFERENCE)")
     args = ap.parse_args()
     tools = Path(args.reference) / "tools"
     sys.path.insert(0, str(tools))

@@ -126,3 +126,98 @@ def test_noalloc_rejects_requests_beyond_its_scratch():
                                                 C.byref(_ptrs(cm, out, 10)), None)
     assert rc == 14  # AEE_EBADPARM
     assert "no-alloc scratch" in calc.last_error()
+
+
+def _noalloc(lib, cm):
+    lib.calculator_rover_pq_search_noalloc.argtypes = [C.c_uint64, C.POINTER(cm.SearchParams), cm._f32p,
+                                                       C.c_int32, cm._i32p, C.c_int32, cm._i32p,
+                                                       C.POINTER(cm.SearchOutputs), C.c_void_p]
+    return lib.calculator_rover_pq_search_noalloc
+
+
+def _chain_index(n=5000):
+    """A path graph 0 -> 1 -> ... -> n-1 whose ADC distances to the zero
+    query fall strictly along the path: a search with a one-entry pool walks
+    the whole chain, claiming one new id per expansion."""
+    from rover_b200 import bundle as B
+    m, ks, sub = 2, 256, 4
+    graph = np.full((n, 1), -1, np.int32)
+    graph[:-1, 0] = np.arange(1, n, dtype=np.int32)
+    book = np.zeros((m, ks, sub), np.float32)
+    book[0] = np.sqrt(250.0 * np.arange(ks, dtype=np.float64))[:, None].astype(np.float32)   # LUT0 ~ 1000 k
+    book[1] = np.sqrt(np.arange(ks, dtype=np.float64) / 4.0)[:, None].astype(np.float32)     # LUT1 ~ k
+    v = (n - 1 - np.arange(n)).astype(np.int64)
+    codes = np.stack([v // 256, v % 256], axis=1).astype(np.uint8)
+    rows = np.zeros((n, m * sub), np.uint8)
+    qp = np.tile(np.array([[0.01, 0.0]], np.float32), (n, 1))
+    return graph, B.PqBundle(B.PqMeta(b"\x05" * 16, n, m * sub, m, ks, sub, m), book, codes, 8,
+                             B.pack_residual_blocks(rows), qp)
+
+
+def test_noalloc_table_overflow_fails_the_call():
+    """A query that claims more ids than its visited table's load limit
+    (half of 4,096 entries here) fails the call with AEE_EFAILED and the
+    overflow message; the query's status says which one, and the scratch is
+    fit for the next call."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from rover_b200 import calculator as cm
+
+    calc = cm.Calculator()
+    fn = _noalloc(calc.lib, cm)
+    graph, bundle = _chain_index()
+    calc.pq_load(graph, 0, bundle)
+    dev = torch.device("cuda", 0)
+    nq = 2
+    q = torch.zeros((nq, 8), dtype=torch.float32, device=dev)
+    pools = torch.ones(nq, dtype=torch.int32, device=dev)
+    out = _device_outputs(torch, nq, 1, 1)
+    params = calc.params(entry_points=1, expand_count=1, correction=0, refine_budget=0, top_k=1, pool_stride=1)
+    rc = fn(calc.handle, C.byref(params), C.cast(C.c_void_p(q.data_ptr()), cm._f32p), nq,
+            C.cast(C.c_void_p(pools.data_ptr()), cm._i32p), 1, None, C.byref(_ptrs(cm, out, 1)), None)
+    torch.cuda.synchronize()
+    assert rc == 1, calc.last_error()   # AEE_EFAILED
+    assert "exceeded its visited table" in calc.last_error()
+    assert torch.equal(out["status"].cpu(), torch.full((nq,), 3, dtype=torch.int32))   # ROVER_QUERY_TABLE_FULL
+    # the allocating entry retries with a larger table and walks the chain to its end
+    r = calc.pq_search(np.zeros((1, 8), np.float32), 1, top_k=1, entry_points=1, expand_count=1, correction=0,
+                       refine_budget=0)
+    assert int(r["ids"][0, 0]) == graph.shape[0] - 1
+    # a request the table holds succeeds on the same scratch afterwards
+    pools_ok = torch.ones(nq, dtype=torch.int32, device=dev)
+    out2 = _device_outputs(torch, nq, 1, 1)
+    short = np.full((graph.shape[0], 1), -1, np.int32)
+    short[:100, 0] = np.arange(1, 101)
+    calc.pq_load(short, 0, bundle)
+    rc = fn(calc.handle, C.byref(params), C.cast(C.c_void_p(q.data_ptr()), cm._f32p), nq,
+            C.cast(C.c_void_p(pools_ok.data_ptr()), cm._i32p), 1, None, C.byref(_ptrs(cm, out2, 1)), None)
+    torch.cuda.synchronize()
+    assert rc == 0, calc.last_error()
+    assert torch.equal(out2["ids"][:, 0].cpu(), torch.full((nq,), 100, dtype=torch.int32))
+
+
+def test_noalloc_refuses_modes_it_does_not_run():
+    """The no-alloc entry runs the exact search over packed rows: a batched,
+    gated or decoded-layout request is refused, not silently run otherwise."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from rover_b200 import calculator as cm
+
+    calc = cm.Calculator()
+    fn = _noalloc(calc.lib, cm)
+    data, graph, bundle, golden, queries = load_fixture("pq8_d64")
+    calc.pq_load(graph, data["graph_entry"], bundle)
+    dev = torch.device("cuda", 0)
+    nq = 4
+    q = torch.from_numpy(np.ascontiguousarray(queries[:nq])).to(dev)
+    pools = torch.full((nq,), 32, dtype=torch.int32, device=dev)
+    for kw in (dict(mode=1), dict(mode=2), dict(layout=2)):
+        out = _device_outputs(torch, nq, 10, 32)
+        params = calc.params(entry_points=4, expand_count=16, correction=1, refine_budget=20, top_k=10,
+                             pool_stride=32, **kw)
+        rc = fn(calc.handle, C.byref(params), C.cast(C.c_void_p(q.data_ptr()), cm._f32p), nq,
+                C.cast(C.c_void_p(pools.data_ptr()), cm._i32p), 32, None, C.byref(_ptrs(cm, out, 10)), None)
+        assert rc == 14, kw   # AEE_EBADPARM
+        assert "ROVER_MODE_EXACT" in calc.last_error()
