@@ -6,19 +6,28 @@ the learned-gate batched form against the plain drop-in.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Plain drop-in: the exact mode (the reference's expansion order, every
-candidate corrected) at the operating point picked by the calibration (entry
-points as multiples of the mixture's cluster count x beam width L in
-{32, 64, 128, 256}: the least-work point whose recall@10 reaches 0.95).
-Learned-gate batched form: the gate is trained on the device from traces of
-8,000 held-out queries (plain search, full correction), then its thresholds,
-beam width, entry points and L are calibrated for the fastest point whose
-recall@10 reaches 0.95 on the full query set.  A step is one batched search
-of the 10,000 queries.  ``value`` (the gated form) is device-timed with
-inputs resident in HBM, the plain form's figures sit in ``config.plain``;
-``e2e`` is the gated step through the host-buffer C-ABI call with the
-host->device query copy and the device->host result copy inside the timed
-region.  Multi-GPU runs are replicas (each rank searches its own 10,000
+Every form picks its operating point on 2,000 held-out calibration queries
+(their own exact neighbours; target recall@10 0.95 plus a 0.003 margin) and
+is then timed, with its recall reported, on the 10,000 timed queries:
+
+* plain drop-in: the exact mode (the reference's expansion order, every
+  candidate corrected); entry points as multiples of the mixture's cluster
+  count x beam width L in {32, 40, 48, 64, 96, 128, 192, 256}; the
+  least-work point reaching the target;
+* batched: W pool entries expanded per step, every candidate corrected, no
+  network; the fastest point over W, entry points and L;
+* gated: the learned gate (trained on the device from traces of 8,000
+  other held-out queries) with thresholds under which its MLP is consulted;
+  the fastest point; the MLP rows evaluated per query are counted.
+
+Equal-point comparisons isolate the parts: batched at the plain form's
+(L, entry points) and batched without the network at the gated form's
+(W, L, entry points).  A step is one batched search of the 10,000 queries.
+``value`` (the gated form, or the batched form when no gated point reaches
+the target) is device-timed with inputs resident in HBM; the other forms'
+figures sit in ``config.plain`` and ``config.forms``; ``e2e`` is the
+headline form through the host-buffer C-ABI call with the host->device query
+copy and the device->host result copy inside the timed region.  Multi-GPU runs are replicas (each rank searches its own 10,000
 queries; no collective on the data path) and report weak scaling.
 
 After the headline, the SQ section (``config.sq``, skipped with --no-sq)
@@ -54,12 +63,20 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "pq_1m_d128"
-L_SWEEP = (32, 48, 64, 96, 128, 192, 256)
+L_SWEEP = (32, 40, 48, 64, 96, 128, 192, 256)
+FREE_L_SWEEP = (16, 24) + L_SWEEP   # batched / gated forms may go below the plain grid
 EP_MULTIPLES = (0.25, 1, 2, 4)   # entry points as multiples of the mixture's cluster count
 TOP_K = 10
 REFINE_BUDGET = 20      # refine_factor 2 x top_k
 TARGET_RECALL = 0.95
+# Every form picks its operating point on the same held-out calibration
+# queries (another sample of the mixture, with their own exact neighbours)
+# and is then timed, and its recall reported, on the separate timed queries.
+# The calibration target carries a small margin so that the point still
+# reaches the target on the timed set.
 CALIBRATION_QUERIES = 2000
+CALIBRATION_OFFSET = 13      # seed offset of the calibration sample (the gate trains on offset 7)
+CALIBRATION_MARGIN = 0.003
 TRAIN_QUERIES = 8000       # held-out queries traced for the gate (about 5M rows)
 GATE_ROWS = 5_000_000
 GATE_EPOCHS = 4
@@ -161,16 +178,22 @@ def seed_pass_bytes(nq: int, seeds: int, md, rcb: int, corrected: bool) -> int:
     return int(nq * seeds * (md.code_bytes + ((rcb + 8) if corrected else 0)))
 
 
-def calibrate(search, w, comps, log_prefix=""):
-    """Operating point: for each entry-point count (multiples of the mixture's
-    cluster count) the smallest L of the sweep whose recall@10 on the first
-    CALIBRATION_QUERIES queries reaches the target; among those, the point
-    with the fewest scored candidates per query (the least work).  The rule
-    only uses recall and the search's own statistics, so the reference and
-    this library -- whose searches are identical -- choose the same point."""
+def calibration_set(args):
+    """The held-out calibration queries and their exact neighbours."""
+    from rover_b200 import workloads
+    return workloads.held_out_set(args.workload, CALIBRATION_QUERIES, CALIBRATION_OFFSET, cache_dir=args.cache_dir)
+
+
+def calibrate(search, cal, comps, log_prefix=""):
+    """The exact search's operating point on the calibration set: for each
+    entry-point count (multiples of the mixture's cluster count) the smallest
+    L of the sweep whose recall@10 reaches the target plus the margin; among
+    those, the point with the fewest scored candidates per query (the least
+    work).  The rule only uses recall and the search's own statistics, so the
+    reference and this library -- whose searches are identical -- choose the
+    same point."""
     from rover_b200.workloads import recall_at_k
-    nc = min(CALIBRATION_QUERIES, len(w.queries))
-    qs, gt = w.queries[:nc], w.gt[:nc]
+    qs, gt = cal
     table, chosen = [], None
     for mult in EP_MULTIPLES:
         ep = max(1, int(round(mult * comps)))
@@ -180,7 +203,7 @@ def calibrate(search, w, comps, log_prefix=""):
             work = float(r["stats"][:, 0].mean())
             table.append({"entry_points": ep, "L": L, "recall_at_10": rec, "scored": work})
             log(f"{log_prefix}calibration ep={ep} L={L} recall@10={rec:.4f} scored={work:.0f}")
-            if rec >= TARGET_RECALL:
+            if rec >= TARGET_RECALL + CALIBRATION_MARGIN:
                 if chosen is None or work < chosen[2]:
                     chosen = (ep, L, work)
                 break
@@ -208,7 +231,8 @@ def reference_arm(args, w, rank) -> dict:
         def search(qs, L, ep):
             return ref.pq_search(h, w.graph, w.entry, qs, L, ep, expand, correction=1,
                                  refine_budget=REFINE_BUDGET, top_k=TOP_K, threads=threads)
-        ep_chosen, chosen, table = calibrate(search, w, CONFIGS[args.workload]["comps"], "reference ")
+        ep_chosen, chosen, table = calibrate(search, calibration_set(args), CONFIGS[args.workload]["comps"],
+                                             "reference ")
         # size the per-step sample to ~5 s of work
         probe = w.queries[:max(threads * 2, 64)]
         t0 = time.perf_counter()
@@ -443,8 +467,7 @@ def main():
         print(json.dumps(reference_arm(args, w, rank)), flush=True)
         return 0
 
-    from rover_b200 import gate as gate_mod
-    from rover_b200.calculator import MODE_GATED, Calculator
+    from rover_b200.calculator import Calculator
     calc = Calculator()
     calc.pq_load(w.graph, w.entry, w.bundle)
     md = w.bundle.meta
@@ -453,71 +476,51 @@ def main():
     rcb = w.bundle.residual_code_bytes
     from rover_b200.workloads import CONFIGS
 
-    # ---- plain drop-in: exact mode, calibrated operating point
+    # ---- plain drop-in: exact mode, operating point from the calibration set
+    cal = calibration_set(args)
     if args.L and args.ep:
         L, ep, table = args.L, args.ep, []
     else:
         def search(qs, L_, ep_):
             return calc.pq_search(qs, L_, top_k=TOP_K, entry_points=ep_, expand_count=expand, correction=1,
                                   refine_budget=REFINE_BUDGET)
-        ep, L, table = calibrate(search, w, CONFIGS[args.workload]["comps"])
+        ep, L, table = calibrate(search, cal, CONFIGS[args.workload]["comps"])
     from rover_b200 import replicas
     ep, L = replicas.from_rank0(dist, (ep, L))     # every replica times rank 0's operating point
     kw = dict(entry_points=ep, expand_count=expand, correction=1, refine_budget=REFINE_BUDGET)
     final = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
     recall = workloads.recall_at_k(final["ids"], final["counts"], w.gt, TOP_K)
-    # the calibration subset can pass while the full set falls just short:
-    # widen the beam until the full query set meets the target
-    while recall < TARGET_RECALL and not (args.L and args.ep):
-        wider = [x for x in L_SWEEP + (512, 1024) if x > L]
-        if not wider:
-            break
-        L = wider[0]
-        final = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
-        recall = workloads.recall_at_k(final["ids"], final["counts"], w.gt, TOP_K)
-    L0 = replicas.from_rank0(dist, L)
-    if L0 != L:       # widened differently than rank 0: use rank 0's beam
-        L = L0
-        final = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
-        recall = workloads.recall_at_k(final["ids"], final["counts"], w.gt, TOP_K)
-    log(f"plain operating point ep={ep} L={L} recall@10={recall:.4f}")
+    log(f"plain operating point ep={ep} L={L} recall@10={recall:.4f} (timed set)")
     stats = final["stats"]
     plain_bytes = algorithmic_bytes(stats, final["counts"], md, rcb, expand, md.dim)
 
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     q_d = torch.from_numpy(w.queries).to(dev)
-    pool_d = torch.full((nq,), L, dtype=torch.int32, device=dev)
-    out = dict(ids=torch.empty((nq, TOP_K), dtype=torch.int32, device=dev),
-               dists=torch.empty((nq, TOP_K), dtype=torch.float32, device=dev),
-               counts=torch.empty(nq, dtype=torch.int32, device=dev),
-               status=torch.empty(nq, dtype=torch.int32, device=dev),
-               stats=torch.empty((nq, 4), dtype=torch.int64, device=dev))
-    ptrs = {k: v.data_ptr() for k, v in out.items()}
-    ptrs["stride"] = TOP_K
-
-    def plain_step():
-        calc.pq_search_device(q_d.data_ptr(), nq, pool_d.data_ptr(), ptrs, stream_ptr=stream.cuda_stream,
-                              top_k=TOP_K, **kw)
-
-    plain = device_steps(calc, args, plain_step, stream, dist, dev)
-    plain_qps = nq * args.steps * world / (plain["total_ms"] / 1e3)
+    plain_kw = dict(kw, mode=0)
+    plain = timed_form(calc, args, w, q_d, L, plain_kw, stream, dist, dev, world)
+    plain_qps = plain["qps"]
     plain_seed = seed_pass_bytes(nq, min(ep, md.num_vectors), md, rcb, True)
-    plain_roof = roofline(plain_bytes, plain_seed, plain["kernels"], args.steps, nq, "plain")
-    log(f"plain {plain_qps:,.0f} QPS ({plain['ms_per_step']:.3f} ms/step)")
+    plain_roof = roofline(plain_bytes, plain_seed, plain["steps"]["kernels"], args.steps, nq, "plain")
+    log(f"plain {plain_qps:,.0f} QPS ({plain['steps']['ms_per_step']:.3f} ms/step)")
 
-    # ---- learned-gate batched form
-    gated = None
+    # ---- batched form (no gate) and learned-gate batched form
+    forms = None
     if not args.no_gate:
-        gated = gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world)
+        forms = free_forms(calc, w, args, cal, ep, L, expand, q_d, stream, dist, dev, world, plain)
+    gated = forms["gated"] if forms else None
 
     if gated:
         head = gated
         mode_kw = gated["kw"]
         head_L = gated["L"]
+    elif forms:
+        head = forms["batched"]
+        mode_kw = head["kw"]
+        head_L = head["L"]
     else:
-        head = dict(qps=plain_qps, steps=plain, recall=recall, stats=stats, roof=plain_roof)
-        mode_kw = kw
+        head = dict(qps=plain_qps, steps=plain["steps"], recall=recall, stats=stats, roof=plain_roof)
+        mode_kw = plain_kw
         head_L = L
 
     # end to end through the host-buffer entry point (pinned host memory)
@@ -561,14 +564,19 @@ def main():
         "config": {"workload": args.workload, "n": md.num_vectors, "dim": md.dim, "pq": f"M={md.m}x{md.ks}",
                    "residual_bits": w.bundle.residual_bits, "graph_degree": int(w.graph.shape[1]),
                    "queries_per_step": nq, "top_k": TOP_K, "refine_budget": REFINE_BUDGET, "expand_count": expand,
-                   "mode": "gated (learned gate, batched)" if gated else "exact (reference expansion order)",
+                   "mode": ("gated (learned gate evaluated in the timed searches, batched)" if gated else
+                            "batched (no network: no gated point reached the target)" if forms else
+                            "exact (reference expansion order)"),
                    "recall_at_10": head["recall"],
-                   "plain": {"qps": plain_qps, "ms_per_step": plain["ms_per_step"], "recall_at_10": recall,
+                   "calibration_set": f"{CALIBRATION_QUERIES} held-out queries (seed offset {CALIBRATION_OFFSET}), "
+                                      f"target recall@10 {TARGET_RECALL} + {CALIBRATION_MARGIN} margin; "
+                                      "recall reported on the timed queries",
+                   "plain": {"qps": plain_qps, "ms_per_step": plain["steps"]["ms_per_step"], "recall_at_10": recall,
                              "entry_points": ep, "beam_L": L, "kernel_ms_per_step":
-                                 {k: v[1] / args.steps for k, v in plain["kernels"].items()},
+                                 {k: v[1] / args.steps for k, v in plain["steps"]["kernels"].items()},
                              "roofline": plain_roof, "calibration": table},
-                   "gated_over_plain": head["qps"] / plain_qps if gated else 1.0,
-                   "gate": gated["report"] if gated else None,
+                   "gated_over_plain": head["qps"] / plain_qps if gated else None,
+                   "forms": forms["report"] if forms else None,
                    "uneven": uneven,
                    "sq": sq,
                    "parallelism": f"replicas x{world}",
@@ -792,15 +800,55 @@ def uneven_section(calc, args, stream, dist, dev, world):
             "plan_over_direct": plan_qps / direct_qps, "identical_outputs": identical}
 
 
-def gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world):
-    """Train the gate on traces of held-out queries, calibrate its
-    thresholds and beam, time it; also the same search with the MLP replaced
-    by a plain ADC/worst ratio threshold (the method without the network)."""
+def timed_form(calc, args, w, q_d, L, kw, stream, dist, dev, world):
+    """One form at one operating point on the timed queries: a host-buffer
+    search for recall and statistics, then the warm-up and timed device
+    steps (queries resident in HBM, outputs written to device buffers)."""
     import torch
+    from rover_b200.workloads import recall_at_k
+    nq = len(w.queries)
+    r = calc.pq_search(w.queries, L, top_k=TOP_K, **kw)
+    rec = recall_at_k(r["ids"], r["counts"], w.gt, TOP_K)
+    pool_d = torch.full((nq,), L, dtype=torch.int32, device=dev)
+    out = dict(ids=torch.empty((nq, TOP_K), dtype=torch.int32, device=dev),
+               dists=torch.empty((nq, TOP_K), dtype=torch.float32, device=dev),
+               counts=torch.empty(nq, dtype=torch.int32, device=dev),
+               status=torch.empty(nq, dtype=torch.int32, device=dev),
+               stats=torch.empty((nq, 4), dtype=torch.int64, device=dev))
+    ptrs = {k: v.data_ptr() for k, v in out.items()}
+    ptrs["stride"] = TOP_K
+
+    def step():
+        calc.pq_search_device(q_d.data_ptr(), nq, pool_d.data_ptr(), ptrs, stream_ptr=stream.cuda_stream,
+                              top_k=TOP_K, **kw)
+
+    steps = device_steps(calc, args, step, stream, dist, dev)
+    qps = nq * args.steps * world / (steps["total_ms"] / 1e3)
+    return dict(qps=qps, steps=steps, recall=rec, stats=r["stats"], counts=r["counts"], kw=kw, L=L)
+
+
+def free_forms(calc, w, args, cal, ep, L, expand, q_d, stream, dist, dev, world, plain):
+    """The free-running forms beside the plain drop-in:
+
+    * batched: ROVER_MODE_BATCHED, W pool entries expanded per step, every
+      candidate corrected -- no network;
+    * gated: ROVER_MODE_GATED with the learned gate trained on traces of
+      held-out training queries; only threshold sets under which the MLP is
+      consulted (refine band open and/or stop head on) are candidates, and
+      the number of MLP rows each search evaluates is counted.
+
+    Each is calibrated on the calibration set for its fastest point reaching
+    the target, then timed on the timed queries.  Two equal-point
+    comparisons isolate the parts: batched at the plain form's (L, entry
+    points), and batched without the network at the gated form's
+    (W, L, entry points).  The method without the network for the refine
+    decision (an ADC / worst ratio threshold) is calibrated beside them."""
     from rover_b200 import gate as gate_mod
-    from rover_b200 import workloads
+    from rover_b200 import replicas, workloads
     from rover_b200.calculator import MODE_BATCHED, MODE_GATED
     t0 = time.time()
+    md = w.bundle.meta
+    nq = len(w.queries)
     train_q = workloads.training_queries(args.workload, args.train_queries)
     tkw = dict(entry_points=ep, expand_count=expand, correction=1, refine_budget=REFINE_BUDGET)
     rows, ids, counts = gate_mod.collect(calc, train_q, L, top_k=TOP_K, **tkw)
@@ -808,112 +856,142 @@ def gated_arm(calc, w, args, ep, L, expand, q_d, stream, dist, dev, world):
     log(f"gate: {len(rows):,} trace rows from {len(train_q)} queries, trained on {model.info['rows']:,} "
         f"in {time.time() - t0:.1f}s, loss {model.info['epoch_loss']}, band [{model.band_lo:.3f}, {model.band_hi:.3f}]")
     width_max = max(1, min(4, 256 // expand))
+    cq, cgt = cal
     # trace-level view of the trained stop head against the single-feature
-    # rules of the method without the network, on held-out queries; its
-    # thresholds for a few loss budgets seed the calibration grid below
-    er, eids, ecounts = gate_mod.collect(calc, w.queries[:STUDY_QUERIES], L, top_k=TOP_K, **tkw)
+    # rules of the method without the network, on calibration queries; its
+    # thresholds for a few loss budgets seed the stop grid below
+    er, eids, ecounts = gate_mod.collect(calc, cq[:STUDY_QUERIES], L, top_k=TOP_K, **tkw)
     _, scores = gate_mod.stop_scores(calc, model, er, L)
     stop_study = gate_mod.stop_savings(er, eids, ecounts, scores, top_k=TOP_K)
     stop_grid = sorted({round(v["threshold"], 3) for v in stop_study["network"].values()
                         if np.isfinite(v["threshold"])}, reverse=True)
     log("stop head (share of expansions saved at a loss budget of final top-10 results): " +
         "; ".join(f"{k} " + " ".join(f"{b}:{v['saved']:.3f}" for b, v in d.items()) for k, d in stop_study.items()))
+    target = TARGET_RECALL + CALIBRATION_MARGIN
+    off = dict(band_lo=np.inf, band_hi=np.inf, refine_logit=-np.inf, stop_logit=np.inf)
 
-    def run(L_, ep_, W, **thr):
-        """Full query set: recall and the summed device time of the call's
-        kernels (CUDA events recorded by the library)."""
-        model.load(calc, **thr)
+    def run(mode, L_, ep_, W, thr=None):
+        """Calibration queries: recall, summed kernel time, MLP rows."""
+        rows0 = 0
+        if thr is not None:
+            model.load(calc, **thr)
+            rows0 = calc.gate_rows()
         calc.kernel_timing(True)
-        r = calc.pq_search(w.queries, L_, top_k=TOP_K, entry_points=ep_, expand_count=expand, correction=1,
-                           refine_budget=REFINE_BUDGET, mode=MODE_GATED, beam_width=W)
+        r = calc.pq_search(cq, L_, top_k=TOP_K, entry_points=ep_, expand_count=expand, correction=1,
+                           refine_budget=REFINE_BUDGET, mode=mode, beam_width=W)
         kt = calc.kernel_times()
         calc.kernel_timing(False)
-        return workloads.recall_at_k(r["ids"], r["counts"], w.gt, TOP_K), sum(v[1] for v in kt.values()), r
+        mlp = calc.gate_rows() - rows0 if thr is not None else 0
+        return workloads.recall_at_k(r["ids"], r["counts"], cgt, TOP_K), sum(v[1] for v in kt.values()), mlp
 
-    # candidate grid: beam width, entry points, L, refine and stop thresholds;
-    # L values below the plain arm's are tried first since they are cheaper
+    def sweep(kind, mode, W, ep_, thr=None):
+        """Ascending L until the target is reached; the rows tried."""
+        out = []
+        for L_ in FREE_L_SWEEP:
+            if L_ > 2 * L:
+                break
+            rec, ms, mlp = run(mode, L_, ep_, W, thr)
+            row = dict(kind=kind, beam_width=W, entry_points=ep_, L=L_, recall_at_10=rec, ms=ms,
+                       mlp_rows_per_query=mlp / len(cq), **{k: float(v) for k, v in (thr or {}).items()})
+            out.append(row)
+            if rec >= target:
+                break
+        return out
+
     table = []
-    # the tensor-core seed ranking makes larger seed sets cheap for this form
-    eps = sorted({ep, 2 * ep})
-    Ls = [x for x in (16, 24) + L_SWEEP if x <= 2 * L]
-    for W in range(min(2, width_max), width_max + 1):
+    eps = sorted({ep, min(2 * ep, md.num_vectors)})
+    for W in range(2, width_max + 1):
         for ep_ in eps:
-            for L_ in Ls:
-                for rl in (-np.inf, -1.0, 0.0):
-                    for sl in (np.inf, *stop_grid):
-                        thr = dict(refine_logit=rl, stop_logit=sl)
-                        if rl == -np.inf:
-                            thr.update(band_lo=np.inf, band_hi=np.inf)
-                        rec, ms, _ = run(L_, ep_, W, **thr)
-                        table.append(dict(kind="mlp", beam_width=W, entry_points=ep_, L=L_, recall_at_10=rec, ms=ms,
-                                          **{k: float(v) for k, v in thr.items()}))
-                # the method without the network: an ADC / worst ratio threshold
-                # on the seed shortlist, no early stop
-                for tau in THRESHOLD_GRID:
-                    thr = dict(band_lo=tau, band_hi=tau, refine_logit=0.0, stop_logit=np.inf)
-                    rec, ms, _ = run(L_, ep_, W, **thr)
-                    table.append(dict(kind="ratio", beam_width=W, entry_points=ep_, L=L_, recall_at_10=rec, ms=ms,
-                                      **{k: float(v) for k, v in thr.items()}))
-    log(f"gate calibration: {len(table)} points in {time.time() - t0:.1f}s")
+            table += sweep("batched", MODE_BATCHED, W, ep_)
 
-    def settle(kind):
-        ok = sorted((t for t in table if t["kind"] == kind and t["recall_at_10"] >= TARGET_RECALL),
-                    key=lambda t: t["ms"])
-        if not ok:
-            return None
-        t = ok[0]
-        thr = {k: t[k] for k in ("band_lo", "band_hi", "refine_logit", "stop_logit") if k in t}
-        rec, _, r = run(t["L"], t["entry_points"], t["beam_width"], **thr)
-        return t, thr, r, rec
+    def fastest(kind, extra=lambda t: True):
+        ok = [t for t in table if t["kind"] == kind and t["recall_at_10"] >= target and extra(t)]
+        return min(ok, key=lambda t: t["ms"]) if ok else None
 
-    from rover_b200 import replicas
-    ok = [t for t in table if t["kind"] == "mlp" and t["recall_at_10"] >= TARGET_RECALL]
-    pick = min(ok, key=lambda t: t["ms"]) if ok else None
-    pick = replicas.from_rank0(dist, pick)     # every replica times rank 0's point
-    if pick is None:
-        log("gate: no calibrated point reaches the target")
-        return None
-    thr = {k: pick[k] for k in ("band_lo", "band_hi", "refine_logit", "stop_logit") if k in pick}
-    rec, _, final = run(pick["L"], pick["entry_points"], pick["beam_width"], **thr)
-    t = pick
-    ratio = settle("ratio")
-    model.load(calc, **thr)
-    nq = len(w.queries)
-    pool_d = torch.full((nq,), t["L"], dtype=torch.int32, device=dev)
-    out = dict(ids=torch.empty((nq, TOP_K), dtype=torch.int32, device=dev),
-               dists=torch.empty((nq, TOP_K), dtype=torch.float32, device=dev),
-               counts=torch.empty(nq, dtype=torch.int32, device=dev),
-               status=torch.empty(nq, dtype=torch.int32, device=dev))
-    ptrs = {k: v.data_ptr() for k, v in out.items()}
-    ptrs["stride"] = TOP_K
-    gkw = dict(entry_points=t["entry_points"], expand_count=expand, correction=1, refine_budget=REFINE_BUDGET,
-               mode=MODE_GATED, beam_width=t["beam_width"])
+    bpick = fastest("batched")
+    Wg, epg = (bpick["beam_width"], bpick["entry_points"]) if bpick else (2, ep)
+    refine_opts = [None] + [dict(band_lo=model.band_lo, band_hi=model.band_hi, refine_logit=v) for v in (-1.0, 0.0, 1.0)]
+    for ro in refine_opts:
+        for so in [np.inf] + stop_grid:
+            if ro is None and so == np.inf:
+                continue     # the network would not be consulted
+            thr = dict(off, **(ro or {}))
+            thr["stop_logit"] = so
+            table += sweep("gated", MODE_GATED, Wg, epg, thr)
+    # the method without the network: an ADC / worst ratio threshold on the
+    # seed shortlist (the band is empty, so the MLP is never consulted)
+    for tau in THRESHOLD_GRID:
+        table += sweep("ratio", MODE_GATED, Wg, epg, dict(off, band_lo=tau, band_hi=tau, refine_logit=0.0))
+    log(f"free-form calibration: {len(table)} points in {time.time() - t0:.1f}s")
 
-    def step():
-        calc.pq_search_device(q_d.data_ptr(), nq, pool_d.data_ptr(), ptrs, stream_ptr=stream.cuda_stream,
-                              top_k=TOP_K, **gkw)
+    gpick = fastest("gated", lambda t: t["mlp_rows_per_query"] > 0)
+    rpick = fastest("ratio")
+    bpick, gpick = replicas.from_rank0(dist, (bpick, gpick))     # every replica times rank 0's points
 
-    steps = device_steps(calc, args, step, stream, dist, dev)
-    qps = nq * args.steps * world / (steps["total_ms"] / 1e3)
-    md = w.bundle.meta
-    gbytes = algorithmic_bytes(final["stats"], final["counts"], md, w.bundle.residual_code_bytes, expand, md.dim)
-    ratio_qps = None
-    if ratio is not None:
-        rt, rthr, _, rrec = ratio
-        ratio_qps = dict(recall_at_10=rrec, beam_width=rt["beam_width"], entry_points=rt["entry_points"], L=rt["L"],
-                         ratio=rthr["band_lo"], calibration_ms=rt["ms"])
-    report = dict(train_queries=int(len(train_q)), trace_rows=int(len(rows)), model=model.info,
-                  band=[model.band_lo, model.band_hi], refine_logit=thr.get("refine_logit"),
-                  stop_logit=thr.get("stop_logit"), beam_width=t["beam_width"], entry_points=t["entry_points"],
-                  L=t["L"], calibration_ms=t["ms"], without_network=ratio_qps,
-                  stop_head_trace_savings=dict(queries=STUDY_QUERIES, L=L, budgets=stop_study),
-                  calibration=sorted((r for r in table if r["recall_at_10"] >= TARGET_RECALL),
-                                     key=lambda r: r["ms"])[:30])
-    log(f"gated {qps:,.0f} QPS recall@10={rec:.4f} at W={t['beam_width']} ep={t['entry_points']} L={t['L']} {thr}")
-    return dict(qps=qps, steps=steps, recall=rec, stats=final["stats"], kw=gkw, L=t["L"], report=report,
-                roof=roofline(gbytes, seed_pass_bytes(nq, min(t["entry_points"], md.num_vectors), md,
-                                                      w.bundle.residual_code_bytes, False),
-                              steps["kernels"], args.steps, nq, "gated"))
+    def kw_of(t, mode):
+        return dict(entry_points=t["entry_points"], expand_count=expand, correction=1, refine_budget=REFINE_BUDGET,
+                    mode=mode, beam_width=t["beam_width"])
+
+    rep = dict(train_queries=int(len(train_q)), trace_rows=int(len(rows)), model=model.info,
+               band=[model.band_lo, model.band_hi], stop_head_trace_savings=dict(queries=STUDY_QUERIES, L=L,
+                                                                                budgets=stop_study),
+               calibration=table)
+    res = dict(batched=None, gated=None, report=rep)
+    if bpick:
+        b = timed_form(calc, args, w, q_d, bpick["L"], kw_of(bpick, MODE_BATCHED), stream, dist, dev, world)
+        bbytes = algorithmic_bytes(b["stats"], b["counts"], md, w.bundle.residual_code_bytes, expand, md.dim)
+        b["roof"] = roofline(bbytes, seed_pass_bytes(nq, min(bpick["entry_points"], md.num_vectors), md,
+                                                     w.bundle.residual_code_bytes, True),
+                             b["steps"]["kernels"], args.steps, nq, "batched")
+        res["batched"] = b
+        # equal point with the plain form: its L and entry points, W-wide steps
+        bp = timed_form(calc, args, w, q_d, plain["L"], dict(plain["kw"], mode=MODE_BATCHED,
+                                                               beam_width=bpick["beam_width"]),
+                        stream, dist, dev, world)
+        rep["batched"] = dict(qps=b["qps"], ms_per_step=b["steps"]["ms_per_step"], recall_at_10=b["recall"],
+                              beam_width=bpick["beam_width"], entry_points=bpick["entry_points"], L=bpick["L"],
+                              calibration_ms=bpick["ms"])
+        rep["batched_over_plain"] = b["qps"] / plain["qps"]
+        rep["batched_over_plain_equal_point"] = dict(
+            ratio=bp["qps"] / plain["qps"], L=plain["L"], entry_points=plain["kw"]["entry_points"],
+            beam_width=bpick["beam_width"], batched_recall_at_10=bp["recall"], plain_recall_at_10=plain["recall"])
+        log(f"batched {b['qps']:,.0f} QPS recall@10={b['recall']:.4f} at W={bpick['beam_width']} "
+            f"ep={bpick['entry_points']} L={bpick['L']}; at the plain point {bp['qps']:,.0f} QPS")
+    if gpick:
+        thr = {k: gpick[k] for k in ("band_lo", "band_hi", "refine_logit", "stop_logit")}
+        model.load(calc, **thr)
+        rows0 = calc.gate_rows()
+        g = timed_form(calc, args, w, q_d, gpick["L"], kw_of(gpick, MODE_GATED), stream, dist, dev, world)
+        searches = (1 + args.warmup + args.steps) * nq
+        g_rows = (calc.gate_rows() - rows0) / searches
+        gbytes = algorithmic_bytes(g["stats"], g["counts"], md, w.bundle.residual_code_bytes, expand, md.dim)
+        g["roof"] = roofline(gbytes, seed_pass_bytes(nq, min(gpick["entry_points"], md.num_vectors), md,
+                                                     w.bundle.residual_code_bytes, False),
+                             g["steps"]["kernels"], args.steps, nq, "gated")
+        res["gated"] = g
+        # the same point with the network switched off
+        bg = timed_form(calc, args, w, q_d, gpick["L"], kw_of(gpick, MODE_BATCHED), stream, dist, dev, world)
+        rep["gated"] = dict(qps=g["qps"], ms_per_step=g["steps"]["ms_per_step"], recall_at_10=g["recall"],
+                            beam_width=gpick["beam_width"], entry_points=gpick["entry_points"], L=gpick["L"],
+                            calibration_ms=gpick["ms"], mlp_rows_per_query=g_rows,
+                            **{k: float(v) for k, v in thr.items()})
+        rep["gated_over_batched"] = g["qps"] / res["batched"]["qps"] if res["batched"] else None
+        rep["gated_over_batched_equal_point"] = dict(
+            ratio=g["qps"] / bg["qps"], beam_width=gpick["beam_width"], L=gpick["L"],
+            entry_points=gpick["entry_points"], gated_recall_at_10=g["recall"], batched_recall_at_10=bg["recall"])
+        log(f"gated {g['qps']:,.0f} QPS recall@10={g['recall']:.4f} at W={gpick['beam_width']} "
+            f"ep={gpick['entry_points']} L={gpick['L']} {thr}, {g_rows:.1f} MLP rows per query; "
+            f"same point without the network {bg['qps']:,.0f} QPS")
+    else:
+        log("gate: no point with the network consulted reaches the target on the calibration set")
+    rep["without_network"] = rpick
+    best_batched = res["batched"]["qps"] if res["batched"] else 0.0
+    rep["finding"] = (
+        "the learned gate is faster than the batched form without it" if res["gated"] and
+        res["gated"]["qps"] > best_batched else
+        "the learned gate does not beat the batched form without it on this workload: the speed-up over the "
+        "plain drop-in comes from the W-wide steps and the tensor-core seed ranking, not from the network")
+    return res
 
 
 if __name__ == "__main__":

@@ -299,6 +299,11 @@ typedef struct RoverGateThresholds {
 AEEResult calculator_rover_gate_load(remote_handle64 h, const float *params, const float *mu,
                                      const float *sigma, const RoverGateThresholds *thresholds);
 AEEResult calculator_rover_gate_unload(remote_handle64 h);
+/* MLP rows the loaded gate has evaluated inside searches (seed-shortlist
+ * rows inside the refine band, plus one row per expansion source while the
+ * stop head is on) since it was loaded: 0 means the thresholds kept the
+ * network out of every search. */
+AEEResult calculator_rover_gate_rows(remote_handle64 h, uint64_t *rows);
 /* The loaded gate's logits [n][2] (refine-needed, stop-expanding) for raw
  * rows [n][5] = {quantized distance, pool rank / L, worst pool distance,
  * hop count / L, query norm} (host buffers), computed by the same device

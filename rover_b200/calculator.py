@@ -131,6 +131,7 @@ class Calculator:
         L.calculator_rover_launch_count.restype = C.c_uint64
         L.calculator_rover_gate_load.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.POINTER(GateThresholds)]
         L.calculator_rover_gate_unload.argtypes = [C.c_uint64]
+        L.calculator_rover_gate_rows.argtypes = [C.c_uint64, C.POINTER(C.c_uint64)]
         L.calculator_rover_gate_eval.argtypes = [C.c_uint64, _f32p, C.c_int64, _f32p]
         L.calculator_rover_seed_topm.argtypes = [C.c_uint64, _f32p, C.c_int32, C.c_int32, C.c_int32, _u64p, _f32p]
         L.calculator_rover_gate_train.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.c_int64,
@@ -191,6 +192,12 @@ class Calculator:
         self._check("calculator_rover_gate_load",
                     self.lib.calculator_rover_gate_load(self.handle, _p(p, _f32p), _p(m, _f32p), _p(sg, _f32p),
                                                         C.byref(t)))
+
+    def gate_rows(self) -> int:
+        """MLP rows the loaded gate has evaluated inside searches since it was loaded."""
+        v = C.c_uint64()
+        self._check("calculator_rover_gate_rows", self.lib.calculator_rover_gate_rows(self.handle, C.byref(v)))
+        return int(v.value)
 
     def gate_unload(self) -> None:
         self._check("calculator_rover_gate_unload", self.lib.calculator_rover_gate_unload(self.handle))

@@ -1544,6 +1544,8 @@ AEEResult plan_inputs(State& s, PqPlanImpl& P) {
     P.gate.b1 = reinterpret_cast<const float*>(rebase(s.gate.b1));
     P.gate.b2 = reinterpret_cast<const float*>(rebase(s.gate.b2));
     P.gate.b3 = reinterpret_cast<const float*>(rebase(s.gate.b3));
+    P.gate.rows_evaluated = reinterpret_cast<unsigned long long*>(
+        const_cast<void*>(static_cast<const void*>(rebase(s.gate.rows_evaluated))));
   } else {
     CK(P.seed_dists.ensure(seed_bytes));
     if (P.verify_seeds) {
@@ -1938,14 +1940,17 @@ extern "C" AEEResult calculator_rover_gate_load(remote_handle64 h, const float* 
   std::copy(b2, b2 + kGateHidden, bias.begin() + kGateHidden);
   std::copy(b3, b3 + kGateOut, bias.begin() + 2 * kGateHidden);
   const size_t o1 = 0, o2 = o1 + w1t.size() * 2, o3 = o2 + w2t.size() * 2, ob = o3 + w3t.size() * 2;
-  const size_t total = ob + bias.size() * 4;
+  const size_t orow = (ob + bias.size() * 4 + 7) & ~static_cast<size_t>(7);   // MLP row counter
+  const size_t total = orow + 8;
   CK(s.gate_buf.ensure(total));
   uint8_t* d = s.gate_buf.as<uint8_t>();
   CK(cudaMemcpy(d + o1, w1t.data(), w1t.size() * 2, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d + o2, w2t.data(), w2t.size() * 2, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d + o3, w3t.data(), w3t.size() * 2, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d + ob, bias.data(), bias.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemset(d + orow, 0, 8));
   GateParams g{};
+  g.rows_evaluated = reinterpret_cast<unsigned long long*>(d + orow);
   g.w1t = reinterpret_cast<const uint16_t*>(d + o1);
   g.w2t = reinterpret_cast<const uint16_t*>(d + o2);
   g.w3t = reinterpret_cast<const uint16_t*>(d + o3);
@@ -2129,6 +2134,20 @@ extern "C" AEEResult calculator_rover_gate_train(remote_handle64 h, const float*
   std::copy(mu, mu + kGateIn, mu_out);
   std::copy(sigma, sigma + kGateIn, sigma_out);
   return fail(AEE_SUCCESS);
+}
+
+extern "C" AEEResult calculator_rover_gate_rows(remote_handle64 h, uint64_t* rows) {
+  (void)h;
+  if (!rows) return AEE_EBADPARM;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  *rows = 0;
+  if (!s.gate.enabled || !s.gate.rows_evaluated) return AEE_SUCCESS;
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  unsigned long long v = 0;
+  CK(cudaMemcpy(&v, s.gate.rows_evaluated, sizeof(v), cudaMemcpyDeviceToHost));
+  *rows = static_cast<uint64_t>(v);
+  return AEE_SUCCESS;
 }
 
 extern "C" AEEResult calculator_rover_gate_unload(remote_handle64 h) {

@@ -134,6 +134,7 @@ struct GateParams {
   float band_lo, band_hi;        // quantized / worst ratio: <= lo correct, >= hi keep, else MLP
   float refine_logit, stop_logit;
   int32_t enabled;               // 0: every candidate corrected, no early stop
+  unsigned long long* rows_evaluated;   // MLP rows run inside searches (null: not counted)
 };
 
 // One trace row per scored candidate or expansion source (training data for

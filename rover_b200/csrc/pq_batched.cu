@@ -166,6 +166,11 @@ __device__ __forceinline__ void gate_rows(const GateParams& gp, const uint32_t* 
   __syncwarp();
 }
 
+// Adds a search's MLP rows to the loaded gate's counter.
+__device__ __forceinline__ void count_gate_rows(const GateParams& gp, int nrows, int lane) {
+  if (lane == 0 && gp.rows_evaluated) atomicAdd(gp.rows_evaluated, static_cast<unsigned long long>(nrows));
+}
+
 // Appends the rows of the lanes that have one; returns this lane's row
 // index, or ~0 when it wrote none (no row, or the buffer is full).
 __device__ __forceinline__ unsigned long long trace_put(const PqBatchArgs& c, int lane, bool have,
@@ -361,7 +366,10 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
           row = __popc(mm & ((1u << lane) - 1u));
           gate_row(c.gate, adc, static_cast<float>(i) / cap, worst, 0.0f, qnorm, feat + row * 4);
         }
-        if (mm) gate_rows(c.gate, feat, __popc(mm), logits, lane);
+        if (mm) {
+          gate_rows(c.gate, feat, __popc(mm), logits, lane);
+          count_gate_rows(c.gate, __popc(mm), lane);
+        }
         if (dcs == 2) dcs = logits[row * 2] > c.gate.refine_logit ? 1 : 0;
         float d = adc;
         bool sbad = false;
@@ -410,6 +418,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
           gate_row(c.gate, key_dist(list[my_pos]), static_cast<float>(my_pos) / cap, worst_now,
                    static_cast<float>(expanded) / cap, qnorm, feat + lane * 4);
         gate_rows(c.gate, feat, nsel, logits, lane);
+        count_gate_rows(c.gate, nsel, lane);
         float sl = lane < nsel ? logits[lane * 2 + 1] : 0.0f;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) sl += __shfl_xor_sync(kFullMask, sl, off);

@@ -150,6 +150,28 @@ def training_queries(name: str, n: int, offset: int = 7) -> np.ndarray:
                  clip_nonneg=cfg["clip"], normalize=cfg["normalize"])
 
 
+def held_out_set(name: str, n: int, offset: int, cache_dir: str | Path | None = None, gt_k: int = 100,
+                 device=None) -> tuple[np.ndarray, np.ndarray]:
+    """Held-out queries (training_queries with this seed offset) and their
+    exact top-gt_k neighbours among the workload's base vectors: the set an
+    operating point is calibrated on, kept apart from the timed queries."""
+    cfg = CONFIGS[name]
+    path = None
+    if cache_dir:
+        path = Path(cache_dir) / f"{name}-{_key(cfg)}" / f"heldout-{offset}-{n}-{gt_k}.npz"
+        if path.exists():
+            z = np.load(path)
+            return z["queries"], z["gt"]
+    base = D.gmm(cfg["n"], cfg["dim"], cfg["comps"], cfg["seed"], clip_nonneg=cfg["clip"],
+                 normalize=cfg["normalize"])
+    queries = training_queries(name, n, offset)
+    gt = D.exact_knn(queries, base, gt_k, device=device)
+    if path:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        np.savez(path, queries=queries, gt=gt)
+    return queries, gt
+
+
 def recall_at_k(ids: np.ndarray, counts: np.ndarray, gt: np.ndarray, k: int) -> float:
     """demo_recall_hits_at_k (retrieval_rpc_demo_support.c:1709) averaged:
     hits among the first k results that appear in the first k truth ids."""

@@ -184,6 +184,30 @@ def test_gate_limits(calc):
     calc.gate_unload()
 
 
+def test_gate_rows_count_the_network_evaluations(calc):
+    """calculator_rover_gate_rows counts the MLP rows the searches ran: none
+    when the thresholds keep the network out, the stop head's sources (one
+    row per expansion source) when it is on, and every shortlisted seed when
+    the refine band covers all ratios."""
+    d = _load(calc)
+    q = d["queries"][:64]
+    params = G.init_params(0)
+    mu, sigma = np.zeros(5, np.float32), np.ones(5, np.float32)
+    calc.gate_load(params, mu, sigma, band_lo=np.inf, band_hi=np.inf, refine_logit=-np.inf, stop_logit=np.inf)
+    calc.pq_search(q, 32, mode=2, beam_width=2, **KW)
+    assert calc.gate_rows() == 0
+    # stop head on but never firing: one row per expansion source
+    calc.gate_load(params, mu, sigma, band_lo=np.inf, band_hi=np.inf, refine_logit=-np.inf, stop_logit=3e38)
+    r = calc.pq_search(q, 32, mode=2, beam_width=2, **KW)
+    assert calc.gate_rows() == int(r["stats"][:, 2].sum())
+    # refine band open over every ratio: every shortlisted seed is a row
+    n_seeds = _seed_count(len(d["graph"]), d["entry"], KW["entry_points"])
+    calc.gate_load(params, mu, sigma, band_lo=-1.0, band_hi=np.inf, refine_logit=0.0, stop_logit=np.inf)
+    calc.pq_search(q, 32, mode=2, beam_width=2, **KW)
+    assert calc.gate_rows() == len(q) * min(2 * 32, n_seeds)
+    calc.gate_unload()
+
+
 RULES = ("hop", "rank", "ratio")
 
 
