@@ -25,6 +25,7 @@
 #include "../../include/rover_b200.h"
 #include "kernels.h"
 #include "rpcmem_compat.h"
+#include "session_bridge.h"
 
 using namespace rover;
 
@@ -125,6 +126,8 @@ struct SqDevice {
 struct State {
   std::mutex mu;
   bool init = false;
+  int session_live[2] = {0, 0};   // lane-protocol sessions (SessionKind) holding an index
+  uint8_t pq_uuid[16] = {};       // index uuid of the pure-PQ DMA index (session LUT checks)
   int device = -1;                // the device current at the first call: index copies, stream, scratch
   int sms = 0;
   cudaStream_t stream = nullptr;
@@ -254,6 +257,14 @@ AEEResult ensure_init(State& s) {
   s.device = dev;
   s.init = true;
   return AEE_SUCCESS;
+}
+
+// A live lane-protocol session reads the index it was started on: loading,
+// replacing or unloading that index is refused until the session returns.
+bool session_busy(const State& s, SessionKind k) {
+  if (!s.session_live[k]) return false;
+  set_error("a %s session is running on the loaded index", k == kSessionPurePq ? "pure-PQ" : "SQMD");
+  return true;
 }
 
 template <class T>
@@ -944,6 +955,7 @@ extern "C" AEEResult calculator_rover_pq_load(remote_handle64 h, const RoverPqIn
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (session_busy(s, kSessionPurePq)) return AEE_EFAILED;
   if (!d || d->num_vectors <= 0 || d->dim <= 0 || d->dim > 1024 || d->m <= 0 ||
       (d->ks != 16 && d->ks != 256) || d->subdim <= 0 || d->m * d->subdim != d->dim ||
       d->code_bytes != (d->ks == 16 ? (d->m + 1) / 2 : d->m) || !d->codes || !d->codebook) {
@@ -1011,6 +1023,7 @@ extern "C" AEEResult calculator_rover_pq_unload(remote_handle64 h) {
   (void)h;
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
+  if (session_busy(s, kSessionPurePq)) return AEE_EFAILED;
   s.pq.release();
   return AEE_SUCCESS;
 }
@@ -2469,6 +2482,7 @@ extern "C" AEEResult calculator_retrieval_load(remote_handle64 h, const int* gra
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (session_busy(s, kSessionSqmd)) return AEE_EFAILED;
   s.legacy.release();
   s.legacy_dma = false;
   if (num_vectors <= 0 || dim <= 0 || graph_k <= 0 || dim > 1024) return AEE_EBADPARM;
@@ -2536,6 +2550,7 @@ extern "C" AEEResult calculator_retrieval_unload(remote_handle64 h) {
   (void)h;
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
+  if (session_busy(s, kSessionSqmd)) return AEE_EFAILED;
   s.legacy.release();
   s.legacy_dma = false;
   return AEE_SUCCESS;
@@ -2549,6 +2564,7 @@ extern "C" AEEResult calculator_retrieval_load_dma(remote_handle64 h, int32 fd_g
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (session_busy(s, kSessionSqmd)) return AEE_EFAILED;
   s.legacy.release();
   s.legacy_dma = false;
   if (fd_graph < -1 || num_vectors <= 0 || dim <= 0 || graph_k <= 0 || dim > 1024) return AEE_EBADPARM;
@@ -2592,6 +2608,7 @@ extern "C" AEEResult calculator_retrieval_unload_dma(remote_handle64 h) {
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   if (!s.legacy_dma) return AEE_SUCCESS;
+  if (session_busy(s, kSessionSqmd)) return AEE_EFAILED;
   s.legacy.release();
   s.legacy_dma = false;
   return AEE_SUCCESS;
@@ -2645,35 +2662,73 @@ extern "C" AEEResult calculator_retrieval_pure_pq_load_dma(
   d.ks = pq_ks;
   d.subdim = pq_subdim;
   d.code_bytes = pq_code_bytes;
-  return calculator_rover_pq_load(h, &d);
+  const AEEResult r = calculator_rover_pq_load(h, &d);
+  if (r == AEE_SUCCESS) {
+    State& s = st();
+    std::lock_guard<std::mutex> lock(s.mu);
+    std::memcpy(s.pq_uuid, index_uuid, 16);
+  }
+  return r;
 }
 
 extern "C" AEEResult calculator_retrieval_pure_pq_unload_dma(remote_handle64 h) {
   return calculator_rover_pq_unload(h);
 }
 
-// Lane-protocol sessions and the remaining legacy services.
-extern "C" AEEResult calculator_retrieval_pure_pq_sqmd_run(remote_handle64 h, int32 fd_sqmd_ctrl, int32 fd_query_lut,
-                                                           int32 lane_count, int32 work_items_cap) {
-  (void)h; (void)fd_sqmd_ctrl; (void)fd_query_lut; (void)lane_count; (void)work_items_cap;
-  set_error("pure-PQ lane sessions are not available in this build");
-  return AEE_EUNSUPPORTED;
+// The lane-protocol sessions (calculator_retrieval_pure_pq_sqmd_run,
+// calculator_retrieval_expand_sqmd(_run)) are served by sessions.cu through
+// the bridge below.
+
+namespace rover {
+
+bool session_acquire(SessionKind kind, SessionIndex* out) {
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (!s.init) {
+    set_error("no index is loaded");
+    return false;
+  }
+  if (s.session_live[kind]) {
+    set_error("a session of this kind is already running");
+    return false;
+  }
+  if (kind == kSessionPurePq) {
+    if (!s.pq.loaded) {
+      set_error("no pure-PQ index is loaded (calculator_retrieval_pure_pq_load_dma)");
+      return false;
+    }
+    out->pq = s.pq.view;
+    std::memcpy(out->pq_uuid, s.pq_uuid, 16);
+  } else {
+    if (!s.legacy.loaded) {
+      set_error("no L1 index is loaded (calculator_retrieval_load / _load_dma)");
+      return false;
+    }
+    out->sq = s.legacy.view;
+  }
+  out->device = s.device;
+  s.session_live[kind] = 1;
+  return true;
 }
 
-extern "C" AEEResult calculator_retrieval_expand_sqmd(remote_handle64 h, const float* query, int queryLen,
-                                                      int32 query_dim, int32 fd_sqmd_ctrl, int32 lane_count,
-                                                      int32 work_items_cap) {
-  (void)h; (void)query; (void)queryLen; (void)query_dim; (void)fd_sqmd_ctrl; (void)lane_count; (void)work_items_cap;
-  set_error("SQMD lane sessions are not available in this build");
-  return AEE_EUNSUPPORTED;
+void session_release(SessionKind kind) {
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  s.session_live[kind] = 0;
 }
 
-extern "C" AEEResult calculator_retrieval_expand_sqmd_run(remote_handle64 h, int32 fd_sqmd_ctrl, int32 lane_count,
-                                                          int32 work_items_cap) {
-  (void)h; (void)fd_sqmd_ctrl; (void)lane_count; (void)work_items_cap;
-  set_error("SQMD lane sessions are not available in this build");
-  return AEE_EUNSUPPORTED;
+void session_count_launches(unsigned n) { g_launches += n; }
+
+void session_error(const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
 }
+
+}  // namespace rover
 
 extern "C" AEEResult calculator_retrieval_search_db(remote_handle64 h, const float* query_a, int query_aLen,
                                                     const float* query_b, int query_bLen, int32 fd_expansion_buf,
