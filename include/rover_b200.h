@@ -86,7 +86,10 @@ typedef struct RoverSearchParams {
     int32_t top_k;           /* results per query when top_ks is NULL */
     int32_t pool_stride;     /* columns of the optional pool output */
     int32_t sq_mode;         /* SQ only: 0 = device search (calculator_retrieval_search),
-                                1 = SQMD session semantics */
+                                1 = SQMD session semantics, 2 = DB-pair search
+                                (calculator_retrieval_search_db: the device search with
+                                each expansion candidate's exact residual distance when
+                                correction is on) */
     int32_t layout;          /* PQ with correction: ROVER_LAYOUT_* */
     int32_t beam_width;      /* BATCHED / GATED: entries expanded per step, 1..4 (0 = the
                                 largest with beam_width * expand_count <= 256) */
@@ -269,7 +272,10 @@ AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, const float *
 
 /* SQ index and batched SQ search (sq_mode 0: calculator_retrieval_search,
  * retrieval_async_dsp_search.c:368; sq_mode 1: the SQMD loop,
- * retrieval_sqmd_common.c:2052 with the exact residual correction). */
+ * retrieval_sqmd_common.c:2052 with the exact residual correction; sq_mode 2:
+ * calculator_retrieval_search_db's per-query search,
+ * retrieval_async_dsp_search.c:1205-1581, with the host correction of
+ * retrieval_rpc_demo_pipeline.c:454-495 applied on the device). */
 AEEResult calculator_rover_sq_load(remote_handle64 h, const RoverSqIndexDesc *desc);
 AEEResult calculator_rover_sq_unload(remote_handle64 h);
 AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSearchParams *params,

@@ -126,7 +126,7 @@ struct SqDevice {
 struct State {
   std::mutex mu;
   bool init = false;
-  int session_live[2] = {0, 0};   // lane-protocol sessions (SessionKind) holding an index
+  int session_live[kSessionKinds] = {};   // sessions / DB-pair calls (SessionKind) holding an index
   uint8_t pq_uuid[16] = {};       // index uuid of the pure-PQ DMA index (session LUT checks)
   int device = -1;                // the device current at the first call: index copies, stream, scratch
   int sms = 0;
@@ -262,8 +262,10 @@ AEEResult ensure_init(State& s) {
 // A live lane-protocol session reads the index it was started on: loading,
 // replacing or unloading that index is refused until the session returns.
 bool session_busy(const State& s, SessionKind k) {
+  if (k == kSessionSqmd && s.session_live[kSessionDb]) k = kSessionDb;
   if (!s.session_live[k]) return false;
-  set_error("a %s session is running on the loaded index", k == kSessionPurePq ? "pure-PQ" : "SQMD");
+  set_error("a %s is running on the loaded index",
+            k == kSessionPurePq ? "pure-PQ session" : k == kSessionSqmd ? "SQMD session" : "DB-pair search");
   return true;
 }
 
@@ -503,7 +505,7 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
   uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * (2ull * a.max_pool + 64ull) * expand));
   CK(s.counter.ensure(sizeof(unsigned int)));
   CK(cudaMemsetAsync(a.status, 0, nq * sizeof(int32_t), stream));
-  for (int attempt = 0; attempt < 4; ++attempt) {
+  for (int attempt = 0; attempt < 8; ++attempt) {
     uint32_t gen_base = 0;
     if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
     if (stream != s.stream) CK(cudaStreamSynchronize(s.stream));
@@ -635,7 +637,7 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
   uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * est));
   CK(s.counter.ensure(sizeof(unsigned int)));
   CK(cudaMemsetAsync(d_out.status, 0, nq * sizeof(int32_t), stream));
-  for (int attempt = 0; attempt < 4; ++attempt) {
+  for (int attempt = 0; attempt < 8; ++attempt) {
     uint32_t gen_base = 0;
     if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
     if (stream != s.stream) {
@@ -734,7 +736,7 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
   uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * (2ull * a.max_pool + 64ull) * expand * W));
   CK(s.counter.ensure(sizeof(unsigned int)));
   CK(cudaMemsetAsync(a.status, 0, nq * sizeof(int32_t), stream));
-  for (int attempt = 0; attempt < 4; ++attempt) {
+  for (int attempt = 0; attempt < 8; ++attempt) {
     uint32_t gen_base = 0;
     if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
     if (stream != s.stream) CK(cudaStreamSynchronize(s.stream));
@@ -807,13 +809,16 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
                          int32_t* d_status, cudaStream_t stream) {
   if (!sq.loaded) { set_error("no SQ index is loaded"); return AEE_EFAILED; }
   int max_pool = 0;
-  for (int32_t v : h_pool) max_pool = std::max(max_pool, mode == kSqModeDsp ? std::min(v, 2000) : v);
+  for (int32_t v : h_pool) max_pool = std::max(max_pool, mode != kSqModeSqmd ? std::min(v, 2000) : v);
   if (max_pool <= 0 || max_pool > 4096) { set_error("pool sizes must be in 1..4096"); return AEE_EBADPARM; }
   const int expand = std::min(p->expand_count, sq.view.degree);
   const long long fbound = mode == kSqModeSqmd
                                ? static_cast<long long>(p->entry_points) + static_cast<long long>(max_pool) * p->expand_count
                                : static_cast<long long>(p->entry_points) + static_cast<long long>(max_pool) * expand;
-  const int fcap = static_cast<int>(std::min<long long>(fbound, 1 << 20));
+  // the DB-pair search grows its frontier up to n entries: start at the
+  // device search's bound and widen on a FRONTIER_FULL report
+  int fcap = static_cast<int>(std::min<long long>(fbound, 1 << 20));
+  if (mode == kSqModeDb) fcap = std::min(fcap, sq.view.n);
   SqSearchArgs a{};
   a.ix = sq.view;
   a.queries = d_queries;
@@ -839,17 +844,25 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
   if (allow_smem(reinterpret_cast<const void*>(sq_search_kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   int blocks = std::max(1, std::min(resident_blocks(reinterpret_cast<const void*>(sq_search_kernel), kSearchWarps * 32, smem, s.sms),
                                     (nq + kSearchWarps - 1) / kSearchWarps));
+  const int max_blocks = blocks;
+  size_t slots = 0;
   // keep the heap scratch under 4 GiB
-  const size_t heap_per_slot = static_cast<size_t>(max_pool + fcap) * 8u;
-  while (blocks > 1 && static_cast<size_t>(blocks) * kSearchWarps * heap_per_slot > (4ull << 30)) blocks >>= 1;
-  const size_t slots = static_cast<size_t>(blocks) * kSearchWarps;
-  CK(s.heaps.ensure(slots * heap_per_slot));
-  a.heaps = s.heaps.as<uint64_t>();
+  auto size_heaps = [&]() -> AEEResult {
+    const size_t heap_per_slot = static_cast<size_t>(max_pool + fcap) * 8u;
+    blocks = max_blocks;
+    while (blocks > 1 && static_cast<size_t>(blocks) * kSearchWarps * heap_per_slot > (4ull << 30)) blocks >>= 1;
+    slots = static_cast<size_t>(blocks) * kSearchWarps;
+    CK(s.heaps.ensure(slots * heap_per_slot));
+    a.heaps = s.heaps.as<uint64_t>();
+    a.frontier_cap = fcap;
+    return AEE_SUCCESS;
+  };
+  if (size_heaps() != AEE_SUCCESS) return AEE_ENOMEMORY;
   const uint64_t est = static_cast<uint64_t>(p->entry_points) * 2 + (2ull * max_pool + 64ull) * static_cast<uint64_t>(std::max(expand, 1));
   uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * est));
   CK(s.counter.ensure(sizeof(unsigned int)));
   CK(cudaMemsetAsync(d_status, 0, nq * sizeof(int32_t), stream));
-  for (int attempt = 0; attempt < 4; ++attempt) {
+  for (int attempt = 0; attempt < 8; ++attempt) {
     uint32_t gen_base = 0;
     if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
     a.visited = s.visited.as<unsigned long long>();
@@ -867,10 +880,17 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
     CK(cudaMemcpyAsync(s.h_status.data(), d_status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     collect_timings();
-    bool retry = false;
-    for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
-    if (!retry) break;
-    entries = next_pow2(static_cast<uint64_t>(entries) * 4);
+    bool retry = false, widen = false;
+    for (int i = 0; i < nq; ++i) {
+      retry |= s.h_status[i] == kStatusTableFull;
+      widen |= mode == kSqModeDb && s.h_status[i] == kStatusFrontierFull && fcap < sq.view.n;
+    }
+    if (!retry && !widen) break;
+    if (retry) entries = next_pow2(static_cast<uint64_t>(entries) * 4);
+    if (widen) {
+      fcap = static_cast<int>(std::min<long long>(4ll * fcap, sq.view.n));
+      if (size_heaps() != AEE_SUCCESS) return AEE_ENOMEMORY;
+    }
     CK(cudaMemsetAsync(d_status, 0, nq * sizeof(int32_t), stream));
   }
   for (int i = 0; i < nq; ++i)
@@ -2419,7 +2439,11 @@ extern "C" AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSe
     return AEE_EBADPARM;
   if (nq == 0) return AEE_SUCCESS;
   if (!s.sq.loaded || !s.sq.view.graph) { set_error("no SQ index with a graph loaded"); return AEE_EFAILED; }
-  if (p->sq_mode == 1 && p->correction && !s.sq.view.residual) { set_error("correction needs residuals"); return AEE_EBADPARM; }
+  if (p->sq_mode < 0 || p->sq_mode > 2) { set_error("sq_mode must be 0, 1 or 2"); return AEE_EBADPARM; }
+  if (p->sq_mode != 0 && p->correction && !s.sq.view.residual) {
+    set_error("correction needs residuals");
+    return AEE_EBADPARM;
+  }
   const int dim = s.sq.view.dim;
   std::vector<int32_t> h_pool(pool_sizes, pool_sizes + nq);
   const int stride = out->out_stride;
@@ -2431,7 +2455,8 @@ extern "C" AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSe
   CK(s.out_counts.ensure(nq * 4));
   CK(s.stats.ensure(static_cast<size_t>(nq) * 32));
   CK(s.status.ensure(nq * 4));
-  AEEResult r = sq_search_core(s, s.sq, p->sq_mode == 1 ? kSqModeSqmd : kSqModeDsp, p, s.in_queries.as<float>(), nq,
+  const int mode = p->sq_mode == 1 ? kSqModeSqmd : p->sq_mode == 2 ? kSqModeDb : kSqModeDsp;
+  AEEResult r = sq_search_core(s, s.sq, mode, p, s.in_queries.as<float>(), nq,
                                s.in_pool.as<int32_t>(), h_pool, p->sq_mode == 1 ? stride : std::min(stride, p->top_k),
                                s.out_ids.as<int32_t>(), s.out_dists.as<float>(), stride, s.out_counts.as<int32_t>(),
                                s.stats.as<unsigned long long>(), s.status.as<int32_t>(), s.stream);
@@ -2688,7 +2713,7 @@ bool session_acquire(SessionKind kind, SessionIndex* out) {
     set_error("no index is loaded");
     return false;
   }
-  if (s.session_live[kind]) {
+  if (s.session_live[kind] && kind != kSessionDb) {
     set_error("a session of this kind is already running");
     return false;
   }
@@ -2705,16 +2730,17 @@ bool session_acquire(SessionKind kind, SessionIndex* out) {
       return false;
     }
     out->sq = s.legacy.view;
+    out->sq_graph_entry = s.legacy.graph_entry;
   }
   out->device = s.device;
-  s.session_live[kind] = 1;
+  ++s.session_live[kind];
   return true;
 }
 
 void session_release(SessionKind kind) {
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
-  s.session_live[kind] = 0;
+  if (s.session_live[kind] > 0) --s.session_live[kind];
 }
 
 void session_count_launches(unsigned n) { g_launches += n; }
@@ -2729,24 +2755,6 @@ void session_error(const char* fmt, ...) {
 }
 
 }  // namespace rover
-
-extern "C" AEEResult calculator_retrieval_search_db(remote_handle64 h, const float* query_a, int query_aLen,
-                                                    const float* query_b, int query_bLen, int32 fd_expansion_buf,
-                                                    int32 entry_points, int32 expand_count, int32 pool_size,
-                                                    int32 num_out, int* candidate_ids_a, int candidate_ids_aLen,
-                                                    float* candidate_dists_a, int candidate_dists_aLen,
-                                                    int32* actual_count_a, int* candidate_ids_b, int candidate_ids_bLen,
-                                                    float* candidate_dists_b, int candidate_dists_bLen,
-                                                    int32* actual_count_b) {
-  (void)h; (void)query_a; (void)query_aLen; (void)query_b; (void)query_bLen; (void)fd_expansion_buf;
-  (void)entry_points; (void)expand_count; (void)pool_size; (void)num_out; (void)candidate_ids_a;
-  (void)candidate_ids_aLen; (void)candidate_dists_a; (void)candidate_dists_aLen; (void)candidate_ids_b;
-  (void)candidate_ids_bLen; (void)candidate_dists_b; (void)candidate_dists_bLen;
-  if (actual_count_a) *actual_count_a = 0;
-  if (actual_count_b) *actual_count_b = 0;
-  set_error("DB-pair search is not available in this build");
-  return AEE_EUNSUPPORTED;
-}
 
 extern "C" AEEResult calculator_retrieval_async_submit(remote_handle64 h, const float* query, int queryLen,
                                                        const int* candidate_ids, int candidate_idsLen,

@@ -248,13 +248,13 @@ void launch_gate_adam(float* p, const float* g, float* m1, float* m2, int count,
 
 // ---- SQ search (heap-exact) ----------------------------------------------
 
-enum SqSearchMode : int32_t { kSqModeDsp = 0, kSqModeSqmd = 1 };
+enum SqSearchMode : int32_t { kSqModeDsp = 0, kSqModeSqmd = 1, kSqModeDb = 2 };
 
 struct SqSearchArgs {
   SqIndexView ix;
   const float* queries; int32_t nq;
   const int32_t* pool_sizes;
-  int32_t mode;                  // kSqModeDsp (a15) or kSqModeSqmd (a12)
+  int32_t mode;                  // kSqModeDsp (a15), kSqModeSqmd (a12) or kSqModeDb (DB-pair)
   int32_t entry_points, graph_entry;
   uint32_t seed;
   int32_t expand_count;
@@ -271,6 +271,47 @@ struct SqSearchArgs {
 };
 
 __global__ void sq_search_kernel(SqSearchArgs a);
+
+// ---- DB-pair search driven step by step by the host (calculator_retrieval_search_db)
+//
+// Two queries (slots), each one search of the reference's DB-pair loop
+// (retrieval_async_dsp_search.c:1205-1581) kept on the device; the host
+// drives it one step at a time through the shared expansion buffers, because
+// each expansion waits for the caller's corrected distances.
+constexpr int kDbSlots = 2;
+constexpr int kDbItems = 32;     // DB_MAX_EXPAND
+enum DbOp : int32_t { kDbNone = 0, kDbInit = 1, kDbStep = 2, kDbFinish = 3 };
+
+struct DbIo {                    // host <-> device per launch (pinned twin on the host)
+  int32_t op[kDbSlots];
+  int32_t count[kDbSlots];       // in (kDbStep): corrections for the last step's ids; out: this step's ids
+  float corr[kDbSlots][kDbItems];
+  int32_t ids[kDbSlots][kDbItems];
+  float coarse[kDbSlots][kDbItems];
+  int32_t finished[kDbSlots];
+  int32_t status[kDbSlots];
+  int32_t out_count[kDbSlots];   // kDbFinish
+};
+
+struct DbSlot {                  // device-resident search state of one query
+  int32_t psize, fsize, finished, last_count;
+  int32_t last_ids[kDbItems];
+  uint8_t qc[1024];
+};
+
+struct DbArgs {
+  SqIndexView ix;
+  const float* queries;          // [kDbSlots][dim]
+  int32_t entry_points, expand_limit, pool_cap, num_out, graph_entry, frontier_cap;
+  DbIo* io;
+  DbSlot* slots;
+  uint64_t* pools;               // [kDbSlots][pool_cap] (id, dist) pairs
+  uint64_t* fronts;              // [kDbSlots][frontier_cap]
+  uint32_t* visited;             // [kDbSlots][(n + 31) / 32]
+  int32_t* out_ids;              // [kDbSlots][num_out]
+  float* out_dists;
+};
+void launch_db_step(const DbArgs& a, cudaStream_t s);
 
 // ---- batched distance kernels ---------------------------------------------
 

@@ -148,6 +148,25 @@ static_assert(offsetof(SqControl, lanes) == 128 && offsetof(SqControl, stats) ==
               sizeof(SqControl) == 20096, "SQMD control layout");
 
 
+// ---- DB-pair expansion buffers ---------------------------------------------
+enum : int32_t { kDbEmpty = 0, kDbDspDone = 1, kDbCpuDone = 2 };
+struct DbExpansion {
+  volatile int32_t state;
+  int32_t count, finished, pad;
+  int32_t neighbor_ids[kItemsMax];
+  float coarse_dists[kItemsMax];
+  float corrected_dists[kItemsMax];
+};
+struct DbSharedStats {
+  volatile uint64_t dsp_wait_cpu_done_us, dsp_invalidate_us, dsp_wait_poll_count;
+};
+struct DbShared {
+  DbExpansion buf[2];
+  DbSharedStats stats;
+};
+static_assert(sizeof(DbExpansion) == 400 && offsetof(DbExpansion, corrected_dists) == 272, "expansion buffer layout");
+static_assert(sizeof(DbShared) == 824, "DB-pair shared layout");
+
 // ---- the GPU side of one service pass ---------------------------------------
 //
 // One device block per session: [offsets: 2 x int64][status: int32, padded to
@@ -676,4 +695,205 @@ extern "C" AEEResult calculator_retrieval_expand_sqmd_run(remote_handle64 h, int
   }
   session_release(kSessionSqmd);
   return rc;
+}
+
+// ---- DB-pair search --------------------------------------------------------
+//
+// retrieval_async_dsp_search.c:1399-1581.  Two queries searched side by side;
+// each expansion's neighbours go to the caller through the shared expansion
+// buffer (DSP_DONE), the caller's correction thread writes their corrected
+// distances back (CPU_DONE), and only then does the search take its next
+// step.  Both searches live on the device (db_step_kernel); this loop moves
+// each step's ids and distances between the expansion buffers and the
+// device, one launch per round for every slot that is ready.
+namespace {
+
+struct DbDevice {
+  cudaStream_t stream = nullptr;
+  void* block = nullptr;
+  DbIo* h_io = nullptr;
+  bool ok = false;
+  DbArgs args{};
+  ~DbDevice() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (block) cudaFree(block);
+    if (h_io) cudaFreeHost(h_io);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  // One allocation: io, slots, queries, pools, frontiers, visited bitmaps, outputs.
+  bool init(const SqIndexView& v, int pool_cap, int num_out) {
+    const size_t n = static_cast<size_t>(v.n), vwords = (n + 31) / 32;
+    auto up = [](size_t x) { return (x + 255) & ~static_cast<size_t>(255); };
+    const size_t o_io = 0, o_slots = up(o_io + sizeof(DbIo)), o_q = up(o_slots + kDbSlots * sizeof(DbSlot)),
+                 o_pool = up(o_q + kDbSlots * v.dim * 4ull), o_front = up(o_pool + kDbSlots * pool_cap * 8ull),
+                 o_vis = up(o_front + kDbSlots * n * 8), o_ids = up(o_vis + kDbSlots * vwords * 4),
+                 o_d = up(o_ids + kDbSlots * num_out * 4ull), total = up(o_d + kDbSlots * num_out * 4ull);
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&block, total) != cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void**>(&h_io), sizeof(DbIo), cudaHostAllocDefault) != cudaSuccess) {
+      session_error("DB-pair set-up: %s", cudaGetErrorString(cudaGetLastError()));
+      return false;
+    }
+    uint8_t* b = static_cast<uint8_t*>(block);
+    args.ix = v;
+    args.io = reinterpret_cast<DbIo*>(b + o_io);
+    args.slots = reinterpret_cast<DbSlot*>(b + o_slots);
+    args.queries = reinterpret_cast<const float*>(b + o_q);
+    args.pools = reinterpret_cast<uint64_t*>(b + o_pool);
+    args.fronts = reinterpret_cast<uint64_t*>(b + o_front);
+    args.visited = reinterpret_cast<uint32_t*>(b + o_vis);
+    args.out_ids = reinterpret_cast<int32_t*>(b + o_ids);
+    args.out_dists = reinterpret_cast<float*>(b + o_d);
+    args.pool_cap = pool_cap;
+    args.num_out = num_out;
+    args.frontier_cap = v.n;     // every id enters the frontier at most once
+    std::memset(h_io, 0, sizeof(DbIo));
+    return ok = true;
+  }
+  bool upload_queries(const float* qa, const float* qb) {
+    float* q = const_cast<float*>(args.queries);
+    const size_t bytes = static_cast<size_t>(args.ix.dim) * 4;
+    return cudaMemcpyAsync(q, qa, bytes, cudaMemcpyHostToDevice, stream) == cudaSuccess &&
+           cudaMemcpyAsync(q + args.ix.dim, qb, bytes, cudaMemcpyHostToDevice, stream) == cudaSuccess;
+  }
+  // h_io -> device, one step, device -> h_io
+  bool launch() {
+    if (cudaMemcpyAsync(args.io, h_io, sizeof(DbIo), cudaMemcpyHostToDevice, stream) != cudaSuccess) return false;
+    launch_db_step(args, stream);
+    if (cudaGetLastError() != cudaSuccess) return false;
+    session_count_launches(1);
+    return cudaMemcpyAsync(h_io, args.io, sizeof(DbIo), cudaMemcpyDeviceToHost, stream) == cudaSuccess &&
+           cudaStreamSynchronize(stream) == cudaSuccess;
+  }
+};
+
+}  // namespace
+
+extern "C" AEEResult calculator_retrieval_search_db(remote_handle64 h, const float* query_a, int query_aLen,
+                                                    const float* query_b, int query_bLen, int32 fd_expansion_buf,
+                                                    int32 entry_points, int32 expand_count, int32 pool_size,
+                                                    int32 num_out, int* candidate_ids_a, int candidate_ids_aLen,
+                                                    float* candidate_dists_a, int candidate_dists_aLen,
+                                                    int32* actual_count_a, int* candidate_ids_b, int candidate_ids_bLen,
+                                                    float* candidate_dists_b, int candidate_dists_bLen,
+                                                    int32* actual_count_b) {
+  (void)h;
+  if (!actual_count_a || !actual_count_b) return AEE_EBADPARM;
+  *actual_count_a = 0;
+  *actual_count_b = 0;
+  DbShared* shared = map_fd<DbShared>(fd_expansion_buf, sizeof(DbShared));
+  if (!shared) {
+    session_error("DB-pair search: the fd names no rpcmem buffer of the needed size");
+    return AEE_EFAILED;
+  }
+  SessionIndex ix;
+  if (!session_acquire(kSessionDb, &ix)) return AEE_EFAILED;
+  struct Release { ~Release() { session_release(kSessionDb); } } release;
+  const SqIndexView& v = ix.sq;
+  if (!v.graph) {
+    session_error("DB-pair search: the loaded L1 index has no graph");
+    return AEE_EFAILED;
+  }
+  if (candidate_ids_aLen < num_out || candidate_dists_aLen < num_out || candidate_ids_bLen < num_out ||
+      candidate_dists_bLen < num_out)
+    return AEE_EBADPARM;
+  // db_search_state_init's refusals (:1213-1224, quantization at :1270)
+  const int expand_limit = std::min(expand_count, v.degree);
+  if (!query_a || !query_b || query_aLen < v.dim || query_bLen < v.dim || entry_points <= 0 || pool_size <= 0 ||
+      num_out <= 0 || expand_limit <= 0 || !(v.l1_scale != 0.0f)) {
+    session_error("DB-pair search: the search state cannot be set up for these arguments");
+    return AEE_ENOMEMORY;
+  }
+  DeviceScope device(ix.device);
+  const int cap = std::min(pool_size, 2000);   // DSP_SEARCH_MAX_POOL
+  DbDevice dev;
+  if (!dev.init(v, cap, num_out) || !dev.upload_queries(query_a, query_b)) return AEE_ENOMEMORY;
+  dev.args.entry_points = entry_points;
+  dev.args.expand_limit = std::min(expand_limit, kItemsMax);
+  dev.args.graph_entry = ix.sq_graph_entry;   // as dsp_search_select_entry_id reads it
+  DbIo& io = *dev.h_io;
+  io.op[0] = io.op[1] = kDbInit;
+  if (!dev.launch() || io.status[0] != kStatusOk || io.status[1] != kStatusOk) {
+    session_error("DB-pair search: entry seeding failed");
+    return AEE_ENOMEMORY;
+  }
+  for (int i = 0; i < 2; ++i) {
+    shared->buf[i].state = kDbEmpty;
+    shared->buf[i].finished = 0;
+    shared->buf[i].count = 0;
+  }
+  shared->stats.dsp_wait_cpu_done_us = shared->stats.dsp_invalidate_us = shared->stats.dsp_wait_poll_count = 0;
+  release_fence();
+  bool fin[2] = {false, false};
+  Backoff idle(idle_limit_us());
+  uint64_t wait_us = 0, polls = 0;
+  while (!fin[0] || !fin[1]) {
+    acquire_fence();
+    bool any = false;
+    for (int i = 0; i < 2; ++i) {
+      io.op[i] = kDbNone;
+      if (fin[i]) continue;
+      DbExpansion& b = shared->buf[i];
+      const int32_t state = b.state;
+      if (state == kDbCpuDone) {
+        acquire_fence();
+        if (b.count < 0 || b.count > kItemsMax) return AEE_ENOMEMORY;   // db_search_apply_corrections refuses
+        for (int j = 0; j < b.count; ++j) io.corr[i][j] = b.corrected_dists[j];
+        io.op[i] = kDbStep;
+      } else if (state == kDbEmpty) {
+        io.op[i] = kDbStep;
+      }
+      any |= io.op[i] != kDbNone;
+    }
+    if (!any) {
+      if (!idle.wait(&polls)) {
+        session_error("DB-pair search: the caller returned no corrections within the idle limit");
+        return AEE_EFAILED;
+      }
+      continue;
+    }
+    idle.woke(&wait_us);
+    if (!dev.launch()) {
+      session_error("DB-pair search: %s", cudaGetErrorString(cudaGetLastError()));
+      return AEE_EFAILED;
+    }
+    for (int i = 0; i < 2; ++i) {
+      if (io.op[i] != kDbStep) continue;
+      if (io.status[i] != kStatusOk) {
+        session_error("DB-pair search: step failed with status %d", io.status[i]);
+        return AEE_ENOMEMORY;
+      }
+      DbExpansion& b = shared->buf[i];
+      if (io.finished[i]) {
+        fin[i] = true;
+        b.finished = 1;
+        b.count = 0;
+      } else {
+        for (int j = 0; j < io.count[i]; ++j) {
+          b.neighbor_ids[j] = io.ids[i][j];
+          b.coarse_dists[j] = io.coarse[i][j];
+        }
+        b.count = io.count[i];
+      }
+      release_fence();
+      b.state = kDbDspDone;
+    }
+  }
+  io.op[0] = io.op[1] = kDbFinish;
+  if (!dev.launch()) return AEE_EFAILED;
+  const int na = io.out_count[0], nb = io.out_count[1];
+  const size_t bytes_a = static_cast<size_t>(na) * 4, bytes_b = static_cast<size_t>(nb) * 4;
+  const bool copied =
+      cudaMemcpyAsync(candidate_ids_a, dev.args.out_ids, bytes_a, cudaMemcpyDeviceToHost, dev.stream) == cudaSuccess &&
+      cudaMemcpyAsync(candidate_dists_a, dev.args.out_dists, bytes_a, cudaMemcpyDeviceToHost, dev.stream) == cudaSuccess &&
+      cudaMemcpyAsync(candidate_ids_b, dev.args.out_ids + num_out, bytes_b, cudaMemcpyDeviceToHost, dev.stream) == cudaSuccess &&
+      cudaMemcpyAsync(candidate_dists_b, dev.args.out_dists + num_out, bytes_b, cudaMemcpyDeviceToHost, dev.stream) == cudaSuccess &&
+      cudaStreamSynchronize(dev.stream) == cudaSuccess;
+  if (!copied) return AEE_EFAILED;
+  *actual_count_a = na;
+  *actual_count_b = nb;
+  shared->stats.dsp_wait_cpu_done_us = wait_us;
+  shared->stats.dsp_wait_poll_count = polls;
+  release_fence();
+  return AEE_SUCCESS;
 }

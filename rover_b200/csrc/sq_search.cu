@@ -10,6 +10,13 @@
 //    seeds from retrieval_sqmd_make_seed_ids (retrieval_sqmd_seed.c:15), and
 //    the exact residual distance (retrieval_rpc_demo_support.c:1397) replacing
 //    the coarse one when correction is on.
+//  * kSqModeDb: one query of calculator_retrieval_search_db, the DB-pair
+//    search (retrieval_async_dsp_search.c:1205-1581): the device search of
+//    kSqModeDsp (entries, pool clamp, neighbour filtering), except that every
+//    expansion candidate enters the pool with the distance the host's
+//    correction thread returns for it (retrieval_rpc_demo_pipeline.c:454-495:
+//    the exact residual distance with correction on, the coarse one with it
+//    off) and that the frontier grows as needed (db_search_reserve_frontier).
 //
 // SQ pool and frontier heaps order by distance only and break ties by heap
 // position (strict '<' replacement, sqmd_common.c:51-80), so results depend
@@ -185,6 +192,7 @@ sq_search_kernel(SqSearchArgs a) {
   vt.slots = a.visited + static_cast<size_t>(slot) * (a.visited_mask + 1ull);
   vt.mask = a.visited_mask;
   const bool sqmd = a.mode == kSqModeSqmd;
+  const bool db = a.mode == kSqModeDb;
 
   for (;;) {
     int qi = 0;
@@ -201,8 +209,10 @@ sq_search_kernel(SqSearchArgs a) {
       continue;
     }
     // frontier capacity the reference allocates for this request
-    const long long fcap_ref = sqmd ? static_cast<long long>(a.entry_points) + static_cast<long long>(cap) * a.expand_count
-                                    : static_cast<long long>(a.entry_points) + static_cast<long long>(cap) * expand;
+    // (the DB-pair search grows its frontier up to n entries)
+    const long long fcap_ref = db ? static_cast<long long>(ix.n)
+                               : sqmd ? static_cast<long long>(a.entry_points) + static_cast<long long>(cap) * a.expand_count
+                                      : static_cast<long long>(a.entry_points) + static_cast<long long>(cap) * expand;
     const int fcap = static_cast<int>(min(fcap_ref, static_cast<long long>(a.frontier_cap)));
     // query and its quantized codes (retrieval_quantize_query_u8/_u4, l1_int8_core.c:13-63)
     const float inv = __frcp_rn(ix.l1_scale);
@@ -343,7 +353,7 @@ sq_search_kernel(SqSearchArgs a) {
         float d = 0.0f;
         if (fresh) {
           d = sq_coarse(ix, qc, nid);
-          if (sqmd && a.correction) d = sq_exact(ix, q, nid);
+          if ((sqmd || db) && a.correction) d = sq_exact(ix, q, nid);
         }
         const int slot_i = __popc(fm & ((1u << lane) - 1u));
         if (fresh) {
@@ -411,5 +421,161 @@ sq_search_kernel(SqSearchArgs a) {
     __syncwarp();
   }
 }
+
+
+// ---------------------------------------------------------------------------
+// DB-pair search, one step per launch (calculator_retrieval_search_db).  Warp
+// w serves slot w when io.op[w] asks for it:
+//   kDbInit   db_search_state_init (retrieval_async_dsp_search.c:1205-1301):
+//             quantized query, cleared visited bitmap, entries (graph entry,
+//             then the LCG of dsp_search_select_entry_id) with their coarse
+//             distances inserted in draw order;
+//   kDbStep   db_search_apply_corrections (:1371-1389) for the ids the last
+//             step returned, with the corrected distances the caller wrote
+//             into io.corr, then db_search_expand_one_step (:1303-1369): pop
+//             (dropping entries worse than a full pool's worst), read up to
+//             expand_limit neighbours, skip invalid and visited ids, and
+//             return the rest with their coarse distances -- or finished;
+//   kDbFinish dsp_heap_sort and the first num_out entries.
+// Heap operations run on lane 0 in the reference's order; lanes compute the
+// coarse distances.
+__global__ void __launch_bounds__(kDbSlots * 32) db_step_kernel(DbArgs a) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  DbIo& io = *a.io;
+  const int op = io.op[w];
+  if (op == kDbNone) return;
+  const SqIndexView& ix = a.ix;
+  DbSlot& s = a.slots[w];
+  HeapEntry* pool = reinterpret_cast<HeapEntry*>(a.pools) + static_cast<size_t>(w) * a.pool_cap;
+  HeapEntry* front = reinterpret_cast<HeapEntry*>(a.fronts) + static_cast<size_t>(w) * a.frontier_cap;
+  const size_t vwords = (static_cast<size_t>(ix.n) + 31) / 32;
+  uint32_t* visited = a.visited + static_cast<size_t>(w) * vwords;
+  __shared__ HeapEntry work[kDbSlots][32];
+  __shared__ int32_t ids[kDbSlots][32];
+  int st = kStatusOk;
+  auto push = [&](int32_t id, float d) {   // lane 0: pool insert, then frontier push
+    if (pool_insert(pool, &s.psize, a.pool_cap, id, d)) {
+      if (s.fsize >= a.frontier_cap) { st = kStatusFrontierFull; return; }
+      front[s.fsize] = HeapEntry{id, d};
+      front_sift_up(front, s.fsize);
+      ++s.fsize;
+    }
+  };
+  auto test_and_set = [&](int32_t id) {     // lane 0 only
+    uint32_t& word = visited[id >> 5];
+    const uint32_t bit = 1u << (id & 31);
+    const bool seen = (word & bit) != 0;
+    word |= bit;
+    return !seen;
+  };
+  if (op == kDbInit) {
+    const float* q = a.queries + static_cast<size_t>(w) * ix.dim;
+    const float inv = __frcp_rn(ix.l1_scale);
+    const int levels = ix.l1_bits == 4 ? 15 : 255;
+    for (int d = lane; d < ix.dim; d += kWarp) {
+      int c = static_cast<int>(roundf(fmul(fsub(q[d], ix.l1_zero), inv)));
+      s.qc[d] = static_cast<uint8_t>(c < 0 ? 0 : (c > levels ? levels : c));
+    }
+    for (size_t i = lane; i < vwords; i += kWarp) visited[i] = 0u;
+    if (lane == 0) { s.psize = s.fsize = s.finished = s.last_count = 0; }
+    __syncwarp();
+    __threadfence_block();
+    const int entries = min(a.entry_points, ix.n);
+    uint32_t lcg = 42u;   // DSP_SEARCH_ENTRY_SEED
+    for (int e0 = 0; e0 < entries && st == kStatusOk; e0 += kWarp) {
+      if (lane == 0) {
+        for (int t = 0; t < kWarp; ++t) {
+          const int i = e0 + t;
+          int32_t id = -1;
+          if (i < entries) {
+            if (i == 0 && a.graph_entry >= 0 && a.graph_entry < ix.n) {
+              id = a.graph_entry;
+            } else {
+              lcg = lcg * 1103515245u + 12345u;
+              id = static_cast<int32_t>((static_cast<uint64_t>(lcg) * static_cast<uint64_t>(ix.n)) >> 32);
+            }
+            if (!test_and_set(id)) id = -1;
+          }
+          ids[w][t] = id;
+        }
+      }
+      __syncwarp();
+      const int32_t id = ids[w][lane];
+      work[w][lane] = HeapEntry{id, id >= 0 ? sq_coarse(ix, s.qc, id) : 0.0f};
+      __syncwarp();
+      if (lane == 0)
+        for (int t = 0; t < kWarp && st == kStatusOk; ++t)
+          if (work[w][t].id >= 0) push(work[w][t].id, work[w][t].dist);
+      st = __shfl_sync(kFullMask, st, 0);
+      __syncwarp();
+    }
+    if (lane == 0) io.status[w] = st;
+    return;
+  }
+  if (op == kDbFinish) {
+    if (lane == 0) {
+      for (int i = s.psize - 1; i > 0; --i) {     // dsp_heap_sort
+        const HeapEntry t = pool[0];
+        pool[0] = pool[i];
+        pool[i] = t;
+        pool_sift_down(pool, i, 0);
+      }
+      const int outn = min(a.num_out, s.psize);
+      for (int i = 0; i < outn; ++i) {
+        a.out_ids[static_cast<size_t>(w) * a.num_out + i] = pool[i].id;
+        a.out_dists[static_cast<size_t>(w) * a.num_out + i] = pool[i].dist;
+      }
+      io.out_count[w] = outn;
+      io.status[w] = kStatusOk;
+    }
+    return;
+  }
+  // kDbStep: the caller's corrections of the last step, then the next step
+  int32_t src = -1;
+  if (lane == 0) {
+    const int nc = s.last_count;
+    for (int t = 0; t < nc && st == kStatusOk; ++t) push(s.last_ids[t], io.corr[w][t]);
+    if (st == kStatusOk) {
+      while (s.fsize > 0 && s.psize >= a.pool_cap && front[0].dist > pool[0].dist) front_pop(front, &s.fsize);
+      if (s.fsize > 0) src = front_pop(front, &s.fsize);
+    }
+  }
+  st = __shfl_sync(kFullMask, st, 0);
+  src = __shfl_sync(kFullMask, src, 0);
+  if (st != kStatusOk || src < 0) {
+    if (lane == 0) {
+      s.finished = src < 0 ? 1 : s.finished;
+      s.last_count = 0;
+      io.count[w] = 0;
+      io.finished[w] = src < 0;
+      io.status[w] = st;
+    }
+    return;
+  }
+  if (lane == 0) {
+    const int32_t* row = ix.graph + static_cast<size_t>(src) * ix.degree;
+    int cnt = 0;
+    for (int j = 0; j < a.expand_limit && cnt < kDbItems; ++j) {
+      const int32_t nid = row[j];
+      if (nid < 0 || nid >= ix.n) continue;
+      if (!test_and_set(nid)) continue;
+      ids[w][cnt++] = nid;
+    }
+    s.last_count = cnt;
+    io.count[w] = cnt;
+    io.finished[w] = 0;
+    io.status[w] = kStatusOk;
+  }
+  __syncwarp();
+  const int cnt = __shfl_sync(kFullMask, lane == 0 ? s.last_count : 0, 0);
+  if (lane < cnt) {
+    const int32_t nid = ids[w][lane];
+    s.last_ids[lane] = nid;
+    io.ids[w][lane] = nid;
+    io.coarse[w][lane] = sq_coarse(ix, s.qc, nid);
+  }
+}
+
+void launch_db_step(const DbArgs& a, cudaStream_t s) { db_step_kernel<<<1, kDbSlots * 32, 0, s>>>(a); }
 
 }  // namespace rover

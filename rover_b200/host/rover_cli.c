@@ -325,7 +325,6 @@ static int parse(int argc, char** argv) {
     c->refine_mode = c->refine ? 1 + (c->third_residual != 0) : 0;
     if (c->third_residual) return refuse("the third-level (ERROR4) refine is not part of this build");
     if (c->split_distance) return refuse("the SQ4 split-distance correction is not part of this build");
-    if (is(c->search_mode, "db_pair")) return refuse("the DB-pair search mode is not part of this build");
     if (is(c->command, "search") &&
         !(c->nq > 0 && c->top_k <= c->n && *c->query && (*c->graph || *c->index_dir)))
         return refuse("search requires query, graph, nq and top-k <= n");
@@ -489,7 +488,9 @@ static int run_search(remote_handle64 h, const RoverBundle* b, const float* quer
        the first-stage factor */
     p.top_k = pq ? cfg.top_k : (refine_budget ? refine_budget : cfg.top_k * cfg.first_factor);
     p.pool_stride = pq ? cfg.pool : 0;
-    p.sq_mode = 1;
+    /* SQ: the SQMD loop, or the DB-pair search (retrieval_rpc_demo_pipeline.c:2496-2700) */
+    const int db_pair = !pq && is(cfg.search_mode, "db_pair");
+    p.sq_mode = db_pair ? 2 : 1;
     const int stride = p.top_k;
     Outputs o;
     memset(&o, 0, sizeof(o));
@@ -523,7 +524,10 @@ static int run_search(remote_handle64 h, const RoverBundle* b, const float* quer
             refine_budget ? (o.pool_counts[i] < refine_budget ? o.pool_counts[i] : refine_budget) : 0);
     } else {
         rc = calculator_rover_sq_search(h, &p, queries, nq, pools, &out);
-        if (!rc && refine_budget) {
+        /* the DB-pair re-rank worker without final refine: demo_rerank_candidates
+           over every candidate (retrieval_rpc_demo_pipeline.c:204-226) */
+        const int rerank = db_pair && !refine_budget && cfg.correction;
+        if (!rc && (refine_budget || rerank)) {
             /* retrieval_final_refine over the first refine_budget entries of the SQMD pool */
             int32_t* cand_counts = (int32_t*)malloc((size_t)nq * 4);
             int32_t* rid = (int32_t*)malloc((size_t)nq * cfg.top_k * 4);
@@ -531,13 +535,13 @@ static int run_search(remote_handle64 h, const RoverBundle* b, const float* quer
             int32_t* rc_counts = (int32_t*)malloc((size_t)nq * 4);
             if (!cand_counts || !rid || !rd || !rc_counts) rc = -1;
             for (int i = 0; !rc && i < nq; ++i) {
-                cand_counts[i] = o.counts[i] < refine_budget ? o.counts[i] : refine_budget;
+                cand_counts[i] = rerank || o.counts[i] < refine_budget ? o.counts[i] : refine_budget;
                 refine_candidates += (unsigned long long)cand_counts[i];
             }
             const unsigned long long r0 = now_us();
             if (!rc)
-                rc = calculator_rover_refine(h, 0, queries, nq, o.ids, stride, cand_counts, cfg.top_k, rid, rd,
-                                             rc_counts, o.status);
+                rc = calculator_rover_refine(h, rerank ? 2 : 0, queries, nq, o.ids, stride, cand_counts, cfg.top_k,
+                                             rid, rd, rc_counts, o.status);
             refine_us = now_us() - r0;
             for (int i = 0; !rc && i < nq; ++i) {
                 memcpy(o.ids + (size_t)i * stride, rid + (size_t)i * cfg.top_k, (size_t)cfg.top_k * 4);

@@ -50,6 +50,12 @@ def cases(data: dict) -> dict:
     return {
         "refine": ["--pool", "32", "--entry-points", "4", "--expand-count", str(min(16, deg)), "--refine", "on"],
         "first_stage": ["--pool", "40", "--entry-points", "8", "--expand-count", str(min(8, deg)), "--refine", "off"],
+        # DB-pair search (calculator_retrieval_search_db with the host's
+        # residual correction); refine off re-ranks with demo_rerank_candidates
+        "db_pair_rerank": ["--search-mode", "db-pair", "--pool", "32", "--entry-points", "4",
+                           "--expand-count", str(min(16, deg)), "--refine", "off"],
+        "db_pair_refine": ["--search-mode", "db-pair", "--pool", "24", "--entry-points", "6",
+                           "--expand-count", str(min(12, deg)), "--refine", "on"],
     }
 
 
