@@ -715,12 +715,31 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
   const size_t smem = slices + static_cast<size_t>(b.filter_bits) / 8;
   if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
-  const bool seed_pass = !gated;      // exact seed distances
-  const bool rank_pass = rows;        // quantized seed distances (tensor cores)
+  // exact seed pools: verified from TF32 ranks of the seeds' decoded rows
+  // when every pool fits kMaxBatch (as the exact decoded search does), else
+  // the all-seeds exact distance pass
+  const bool verify = !gated && !tracing && a.max_pool <= kMaxBatch;
+  const bool seed_pass = !gated && !verify;   // exact seed distances
+  const bool rank_pass = rows;                // quantized seed distances (tensor cores)
   if (rank_pass && ensure_seed_recon(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
-  const size_t per_query = static_cast<size_t>(ss.count) * sizeof(float) * ((seed_pass ? 1 : 0) + (rank_pass ? 1 : 0));
+  if (verify) {
+    if (ensure_seed_drows(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
+    b.seed_verify = 1;
+    b.seed_norms = ss.drow_norms.as<float>();
+    b.seed_norm_max = ss.drow_norm_max;
+    b.seed_stride = (ss.count + 3) / 4 * 4;   // rank rows are read as float4
+    b.top_m = seed_top_m(ss.count, a.max_pool);
+  }
+  const size_t row_floats = verify ? static_cast<size_t>(b.seed_stride) : static_cast<size_t>(ss.count);
+  const size_t per_query = row_floats * sizeof(float) * ((seed_pass || verify ? 1 : 0) + (rank_pass ? 1 : 0));
   const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(nq, kSeedDistBudget / per_query)));
-  if (seed_pass) CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
+  if (seed_pass || verify) CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * row_floats * sizeof(float)));
+  if (verify) {
+    CK(s.seed_top.ensure(static_cast<size_t>(chunk) * b.top_m * sizeof(uint64_t)));
+    CK(s.seed_top_next.ensure(static_cast<size_t>(chunk) * sizeof(float)));
+    b.seed_top = s.seed_top.as<uint64_t>();
+    b.seed_top_next = s.seed_top_next.as<float>();
+  }
   if (rank_pass) {
     CK(s.seed_rank.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
     b.top_m = seed_top_m(ss.count, a.max_pool);
@@ -729,7 +748,7 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
     b.seed_top = s.seed_top.as<uint64_t>();
     b.seed_top_next = s.seed_top_next.as<float>();
   }
-  b.seed_dists = seed_pass ? s.seed_dists.as<float>() : nullptr;
+  b.seed_dists = seed_pass || verify ? s.seed_dists.as<float>() : nullptr;
   c.seed_rank = rank_pass ? s.seed_rank.as<float>() : nullptr;
   const int blocks_cap = std::max(1, std::min(max_blocks, (chunk + kSearchWarps - 1) / kSearchWarps));
   const size_t slots = static_cast<size_t>(blocks_cap) * kSearchWarps;
@@ -755,6 +774,17 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
         }
         CK(cudaGetLastError());
         ++g_launches;
+      }
+      if (verify) {
+        {
+          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
+          launch_pq_seed_rank(a.queries, q0, q1, pq.view.dim, ss.drows.as<float>(), ss.drow_norms.as<float>(),
+                              b.n_seeds, s.seed_dists.as<float>(), stream, b.seed_stride);
+          launch_pq_seed_topm(s.seed_dists.as<float>(), b.seed_stride, b.n_seeds, q1 - q0, b.top_m,
+                              s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
+        }
+        CK(cudaGetLastError());
+        g_launches += 2;
       }
       if (rank_pass) {
         {

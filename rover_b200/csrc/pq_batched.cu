@@ -33,6 +33,7 @@
 #include <cuda_bf16.h>
 
 #include "pq_common.cuh"
+#include "pq_seed_pool.cuh"
 
 namespace rover {
 
@@ -313,14 +314,27 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
     }
 
     if (!kGated) {
-      // ---- exact seed pool from the all-seeds distance pass
+      // ---- exact seed pool: verified from the TF32 seed ranks (every pool
+      // within kMaxBatch, not tracing), else from the all-seeds distance pass
       corrected = static_cast<unsigned long long>(b.n_seeds);
-      const float* drow = b.seed_dists + seed_row;
-      if (st == kStatusOk &&
-          !(cap <= kMaxBatch
-                ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)
-                : select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)))
-        st = kStatusNumeric;
+      if (!tracing && b.seed_verify) {
+        const float* arow = b.seed_dists + seed_row_index * b.seed_stride;
+        if (st == kStatusOk) {
+          if (cap > kMaxBatch) st = kStatusBadParam;
+          else if (!verified_seed_pool<D>(list, &size, cap, stage, batch, b, arow,
+                                          b.seed_top ? b.seed_top + seed_row_index * b.top_m : nullptr,
+                                          b.seed_top ? b.seed_top_next[seed_row_index] : 0.0f, q, dim, &cursor,
+                                          lane))
+            st = kStatusNumeric;
+        }
+      } else {
+        const float* drow = b.seed_dists + seed_row;
+        if (st == kStatusOk &&
+            !(cap <= kMaxBatch
+                  ? select_top_lanes(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)
+                  : select_top(list, &size, cap, stage, b.n_seeds, SeedRowKeys{drow, b.seed_ids}, &cursor, lane)))
+          st = kStatusNumeric;
+      }
       if (st == kStatusOk && check_adc) {
         bool adc_bad = false;
         for (int e = lane; e < b.n_seeds; e += kWarp) {
