@@ -397,13 +397,16 @@ def device_steps(calc, args, step, stream, dist=None, dev=None):
 
 
 SEED_KERNELS = ("pq_seeds", "pq_seed_rank")
-# DRAM bytes per query of the search kernels, read from one ncu capture each
-# (dram__bytes_read.sum + dram__bytes_write.sum over the queries of a
-# 2,000-query launch at the headline operating points); scaled to a launch by
-# its query count.
+# DRAM bytes per query of each form's search kernel, from one ncu capture of
+# a 2,000-query launch at the benchmark's operating point
+# (dram__bytes_read.sum + dram__bytes_write.sum / 2,000); scaled to a launch
+# by its query count, since traffic grows with the queries searched.
 PROFILED_TRAFFIC = {
-    "pq_batched": (226.0e3, "profiles/pq_batched_gated_pq1m_2000q.md (W=2, L=32, 4,096 entry points)"),
-    "pq_decoded": (None, None),
+    "plain": (219.8e3, "ncu DRAM bytes of pq_decoded_search_kernel<128>, 2,000 queries, L=40, 4,096 entry points"),
+    "batched": (184.3e3, "ncu DRAM bytes of pq_batched_search_kernel<128,kBatchFull>, 2,000 queries, W=3, L=24, "
+                         "8,192 entry points"),
+    "gated": (191.0e3, "ncu DRAM bytes of pq_batched_search_kernel<128,kBatchGated>, 2,000 queries, W=3, L=24, "
+                       "8,192 entry points"),
 }
 
 
@@ -418,7 +421,7 @@ def roofline(bytes_per_call, seed_bytes_per_call, kernels, steps, nq, label):
     launch_s = total_ms / max(1, launches) / 1e3
     per_launch = (bytes_per_call - seed_bytes_per_call) * steps / max(1, launches)
     achieved = per_launch / launch_s / 1e9
-    per_query, source = PROFILED_TRAFFIC.get(top, (None, None))
+    per_query, source = PROFILED_TRAFFIC.get(label, (None, None))
     traffic = per_query * nq * steps / max(1, launches) if per_query else None
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "traffic_source": source, "peak_kind": peak_kind, "kernel": top,

@@ -14,7 +14,16 @@ residual rows), ``batched`` (W-wide steps, full correction) and ``gated``
 (the batched kernel with a loaded gate whose thresholds correct every
 shortlisted seed and never stop -- the configuration bench.py's calibration
 keeps on the 1M x 128 workload).
+
+``--form score --kind K`` runs one of the batched distance kernels of
+calculator_rover_score instead (K: 0 ADC, 1 packed residual, 2 SQ8 code
+distance, 3 SQ exact residual, 4 decoded-row rescore) on --queries queries x
+--ids uniformly random ids over the index; ``--form refine`` the FP64 final
+refine of 128 candidates per query.  SQ kinds encode the same base vectors
+with the global 8-bit SQ codec.  With ``--adc-n N`` (kind 0) the index is a
+synthetic one of N random M=16 codes, so that the gathered codes exceed L2.
 """
+
 from __future__ import annotations
 
 import argparse
@@ -27,7 +36,10 @@ import numpy as np
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--form", default="gated", choices=("plain", "packed", "batched", "gated"))
+    ap.add_argument("--form", default="gated", choices=("plain", "packed", "batched", "gated", "score", "refine"))
+    ap.add_argument("--kind", type=int, default=4)
+    ap.add_argument("--ids", type=int, default=8192)
+    ap.add_argument("--adc-n", type=int, default=0)
     ap.add_argument("--workload", default="pq_1m_d128")
     ap.add_argument("--queries", type=int, default=2000)
     ap.add_argument("--L", type=int, default=32)
@@ -39,6 +51,8 @@ def main(argv=None) -> int:
 
     from . import workloads
     from .calculator import GATE_PARAMS, MODE_BATCHED, MODE_EXACT, MODE_GATED, Calculator
+    if args.form in ("score", "refine"):
+        return distance_case(args)
     w = workloads.build_pq(args.workload, cache_dir=args.cache_dir, verbose=False)
     calc = Calculator()
     calc.pq_load(w.graph, w.entry, w.bundle)
@@ -66,6 +80,57 @@ def main(argv=None) -> int:
     calc.kernel_timing(False)
     print(json.dumps(dict(form=args.form, workload=args.workload, queries=len(q), L=args.L, entry_points=args.ep,
                           beam_width=args.W if args.form in ("batched", "gated") else None,
+                          warm_launches=warm, kernel_ms=times)), flush=True)
+    calc.close()
+    return 0
+
+
+def distance_case(args) -> int:
+    """One warm-up call and --repeat timed calls of a distance kernel."""
+    from . import bundle as B
+    from . import datasets as D
+    from . import workloads
+    from .calculator import Calculator
+    rng = np.random.default_rng(7)
+    calc = Calculator()
+    if args.form == "score" and args.kind == 0 and args.adc_n:
+        n, dim, m = args.adc_n, 128, 16
+        book = rng.normal(size=(m, 256, dim // m)).astype(np.float32)
+        codes = rng.integers(0, 256, size=(n, m), dtype=np.uint8)
+        bundle = B.PqBundle(B.PqMeta(b"\x07" * 16, n, dim, m, 256, dim // m, m), book, codes)
+        calc.pq_load(None, -1, bundle)
+        q = rng.normal(size=(args.queries, dim)).astype(np.float32)
+        label = f"synthetic {n:,} x M=16 codes"
+    else:
+        w = workloads.build_pq(args.workload, cache_dir=args.cache_dir, verbose=False)
+        n = w.bundle.meta.num_vectors
+        q = np.ascontiguousarray(w.queries[:args.queries])
+        label = args.workload
+        if args.form == "score" and args.kind in (2, 3):
+            cfg = workloads.CONFIGS[args.workload]
+            base = D.gmm(cfg["n"], cfg["dim"], cfg["comps"], cfg["seed"], clip_nonneg=cfg["clip"],
+                         normalize=cfg["normalize"])
+            s, z, l1, res, qp = D.sq_encode(base, 8, 8)
+            del base
+            calc.sq_load(w.graph, w.entry, B.SqBundle(n, cfg["dim"], 8, float(s), float(z), l1, 8, res, qp))
+        else:
+            calc.pq_load(w.graph, w.entry, w.bundle)
+    if args.form == "score":
+        lists = list(rng.integers(0, n, size=(len(q), args.ids), dtype=np.int64).astype(np.int32))
+        run = lambda: calc.score(args.kind, q, lists)
+    else:
+        cand = ((rng.integers(0, n, size=(len(q), 1)) + np.arange(128)[None, :] * 7919) % n).astype(np.int32)
+        run = lambda: calc.refine(1, q, cand, np.full(len(q), 128, np.int32), 10)
+    l0 = calc.launch_count()
+    run()
+    warm = calc.launch_count() - l0
+    calc.kernel_timing(True)
+    for _ in range(args.repeat):
+        run()
+    times = {k: v[1] / args.repeat for k, v in calc.kernel_times().items() if v[0] > 0}
+    calc.kernel_timing(False)
+    print(json.dumps(dict(form=args.form, kind=args.kind if args.form == "score" else None, index=label,
+                          queries=len(q), ids_per_query=args.ids if args.form == "score" else 128,
                           warm_launches=warm, kernel_ms=times)), flush=True)
     calc.close()
     return 0
