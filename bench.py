@@ -396,7 +396,7 @@ def device_steps(calc, args, step, stream, dist=None, dev=None):
                 clocks=clocks.summary())
 
 
-SEED_KERNELS = ("pq_seeds", "pq_seed_rank")
+SEED_KERNELS = ("pq_seeds", "pq_seed_rank", "pq_seed_topm")
 # DRAM bytes per query of each form's search kernel, from one ncu capture of
 # a 2,000-query launch at the benchmark's operating point
 # (dram__bytes_read.sum + dram__bytes_write.sum / 2,000); scaled to a launch

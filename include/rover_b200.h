@@ -328,6 +328,15 @@ AEEResult calculator_rover_gate_eval(remote_handle64 h, const float *rows, int64
 AEEResult calculator_rover_seed_topm(remote_handle64 h, const float *rank, int32_t rows, int32_t n_seeds, int32_t m,
                                      uint64_t *keys, float *next);
 
+/* The seed ranking of the verified seed pool on host buffers:
+ * out[nq][n_rows] = max(|q|^2 + |x|^2 - 2 q . x, 0) with the dot products on
+ * the tensor cores from TF32-rounded operands -- tcgen05 (TMA-fed, TMEM
+ * accumulators) for dim 32..128 in steps of 32, mma.sync otherwise or with
+ * ROVER_SEED_RANK=mma in the environment.  Runs the device code the searches
+ * run (pq_seed_rank, pq_seed_pool.cuh bounds its error). */
+AEEResult calculator_rover_seed_rank(remote_handle64 h, const float *queries, int32_t num_queries,
+                                     const float *rows, int32_t num_rows, int32_t dim, float *out);
+
 /* One training row per scored candidate or expansion source. */
 typedef struct RoverGateTraceRow {
     int32_t query, hop, id;
@@ -404,6 +413,7 @@ uint64_t calculator_rover_launch_count(void);
 #define ROVER_KERNEL_REFINE 11      /* calculator_rover_refine */
 #define ROVER_KERNEL_PQ_RESCORE 12  /* kind 4: corrected distances from decoded rows */
 #define ROVER_KERNEL_PLAN 13        /* search plans: bookkeeping kernels */
+#define ROVER_KERNEL_PQ_SEED_TOPM 14 /* per-query top-M of the seed ranks */
 #define ROVER_KERNEL_KINDS 16
 void calculator_rover_kernel_timing(int32_t enable);
 int32_t calculator_rover_kernel_times(int64_t *launches, double *ms, int32_t kinds);

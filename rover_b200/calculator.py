@@ -132,6 +132,7 @@ class Calculator:
         L.calculator_rover_gate_load.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.POINTER(GateThresholds)]
         L.calculator_rover_gate_unload.argtypes = [C.c_uint64]
         L.calculator_rover_gate_rows.argtypes = [C.c_uint64, C.POINTER(C.c_uint64)]
+        L.calculator_rover_seed_rank.argtypes = [C.c_uint64, _f32p, C.c_int32, _f32p, C.c_int32, C.c_int32, _f32p]
         L.calculator_rover_gate_eval.argtypes = [C.c_uint64, _f32p, C.c_int64, _f32p]
         L.calculator_rover_seed_topm.argtypes = [C.c_uint64, _f32p, C.c_int32, C.c_int32, C.c_int32, _u64p, _f32p]
         L.calculator_rover_gate_train.argtypes = [C.c_uint64, _f32p, _f32p, _f32p, C.c_int64,
@@ -181,7 +182,7 @@ class Calculator:
         return int(self.lib.calculator_rover_launch_count())
 
     KERNEL_KINDS = ("pq_packed", "pq_seeds", "pq_decoded", "pq_batched", "sq", "pq_seed_rank", "pq_lut", "pq_adc",
-                    "pq_residual", "sq_coarse", "sq_exact", "refine", "pq_rescore", "plan")
+                    "pq_residual", "sq_coarse", "sq_exact", "refine", "pq_rescore", "plan", "pq_seed_topm")
 
     # -- learned gate
     def gate_load(self, params, mu, sigma, band_lo=0.0, band_hi=0.0, refine_logit=0.0, stop_logit=1e30) -> None:
@@ -192,6 +193,16 @@ class Calculator:
         self._check("calculator_rover_gate_load",
                     self.lib.calculator_rover_gate_load(self.handle, _p(p, _f32p), _p(m, _f32p), _p(sg, _f32p),
                                                         C.byref(t)))
+
+    def seed_rank(self, queries, rows) -> np.ndarray:
+        """[nq][n_rows] TF32 tensor-core ranks |q|^2 + |x|^2 - 2 q.x (clamped at 0)."""
+        q = np.ascontiguousarray(queries, dtype=np.float32)
+        x = np.ascontiguousarray(rows, dtype=np.float32)
+        out = np.empty((q.shape[0], x.shape[0]), np.float32)
+        self._check("calculator_rover_seed_rank",
+                    self.lib.calculator_rover_seed_rank(self.handle, _p(q, _f32p), q.shape[0], _p(x, _f32p),
+                                                        x.shape[0], q.shape[1], _p(out, _f32p)))
+        return out
 
     def gate_rows(self) -> int:
         """MLP rows the loaded gate has evaluated inside searches since it was loaded."""

@@ -83,9 +83,16 @@ struct SeedSet {
   DevBuf recon, recon_norms;
   bool drows_ready = false;        // decoded rows for the verified exact seed pool
   DevBuf drows, drow_norms;
+  // TF32-rounded copies of recon / drows named by TMA descriptors, for the
+  // tensor-core seed ranking (valid == 0: the mma.sync ranking is used)
+  DevBuf recon_tc, drows_tc;
+  TcSeedMap recon_map{}, drows_map{};
   float drow_norm_max = 0.0f;      // largest of drow_norms (+inf if one is not finite)
   void release() {
     ids.release(); bits.release(); recon.release(); recon_norms.release(); drows.release(); drow_norms.release();
+    recon_tc.release(); drows_tc.release();
+    recon_map.valid = 0;
+    drows_map.valid = 0;
     valid = false;
     recon_ready = false;
     drows_ready = false;
@@ -139,6 +146,7 @@ struct State {
   // scratch
   DevBuf visited, heaps, counter, status, stats, luts, seed_dists, seed_rank;
   DevBuf seed_top, seed_top_next;  // per query: top-M seed ranks (pq_seed_topm_kernel)
+  DevBuf tc_err;                   // set by the tensor-core seed ranking if a bounded wait ran out
   DevBuf gate_buf;                // BF16 transposed weights + FP32 biases of the loaded gate
   GateParams gate{};              // enabled == 0: no gate loaded
   DevBuf trace_rows, trace_count; // calculator_rover_pq_trace
@@ -400,6 +408,58 @@ AEEResult ensure_seeds(State& s, PqDevice& pq, int32_t entry_points, uint32_t se
 }
 
 // PQ reconstructions of the current seed set (for the tensor-core ranking).
+// The tensor-core seed ranking runs where its descriptor could be made
+// (dim 32..128 in steps of 32) unless ROVER_SEED_RANK=mma asks for the
+// mma.sync kernel.
+bool tc_rank_wanted() {
+  static const bool want = [] {
+    const char* v = std::getenv("ROVER_SEED_RANK");
+    return !(v && std::strcmp(v, "mma") == 0);
+  }();
+  return want;
+}
+
+// A TF32-rounded copy of [count][dim] seed rows and its TMA descriptor.
+AEEResult make_tc_rows(State& s, const DevBuf& rows, int count, int dim, DevBuf& copy, TcSeedMap& map) {
+  map.valid = 0;
+  if (!tc_rank_wanted() || !seed_rank_tc_supported(dim) || count <= 0) return AEE_SUCCESS;
+  CK(copy.ensure(static_cast<size_t>(count) * dim * sizeof(float)));
+  launch_tf32_round(rows.as<float>(), copy.as<float>(), static_cast<size_t>(count) * dim, s.stream);
+  CK(cudaGetLastError());
+  ++g_launches;
+  if (!s.tc_err.p) {
+    CK(s.tc_err.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(s.tc_err.p, 0, sizeof(int), s.stream));
+  }
+  tc_seed_map_encode(&map, copy.as<float>(), count, dim);   // invalid map: the mma.sync ranking
+  return AEE_SUCCESS;
+}
+
+// Seed ranks of queries [q0, q1) into out: tensor cores when the rows have
+// a descriptor, else mma.sync.
+AEEResult seed_rank(State& s, const float* queries, int q0, int q1, int dim, const TcSeedMap& map,
+                    const DevBuf& rows, const DevBuf& norms, int n_seeds, float* out, int stride, cudaStream_t st) {
+  if (map.valid && launch_pq_seed_rank_tc(map, queries, q0, q1, dim, norms.as<float>(), n_seeds, out, stride,
+                                          s.tc_err.as<int>(), s.sms, st))
+    return AEE_SUCCESS;
+  launch_pq_seed_rank(queries, q0, q1, dim, rows.as<float>(), norms.as<float>(), n_seeds, out, st, stride);
+  CK(cudaGetLastError());
+  return AEE_SUCCESS;
+}
+
+// After a search: fails the call if the tensor-core ranking gave up waiting.
+AEEResult check_tc_err(State& s) {
+  if (!s.tc_err.p) return AEE_SUCCESS;
+  int e = 0;
+  CK(cudaMemcpy(&e, s.tc_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    CK(cudaMemset(s.tc_err.p, 0, sizeof(int)));
+    set_error("the tensor-core seed ranking gave up waiting on its pipeline; the search was not completed");
+    return AEE_EFAILED;
+  }
+  return AEE_SUCCESS;
+}
+
 AEEResult ensure_seed_recon(State& s, PqDevice& pq) {
   SeedSet& ss = pq.seeds;
   if (ss.recon_ready) return AEE_SUCCESS;
@@ -409,6 +469,7 @@ AEEResult ensure_seed_recon(State& s, PqDevice& pq) {
                        s.stream);
   CK(cudaGetLastError());
   ++g_launches;
+  if (make_tc_rows(s, ss.recon, ss.count, pq.view.dim, ss.recon_tc, ss.recon_map) != AEE_SUCCESS) return AEE_EFAILED;
   CK(cudaStreamSynchronize(s.stream));
   ss.recon_ready = true;
   return AEE_SUCCESS;
@@ -425,6 +486,7 @@ AEEResult ensure_seed_drows(State& s, PqDevice& pq) {
                         ss.drow_norms.as<float>(), s.stream);
   CK(cudaGetLastError());
   ++g_launches;
+  if (make_tc_rows(s, ss.drows, ss.count, pq.view.dim, ss.drows_tc, ss.drows_map) != AEE_SUCCESS) return AEE_EFAILED;
   std::vector<float> norms(ss.count);
   CK(cudaMemcpyAsync(norms.data(), ss.drow_norms.p, norms.size() * sizeof(float), cudaMemcpyDeviceToHost, s.stream));
   CK(cudaStreamSynchronize(s.stream));
@@ -516,9 +578,13 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
     for (int q0 = 0; q0 < nq; q0 += chunk) {
       const int q1 = std::min(nq, q0 + chunk);
       if (verify) {
-        TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
-        launch_pq_seed_rank(a.queries, q0, q1, pq.view.dim, ss.drows.as<float>(), ss.drow_norms.as<float>(),
-                            b.n_seeds, s.seed_dists.as<float>(), stream, b.seed_stride);
+        {
+          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
+          if (seed_rank(s, a.queries, q0, q1, pq.view.dim, ss.drows_map, ss.drows_tc.p ? ss.drows_tc : ss.drows,
+                        ss.drow_norms, b.n_seeds, s.seed_dists.as<float>(), b.seed_stride, stream) != AEE_SUCCESS)
+            return AEE_EFAILED;
+        }
+        TimedLaunch tl(ROVER_KERNEL_PQ_SEED_TOPM, stream);
         launch_pq_seed_topm(s.seed_dists.as<float>(), b.seed_stride, b.n_seeds, q1 - q0, b.top_m,
                             s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
         ++g_launches;
@@ -544,6 +610,7 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
     CK(cudaMemcpyAsync(s.h_status.data(), a.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     collect_timings();
+    if (check_tc_err(s) != AEE_SUCCESS) return AEE_EFAILED;
     bool retry = false;
     for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
     if (!retry) break;
@@ -731,7 +798,10 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
     b.top_m = seed_top_m(ss.count, a.max_pool);
   }
   const size_t row_floats = verify ? static_cast<size_t>(b.seed_stride) : static_cast<size_t>(ss.count);
-  const size_t per_query = row_floats * sizeof(float) * ((seed_pass || verify ? 1 : 0) + (rank_pass ? 1 : 0));
+  // quantized rank rows padded to a multiple of 4 floats (vector stores)
+  c.rank_stride = rank_pass ? (ss.count + 3) / 4 * 4 : 0;
+  const size_t per_query = row_floats * sizeof(float) * (seed_pass || verify ? 1 : 0) +
+                           static_cast<size_t>(c.rank_stride) * sizeof(float);
   const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(nq, kSeedDistBudget / per_query)));
   if (seed_pass || verify) CK(s.seed_dists.ensure(static_cast<size_t>(chunk) * row_floats * sizeof(float)));
   if (verify) {
@@ -741,7 +811,7 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
     b.seed_top_next = s.seed_top_next.as<float>();
   }
   if (rank_pass) {
-    CK(s.seed_rank.ensure(static_cast<size_t>(chunk) * ss.count * sizeof(float)));
+    CK(s.seed_rank.ensure(static_cast<size_t>(chunk) * c.rank_stride * sizeof(float)));
     b.top_m = seed_top_m(ss.count, a.max_pool);
     CK(s.seed_top.ensure(static_cast<size_t>(chunk) * b.top_m * sizeof(uint64_t)));
     CK(s.seed_top_next.ensure(static_cast<size_t>(chunk) * sizeof(float)));
@@ -778,8 +848,12 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
       if (verify) {
         {
           TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
-          launch_pq_seed_rank(a.queries, q0, q1, pq.view.dim, ss.drows.as<float>(), ss.drow_norms.as<float>(),
-                              b.n_seeds, s.seed_dists.as<float>(), stream, b.seed_stride);
+          if (seed_rank(s, a.queries, q0, q1, pq.view.dim, ss.drows_map, ss.drows_tc.p ? ss.drows_tc : ss.drows,
+                        ss.drow_norms, b.n_seeds, s.seed_dists.as<float>(), b.seed_stride, stream) != AEE_SUCCESS)
+            return AEE_EFAILED;
+        }
+        {
+          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_TOPM, stream);
           launch_pq_seed_topm(s.seed_dists.as<float>(), b.seed_stride, b.n_seeds, q1 - q0, b.top_m,
                               s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
         }
@@ -789,9 +863,14 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
       if (rank_pass) {
         {
           TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
-          launch_pq_seed_rank(a.queries, q0, q1, pq.view.dim, pq.seeds.recon.as<float>(),
-                              pq.seeds.recon_norms.as<float>(), b.n_seeds, s.seed_rank.as<float>(), stream);
-          launch_pq_seed_topm(s.seed_rank.as<float>(), b.n_seeds, b.n_seeds, q1 - q0, b.top_m,
+          if (seed_rank(s, a.queries, q0, q1, pq.view.dim, pq.seeds.recon_map,
+                        pq.seeds.recon_tc.p ? pq.seeds.recon_tc : pq.seeds.recon, pq.seeds.recon_norms, b.n_seeds,
+                        s.seed_rank.as<float>(), c.rank_stride, stream) != AEE_SUCCESS)
+            return AEE_EFAILED;
+        }
+        {
+          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_TOPM, stream);
+          launch_pq_seed_topm(s.seed_rank.as<float>(), c.rank_stride, b.n_seeds, q1 - q0, b.top_m,
                               s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
         }
         CK(cudaGetLastError());
@@ -812,6 +891,7 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
     CK(cudaMemcpyAsync(s.h_status.data(), a.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     collect_timings();
+    if (check_tc_err(s) != AEE_SUCCESS) return AEE_EFAILED;
     bool retry = false;
     for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
     if (!retry) break;
@@ -2197,6 +2277,37 @@ extern "C" AEEResult calculator_rover_gate_train(remote_handle64 h, const float*
   std::copy(mu, mu + kGateIn, mu_out);
   std::copy(sigma, sigma + kGateIn, sigma_out);
   return fail(AEE_SUCCESS);
+}
+
+extern "C" AEEResult calculator_rover_seed_rank(remote_handle64 h, const float* queries, int32_t nq,
+                                                const float* rows, int32_t n_rows, int32_t dim, float* out) {
+  (void)h;
+  if (!queries || !rows || !out || nq <= 0 || n_rows <= 0 || dim <= 0 || dim % 4 != 0 || dim > 1024)
+    return AEE_EBADPARM;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  struct Bufs {
+    DevBuf q, x, xtc, xn, o;
+    ~Bufs() { q.release(); x.release(); xtc.release(); xn.release(); o.release(); }
+  } b;
+  if (upload(b.q, queries, static_cast<size_t>(nq) * dim, s.stream) ||
+      upload(b.x, rows, static_cast<size_t>(n_rows) * dim, s.stream))
+    return AEE_ENOMEMORY;
+  CK(b.xn.ensure(static_cast<size_t>(n_rows) * sizeof(float)));
+  CK(b.o.ensure(static_cast<size_t>(nq) * n_rows * sizeof(float)));
+  launch_row_norms(b.x.as<float>(), n_rows, dim, b.xn.as<float>(), s.stream);
+  CK(cudaGetLastError());
+  ++g_launches;
+  TcSeedMap map{};
+  if (make_tc_rows(s, b.x, n_rows, dim, b.xtc, map) != AEE_SUCCESS) return AEE_EFAILED;
+  if (seed_rank(s, b.q.as<float>(), 0, nq, dim, map, b.xtc.p ? b.xtc : b.x, b.xn, n_rows, b.o.as<float>(), n_rows,
+                s.stream) != AEE_SUCCESS)
+    return AEE_EFAILED;
+  ++g_launches;
+  CK(cudaMemcpyAsync(out, b.o.p, static_cast<size_t>(nq) * n_rows * sizeof(float), cudaMemcpyDeviceToHost, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+  return check_tc_err(s);
 }
 
 extern "C" AEEResult calculator_rover_gate_rows(remote_handle64 h, uint64_t* rows) {

@@ -153,7 +153,8 @@ struct PqBatchArgs {
   GateTraceRow* trace;            // null = no trace
   unsigned long long* trace_count;
   int64_t trace_cap;
-  const float* seed_rank;         // [q_end - q_begin][n_seeds] quantized seed distances (gated, traces)
+  const float* seed_rank;         // [q_end - q_begin][rank_stride] quantized seed distances (gated, traces)
+  int32_t rank_stride;            // floats between seed_rank rows (0 = n_seeds)
   int32_t short_cap;              // gated seeds: ADC shortlist capacity
   int32_t smem_ids_offset, smem_short_offset, smem_feat_offset, smem_logit_offset;
 };
@@ -207,6 +208,20 @@ void launch_pq_seed_recon(const PqIndexView& ix, const int32_t* seed_ids, int n_
                           cudaStream_t s);
 // Quantized seed distances for ranking (TF32 tensor cores):
 // out[q - q_begin][u] = |q|^2 + |x~_u|^2 - 2 q . x~_u.  dim % 4 == 0.
+// The same ranks on tcgen05 tensor cores (seed_rank_tc.cu) for dim in
+// {32, 64, 96, 128}: the seed rows are a TF32-rounded copy named by a TMA
+// descriptor.  *err is set if a bounded wait inside the kernel ran out.
+struct alignas(64) TcSeedMap {
+  unsigned char bytes[128];   // CUtensorMap
+  int32_t valid;
+};
+bool seed_rank_tc_supported(int dim);
+bool tc_seed_map_encode(TcSeedMap* m, const float* rows_tf32, int n_seeds, int dim);
+void launch_tf32_round(const float* in, float* out, size_t n, cudaStream_t s);
+void launch_row_norms(const float* rows, int n, int dim, float* norms, cudaStream_t s);
+bool launch_pq_seed_rank_tc(const TcSeedMap& m, const float* queries, int q_begin, int q_end, int dim,
+                            const float* norms, int n_seeds, float* out, int out_stride, int* err, int sms,
+                            cudaStream_t s);
 void launch_pq_seed_rank(const float* queries, int q_begin, int q_end, int dim, const float* rows, const float* norms,
                          int n_seeds, float* out, cudaStream_t s, int out_stride = 0);   // 0: rows of n_seeds
 

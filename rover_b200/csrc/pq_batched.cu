@@ -293,7 +293,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
     // ---- ADC shortlist of the seeds (gated search, traces)
     if (adc_rows) {
       const int scap = min(c.short_cap, 2 * cap);
-      const float* arow = c.seed_rank + seed_row;
+      const float* arow = c.seed_rank + seed_row_index * (c.rank_stride ? c.rank_stride : b.n_seeds);
       const float next = b.seed_top ? b.seed_top_next[seed_row_index] : 0.0f;
       if (b.seed_top && next == next && scap <= b.top_m) {
         // the row's top ranks, selected by pq_seed_topm_kernel: (rank, seed index) -> (rank, id)
