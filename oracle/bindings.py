@@ -246,6 +246,29 @@ class _SqIndex(C.Structure):
                 ("residual_bits", C.c_int32), ("residual_code_bytes", C.c_int32), ("qparams", _f32p)]
 
 
+class _Error4(C.Structure):
+    _fields_ = [("qparams", _f32p), ("blocks", _u8p), ("code_bytes", C.c_int32),
+                ("vectors_per_block", C.c_int32)]
+
+
+class _SplitQuery(C.Structure):
+    _fields_ = [("q", C.c_uint8 * 1024), ("sum_q", C.c_uint64)]
+
+
+def read_error4(path, n: int, dim: int):
+    """The ERROR4 artifact's payload (256-byte header skipped): per-row
+    {scale, zero} and the 4096-byte code blocks."""
+    raw = np.fromfile(path, dtype=np.uint8)
+    qp = raw[256:256 + 8 * n].view(np.float32).reshape(n, 2).copy()
+    blocks = raw[256 + 8 * n:].copy()
+    return qp, blocks, (dim + 1) // 2, 4096 // ((dim + 1) // 2)
+
+
+def read_bias(path, n: int):
+    """The split-distance bias payload (64-byte header skipped)."""
+    return np.fromfile(path, dtype=np.uint8)[64:64 + 4 * n].view(np.float32).copy()
+
+
 class Port:
     """This project's C restatement of the path (oracle/rover_oracle.c)."""
 
@@ -272,6 +295,17 @@ class Port:
                                         C.c_int, _i32p, _f32p]
         L.oracle_refine.argtypes = [C.c_int, C.c_void_p, _f32p, _i32p, C.c_int, C.c_int, _i32p, _f32p]
         L.oracle_sq_rerank.argtypes = [C.POINTER(_SqIndex), _f32p, _i32p, _f32p, C.c_int, C.c_int, _i32p, _f32p]
+        L.oracle_refine_ex.argtypes = [C.c_int, C.c_void_p, C.POINTER(_Error4), _f32p, _i32p, C.c_int, C.c_int,
+                                       _i32p, _f32p]
+        L.oracle_split_query.argtypes = [C.POINTER(_SqIndex), _f32p, C.POINTER(_SplitQuery)]
+        for f in ("oracle_split_coarse",):
+            getattr(L, f).argtypes = [C.POINTER(_SqIndex), C.POINTER(_SplitQuery), C.c_int]
+            getattr(L, f).restype = C.c_float
+        for f in ("oracle_split_delta", "oracle_split_distance"):
+            getattr(L, f).argtypes = [C.POINTER(_SqIndex), _f32p, C.POINTER(_SplitQuery), C.c_int]
+            getattr(L, f).restype = C.c_float
+        L.oracle_sqmd_search_split.argtypes = [C.POINTER(_SqIndex), _f32p, _f32p, C.c_int, C.c_int, C.c_uint32,
+                                               C.c_int, C.c_int, _i32p, _f32p, C.c_int, _u64p]
 
     def pq_index(self, graph, bundle):
         """(struct, keepalive) for a rover_b200.bundle.PqBundle + graph."""
@@ -408,3 +442,53 @@ class Port:
         if c < 0:
             raise RuntimeError("oracle_refine failed")
         return out_ids[:c], out_d[:c]
+
+    def error4(self, path, n: int, dim: int):
+        """(struct, keepalive) of an ERROR4 artifact file."""
+        qp, blocks, cb, vpb = read_error4(path, n, dim)
+        return _Error4(_p(qp, _f32p), _p(blocks, _u8p), cb, vpb), (qp, blocks)
+
+    def refine_ex(self, kind, ix, e4, query, ids, top_k):
+        """Final refine; mode ERROR4 with e4 (from error4()), else CURRENT."""
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        out_ids = np.full(top_k, -1, dtype=np.int32)
+        out_d = np.zeros(top_k, dtype=np.float32)
+        c = self.lib.oracle_refine_ex(kind, C.cast(C.byref(ix[0]), C.c_void_p), C.byref(e4[0]) if e4 else None,
+                                      _p(q, _f32p), _p(ids, _i32p), len(ids), top_k, _p(out_ids, _i32p),
+                                      _p(out_d, _f32p))
+        if c < 0:
+            raise RuntimeError("oracle_refine_ex failed")
+        return out_ids[:c], out_d[:c]
+
+    def split_query(self, ix, query):
+        sq = _SplitQuery()
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        if self.lib.oracle_split_query(C.byref(ix[0]), _p(q, _f32p), C.byref(sq)) != 0:
+            raise RuntimeError("oracle_split_query failed")
+        return sq
+
+    def split_parts(self, ix, bias, query, ids):
+        """(coarse, delta, seed distance) of each id under the split distance."""
+        sq = self.split_query(ix, query)
+        b = np.ascontiguousarray(bias, dtype=np.float32)
+        out = np.array([(self.lib.oracle_split_coarse(C.byref(ix[0]), C.byref(sq), int(i)),
+                         self.lib.oracle_split_delta(C.byref(ix[0]), _p(b, _f32p), C.byref(sq), int(i)),
+                         self.lib.oracle_split_distance(C.byref(ix[0]), _p(b, _f32p), C.byref(sq), int(i)))
+                        for i in ids], dtype=np.float32)
+        return out
+
+    def sqmd_search_split(self, ix, bias, graph_entry, query, pool, entry_points, expand_count, seed=42,
+                          out_cap=None):
+        q = np.ascontiguousarray(query, dtype=np.float32)
+        b = np.ascontiguousarray(bias, dtype=np.float32)
+        cap = out_cap or pool
+        ids = np.full(cap, -1, dtype=np.int32)
+        d = np.zeros(cap, dtype=np.float32)
+        stats = np.zeros(4, dtype=np.uint64)
+        c = self.lib.oracle_sqmd_search_split(C.byref(ix[0]), _p(b, _f32p), _p(q, _f32p), entry_points,
+                                              graph_entry, seed, expand_count, pool, _p(ids, _i32p), _p(d, _f32p),
+                                              cap, _p(stats, _u64p))
+        if c < 0:
+            raise RuntimeError("oracle_sqmd_search_split failed")
+        return ids[:c], d[:c], stats

@@ -472,6 +472,77 @@ int oracle_sq_seed_ids(int n, int entry_points, int graph_entry, uint32_t seed, 
     return count;
 }
 
+/* SQ4 split distance ------------------------------------------------ */
+
+/* retrieval_quantize_query_l1_aligned_u8, retrieval_l1_int8_core.c:65-111:
+ * codes on the 4-bit L1 grid refined 17-fold, in double, lround, clamped. */
+int oracle_split_query(const OracleSqIndex *ix, const float *query, OracleSplitQuery *out) {
+    const double qs = (double)ix->l1_scale / 17.0;
+    if (!query || !out || ix->dim <= 0 || ix->dim > 1024 || !isfinite(ix->l1_scale) ||
+        !isfinite(ix->l1_zero) || ix->l1_scale <= 0.0f || !isfinite(qs) || qs <= 0.0)
+        return -1;
+    out->sum_q = 0;
+    for (int i = 0; i < ix->dim; i++) {
+        double raw = ((double)query[i] - (double)ix->l1_zero) / qs;
+        long code;
+        if (!isfinite(query[i]) || !isfinite(raw)) return -1;
+        code = lround(raw);
+        if (code < 0) code = 0;
+        else if (code > 255) code = 255;
+        out->q[i] = (uint8_t)code;
+        out->sum_q += (uint64_t)code;
+    }
+    return 0;
+}
+
+/* retrieval_compute_u8_u4_l1_distance_scalar (:171-191) */
+float oracle_split_coarse(const OracleSqIndex *ix, const OracleSplitQuery *sq, int id) {
+    const uint8_t *x = ix->l1 + (size_t)id * ix->l1_code_bytes;
+    const double qs = (double)ix->l1_scale / 17.0;
+    int64_t acc = 0;
+    if (ix->dim <= 0 || ix->dim > 33025 || !isfinite(ix->l1_scale) || ix->l1_scale <= 0.0f) return FLT_MAX;
+    for (int i = 0; i < ix->dim; i++) {
+        int32_t diff = (int32_t)sq->q[i] - 17 * (int32_t)code4(x, i);
+        acc += (int64_t)diff * (int64_t)diff;
+    }
+    return (float)((double)acc * qs * qs);
+}
+
+/* sqmd_split_residual_delta_fn (retrieval_rpc_demo_pipeline.c:935-976) over
+ * retrieval_compute_u8_u4 / u8_u8_residual_dot_scalar (:193-263):
+ * bias[id] - 2 <q, r> with the dot product expanded over the integer sums. */
+float oracle_split_delta(const OracleSqIndex *ix, const float *bias, const OracleSplitQuery *sq, int id) {
+    const uint8_t *r = ix->residual + (size_t)id * ix->residual_code_bytes;
+    const float rs = ix->qparams[2 * (size_t)id], rz = ix->qparams[2 * (size_t)id + 1];
+    const double qs = (double)ix->l1_scale / 17.0;
+    uint64_t sum_qv = 0, sum_v = 0;
+    double dot, delta;
+    if (!isfinite(ix->l1_scale) || !isfinite(ix->l1_zero) || !isfinite(rs) || !isfinite(rz) ||
+        ix->l1_scale <= 0.0f || rs < 0.0f)
+        return NAN;
+    for (int i = 0; i < ix->dim; i++) {
+        uint8_t v = ix->residual_bits == 4 ? (uint8_t)code4(r, i) : r[i];
+        sum_qv += (uint64_t)sq->q[i] * (uint64_t)v;
+        sum_v += (uint64_t)v;
+    }
+    dot = qs * (double)rs * (double)sum_qv + qs * (double)rz * (double)sq->sum_q +
+          (double)ix->l1_zero * (double)rs * (double)sum_v +
+          (double)ix->dim * (double)ix->l1_zero * (double)rz;
+    delta = (double)bias[id] - 2.0 * dot;
+    return isfinite(delta) ? (float)delta : NAN;
+}
+
+/* sqmd_split_distance_for_id (retrieval_rpc_demo_pipeline.c:978-995): the
+ * seeds' distance; FLT_MAX when either part is not finite. */
+float oracle_split_distance(const OracleSqIndex *ix, const float *bias, const OracleSplitQuery *sq, int id) {
+    float coarse = oracle_split_coarse(ix, sq, id);
+    float delta = oracle_split_delta(ix, bias, sq, id);
+    if (!isfinite(coarse) || !isfinite(delta)) return FLT_MAX;
+    coarse += delta;
+    if (coarse < 0.0f && coarse > -1.0e-4f) coarse = 0.0f;
+    return coarse;
+}
+
 /* Distance-only heaps with the reference's tie behaviour:
  * sqmd_heap_sift_up/down, sqmd_frontier_*, sqmd_candidate_insert,
  * sqmd_heap_sort (retrieval_sqmd_common.c:9-144); the DSP copies
@@ -562,15 +633,16 @@ static int sq_front_pop(Cand *f, int *size) {
  * seeds and seed distances from sqmd_make_seed (pipeline.c:1013-1055).
  * stats: {work_items, exact_corrected, turns, dedup_skips}.
  */
-int oracle_sqmd_search(const OracleSqIndex *ix, const float *query, int entry_points,
-                       int graph_entry, uint32_t seed, int expand_count, int pool_capacity,
-                       int correction, int32_t *out_ids, float *out_dists, int out_capacity,
-                       uint64_t *stats) {
+static int sqmd_search_core(const OracleSqIndex *ix, const float *bias, const float *query,
+                            int entry_points, int graph_entry, uint32_t seed, int expand_count,
+                            int pool_capacity, int correction, int32_t *out_ids, float *out_dists,
+                            int out_capacity, uint64_t *stats) {
     int n = ix->n, pool_size = 0, front_size = 0, result = -1, seed_count;
     size_t front_cap = (size_t)entry_points + (size_t)pool_capacity * (size_t)expand_count;
     int expand = expand_count < ix->degree ? expand_count : ix->degree;
     uint64_t work = 0, corrected = 0, turns = 0, dedup = 0;
     uint8_t qc[1024];
+    OracleSplitQuery split;
     Cand *pool = calloc((size_t)pool_capacity, sizeof(Cand));
     Cand *front = calloc(front_cap ? front_cap : 1, sizeof(Cand));
     uint32_t *visited = calloc(((size_t)n + 31) / 32, sizeof(uint32_t));
@@ -579,13 +651,17 @@ int oracle_sqmd_search(const OracleSqIndex *ix, const float *query, int entry_po
     if (!pool || !front || !visited || !seeds || ix->dim > 1024 || pool_capacity <= 0 ||
         entry_points <= 0 || expand_count <= 0 || oracle_sq_quantize(ix, query, qc) != 0)
         goto done;
+    /* sqmd_split_query_init (pipeline.c:916-933): 4-bit codes, residuals */
+    if (bias && (!correction || ix->l1_bits != 4 || !ix->residual || !ix->qparams ||
+                 oracle_split_query(ix, query, &split) != 0))
+        goto done;
     seed_count = oracle_sq_seed_ids(n, entry_points, graph_entry, seed, seeds, entry_points);
     if (seed_count <= 0) goto done;
     for (int i = 0; i < seed_count; i++) {
         int id = seeds[i];
         float d;
         if (correction) {
-            d = oracle_sq_exact(ix, query, id);
+            d = bias ? oracle_split_distance(ix, bias, &split, id) : oracle_sq_exact(ix, query, id);
             if (!isfinite(d) || d < 0.0f) goto done;
         } else {
             d = oracle_sq_coarse(ix, qc, id);
@@ -618,7 +694,17 @@ int oracle_sqmd_search(const OracleSqIndex *ix, const float *query, int entry_po
         for (int w = 0; w < nw; w++) visited[wl[w] >> 5] |= 1u << (wl[w] & 31);
         for (int w = 0; w < nw; w++) {
             float d = oracle_sq_coarse(ix, qc, wl[w]);
-            if (correction) d = oracle_sq_exact(ix, query, wl[w]);
+            if (bias) {
+                /* sqmd_source_job_commit (sqmd_common.c:1533-1556): the
+                 * lane's split coarse distance plus the host's delta */
+                float delta = oracle_split_delta(ix, bias, &split, wl[w]);
+                if (!isfinite(delta)) goto done;
+                d = oracle_split_coarse(ix, &split, wl[w]) + delta;
+                if (d < 0.0f && d > -1.0e-4f) d = 0.0f;
+                if (!isfinite(d) || d < 0.0f) goto done;
+            } else if (correction) {
+                d = oracle_sq_exact(ix, query, wl[w]);
+            }
             if (sq_pool_insert(pool, &pool_size, pool_capacity, wl[w], d) &&
                 (size_t)front_size < front_cap) {
                 front[front_size].id = wl[w]; front[front_size].dist = d;
@@ -634,6 +720,25 @@ int oracle_sqmd_search(const OracleSqIndex *ix, const float *query, int entry_po
 done:
     free(pool); free(front); free(visited); free(seeds);
     return result;
+}
+
+int oracle_sqmd_search(const OracleSqIndex *ix, const float *query, int entry_points,
+                       int graph_entry, uint32_t seed, int expand_count, int pool_capacity,
+                       int correction, int32_t *out_ids, float *out_dists, int out_capacity,
+                       uint64_t *stats) {
+    return sqmd_search_core(ix, NULL, query, entry_points, graph_entry, seed, expand_count, pool_capacity,
+                            correction, out_ids, out_dists, out_capacity, stats);
+}
+
+/* The SQMD session path with SQMD_SPLIT_DISTANCE on
+ * (sqmd_cpu_state_run_source_pipeline_split, sqmd_common.c:2028-2050). */
+int oracle_sqmd_search_split(const OracleSqIndex *ix, const float *bias, const float *query,
+                             int entry_points, int graph_entry, uint32_t seed, int expand_count,
+                             int pool_capacity, int32_t *out_ids, float *out_dists, int out_capacity,
+                             uint64_t *stats) {
+    if (!bias) return -1;
+    return sqmd_search_core(ix, bias, query, entry_points, graph_entry, seed, expand_count, pool_capacity,
+                            1, out_ids, out_dists, out_capacity, stats);
 }
 
 /*
@@ -744,8 +849,29 @@ static int refine_decode_sq(const OracleSqIndex *ix, int id, float *out) {
     return 0;
 }
 
+/* decode_vector's ERROR4 term (retrieval_final_refine.c:221-246): the
+ * storage row's int4 code, scale and zero added to the base decode, each
+ * product and sum rounded to float; the row is the graph id here (no
+ * storage map). */
+static int refine_add_error4(const OracleError4 *e4, int row, int dim, float *v) {
+    const uint8_t *codes = e4->blocks + (size_t)(row / e4->vectors_per_block) * 4096u +
+                           (size_t)(row % e4->vectors_per_block) * (size_t)e4->code_bytes;
+    float s = e4->qparams[2 * (size_t)row], z = e4->qparams[2 * (size_t)row + 1];
+    for (int d = 0; d < dim; d++) {
+        volatile float value = v[d] + refine_decode_value((unsigned)code4(codes, d), s, z);
+        if (!isfinite(value)) return -1;
+        v[d] = value;
+    }
+    return 0;
+}
+
 int oracle_refine(int kind, const void *index, const float *query, const int32_t *ids,
                   int count, int output_k, int32_t *out_ids, float *out_dists) {
+    return oracle_refine_ex(kind, index, NULL, query, ids, count, output_k, out_ids, out_dists);
+}
+
+int oracle_refine_ex(int kind, const void *index, const OracleError4 *e4, const float *query,
+                     const int32_t *ids, int count, int output_k, int32_t *out_ids, float *out_dists) {
     int dim = kind == 0 ? ((const OracleSqIndex *)index)->dim : ((const OraclePqIndex *)index)->dim;
     int n = kind == 0 ? ((const OracleSqIndex *)index)->n : ((const OraclePqIndex *)index)->n;
     RefineItem *items = malloc((size_t)(count > 0 ? count : 1) * sizeof(RefineItem));
@@ -763,6 +889,7 @@ int oracle_refine(int kind, const void *index, const float *query, const int32_t
         int drc = kind == 0 ? refine_decode_sq((const OracleSqIndex *)index, items[i].id, v)
                             : oracle_pq_decode((const OraclePqIndex *)index, items[i].id, v);
         if (drc != 0) goto done;
+        if (e4 && refine_add_error4(e4, items[i].id, dim, v) != 0) goto done;
         items[i].dist = 0;
         for (int d = 0; d < dim; d++) {
             double delta = (double)query[d] - (double)v[d];

@@ -73,6 +73,36 @@ int oracle_dsp_search(const OracleSqIndex *ix, const float *query, int entry_poi
 int oracle_refine(int kind, const void *index, const float *query, const int32_t *ids,
                   int count, int output_k, int32_t *out_ids, float *out_dists);
 
+/* Third-level ERROR4 artifact payload (PQERR4V1 / SQERR4V1 after the
+ * 256-byte header): per storage row {scale, zero}, then 4096-byte blocks of
+ * ceil(dim/2)-byte int4 codes, low nibble first. */
+typedef struct {
+    const float *qparams;        /* [n][2]                                 */
+    const uint8_t *blocks;       /* vectors_per_block rows per 4096 bytes  */
+    int32_t code_bytes, vectors_per_block;
+} OracleError4;
+
+/* final refine in mode ERROR4 when e4 != NULL (mode CURRENT otherwise) */
+int oracle_refine_ex(int kind, const void *index, const OracleError4 *e4, const float *query,
+                     const int32_t *ids, int count, int output_k, int32_t *out_ids, float *out_dists);
+
+/* SQ4 split distance: the L1-aligned u8 query, the u8-vs-4-bit L1 code
+ * distance, the residual delta bias[id] - 2 q.r and their sum. */
+typedef struct {
+    uint8_t q[1024];
+    uint64_t sum_q;
+} OracleSplitQuery;
+
+int oracle_split_query(const OracleSqIndex *ix, const float *query, OracleSplitQuery *out);
+float oracle_split_coarse(const OracleSqIndex *ix, const OracleSplitQuery *sq, int id);
+float oracle_split_delta(const OracleSqIndex *ix, const float *bias, const OracleSplitQuery *sq, int id);
+float oracle_split_distance(const OracleSqIndex *ix, const float *bias, const OracleSplitQuery *sq, int id);
+/* oracle_sqmd_search with split distances (correction on, 4-bit L1 codes) */
+int oracle_sqmd_search_split(const OracleSqIndex *ix, const float *bias, const float *query,
+                             int entry_points, int graph_entry, uint32_t seed, int expand_count,
+                             int pool_capacity, int32_t *out_ids, float *out_dists, int out_capacity,
+                             uint64_t *stats);
+
 /* batch helpers (threads over queries) */
 int oracle_pq_search_batch(const OraclePqIndex *ix, const float *queries, int nq,
                            const int32_t *pool_sizes, int entry_points, int graph_entry,

@@ -37,8 +37,23 @@ GOLDEN = Path(__file__).resolve().parent
 FIXTURES = ["pq8_d64", "pq4_d24", "sq8_d32", "sq4_d24"]
 
 
-def cases(data: dict) -> dict:
+def cases(data: dict, d: Path) -> dict:
     deg = int(data["graph_degree"])
+    # the final refine's mode 2 (ERROR4 term) and the SQ4 split distance,
+    # over the artifacts tests/golden/make_refine_artifacts.py wrote
+    error4 = ["--third-residual", "on", "--error4", str(d / "error4.refine")]
+    extra = {}
+    if (d / "error4.refine").exists():
+        extra["third_residual"] = ["--pool", "32", "--entry-points", "4", "--expand-count", str(min(16, deg)),
+                                   "--refine", "on"] + error4
+    if (d / "correction_bias.f32").exists():
+        split = ["--split-distance", "on", "--bias", str(d / "correction_bias.f32")]
+        extra["split_refine"] = ["--pool", "32", "--entry-points", "4", "--expand-count", str(min(16, deg)),
+                                 "--refine", "on"] + split
+        extra["split_first_stage"] = ["--pool", "40", "--entry-points", "8", "--expand-count", str(min(8, deg)),
+                                      "--refine", "off"] + split
+        extra["split_third_residual"] = ["--pool", "24", "--entry-points", "6", "--expand-count",
+                                         str(min(12, deg)), "--refine", "on"] + split + error4
     if data["method"] == "pq":
         return {
             "refine": ["--pool", "32", "--entry-points", "4", "--expand-count", str(min(16, deg)), "--refine", "on"],
@@ -46,6 +61,7 @@ def cases(data: dict) -> dict:
                             "--refine", "off"],
             "refine_all": ["--pool", "24", "--entry-points", "1", "--expand-count", str(deg), "--refine-all",
                            "--refine", "on", "--top-k", "5", "--seed", "7"],
+            **extra,
         }
     return {
         "refine": ["--pool", "32", "--entry-points", "4", "--expand-count", str(min(16, deg)), "--refine", "on"],
@@ -56,6 +72,7 @@ def cases(data: dict) -> dict:
                            "--expand-count", str(min(16, deg)), "--refine", "off"],
         "db_pair_refine": ["--search-mode", "db-pair", "--pool", "24", "--entry-points", "6",
                            "--expand-count", str(min(12, deg)), "--refine", "on"],
+        **extra,
     }
 
 
@@ -87,6 +104,7 @@ def main():
     ap.add_argument("--reference", default=os.environ.get("ROVER_REFERENCE"),
                     required="ROVER_REFERENCE" not in os.environ,
                     help="reference checkout (default: $ROVER_REFERENCE)")
+    ap.add_argument("--tags", nargs="*", help="record only these cases (the others stay as recorded)")
     args = ap.parse_args()
     bindings.build(args.reference)
     rover_ref = ROOT / "oracle" / "_ref" / "rover_ref"
@@ -99,9 +117,13 @@ def main():
         key = "search_on_ids" if data["method"] == "pq" else "sqmd_on_ids"
         gt = np.full((nq, 100), -1, np.int32)
         gt[:, :10] = g[key][:, :10]
-        B.write_ivecs(d / "cli_gt.ivecs", gt)
-        record = {}
-        for tag, extra in cases(data).items():
+        if not args.tags:
+            B.write_ivecs(d / "cli_gt.ivecs", gt)
+        cases_file = d / "cli_cases.json"
+        record = json.loads(cases_file.read_text()) if args.tags and cases_file.exists() else {}
+        for tag, extra in cases(data, d).items():
+            if args.tags and tag not in args.tags:
+                continue
             with tempfile.TemporaryDirectory() as tmp:
                 out, met = Path(tmp) / "results.jsonl", Path(tmp) / "metrics.csv"
                 full = base_args(d, data, nq, d / "cli_gt.ivecs") + extra + ["--output", str(out), "--metrics", str(met)]
