@@ -93,7 +93,14 @@ typedef struct RoverSearchParams {
     int32_t layout;          /* PQ with correction: ROVER_LAYOUT_* */
     int32_t beam_width;      /* BATCHED / GATED: entries expanded per step, 1..4 (0 = the
                                 largest with beam_width * expand_count <= 256) */
-    int32_t reserved[4];
+    int32_t third_residual;  /* PQ with refine_budget > 0: the final refine in mode ERROR4
+                                (retrieval_final_refine.c:118-166, :221-246), adding the
+                                artifact loaded by calculator_rover_error4_load to every
+                                decoded candidate */
+    int32_t split_distance;  /* SQ, sq_mode 1 with correction: the SQ4 split distance
+                                (SQMD_SPLIT_DISTANCE on, retrieval_rpc_demo_pipeline.c:909-995)
+                                with the bias loaded by calculator_rover_sq_split_load */
+    int32_t reserved[2];
 } RoverSearchParams;
 
 /* Per-call outputs.  Host pointers for calculator_rover_*_search, device
@@ -258,12 +265,33 @@ AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, const float *q
 AEEResult calculator_rover_pq_lut(remote_handle64 h, const float *queries, int32_t num_queries,
                                   float *out_luts, int32_t *out_status);
 
+/* The third-level ERROR4 artifact of the loaded index (kind 0 = the SQ index
+ * of calculator_rover_sq_load, 1 = the PQ index): the payload of a
+ * SQERR4V1 / PQERR4V1 file after its 256-byte header (retrieval_final_refine.c:
+ * 118-166 validates the header; the host does that before calling), i.e.
+ * qparams[num_vectors][2] {scale >= 0, zero}, then code_blocks: 4096-byte
+ * blocks of 4096 / ceil(dim/2) rows of ceil(dim/2) int4 codes, low nibble
+ * first.  Rows are graph ids (no storage map).  Unloading or replacing the
+ * index drops it. */
+AEEResult calculator_rover_error4_load(remote_handle64 h, int32_t kind, const float *qparams,
+                                       const uint8_t *code_blocks, int64_t code_blocks_bytes,
+                                       int32_t num_vectors, int32_t dim);
+AEEResult calculator_rover_error4_unload(remote_handle64 h, int32_t kind);
+
+/* The SQ4 split-distance bias of the loaded SQ index (the payload of a
+ * SQMDBIAS file after its 64-byte header, one finite float per vector;
+ * sqmd_load_correction_bias, retrieval_rpc_demo_support.c:237-297, holds the
+ * header checks).  Needs 4-bit L1 codes and residuals. */
+AEEResult calculator_rover_sq_split_load(remote_handle64 h, const float *bias, int32_t num_vectors);
+
 /* Final refine of host-supplied candidate lists (refine_impl,
  * retrieval_final_refine.c:256): kind 0 = SQ decode, 1 = PQ residual decode.
  * kind 2 = the legacy SQ re-rank demo_rerank_candidates
  * (retrieval_rpc_demo_support.c:1833): stable sort by id, exact residual
  * distance (retrieval_demo_exact_distance_residual, :1397; FLT_MAX for an id
  * outside the index), stable sort by distance, first top_k; no reorder map.
+ * kinds 3 / 4 = kinds 0 / 1 in mode ERROR4 (the index's loaded ERROR4
+ * artifact added to each decode, decode_vector :221-246).
  * At most 2048 candidates per query. */
 AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, const float *queries,
                                   int32_t num_queries, const int32_t *cand_ids, int32_t cand_stride,

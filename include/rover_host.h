@@ -80,6 +80,11 @@ typedef struct RoverBundle {
     uint8_t *sq_l1;
     uint8_t *sq_residual_rows;      /* unpacked [n][residual code bytes] */
     float *sq_qparams;
+    /* the member files the index came from: PQ codes, residual, qparams (or
+       SQ l1, residual, qparams), and the PQ codebook -- the digests the
+       correction artifacts below are bound to */
+    char base_paths[3][4096];
+    char pq_book_path[4096];
 } RoverBundle;
 
 /* A rover.index.v1 directory: validate index.json (schema, method, sizes,
@@ -99,6 +104,26 @@ int rover_bundle_open_sq(const char *graph_path, const char *graph_format, int32
 void rover_bundle_close(RoverBundle *b);
 
 const char *rover_host_error(void);
+
+/* ---- correction artifacts ---- */
+/* The final refine's third-level ERROR4 file (PQERR4V1 / SQERR4V1), checked
+ * as retrieval_final_refine.c:118-166 does against the bundle it refines
+ * (the base members' and the PQ codebook's SHA-256, the id maps: the order
+ * map graph -> original when one is used, else none) and loaded. */
+typedef struct RoverError4 {
+    int32_t num_vectors, dim;
+    float *qparams;                 /* [n][2] {scale >= 0, zero}            */
+    const uint8_t *blocks;          /* 4096-byte code blocks                */
+    int64_t blocks_bytes;
+    uint8_t *file;                  /* owns blocks                          */
+} RoverError4;
+int rover_error4_open(const RoverBundle *b, const char *path, const int32_t *graph_to_original, RoverError4 **out);
+void rover_error4_close(RoverError4 *e);
+/* The SQMD split-distance bias (SQMDBIAS, retrieval_rpc_demo_support.c:
+ * 237-297): *out is malloc'd [n] floats. */
+int rover_split_bias_open(const RoverBundle *b, const char *path, float **out);
+/* message of the last failed artifact call on this thread */
+const char *rover_artifact_error(void);
 
 #ifdef __cplusplus
 }

@@ -26,7 +26,7 @@ HOST_DIR = HERE / "host"
 HOST_LIB = LIB_DIR / "librover_host.so"
 BIN_DIR = HERE / "bin"
 ROVER = BIN_DIR / "Rover"
-HOST_SOURCES = ["sha256.c", "json.c", "bundle.c"]
+HOST_SOURCES = ["sha256.c", "json.c", "bundle.c", "artifacts.c"]
 
 SOURCES = ["calculator.cu", "pq_search.cu", "pq_decoded.cu", "pq_batched.cu", "gate_train.cu", "plan.cu", "sq_search.cu", "distance.cu", "sessions.cu", "seed_rank_tc.cu", "rpcmem_compat.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

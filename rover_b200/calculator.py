@@ -55,7 +55,8 @@ class SearchParams(C.Structure):
     _fields_ = [("size", C.c_int32), ("mode", C.c_int32), ("entry_points", C.c_int32), ("seed", C.c_uint32),
                 ("expand_count", C.c_int32), ("correction", C.c_int32), ("refine_budget", C.c_int32),
                 ("top_k", C.c_int32), ("pool_stride", C.c_int32), ("sq_mode", C.c_int32),
-                ("layout", C.c_int32), ("beam_width", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("layout", C.c_int32), ("beam_width", C.c_int32), ("third_residual", C.c_int32),
+                ("split_distance", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class GateThresholds(C.Structure):
@@ -165,6 +166,10 @@ class Calculator:
         L.calculator_rover_sq_unload.argtypes = [C.c_uint64]
         L.calculator_rover_sq_search.argtypes = [C.c_uint64, C.POINTER(SearchParams), _f32p, C.c_int32, _i32p,
                                                  C.POINTER(SearchOutputs)]
+        L.calculator_rover_error4_load.argtypes = [C.c_uint64, C.c_int32, _f32p, _u8p, C.c_int64, C.c_int32,
+                                                   C.c_int32]
+        L.calculator_rover_error4_unload.argtypes = [C.c_uint64, C.c_int32]
+        L.calculator_rover_sq_split_load.argtypes = [C.c_uint64, _f32p, C.c_int32]
         self.handle = C.c_uint64(0)
         self._check("calculator_open", L.calculator_open(b"file:///libcalculator_skel.so", C.byref(self.handle)))
         self._keep = {}
@@ -360,7 +365,8 @@ class Calculator:
 
     @staticmethod
     def params(entry_points=1, expand_count=32, correction=1, refine_budget=0, top_k=10, seed=42,
-               pool_stride=0, sq_mode=0, mode=0, layout=0, beam_width=0) -> SearchParams:
+               pool_stride=0, sq_mode=0, mode=0, layout=0, beam_width=0, third_residual=0,
+               split_distance=0) -> SearchParams:
         p = SearchParams()
         p.size = C.sizeof(SearchParams)
         p.mode = mode
@@ -374,6 +380,8 @@ class Calculator:
         p.sq_mode = sq_mode
         p.layout = layout
         p.beam_width = beam_width
+        p.third_residual = third_residual
+        p.split_distance = split_distance
         return p
 
     def pq_search(self, queries, pool_sizes, top_k=10, top_ks=None, pool_stride=0, stats=True, check=True,
@@ -479,6 +487,25 @@ class Calculator:
                                                      _p(od, _f32p), _p(oc, _i32p), _p(st, _i32p)))
         return oi, od, oc
 
+    def error4_load(self, kind: int, qparams, code_blocks) -> None:
+        """The ERROR4 artifact payload (qparams [n][2], 4096-byte code blocks)
+        of the loaded SQ (kind 0) or PQ (kind 1) index."""
+        qp = np.ascontiguousarray(qparams, dtype=np.float32)
+        blocks = np.ascontiguousarray(code_blocks, dtype=np.uint8).reshape(-1)
+        dim = self.pq_dim if kind == 1 else self._keep["sq_dim"]
+        self._check("calculator_rover_error4_load",
+                    self.lib.calculator_rover_error4_load(self.handle, kind, _p(qp, _f32p), _p(blocks, _u8p),
+                                                          blocks.size, qp.shape[0], dim))
+
+    def error4_unload(self, kind: int) -> None:
+        self._check("calculator_rover_error4_unload", self.lib.calculator_rover_error4_unload(self.handle, kind))
+
+    def sq_split_load(self, bias) -> None:
+        """The SQ4 split-distance bias of the loaded SQ index."""
+        b = np.ascontiguousarray(bias, dtype=np.float32)
+        self._check("calculator_rover_sq_split_load",
+                    self.lib.calculator_rover_sq_split_load(self.handle, _p(b, _f32p), b.size))
+
     # -- extension: SQ
     def sq_load(self, graph, graph_entry: int, b) -> None:
         g = None if graph is None else np.ascontiguousarray(graph, dtype=np.int32)
@@ -490,6 +517,7 @@ class Calculator:
                            _p(l1, _u8p), b.l1_bits, b.l1_scale, b.l1_zero, _p(res, _u8p), b.residual_bits,
                            _p(qp, _f32p))
         self._check("calculator_rover_sq_load", self.lib.calculator_rover_sq_load(self.handle, C.byref(desc)))
+        self._keep["sq_dim"] = b.dim
 
     def sq_unload(self) -> None:
         self._check("calculator_rover_sq_unload", self.lib.calculator_rover_sq_unload(self.handle))

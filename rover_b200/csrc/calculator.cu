@@ -101,6 +101,7 @@ struct SeedSet {
 
 struct PqDevice {
   DevBuf graph, codes, codebook, residual, qparams;
+  DevBuf e4_qparams, e4_blocks;   // ERROR4 artifact (calculator_rover_error4_load)
   DevBuf decoded;                 // [n][dim] FP32 reconstructions, built on first use
   bool decoded_ready = false;
   SeedSet seeds;
@@ -111,7 +112,8 @@ struct PqDevice {
   uint64_t epoch = 0;             // bumped whenever the device copy is released (plans check it)
   void release() {
     graph.release(); codes.release(); codebook.release(); residual.release(); qparams.release();
-    decoded.release(); seeds.release();
+    decoded.release(); seeds.release(); e4_qparams.release(); e4_blocks.release();
+    view.e4 = Error4View{};
     decoded_ready = false;
     loaded = false;
     has_graph = false;
@@ -121,11 +123,16 @@ struct PqDevice {
 
 struct SqDevice {
   DevBuf graph, l1, residual, qparams;
+  DevBuf e4_qparams, e4_blocks;   // ERROR4 artifact (calculator_rover_error4_load)
+  DevBuf split_bias;              // SQ4 split-distance bias (calculator_rover_sq_split_load)
   SqIndexView view{};
   int32_t graph_entry = -1;
   bool loaded = false;
   void release() {
     graph.release(); l1.release(); residual.release(); qparams.release();
+    e4_qparams.release(); e4_blocks.release(); split_bias.release();
+    view.e4 = Error4View{};
+    view.split_bias = nullptr;
     loaded = false;
   }
 };
@@ -640,6 +647,10 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
   if (max_pool <= 0 || max_pool > 4096) { set_error("pool sizes must be in 1..4096"); return AEE_EBADPARM; }
   if (p->correction && pq.view.residual_bits == 0) { set_error("correction needs residuals"); return AEE_EBADPARM; }
   if (p->refine_budget > 0 && pq.view.residual_bits == 0) { set_error("refine needs residuals"); return AEE_EBADPARM; }
+  if (p->third_residual && (!pq.view.e4.qparams || p->refine_budget <= 0)) {
+    set_error("third_residual needs a loaded ERROR4 artifact and a refine budget");
+    return AEE_EBADPARM;
+  }
   const int expand = std::min(p->expand_count, pq.view.degree);
   if (expand > kMaxBatch) { set_error("expand_count above %d", kMaxBatch); return AEE_EBADPARM; }
 
@@ -656,6 +667,7 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
   a.expand_count = p->expand_count;
   a.correction = p->correction;
   a.refine_budget = p->refine_budget;
+  a.third_residual = p->third_residual;
   a.max_pool = max_pool;
   a.pool_ids = d_out.pool_ids;
   a.pool_dists = d_out.pool_dists;
@@ -940,6 +952,7 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
   a.seed = p->seed;
   a.expand_count = p->expand_count;
   a.correction = p->correction;
+  a.split = p->split_distance;
   a.num_out = num_out;
   a.max_pool = max_pool;
   a.frontier_cap = fcap;
@@ -951,8 +964,9 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
   a.status = d_status;
   const size_t per_warp = ((sq.view.dim * 4 + 15) & ~15) + ((sq.view.dim + 15) & ~15) + 64 * 8;
   const size_t smem = per_warp * kSearchWarps;
-  if (allow_smem(reinterpret_cast<const void*>(sq_search_kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
-  int blocks = std::max(1, std::min(resident_blocks(reinterpret_cast<const void*>(sq_search_kernel), kSearchWarps * 32, smem, s.sms),
+  const SqSearchFn sq_kernel = sq_search_kernel_for(a.split != 0);
+  if (allow_smem(reinterpret_cast<const void*>(sq_kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
+  int blocks = std::max(1, std::min(resident_blocks(reinterpret_cast<const void*>(sq_kernel), kSearchWarps * 32, smem, s.sms),
                                     (nq + kSearchWarps - 1) / kSearchWarps));
   const int max_blocks = blocks;
   size_t slots = 0;
@@ -982,7 +996,7 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
     CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
     {
       TimedLaunch tl(ROVER_KERNEL_SQ, stream);
-      sq_search_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
+      sq_kernel<<<blocks, kSearchWarps * 32, smem, stream>>>(a);
     }
     CK(cudaGetLastError());
     ++g_launches;
@@ -1394,6 +1408,7 @@ PqSearchArgs plan_args(const State& s, const PqPlanImpl& P, const float* queries
   a.expand_count = P.p.expand_count;
   a.correction = P.p.correction;
   a.refine_budget = P.p.refine_budget;
+  a.third_residual = P.p.third_residual;
   a.max_pool = P.max_pool;
   a.pool_ids = o.pool_ids;
   a.pool_dists = o.pool_dists;
@@ -1732,6 +1747,10 @@ AEEResult plan_setup(State& s, PqPlanImpl& P, const RoverSearchParams* p, int32_
   }
   if (p->correction && pq.view.residual_bits == 0) { set_error("correction needs residuals"); return AEE_EBADPARM; }
   if (p->refine_budget > 0 && pq.view.residual_bits == 0) { set_error("refine needs residuals"); return AEE_EBADPARM; }
+  if (p->third_residual && (!pq.view.e4.qparams || p->refine_budget <= 0)) {
+    set_error("third_residual needs a loaded ERROR4 artifact and a refine budget");
+    return AEE_EBADPARM;
+  }
   P.expand = std::min(p->expand_count, pq.view.degree);
   if (P.expand > kMaxBatch) { set_error("expand_count above %d", kMaxBatch); return AEE_EBADPARM; }
   P.decodable = p->correction != 0 && pq.view.dim % 4 == 0;
@@ -2500,8 +2519,15 @@ extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, co
   State& s = st();
   std::lock_guard<std::mutex> lock(s.mu);
   if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
-  if (nq <= 0 || !queries || !cand_ids || !cand_counts || top_k <= 0 || cand_stride <= 0 || kind < 0 || kind > 2)
+  if (nq <= 0 || !queries || !cand_ids || !cand_counts || top_k <= 0 || cand_stride <= 0 || kind < 0 || kind > 4)
     return AEE_EBADPARM;
+  // kinds 3 / 4: kinds 0 / 1 in mode ERROR4 (the index's third-level term)
+  const bool error4 = kind >= 3;
+  if (error4) {
+    kind -= 3;
+    const Error4View& e = kind == 1 ? s.pq.view.e4 : s.sq.view.e4;
+    if (!e.qparams) { set_error("no ERROR4 artifact is loaded for this index"); return AEE_EFAILED; }
+  }
   if (kind == 1 && (!s.pq.loaded || !s.pq.view.residual_bits)) { set_error("no PQ residual index"); return AEE_EFAILED; }
   if (kind == 0 && (!s.sq.loaded || !s.sq.view.residual)) { set_error("no SQ residual index"); return AEE_EFAILED; }
   if (kind == 2 && !s.sq.loaded) { set_error("no SQ index loaded"); return AEE_EFAILED; }
@@ -2536,7 +2562,7 @@ extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, co
     TimedLaunch tl(ROVER_KERNEL_REFINE, s.stream);
     launch_refine(kind, s.pq.view, s.sq.view, decoded, s.in_queries.as<float>(), nq, s.in_ids.as<int32_t>(), cand_stride,
                   s.in_pool.as<int32_t>(), top_k, cap, s.out_ids.as<int32_t>(), s.out_dists.as<float>(),
-                  s.out_counts.as<int32_t>(), s.status.as<int32_t>(), s.stream);
+                  s.out_counts.as<int32_t>(), s.status.as<int32_t>(), s.stream, error4);
   }
   CK(cudaGetLastError());
   ++g_launches;
@@ -2569,6 +2595,86 @@ extern "C" AEEResult calculator_rover_sq_unload(remote_handle64 h) {
   return AEE_SUCCESS;
 }
 
+// The ERROR4 payload of retrieval_final_refine's mode 2 (the host validated
+// the artifact's header, retrieval_final_refine.c:118-166; the qparams
+// checks of :160-163 are repeated here).
+extern "C" AEEResult calculator_rover_error4_load(remote_handle64 h, int32_t kind, const float* qparams,
+                                                  const uint8_t* code_blocks, int64_t code_blocks_bytes,
+                                                  int32_t num_vectors, int32_t dim) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if ((kind != 0 && kind != 1) || !qparams || !code_blocks || num_vectors <= 0 || dim <= 0 || dim > 8192)
+    return AEE_EBADPARM;
+  const bool pq = kind == 1;
+  if (pq ? !s.pq.loaded : !s.sq.loaded) { set_error("no index of this kind is loaded"); return AEE_EFAILED; }
+  if (pq ? session_busy(s, kSessionPurePq) : session_busy(s, kSessionSqmd)) return AEE_EFAILED;
+  const int32_t n = pq ? s.pq.view.n : s.sq.view.n;
+  const int32_t idim = pq ? s.pq.view.dim : s.sq.view.dim;
+  const int cb = (dim + 1) / 2, vpb = 4096 / cb;
+  if (num_vectors != n || dim != idim || vpb <= 0 ||
+      code_blocks_bytes != static_cast<int64_t>((num_vectors + vpb - 1) / vpb) * 4096) {
+    set_error("ERROR4 artifact does not match the loaded index");
+    return AEE_EBADPARM;
+  }
+  for (int64_t i = 0; i < num_vectors; ++i)
+    if (!std::isfinite(qparams[2 * i]) || qparams[2 * i] < 0.0f || !std::isfinite(qparams[2 * i + 1])) {
+      set_error("ERROR4 qparams of row %lld are invalid", static_cast<long long>(i));
+      return AEE_EBADPARM;
+    }
+  DevBuf& q = pq ? s.pq.e4_qparams : s.sq.e4_qparams;
+  DevBuf& b = pq ? s.pq.e4_blocks : s.sq.e4_blocks;
+  if (upload(q, qparams, static_cast<size_t>(num_vectors) * 2, s.stream) != AEE_SUCCESS ||
+      upload(b, code_blocks, static_cast<size_t>(code_blocks_bytes), s.stream) != AEE_SUCCESS)
+    return AEE_ENOMEMORY;
+  CK(cudaStreamSynchronize(s.stream));
+  Error4View& e = pq ? s.pq.view.e4 : s.sq.view.e4;
+  e.qparams = q.as<float>();
+  e.blocks = b.as<uint8_t>();
+  e.code_bytes = cb;
+  e.vpb = vpb;
+  return AEE_SUCCESS;
+}
+
+extern "C" AEEResult calculator_rover_error4_unload(remote_handle64 h, int32_t kind) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (kind != 0 && kind != 1) return AEE_EBADPARM;
+  if (kind == 1) {
+    s.pq.e4_qparams.release(); s.pq.e4_blocks.release(); s.pq.view.e4 = Error4View{};
+  } else {
+    s.sq.e4_qparams.release(); s.sq.e4_blocks.release(); s.sq.view.e4 = Error4View{};
+  }
+  return AEE_SUCCESS;
+}
+
+// The SQMD split-distance bias (sqmd_load_correction_bias,
+// retrieval_rpc_demo_support.c:237-297; the host checked the header and the
+// payload hash).  Split distance needs 4-bit L1 codes and residuals
+// (sqmd_split_query_init, retrieval_rpc_demo_pipeline.c:916-933).
+extern "C" AEEResult calculator_rover_sq_split_load(remote_handle64 h, const float* bias, int32_t num_vectors) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!bias || num_vectors <= 0) return AEE_EBADPARM;
+  SqDevice& d = s.sq;
+  if (!d.loaded || num_vectors != d.view.n) { set_error("the bias does not match the loaded SQ index"); return AEE_EBADPARM; }
+  if (d.view.l1_bits != 4 || !d.view.residual || !d.view.qparams || !std::isfinite(d.view.l1_scale) ||
+      !(d.view.l1_scale > 0.0f) || !std::isfinite(d.view.l1_zero)) {
+    set_error("split distance needs 4-bit L1 codes, residuals and a valid L1 scale");
+    return AEE_EBADPARM;
+  }
+  for (int32_t i = 0; i < num_vectors; ++i)
+    if (!std::isfinite(bias[i])) { set_error("bias of row %d is not finite", i); return AEE_EBADPARM; }
+  if (upload(d.split_bias, bias, static_cast<size_t>(num_vectors), s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  CK(cudaStreamSynchronize(s.stream));
+  d.view.split_bias = d.split_bias.as<float>();
+  return AEE_SUCCESS;
+}
+
 extern "C" AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSearchParams* p, const float* queries,
                                                 int32_t nq, const int32_t* pool_sizes, const RoverSearchOutputs* out) {
   (void)h;
@@ -2583,6 +2689,10 @@ extern "C" AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSe
   if (p->sq_mode < 0 || p->sq_mode > 2) { set_error("sq_mode must be 0, 1 or 2"); return AEE_EBADPARM; }
   if (p->sq_mode != 0 && p->correction && !s.sq.view.residual) {
     set_error("correction needs residuals");
+    return AEE_EBADPARM;
+  }
+  if (p->split_distance && (p->sq_mode != 1 || !p->correction || !s.sq.view.split_bias)) {
+    set_error("split_distance needs sq_mode 1, correction and a loaded split bias");
     return AEE_EBADPARM;
   }
   const int dim = s.sq.view.dim;
@@ -2990,8 +3100,9 @@ extern "C" AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const
     return AEE_EBADPARM;
   }
   // this entry runs the exact search over packed residual rows only
-  if (p->mode != ROVER_MODE_EXACT || p->layout == ROVER_LAYOUT_DECODED) {
-    set_error("the no-alloc search runs mode ROVER_MODE_EXACT with the packed (or auto) layout only");
+  if (p->mode != ROVER_MODE_EXACT || p->layout == ROVER_LAYOUT_DECODED || p->third_residual) {
+    set_error("the no-alloc search runs mode ROVER_MODE_EXACT with the packed (or auto) layout and the "
+              "mode-1 final refine only");
     return AEE_EBADPARM;
   }
   if (nq == 0) return AEE_SUCCESS;
@@ -3004,6 +3115,10 @@ extern "C" AEEResult calculator_rover_pq_search_noalloc(remote_handle64 h, const
   if (max_pool <= 0 || max_pool > 4096) { set_error("max_pool must be in 1..4096"); return AEE_EBADPARM; }
   if (p->correction && pq.view.residual_bits == 0) { set_error("correction needs residuals"); return AEE_EBADPARM; }
   if (p->refine_budget > 0 && pq.view.residual_bits == 0) { set_error("refine needs residuals"); return AEE_EBADPARM; }
+  if (p->third_residual && (!pq.view.e4.qparams || p->refine_budget <= 0)) {
+    set_error("third_residual needs a loaded ERROR4 artifact and a refine budget");
+    return AEE_EBADPARM;
+  }
   const int expand = std::min(p->expand_count, pq.view.degree);
   if (expand > kMaxBatch) { set_error("expand_count above %d", kMaxBatch); return AEE_EBADPARM; }
   int dev = 0;

@@ -24,6 +24,16 @@ enum QueryStatus : int32_t {
   kStatusFrontierFull = 5,  // SQ frontier exceeded the reference's bound
 };
 
+// The final refine's third-level ERROR4 term (retrieval_final_refine.c:
+// 118-166, :221-246): per storage row an int4 code per dimension, packed
+// low nibble first into ceil(dim/2) bytes, vpb rows per 4096-byte block, and
+// a {scale, zero} pair.  qparams == nullptr when no artifact is loaded.
+struct Error4View {
+  const float* qparams;     // [n][2]
+  const uint8_t* blocks;
+  int32_t code_bytes, vpb;
+};
+
 struct PqIndexView {
   const int32_t* graph;     // [n][degree]
   int32_t n, degree, dim;
@@ -34,6 +44,7 @@ struct PqIndexView {
   int32_t residual_bits, rcb, vpb;
   const float* qparams;     // [n][2] {scale, zero}
   float codebook_absmax;    // max |codebook entry| (bounds every LUT entry)
+  Error4View e4;            // ERROR4 artifact of this index (optional)
 };
 
 struct SqIndexView {
@@ -45,6 +56,8 @@ struct SqIndexView {
   const uint8_t* residual;  // [n][rcb] flat rows (may be null)
   int32_t residual_bits, rcb;
   const float* qparams;     // [n][2]
+  Error4View e4;            // ERROR4 artifact of this index (optional)
+  const float* split_bias;  // [n] SQ4 split-distance bias (optional)
 };
 
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
@@ -56,10 +69,23 @@ __device__ __forceinline__ int nibble(const uint8_t* p, int i) {
   return (i & 1) ? (b >> 4) : (b & 15);
 }
 
+// decode_vector's ERROR4 step for dimension d of one row: x + (code * scale
+// + zero), each product and sum rounded to float (decode_value, add_f32).
+__device__ __forceinline__ float error4_add(float x, const uint8_t* codes, float2 qp, int d);
+
 // Exact small-integer to float: byte b -> float(b) by placing b in the
 // mantissa of 2^23 and subtracting 2^23 (exact for b < 2^23).
 __device__ __forceinline__ float u8f(uint32_t b) {
   return __fsub_rn(__uint_as_float(0x4B000000u | b), 8388608.0f);
+}
+
+__device__ __forceinline__ float error4_add(float x, const uint8_t* codes, float2 qp, int d) {
+  return fadd(x, fadd(fmul(u8f(static_cast<uint32_t>(nibble(codes, d))), qp.x), qp.y));
+}
+
+// The ERROR4 codes of storage row `row`.
+__device__ __forceinline__ const uint8_t* error4_row(const Error4View& e, int32_t row) {
+  return e.blocks + static_cast<size_t>(row / e.vpb) * 4096u + static_cast<size_t>(row % e.vpb) * e.code_bytes;
 }
 
 // Candidate keys: (distance bits << 32) | id.  Distances are squared norms

@@ -13,6 +13,7 @@
 // Each query's id list is offsets[q] .. offsets[q+1] of a flat id array.
 
 #include "pq_common.cuh"
+#include "sq_split.cuh"
 
 namespace rover {
 
@@ -290,6 +291,28 @@ __global__ void sq_coarse_kernel(SqIndexView ix, const float* __restrict__ queri
   if (bad) status[qi] = kStatusBadParam;
 }
 
+// The lane side of the split distance (sqmd_dsp_distance_fn with the
+// ALIGNED_U8 query contract, retrieval_async_dsp_search.c:993-1016): the
+// u8-vs-4-bit L1 distance of each id against the host's aligned query.
+__global__ void sq_aligned_coarse_kernel(SqIndexView ix, const uint8_t* __restrict__ queries_u8, int nq,
+                                         const int32_t* __restrict__ ids, const int64_t* __restrict__ offsets,
+                                         float* __restrict__ out, int32_t* status) {
+  extern __shared__ __align__(16) uint8_t qu[];
+  const int qi = blockIdx.y;
+  for (int d = threadIdx.x; d < ix.dim; d += blockDim.x) qu[d] = queries_u8[static_cast<size_t>(qi) * ix.dim + d];
+  __syncthreads();
+  const double step = split_step(ix.l1_scale);
+  const int64_t begin = offsets[qi], end = offsets[qi + 1];
+  bool bad = false;
+  for (int64_t i = begin + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < end;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t id = __ldg(ids + i);
+    if (id < 0 || id >= ix.n) { bad = true; continue; }
+    out[i] = split_coarse(ix, qu, id, step);
+  }
+  if (bad) status[qi] = kStatusBadParam;
+}
+
 // retrieval_demo_exact_distance_residual_scalar (support.c:1397) of one
 // vector: x = (l1*s + z) + (r*rs + rz) per dimension, sequential FP32 sum.
 __device__ __forceinline__ float sq_exact_one(const SqIndexView& ix, const float* q, int32_t id) {
@@ -392,11 +415,13 @@ __device__ __forceinline__ bool refine_value(int kind, const PqIndexView& pq, co
 
 // One warp per query: FP64 distances of the candidates on their decoded
 // vectors, sorted by (distance, id), top k kept.
-__global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const float* __restrict__ decoded,
-                              const float* __restrict__ queries,
+__global__ void refine_kernel(int kind, bool error4, PqIndexView pq, SqIndexView sq,
+                              const float* __restrict__ decoded, const float* __restrict__ queries,
                               int nq, const int32_t* __restrict__ cand_ids, int cand_stride,
                               const int32_t* __restrict__ cand_counts, int top_k, int capacity,
                               int32_t* out_ids, float* out_dists, int32_t* out_counts, int32_t* status) {
+  // mode ERROR4: the index's third-level term on top of every decode
+  const Error4View& e4 = kind == 1 ? pq.e4 : sq.e4;
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int qi = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -435,11 +460,14 @@ __global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const fl
       if (i < count) {
         double dist = 0.0;
         const float4* x4 = reinterpret_cast<const float4*>(tile + lane * rs);
+        const uint8_t* e4c = error4 ? error4_row(e4, id) : nullptr;
+        const float2 e4q = e4c ? __ldg(reinterpret_cast<const float2*>(e4.qparams) + id) : make_float2(0.f, 0.f);
         for (int t = 0; t < dim / 4; ++t) {
           const float4 x = x4[t];
-          const float xv[4] = {x.x, x.y, x.z, x.w};
+          float xv[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
+            if (e4c) xv[u] = error4_add(xv[u], e4c, e4q, 4 * t + u);
             if (!isfinite(xv[u])) bad = true;
             const double delta = __dsub_rn(static_cast<double>(q[4 * t + u]), static_cast<double>(xv[u]));
             dist = __dadd_rn(dist, __dmul_rn(delta, delta));
@@ -475,9 +503,15 @@ __global__ void refine_kernel(int kind, PqIndexView pq, SqIndexView sq, const fl
               !isfinite(qp.x) || qp.x < 0.0f || !isfinite(qp.y)) bad = true;
         }
         double dist = 0.0;
+        const uint8_t* e4c = error4 ? error4_row(e4, id) : nullptr;
+        const float2 e4q = e4c ? __ldg(reinterpret_cast<const float2*>(e4.qparams) + id) : make_float2(0.f, 0.f);
         for (int d = 0; d < dim; ++d) {
           float x;
           if (!refine_value(kind, pq, sq, id, d, a, b, qp, &x)) bad = true;
+          if (e4c) {
+            x = error4_add(x, e4c, e4q, d);
+            if (!isfinite(x)) bad = true;
+          }
           const double delta = __dsub_rn(static_cast<double>(q[d]), static_cast<double>(x));
           dist = __dadd_rn(dist, __dmul_rn(delta, delta));
         }
@@ -780,6 +814,13 @@ void launch_sq_coarse(const SqIndexView& ix, const float* queries, int nq, const
   sq_coarse_kernel<<<grid, 128, (ix.dim + 15) & ~15, s>>>(ix, queries, nq, ids, offsets, out, status);
 }
 
+void launch_sq_aligned_coarse(const SqIndexView& ix, const uint8_t* queries_u8, int nq, const int32_t* ids,
+                              const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
+  if (nq <= 0 || ix.l1_bits != 4) return;
+  dim3 grid(8, nq);
+  sq_aligned_coarse_kernel<<<grid, 128, (ix.dim + 15) & ~15, s>>>(ix, queries_u8, nq, ids, offsets, out, status);
+}
+
 void launch_sq_exact(const SqIndexView& ix, const float* queries, int nq, const int32_t* ids,
                      const int64_t* offsets, float* out, int32_t* status, cudaStream_t s) {
   if (nq <= 0) return;
@@ -811,7 +852,7 @@ void launch_rerank(const SqIndexView& ix, const float* queries, int nq, const in
 void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const float* decoded, const float* queries,
                    int nq, const int32_t* cand_ids, int cand_stride, const int32_t* cand_counts,
                    int top_k, int capacity, int32_t* out_ids, float* out_dists,
-                   int32_t* out_counts, int32_t* status, cudaStream_t s) {
+                   int32_t* out_counts, int32_t* status, cudaStream_t s, bool error4) {
   if (nq <= 0) return;
   int cap = 1;
   while (cap < capacity) cap <<= 1;
@@ -824,7 +865,7 @@ void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const
     smem = static_cast<size_t>(warps) * cap * 12;
   }
   if (smem > 48 * 1024) cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  refine_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, s>>>(kind, pq, sq, decoded, queries, nq, cand_ids,
+  refine_kernel<<<(nq + warps - 1) / warps, warps * 32, smem, s>>>(kind, error4, pq, sq, decoded, queries, nq, cand_ids,
                                                                    cand_stride,
                                                                    cand_counts, top_k, cap, out_ids, out_dists,
                                                                    out_counts, status);

@@ -25,6 +25,7 @@ struct PqSearchArgs {
   int32_t expand_count;
   int32_t correction;
   int32_t refine_budget;         // 0 = no final refine
+  int32_t third_residual;        // final refine in mode ERROR4 (ix.e4 loaded)
   int32_t max_pool;              // list capacity per warp (>= every pool size)
   // outputs (device)
   int32_t* pool_ids; float* pool_dists; int32_t pool_stride; int32_t* pool_counts;
@@ -274,6 +275,7 @@ struct SqSearchArgs {
   uint32_t seed;
   int32_t expand_count;
   int32_t correction;            // SQMD only
+  int32_t split;                 // SQMD with the SQ4 split distance (ix.split_bias)
   int32_t num_out;               // DSP mode: outputs per query
   int32_t max_pool;              // pool heap capacity per slot
   int32_t frontier_cap;          // frontier heap capacity per slot
@@ -285,7 +287,10 @@ struct SqSearchArgs {
   unsigned int* next_query;
 };
 
-__global__ void sq_search_kernel(SqSearchArgs a);
+using SqSearchFn = void (*)(SqSearchArgs);
+// The SQ search kernel (a __global__ function): with the split distance
+// compiled in or out, so the plain searches keep their register budget.
+SqSearchFn sq_search_kernel_for(bool split);
 
 // ---- DB-pair search driven step by step by the host (calculator_retrieval_search_db)
 //
@@ -347,9 +352,14 @@ void launch_rerank(const SqIndexView& ix, const float* queries, int nq, const in
                    const int32_t* cand_counts, int top_k, int capacity, int32_t* out_ids, float* out_dists,
                    int32_t* out_counts, int32_t* status, cudaStream_t s);
 // decoded: the PQ index's decoded rows (kind 1, dim % 4 == 0) or null.
+// error4: mode ERROR4, the index view's e4 term added to every decode.
 void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const float* decoded, const float* queries,
                    int nq, const int32_t* cand_ids, int cand_stride, const int32_t* cand_counts,
                    int top_k, int capacity, int32_t* out_ids, float* out_dists,
-                   int32_t* out_counts, int32_t* status, cudaStream_t s);
+                   int32_t* out_counts, int32_t* status, cudaStream_t s, bool error4 = false);
+// The split distance's lane part (retrieval_compute_u8_u4_l1_distance) of
+// ids[offsets[q]..offsets[q+1]) against the aligned u8 queries [nq][dim].
+void launch_sq_aligned_coarse(const SqIndexView& ix, const uint8_t* queries_u8, int nq, const int32_t* ids,
+                              const int64_t* offsets, float* out, int32_t* status, cudaStream_t s);
 
 }  // namespace rover

@@ -263,20 +263,25 @@ __device__ __forceinline__ bool pq_residual_fixed(const PqIndexView& ix, const f
 static __device__ void pq_refine_warp(const PqIndexView& ix, const float* q, const uint64_t* list,
                                int count, int k, double* sd, int32_t* si, int lane,
                                int32_t* out_ids, float* out_dists, int32_t* out_count,
-                               int32_t* status, const float* decoded = nullptr) {
+                               int32_t* status, const float* decoded = nullptr, bool error4 = false) {
   int np2 = 1;
   while (np2 < count) np2 <<= 1;
   bool bad = false;
   for (int i = lane; i < np2; i += kWarp) {
+    // mode ERROR4: the storage row's third-level term on top of the decode
+    const int32_t row = i < count ? key_id(list[i]) : 0;
+    const uint8_t* e4c = error4 && i < count ? error4_row(ix.e4, row) : nullptr;
+    const float2 e4q = e4c ? __ldg(reinterpret_cast<const float2*>(ix.e4.qparams) + row) : make_float2(0.f, 0.f);
     if (i < count && decoded) {
       const int32_t id = key_id(list[i]);
       const float4* x4 = reinterpret_cast<const float4*>(decoded + static_cast<size_t>(id) * ix.dim);
       double dist = 0.0;
       for (int t = 0; t < ix.dim / 4; ++t) {
         const float4 x = __ldg(x4 + t);
-        const float xv[4] = {x.x, x.y, x.z, x.w};
+        float xv[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
+          if (e4c) xv[u] = error4_add(xv[u], e4c, e4q, 4 * t + u);
           if (!isfinite(xv[u])) bad = true;
           const double delta = __dsub_rn(static_cast<double>(q[4 * t + u]), static_cast<double>(xv[u]));
           dist = __dadd_rn(dist, __dmul_rn(delta, delta));
@@ -299,7 +304,8 @@ static __device__ void pq_refine_warp(const PqIndexView& ix, const float* q, con
         for (int j = 0; j < ix.subdim; ++j, ++dim) {
           const uint32_t r = ix.residual_bits == 4 ? static_cast<uint32_t>(nibble(res, dim))
                                                    : static_cast<uint32_t>(__ldg(res + dim));
-          const float x = fadd(fadd(__ldg(cen + j), fmul(u8f(r), qp.x)), qp.y);
+          float x = fadd(fadd(__ldg(cen + j), fmul(u8f(r), qp.x)), qp.y);
+          if (e4c) x = error4_add(x, e4c, e4q, dim);
           if (!isfinite(x)) bad = true;
           const double delta = __dsub_rn(static_cast<double>(q[dim]), static_cast<double>(x));
           dist = __dadd_rn(dist, __dmul_rn(delta, delta));
@@ -713,7 +719,8 @@ __device__ __forceinline__ void pq_finish_query(const PqSearchArgs& a, const flo
       double* sd = reinterpret_cast<double*>(base + a.smem_refine_offset);
       int32_t* si = reinterpret_cast<int32_t*>(sd + a.refine_capacity);
       int32_t rs = kStatusOk;
-      pq_refine_warp(ix, q, list, cnt, k, sd, si, lane, oi, od, a.out_counts + qi, &rs, decoded);
+      pq_refine_warp(ix, q, list, cnt, k, sd, si, lane, oi, od, a.out_counts + qi, &rs, decoded,
+                     a.third_residual != 0);
       rs = __shfl_sync(kFullMask, rs, 0);
       if (rs != kStatusOk && lane == 0) *status = rs;
     } else {

@@ -207,17 +207,19 @@ class GpuPass {
   int32_t* ids() { return reinterpret_cast<int32_t*>(static_cast<uint8_t*>(h_block_) + kOffIds); }
   const float* out() const { return reinterpret_cast<const float*>(static_cast<const uint8_t*>(h_block_) + kOffOut); }
 
-  // The per-query table: the PQ lookup table (m * ks floats) or the FP32 query.
-  bool upload_table(const float* src, size_t floats) {
-    if (floats > table_floats_) return false;
-    if (cudaMemcpyAsync(d_table_, src, floats * sizeof(float), cudaMemcpyHostToDevice, stream_) != cudaSuccess)
+  // The per-query table: the PQ lookup table (m * ks floats), the FP32
+  // query, or the aligned u8 query of the split distance (bytes).
+  bool upload_table(const void* src, size_t bytes) {
+    if (bytes > table_floats_ * sizeof(float)) return false;
+    if (cudaMemcpyAsync(d_table_, src, bytes, cudaMemcpyHostToDevice, stream_) != cudaSuccess)
       return fail("table upload");
     return cudaStreamSynchronize(stream_) == cudaSuccess || fail("table upload");
   }
 
-  // Distances of ids()[0, n): PQ ADC (pq != nullptr) or SQ L1 distance.
-  // False on a CUDA error or a kernel-reported failure.
-  bool run(const PqIndexView* pq, const SqIndexView* sq, int n, uint64_t* gpu_us) {
+  // Distances of ids()[0, n): PQ ADC (pq != nullptr), or SQ L1 distance
+  // (against the aligned u8 query when `aligned`).  False on a CUDA error or
+  // a kernel-reported failure.
+  bool run(const PqIndexView* pq, const SqIndexView* sq, int n, uint64_t* gpu_us, bool aligned = false) {
     const auto t0 = std::chrono::steady_clock::now();
     uint8_t* hb = static_cast<uint8_t*>(h_block_);
     int64_t* off = reinterpret_cast<int64_t*>(hb);
@@ -233,6 +235,8 @@ class GpuPass {
     float* d_out = reinterpret_cast<float*>(db + kOffOut);
     const int32_t* d_ids = reinterpret_cast<const int32_t*>(db + kOffIds);
     if (pq) launch_pq_adc(*pq, d_table_, 1, d_ids, d_off, d_out, d_status, stream_);
+    else if (aligned) launch_sq_aligned_coarse(*sq, reinterpret_cast<const uint8_t*>(d_table_), 1, d_ids, d_off, d_out,
+                                               d_status, stream_);
     else launch_sq_coarse(*sq, d_table_, 1, d_ids, d_off, d_out, d_status, stream_);
     if (cudaGetLastError() != cudaSuccess) return fail("distance kernel launch");
     session_count_launches(1);
@@ -398,7 +402,7 @@ AEEResult serve_pure_pq(const SessionIndex& ix, PqControl* ctl, PqLutHeader* hdr
       }
     }
     if (!bad && gen != table_gen) {
-      if (!gpu.upload_table(lut, static_cast<size_t>(entries))) bad = "lookup-table upload";
+      if (!gpu.upload_table(lut, static_cast<size_t>(entries) * sizeof(float))) bad = "lookup-table upload";
       else table_gen = gen;
     }
     if (!bad && nids > 0 && !gpu.run(&v, nullptr, nids, &compute_us)) bad = "ADC kernel (non-finite distance or CUDA error)";
@@ -487,8 +491,9 @@ AEEResult serve_sqmd(const SessionIndex& ix, SqControl* ctl, const float* call_q
     return rc;
   }
   int table_gen = -1;
+  bool aligned = false;   // the current query uses the ALIGNED_U8 contract
   if (!persistent) {
-    if (!gpu.upload_table(call_query, static_cast<size_t>(v.dim))) return AEE_EFAILED;
+    if (!gpu.upload_table(call_query, static_cast<size_t>(v.dim) * sizeof(float))) return AEE_EFAILED;
     table_gen = 0;
   }
   release_fence();
@@ -534,16 +539,29 @@ AEEResult serve_sqmd(const SessionIndex& ix, SqControl* ctl, const float* call_q
     SqLaneBuffer* failed = nullptr;
     int32_t fail_status = 0;
     if (persistent && ctl->query_slot.query_gen != table_gen) {
+      // the lane worker's query refresh (retrieval_async_dsp_search.c:1095-1127):
+      // the legacy contract quantizes the FP32 query; the ALIGNED_U8
+      // contract (split distance) hands over the host's u8 query, which
+      // needs 4-bit L1 codes and the index's dimension
       const SqQuerySlot& qs = ctl->query_slot;
-      if (qs.contract_id != kContractLegacy || !(v.l1_scale != 0.0f) ||
-          !gpu.upload_table(qs.query, static_cast<size_t>(v.dim))) {
+      const bool want_aligned = qs.contract_id == kContractAlignedU8;
+      bool ok;
+      if (want_aligned) {
+        ok = qs.query_dim == v.dim && v.l1_bits == 4 && std::isfinite(v.l1_scale) && v.l1_scale > 0.0f &&
+             gpu.upload_table(const_cast<const uint8_t*>(qs.query_u8), static_cast<size_t>(v.dim));
+      } else {
+        ok = qs.contract_id == kContractLegacy && v.l1_scale != 0.0f &&
+             gpu.upload_table(const_cast<const float*>(qs.query), static_cast<size_t>(v.dim) * sizeof(float));
+      }
+      if (!ok) {
         failed = &ctl->lanes[ready[0].lane].buf[ready[0].index];
         fail_status = kSqStatusBadParam;
-        session_error(qs.contract_id != kContractLegacy
-                          ? "SQMD session: the aligned-u8 query contract (split distance) is not served"
-                          : "SQMD session: the query cannot be quantized");
+        session_error(want_aligned ? "SQMD session: the aligned-u8 query does not fit this index"
+                      : qs.contract_id != kContractLegacy ? "SQMD session: unknown query contract"
+                                                          : "SQMD session: the query cannot be quantized");
       } else {
         table_gen = qs.query_gen;
+        aligned = want_aligned;
       }
     }
     for (int r = 0; r < nready && !failed; ++r) {
@@ -557,7 +575,7 @@ AEEResult serve_sqmd(const SessionIndex& ix, SqControl* ctl, const float* call_q
         gpu.ids()[nids++] = id;
       }
     }
-    if (!failed && nids > 0 && !gpu.run(nullptr, &v, nids, &compute_us)) {
+    if (!failed && nids > 0 && !gpu.run(nullptr, &v, nids, &compute_us, aligned)) {
       failed = &ctl->lanes[ready[0].lane].buf[ready[0].index];
       fail_status = kSqStatusBadParam;
     }

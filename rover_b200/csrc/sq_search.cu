@@ -26,6 +26,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "sq_split.cuh"
 
 namespace rover {
 
@@ -171,8 +172,9 @@ __device__ __forceinline__ bool first_of_equal(bool active, int32_t id, int lane
   return active && (__ffs(same) - 1) == lane;
 }
 
+template <bool kSplit>
 __global__ void __launch_bounds__(kSearchWarps * 32)
-sq_search_kernel(SqSearchArgs a) {
+sq_search_kernel_t(SqSearchArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -193,6 +195,7 @@ sq_search_kernel(SqSearchArgs a) {
   vt.mask = a.visited_mask;
   const bool sqmd = a.mode == kSqModeSqmd;
   const bool db = a.mode == kSqModeDb;
+  const bool split = kSplit && sqmd && a.correction;   // the host checks the index supports it
 
   for (;;) {
     int qi = 0;
@@ -214,15 +217,35 @@ sq_search_kernel(SqSearchArgs a) {
                                : sqmd ? static_cast<long long>(a.entry_points) + static_cast<long long>(cap) * a.expand_count
                                       : static_cast<long long>(a.entry_points) + static_cast<long long>(cap) * expand;
     const int fcap = static_cast<int>(min(fcap_ref, static_cast<long long>(a.frontier_cap)));
-    // query and its quantized codes (retrieval_quantize_query_u8/_u4, l1_int8_core.c:13-63)
+    // query and its quantized codes (retrieval_quantize_query_u8/_u4,
+    // l1_int8_core.c:13-63); with the split distance the codes of the
+    // 17-fold refined grid instead (sq_split.cuh) and their sum
     const float inv = __frcp_rn(ix.l1_scale);
     const int levels = ix.l1_bits == 4 ? 15 : 255;
+    const double step = split ? split_step(ix.l1_scale) : 0.0;
+    unsigned long long sum_q = 0;
+    bool qbad = false;
     for (int d = lane; d < ix.dim; d += kWarp) {
       const float v = a.queries[static_cast<size_t>(qi) * ix.dim + d];
       q[d] = v;
-      int c = static_cast<int>(roundf(fmul(fsub(v, ix.l1_zero), inv)));
-      c = c < 0 ? 0 : (c > levels ? levels : c);
-      qc[d] = static_cast<uint8_t>(c);
+      if (split) {
+        uint8_t c = 0;
+        qbad |= !split_code(v, ix.l1_zero, step, &c);
+        qc[d] = c;
+        sum_q += c;
+      } else {
+        int c = static_cast<int>(roundf(fmul(fsub(v, ix.l1_zero), inv)));
+        c = c < 0 ? 0 : (c > levels ? levels : c);
+        qc[d] = static_cast<uint8_t>(c);
+      }
+    }
+    if (split) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) sum_q += __shfl_xor_sync(kFullMask, sum_q, off);
+      if (__any_sync(kFullMask, qbad)) {
+        if (lane == 0) *status = kStatusNumeric;
+        continue;
+      }
     }
     __syncwarp();
     vt.gen = a.gen_base + static_cast<uint32_t>(qi);
@@ -299,7 +322,8 @@ sq_search_kernel(SqSearchArgs a) {
       }
       float d = 0.0f;
       if (fresh) {
-        d = (sqmd && a.correction) ? sq_exact(ix, q, id) : sq_coarse(ix, qc, id);
+        d = split ? split_seed_distance(ix, qc, sum_q, id, step)
+                  : (sqmd && a.correction) ? sq_exact(ix, q, id) : sq_coarse(ix, qc, id);
         if (sqmd && a.correction && (!isfinite(d) || d < 0.0f)) st = kStatusNumeric;
       }
       if (__any_sync(kFullMask, st != kStatusOk)) { st = st != kStatusOk ? st : kStatusNumeric; break; }
@@ -351,10 +375,18 @@ sq_search_kernel(SqSearchArgs a) {
         }
         const unsigned fm = __ballot_sync(kFullMask, fresh);
         float d = 0.0f;
-        if (fresh) {
+        bool dbad = false;
+        if (fresh && split) {
+          // sqmd_source_job_commit (sqmd_common.c:1533-1556): the lane's
+          // coarse distance plus the host's delta, tiny negatives clamped
+          const float dl = split_delta(ix, qc, sum_q, nid, step);
+          d = split_sum(split_coarse(ix, qc, nid, step), dl);
+          dbad = !isfinite(dl) || !isfinite(d) || d < 0.0f;
+        } else if (fresh) {
           d = sq_coarse(ix, qc, nid);
           if ((sqmd || db) && a.correction) d = sq_exact(ix, q, nid);
         }
+        if (split && __any_sync(kFullMask, dbad)) { st = kStatusNumeric; break; }
         const int slot_i = __popc(fm & ((1u << lane) - 1u));
         if (fresh) {
           work[slot_i].id = nid;
@@ -422,6 +454,10 @@ sq_search_kernel(SqSearchArgs a) {
   }
 }
 
+
+SqSearchFn sq_search_kernel_for(bool split) {
+  return split ? sq_search_kernel_t<true> : sq_search_kernel_t<false>;
+}
 
 // ---------------------------------------------------------------------------
 // DB-pair search, one step per launch (calculator_retrieval_search_db).  Warp

@@ -340,6 +340,10 @@ int rover_bundle_open_pq(const char* graph_path, const char* graph_format, int32
     b->dim = dim;
     b->degree = degree;
     b->graph_entry = graph_entry;
+    snprintf(b->base_paths[0], sizeof(b->base_paths[0]), "%s", pq_codes ? pq_codes : "");
+    snprintf(b->base_paths[1], sizeof(b->base_paths[1]), "%s", pq_residual ? pq_residual : "");
+    snprintf(b->base_paths[2], sizeof(b->base_paths[2]), "%s", pq_qparams ? pq_qparams : "");
+    snprintf(b->pq_book_path, sizeof(b->pq_book_path), "%s", pq_book ? pq_book : "");
     if (rover_read_graph(graph_path, graph_format, n, dim, degree, &b->graph) != 0 ||
         (verify && rover_check_graph(b->graph, n, degree) != 0) ||
         open_pq_members(b, pq_book, pq_codes, pq_residual, pq_qparams, residual_bits, verify) != 0) {
@@ -363,6 +367,9 @@ int rover_bundle_open_sq(const char* graph_path, const char* graph_format, int32
     b->dim = dim;
     b->degree = degree;
     b->graph_entry = graph_entry;
+    snprintf(b->base_paths[0], sizeof(b->base_paths[0]), "%s", l1 ? l1 : "");
+    snprintf(b->base_paths[1], sizeof(b->base_paths[1]), "%s", residual ? residual : "");
+    snprintf(b->base_paths[2], sizeof(b->base_paths[2]), "%s", qparams ? qparams : "");
     uint8_t* raw = NULL;
     size_t len = 0;
     int rc = -1;

@@ -323,8 +323,13 @@ static int parse(int argc, char** argv) {
         c->search_mode = "db_pair";
     }
     c->refine_mode = c->refine ? 1 + (c->third_residual != 0) : 0;
-    if (c->third_residual) return refuse("the third-level (ERROR4) refine is not part of this build");
-    if (c->split_distance) return refuse("the SQ4 split-distance correction is not part of this build");
+    if (c->third_residual) {
+        /* the artifact must exist and hash (config.c:118); it is checked
+           against the index when the refine opens it */
+        uint8_t digest[32];
+        if (!*c->error4 || rover_sha256_file(c->error4, 0, digest) != 0)
+            return refuse("missing or unreadable third residual artifact");
+    }
     if (is(c->command, "search") &&
         !(c->nq > 0 && c->top_k <= c->n && *c->query && (*c->graph || *c->index_dir)))
         return refuse("search requires query, graph, nq and top-k <= n");
@@ -483,6 +488,10 @@ static int run_search(remote_handle64 h, const RoverBundle* b, const float* quer
     p.expand_count = cfg.expand_count;
     p.correction = cfg.correction;
     p.refine_budget = pq ? refine_budget : 0;
+    p.third_residual = pq && cfg.refine_mode == 2;
+    /* SQMD_SPLIT_DISTANCE (retrieval_rpc_demo_pipeline.c:2776, set from
+       --split-distance by config.c:122) */
+    p.split_distance = !pq && cfg.split_distance;
     /* the SQMD driver asks its search for rerank_count results
        (retrieval_rpc_demo_pipeline.c:2754): the refine budget, or top-k x
        the first-stage factor */
@@ -524,9 +533,10 @@ static int run_search(remote_handle64 h, const RoverBundle* b, const float* quer
             refine_budget ? (o.pool_counts[i] < refine_budget ? o.pool_counts[i] : refine_budget) : 0);
     } else {
         rc = calculator_rover_sq_search(h, &p, queries, nq, pools, &out);
-        /* the DB-pair re-rank worker without final refine: demo_rerank_candidates
-           over every candidate (retrieval_rpc_demo_pipeline.c:204-226) */
-        const int rerank = db_pair && !refine_budget && cfg.correction;
+        /* without final refine, demo_rerank_candidates over every candidate:
+           the DB-pair re-rank worker (retrieval_rpc_demo_pipeline.c:204-226)
+           and the split-distance SQMD path (:3310-3320) */
+        const int rerank = !refine_budget && ((db_pair && cfg.correction) || cfg.split_distance);
         if (!rc && (refine_budget || rerank)) {
             /* retrieval_final_refine over the first refine_budget entries of the SQMD pool */
             int32_t* cand_counts = (int32_t*)malloc((size_t)nq * 4);
@@ -540,8 +550,8 @@ static int run_search(remote_handle64 h, const RoverBundle* b, const float* quer
             }
             const unsigned long long r0 = now_us();
             if (!rc)
-                rc = calculator_rover_refine(h, rerank ? 2 : 0, queries, nq, o.ids, stride, cand_counts, cfg.top_k,
-                                             rid, rd, rc_counts, o.status);
+                rc = calculator_rover_refine(h, rerank ? 2 : cfg.refine_mode == 2 ? 3 : 0, queries, nq, o.ids,
+                                             stride, cand_counts, cfg.top_k, rid, rd, rc_counts, o.status);
             refine_us = now_us() - r0;
             for (int i = 0; !rc && i < nq; ++i) {
                 memcpy(o.ids + (size_t)i * stride, rid + (size_t)i * cfg.top_k, (size_t)cfg.top_k * 4);
@@ -628,6 +638,42 @@ static int run_search(remote_handle64 h, const RoverBundle* b, const float* quer
     return bad ? -1 : 0;
 }
 
+/* The split-distance bias, checked as sqmd_load_correction_bias does
+   (retrieval_rpc_demo_pipeline.c:3000-3019 prints the same refusal). */
+static int load_split_bias(remote_handle64 h, const RoverBundle* b) {
+    float* bias = NULL;
+    if (rover_split_bias_open(b, cfg.bias, &bias) != 0) {
+        printf("  ERROR: split distance requires verified U4/U4 or U4/U8 bias artifact %s\n", cfg.bias);
+        fprintf(stderr, "Rover: %s\n", rover_artifact_error());
+        return -1;
+    }
+    printf("  SQMD split distance: ON bias=%s bytes=%llu\n", cfg.bias, (unsigned long long)b->n * 4ull);
+    const int rc = calculator_rover_sq_split_load(h, bias, b->n);
+    if (rc) fprintf(stderr, "Rover: split bias load failed (%d): %s\n", rc, calculator_rover_last_error());
+    free(bias);
+    return rc ? -1 : 0;
+}
+
+/* The ERROR4 artifact of the final refine's mode 2, checked as
+   retrieval_final_refine.c:118-166 does (the reference's two open-failure
+   messages, retrieval_rpc_demo_pure_pq.c:530-533 and
+   retrieval_rpc_demo_pipeline.c:3040-3043). */
+static int load_error4(remote_handle64 h, const RoverBundle* b) {
+    RoverError4* e = NULL;
+    const int pq = b->method == 1;
+    if (rover_error4_open(b, cfg.error4, sink.to_original, &e) != 0) {
+        printf(pq ? "ERROR: PQ final refinement identity/open failed\n"
+                  : "  ERROR: Phase15 refinement artifact/provider validation failed\n");
+        fprintf(stderr, "Rover: %s\n", rover_artifact_error());
+        return -1;
+    }
+    const int rc = calculator_rover_error4_load(h, pq ? 1 : 0, e->qparams, e->blocks, e->blocks_bytes,
+                                                e->num_vectors, e->dim);
+    if (rc) fprintf(stderr, "Rover: ERROR4 load failed (%d): %s\n", rc, calculator_rover_last_error());
+    rover_error4_close(e);
+    return rc ? -1 : 0;
+}
+
 static int search(remote_handle64 h) {
     RoverBundle* b = NULL;
     const int pq = !strcmp(cfg.method, "pq");
@@ -688,7 +734,9 @@ static int search(remote_handle64 h) {
     }
     fflush(stdout);
     if (rc) fprintf(stderr, "Rover: index load failed (%d): %s\n", rc, calculator_rover_last_error());
-    else rc = run_search(h, b, queries, gt);
+    if (!rc && cfg.split_distance) rc = load_split_bias(h, b);
+    if (!rc && cfg.refine_mode == 2) rc = load_error4(h, b);
+    if (!rc) rc = run_search(h, b, queries, gt);
     if (pq) calculator_rover_pq_unload(h);
     else calculator_rover_sq_unload(h);
     rover_bundle_close(b);
