@@ -265,6 +265,23 @@ AEEResult calculator_rover_score(remote_handle64 h, int32_t kind, const float *q
 AEEResult calculator_rover_pq_lut(remote_handle64 h, const float *queries, int32_t num_queries,
                                   float *out_luts, int32_t *out_status);
 
+/* PQ codebook training on the GPU: retrieval_pq_train
+ * (retrieval_pq_core.c:202-224 over retrieval_pq_train_subspace :97-200),
+ * bit for bit: per subspace, centroid k starts as training vector
+ * k (count-1) / (ks-1) and kmeans_iters (at least 1) Lloyd iterations follow,
+ * with the reference's FP32 distances, first-minimum ties and member sums in
+ * vector order.  train_vectors [train_count][dim] (host, finite), codebook
+ * out [m][ks][dim/m] (host).  ks in 1..256, dim % m == 0. */
+AEEResult calculator_rover_pq_train(remote_handle64 h, const float *train_vectors, int32_t train_count,
+                                    int32_t dim, int32_t m, int32_t ks, int32_t kmeans_iters,
+                                    float *out_codebook);
+/* PQ encoding on the GPU: retrieval_pq_encode_batch (retrieval_pq_core.c:
+ * 226-268): the nearest centroid of every subspace (first minimum), codes
+ * [count][code_bytes] with two 4-bit codes per byte (low nibble first) when
+ * ks <= 16.  AEE_EBADPARM on a non-finite distance, as the reference fails. */
+AEEResult calculator_rover_pq_encode(remote_handle64 h, const float *vectors, int64_t count, int32_t dim,
+                                     const float *codebook, int32_t m, int32_t ks, uint8_t *out_codes);
+
 /* The third-level ERROR4 artifact of the loaded index (kind 0 = the SQ index
  * of calculator_rover_sq_load, 1 = the PQ index): the payload of a
  * SQERR4V1 / PQERR4V1 file after its 256-byte header (retrieval_final_refine.c:
@@ -442,6 +459,7 @@ uint64_t calculator_rover_launch_count(void);
 #define ROVER_KERNEL_PQ_RESCORE 12  /* kind 4: corrected distances from decoded rows */
 #define ROVER_KERNEL_PLAN 13        /* search plans: bookkeeping kernels */
 #define ROVER_KERNEL_PQ_SEED_TOPM 14 /* per-query top-M of the seed ranks */
+#define ROVER_KERNEL_PQ_TRAIN 15    /* calculator_rover_pq_train / _pq_encode */
 #define ROVER_KERNEL_KINDS 16
 void calculator_rover_kernel_timing(int32_t enable);
 int32_t calculator_rover_kernel_times(int64_t *launches, double *ms, int32_t kinds);

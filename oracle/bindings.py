@@ -48,6 +48,12 @@ def port_available() -> bool:
     return PORT_LIB.is_file()
 
 
+class _PqConfig(C.Structure):
+    """RetrievalPqConfig (retrieval_pq_core.h:10-17)."""
+    _fields_ = [("m", C.c_int), ("ks", C.c_int), ("subdim", C.c_int), ("dim", C.c_int), ("train_max", C.c_int),
+                ("kmeans_iters", C.c_int)]
+
+
 class Reference:
     """The reference's own functions, driven in batches."""
 
@@ -79,6 +85,32 @@ class Reference:
         L.ref_dsp_search_batch.argtypes = [C.c_int, _i32p, C.c_int, C.c_int, C.c_int, _u8p, C.c_int, C.c_int,
                                            C.c_float, C.c_float, _f32p, C.c_int, _i32p, C.c_int, C.c_int,
                                            C.c_int, C.c_int, _i32p, _f32p, C.c_int, _i32p]
+
+    # -- PQ training and encoding (retrieval_pq_core.c:97-268, called directly)
+    def pq_train(self, vectors, m: int, ks: int, iters: int):
+        x = np.ascontiguousarray(vectors, dtype=np.float32)
+        n, dim = x.shape
+        cfg = _PqConfig(m, ks, dim // m, dim, n, iters)
+        book = np.zeros((m, ks, dim // m), np.float32)
+        self.lib.retrieval_pq_train.argtypes = [_f32p, C.c_int, C.POINTER(_PqConfig), _f32p]
+        rc = self.lib.retrieval_pq_train(_p(x, _f32p), n, C.byref(cfg), _p(book, _f32p))
+        if rc != 0:
+            raise RuntimeError(f"retrieval_pq_train failed: {rc}")
+        return book
+
+    def pq_encode(self, vectors, book):
+        x = np.ascontiguousarray(vectors, dtype=np.float32)
+        b = np.ascontiguousarray(book, dtype=np.float32)
+        m, ks, subdim = b.shape
+        cfg = _PqConfig(m, ks, subdim, m * subdim, 0, 1)
+        cb = (m + 1) // 2 if ks <= 16 else m
+        codes = np.zeros((x.shape[0], cb), np.uint8)
+        self.lib.retrieval_pq_encode_batch.argtypes = [_f32p, C.c_int, _f32p, C.POINTER(_PqConfig), _u8p]
+        rc = self.lib.retrieval_pq_encode_batch(_p(x, _f32p), x.shape[0], _p(b, _f32p), C.byref(cfg),
+                                                _p(codes, _u8p))
+        if rc != 0:
+            raise RuntimeError(f"retrieval_pq_encode_batch failed: {rc}")
+        return codes
 
     # -- PQ
     def pq_open(self, prefix, residual_bits: int, chunk_vectors: int = 262144):

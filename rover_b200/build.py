@@ -28,7 +28,7 @@ BIN_DIR = HERE / "bin"
 ROVER = BIN_DIR / "Rover"
 HOST_SOURCES = ["sha256.c", "json.c", "bundle.c", "artifacts.c"]
 
-SOURCES = ["calculator.cu", "pq_search.cu", "pq_decoded.cu", "pq_batched.cu", "gate_train.cu", "plan.cu", "sq_search.cu", "distance.cu", "sessions.cu", "seed_rank_tc.cu", "rpcmem_compat.cpp"]
+SOURCES = ["calculator.cu", "pq_search.cu", "pq_decoded.cu", "pq_batched.cu", "gate_train.cu", "plan.cu", "sq_search.cu", "distance.cu", "sessions.cu", "seed_rank_tc.cu", "pq_train.cu", "rpcmem_compat.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

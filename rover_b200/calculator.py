@@ -170,6 +170,10 @@ class Calculator:
                                                    C.c_int32]
         L.calculator_rover_error4_unload.argtypes = [C.c_uint64, C.c_int32]
         L.calculator_rover_sq_split_load.argtypes = [C.c_uint64, _f32p, C.c_int32]
+        L.calculator_rover_pq_train.argtypes = [C.c_uint64, _f32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                                C.c_int32, _f32p]
+        L.calculator_rover_pq_encode.argtypes = [C.c_uint64, _f32p, C.c_int64, C.c_int32, _f32p, C.c_int32,
+                                                 C.c_int32, _u8p]
         self.handle = C.c_uint64(0)
         self._check("calculator_open", L.calculator_open(b"file:///libcalculator_skel.so", C.byref(self.handle)))
         self._keep = {}
@@ -187,7 +191,8 @@ class Calculator:
         return int(self.lib.calculator_rover_launch_count())
 
     KERNEL_KINDS = ("pq_packed", "pq_seeds", "pq_decoded", "pq_batched", "sq", "pq_seed_rank", "pq_lut", "pq_adc",
-                    "pq_residual", "sq_coarse", "sq_exact", "refine", "pq_rescore", "plan", "pq_seed_topm")
+                    "pq_residual", "sq_coarse", "sq_exact", "refine", "pq_rescore", "plan", "pq_seed_topm",
+                    "pq_train")
 
     # -- learned gate
     def gate_load(self, params, mu, sigma, band_lo=0.0, band_hi=0.0, refine_logit=0.0, stop_logit=1e30) -> None:
@@ -486,6 +491,28 @@ class Calculator:
                                                      ids.shape[1], _p(counts, _i32p), top_k, _p(oi, _i32p),
                                                      _p(od, _f32p), _p(oc, _i32p), _p(st, _i32p)))
         return oi, od, oc
+
+    def pq_train(self, vectors, m: int, ks: int, iters: int) -> np.ndarray:
+        """retrieval_pq_train on the GPU: codebook [m][ks][dim/m]."""
+        x = np.ascontiguousarray(vectors, dtype=np.float32)
+        n, dim = x.shape
+        book = np.zeros((m, ks, dim // m), np.float32)
+        self._check("calculator_rover_pq_train",
+                    self.lib.calculator_rover_pq_train(self.handle, _p(x, _f32p), n, dim, m, ks, iters,
+                                                       _p(book, _f32p)))
+        return book
+
+    def pq_encode(self, vectors, codebook) -> np.ndarray:
+        """retrieval_pq_encode_batch on the GPU: codes [n][code_bytes]."""
+        x = np.ascontiguousarray(vectors, dtype=np.float32)
+        book = np.ascontiguousarray(codebook, dtype=np.float32)
+        m, ks, _ = book.shape
+        cb = (m + 1) // 2 if ks <= 16 else m
+        codes = np.zeros((x.shape[0], cb), np.uint8)
+        self._check("calculator_rover_pq_encode",
+                    self.lib.calculator_rover_pq_encode(self.handle, _p(x, _f32p), x.shape[0], x.shape[1],
+                                                        _p(book, _f32p), m, ks, _p(codes, _u8p)))
+        return codes
 
     def error4_load(self, kind: int, qparams, code_blocks) -> None:
         """The ERROR4 artifact payload (qparams [n][2], 4096-byte code blocks)

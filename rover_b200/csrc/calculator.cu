@@ -2595,6 +2595,74 @@ extern "C" AEEResult calculator_rover_sq_unload(remote_handle64 h) {
   return AEE_SUCCESS;
 }
 
+// retrieval_pq_train (retrieval_pq_core.c:202-224) on the device.
+extern "C" AEEResult calculator_rover_pq_train(remote_handle64 h, const float* train_vectors, int32_t train_count,
+                                               int32_t dim, int32_t m, int32_t ks, int32_t kmeans_iters,
+                                               float* out_codebook) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  // retrieval_pq_validate_config (:84-93) and the input checks of :108-129
+  if (!train_vectors || !out_codebook || train_count <= 0 || m <= 0 || ks <= 0 || ks > 256 || dim <= 0 ||
+      dim % m != 0)
+    return AEE_EBADPARM;
+  const size_t values = static_cast<size_t>(train_count) * dim;
+  for (size_t i = 0; i < values; ++i)
+    if (!std::isfinite(train_vectors[i])) { set_error("training vector %zu is not finite", i / dim); return AEE_EBADPARM; }
+  DevBuf x, book;
+  const size_t book_floats = static_cast<size_t>(ks) * dim;   // m * ks * subdim
+  if (upload(x, train_vectors, values, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  CK(book.ensure(book_floats * sizeof(float)));
+  PqTrainScratch scratch;
+  {
+    TimedLaunch tl(ROVER_KERNEL_PQ_TRAIN, s.stream);
+    CK(pq_train_device(x.as<float>(), train_count, dim, m, ks, kmeans_iters, book.as<float>(), &scratch, s.stream));
+  }
+  g_launches += static_cast<unsigned long long>(pq_train_launches(kmeans_iters));
+  if (download(out_codebook, book.p, book_floats, s.stream)) return AEE_EFAILED;
+  CK(cudaStreamSynchronize(s.stream));
+  return AEE_SUCCESS;
+}
+
+// retrieval_pq_encode_batch (retrieval_pq_core.c:226-268) on the device, in
+// chunks of at most 1M vectors.
+extern "C" AEEResult calculator_rover_pq_encode(remote_handle64 h, const float* vectors, int64_t count, int32_t dim,
+                                                const float* codebook, int32_t m, int32_t ks, uint8_t* out_codes) {
+  (void)h;
+  State& s = st();
+  std::lock_guard<std::mutex> lock(s.mu);
+  if (ensure_init(s) != AEE_SUCCESS) return AEE_EFAILED;
+  if (!vectors || !codebook || !out_codes || count < 0 || m <= 0 || ks <= 0 || ks > 256 || dim <= 0 ||
+      dim % m != 0)
+    return AEE_EBADPARM;
+  if (count == 0) return AEE_SUCCESS;
+  const int code_bytes = ks <= 16 ? m / 2 + m % 2 : m;
+  DevBuf book, x, codes, bad;
+  if (upload(book, codebook, static_cast<size_t>(ks) * dim, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  CK(bad.ensure(sizeof(int)));
+  CK(cudaMemsetAsync(bad.p, 0, sizeof(int), s.stream));
+  const int64_t chunk = 1 << 20;
+  for (int64_t begin = 0; begin < count; begin += chunk) {
+    const int64_t nc = std::min<int64_t>(chunk, count - begin);
+    if (upload(x, vectors + begin * dim, static_cast<size_t>(nc) * dim, s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+    CK(codes.ensure(static_cast<size_t>(nc) * code_bytes));
+    {
+      TimedLaunch tl(ROVER_KERNEL_PQ_TRAIN, s.stream);
+      launch_pq_encode(x.as<float>(), nc, dim, m, ks, book.as<float>(), codes.as<uint8_t>(), bad.as<int>(), s.stream);
+    }
+    CK(cudaGetLastError());
+    ++g_launches;
+    if (download(out_codes + begin * code_bytes, codes.p, static_cast<size_t>(nc) * code_bytes, s.stream))
+      return AEE_EFAILED;
+  }
+  int h_bad = 0;
+  CK(cudaMemcpyAsync(&h_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+  CK(cudaStreamSynchronize(s.stream));
+  if (h_bad) { set_error("a subspace distance is not finite"); return AEE_EBADPARM; }
+  return AEE_SUCCESS;
+}
+
 // The ERROR4 payload of retrieval_final_refine's mode 2 (the host validated
 // the artifact's header, retrieval_final_refine.c:118-166; the qparams
 // checks of :160-163 are repeated here).

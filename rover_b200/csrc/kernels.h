@@ -362,4 +362,26 @@ void launch_refine(int kind, const PqIndexView& pq, const SqIndexView& sq, const
 void launch_sq_aligned_coarse(const SqIndexView& ix, const uint8_t* queries_u8, int nq, const int32_t* ids,
                               const int64_t* offsets, float* out, int32_t* status, cudaStream_t s);
 
+// ---- PQ codebook training and encoding (pq_train.cu)
+//
+// retrieval_pq_train (retrieval_pq_core.c:97-224) over x [n][dim] on the
+// device, all m subspaces at once; book [m][ks][dim/m] receives the
+// codebook.  The scratch (assignments, per-block histograms, member lists)
+// is owned by the caller's PqTrainScratch.
+struct PqTrainScratch {
+  uint8_t* assign = nullptr;
+  int* block_hist = nullptr;
+  int* counts = nullptr;
+  int* members = nullptr;
+  ~PqTrainScratch();
+  void release();
+};
+cudaError_t pq_train_device(const float* x, int n, int dim, int m, int ks, int iters, float* book,
+                            PqTrainScratch* scratch, cudaStream_t s);
+int pq_train_launches(int iters);
+// retrieval_pq_encode_batch (:226-268): codes [n][code_bytes], 4-bit codes
+// packed low nibble first when ks <= 16; *bad = 1 on a non-finite distance.
+void launch_pq_encode(const float* x, long long n, int dim, int m, int ks, const float* book, uint8_t* codes,
+                      int* bad, cudaStream_t s);
+
 }  // namespace rover
