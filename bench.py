@@ -88,6 +88,11 @@ UNEVEN_L = (16, 512)
 UNEVEN_K = (1, 10, 100)
 UNEVEN_REFINE = 200               # refine_factor 2 x the largest k
 UNEVEN_EPS = (256, 1024, 4096)
+LARGE_WORKLOAD = "pq_10m_d128"    # --config5: 10M x 128, SQ4 + PQ32, uneven L in [32, 256]
+LARGE_L = (32, 256)
+LARGE_EPS = (4096, 8192, 16384)
+LARGE_REFINE = 20
+LARGE_W = 2
 METRIC = "QPS at recall@10>=0.95 on 1 B200 (pure-PQ graph search, 1M x 128): learned-gate batched vs plain"
 
 
@@ -446,6 +451,9 @@ def main():
     ap.add_argument("--train-queries", type=int, default=TRAIN_QUERIES)
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch plan section")
     ap.add_argument("--no-sq", action="store_true", help="skip the SQ section")
+    ap.add_argument("--large-workload", default=LARGE_WORKLOAD, help="with --config5: workloads.LARGE_CONFIGS name")
+    ap.add_argument("--config5", action="store_true",
+                    help="only the large combined configuration (10M x 128, SQ4 + PQ32, uneven L): one JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -462,6 +470,18 @@ def main():
         dist = replicas.init("nccl", timeout_s=600)
     if torch.cuda.is_available():
         torch.cuda.set_device(local)
+
+    if args.config5:
+        from rover_b200.calculator import Calculator
+        calc = Calculator()
+        dev = torch.device("cuda", local)
+        c5 = config5_section(calc, args, torch.cuda.current_stream(dev), dist, dev, world)
+        if rank == 0:
+            print(json.dumps({"metric": "QPS at recall@10 on 1 B200, large combined configuration "
+                                        "(10M x 128, SQ4 + PQ32, uneven L)", "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "data": "synthetic (seeded Gaussian mixture)",
+                              "config5": c5}, default=float), flush=True)
+        return 0
 
     from rover_b200 import workloads
     w = workloads.build_pq(args.workload, cache_dir=args.cache_dir, verbose=rank == 0)
@@ -801,6 +821,106 @@ def uneven_section(calc, args, stream, dist, dev, world):
                        "kernel_ms_per_step": {k: v[1] / args.steps for k, v in direct["kernels"].items()},
                        "gpu_launches_per_step": direct["launches"] / args.steps},
             "plan_over_direct": plan_qps / direct_qps, "identical_outputs": identical}
+
+
+def config5_section(calc, args, stream, dist, dev, world) -> dict:
+    """The large combined configuration (workloads.LARGE_CONFIGS): 100,000
+    queries with beams uniform in [32, 256] and k = 10 on the 10M x 128 PQ32
+    index, one batch per step through a search plan replayed from a CUDA
+    graph, for the plain exact form, the W-wide batched form and the gated
+    form (gate trained on traces of 2,000 further queries); recall@10 on the
+    first 10,000 queries.  Entry points: the fewest of LARGE_EPS reaching
+    recall@10 >= 0.95 for the plain form.  Then the SQ4 component over the
+    same vectors: the SQMD search with 4-bit codes and 8-bit residual
+    correction, top 20 refined to 10, on the ground-truth queries."""
+    import torch
+    from rover_b200 import datasets as D
+    from rover_b200 import gate as gate_mod
+    from rover_b200 import workloads
+    from rover_b200.workloads import recall_at_k
+    w = workloads.build_large(args.large_workload, calc)
+    cfg = workloads.LARGE_CONFIGS[args.large_workload]
+    log(f"config5 workload ready in {w.build_seconds:.1f}s")
+    calc.pq_load(w.graph, w.entry, w.pq)
+    nq, gq = len(w.queries), len(w.gt)
+    expand = int(w.graph.shape[1])
+    pools = np.random.default_rng(2026).integers(LARGE_L[0], LARGE_L[1] + 1, nq).astype(np.int32)
+    table, ep = [], LARGE_EPS[-1]
+    for ep_ in LARGE_EPS:
+        r = calc.pq_search(w.queries[:gq], pools[:gq], top_k=TOP_K, stats=True, entry_points=ep_,
+                           expand_count=expand, correction=1, refine_budget=LARGE_REFINE)
+        rec = recall_at_k(r["ids"], r["counts"], w.gt, TOP_K)
+        table.append(dict(entry_points=ep_, recall_at_10=rec, scored=float(r["stats"][:, 0].mean()),
+                          expanded=float(r["stats"][:, 2].mean())))
+        log(f"config5 calibration ep={ep_} recall@10={rec:.4f}")
+        if rec >= TARGET_RECALL:
+            ep = ep_
+            break
+    base_kw = dict(entry_points=ep, expand_count=expand, correction=1, refine_budget=LARGE_REFINE)
+    q_d = torch.from_numpy(np.ascontiguousarray(w.queries)).to(dev)
+    out = dict(ids=torch.empty((nq, TOP_K), dtype=torch.int32, device=dev),
+               dists=torch.empty((nq, TOP_K), dtype=torch.float32, device=dev),
+               counts=torch.empty(nq, dtype=torch.int32, device=dev),
+               status=torch.empty(nq, dtype=torch.int32, device=dev))
+    ptrs = {k: v.data_ptr() for k, v in out.items()}
+    ptrs["stride"] = TOP_K
+
+    def form(label, kw):
+        plan = calc.pq_plan(nq, pools, tune_queries_ptr=q_d.data_ptr(), top_k=TOP_K, **kw)
+        info = plan.describe()
+        graph = torch.cuda.CUDAGraph()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph):
+            plan.launch(q_d.data_ptr(), ptrs, torch.cuda.current_stream().cuda_stream)
+        t = device_steps(calc, args, graph.replay, stream, dist, dev)
+        torch.cuda.synchronize()
+        ok = bool(torch.equal(out["status"], torch.zeros_like(out["status"])))
+        ids, counts = out["ids"][:gq].cpu().numpy(), out["counts"][:gq].cpu().numpy()
+        rec = recall_at_k(ids, counts, w.gt, TOP_K)
+        del graph
+        plan.destroy()
+        qps = nq * args.steps * world / (t["total_ms"] / 1e3)
+        log(f"config5 {label}: {qps:,.0f} QPS ({t['ms_per_step']:.2f} ms/step) recall@10={rec:.4f} status_ok={ok}")
+        return dict(qps=qps, ms_per_step=t["ms_per_step"], recall_at_10=rec, all_queries_ok=ok,
+                    kernel_ms_per_step={k: v[1] / args.steps for k, v in t["kernels"].items()},
+                    plan={k: info[k] for k in ("classes", "warps_per_cta", "shared_visited_slots", "layout")},
+                    clocks=t["clocks"])
+
+    res = {"plain": form("plain", dict(base_kw, mode=0))}
+    res["batched"] = form(f"batched W={LARGE_W}", dict(base_kw, mode=1, beam_width=LARGE_W))
+    # the learned gate: traces of 2,000 queries drawn apart from the timed ones
+    train_q = D.gmm(2000, cfg["dim"], cfg["comps"], cfg["seed"] + 7, centers_seed=cfg["seed"], clip_nonneg=True)
+    rows, ids, counts = gate_mod.collect(calc, train_q, 64, top_k=TOP_K, entry_points=ep, expand_count=expand,
+                                         correction=1, refine_budget=LARGE_REFINE)
+    model = gate_mod.train(calc, rows, ids, counts, 64, top_k=TOP_K, max_rows=GATE_ROWS, epochs=GATE_EPOCHS)
+    model.load(calc, refine_logit=0.0, stop_logit=float("inf"))
+    res["gated"] = form(f"gated W={LARGE_W}", dict(base_kw, mode=2, beam_width=LARGE_W))
+    res["gated"]["gate"] = dict(band=[model.band_lo, model.band_hi], refine_logit=0.0, stop_logit="inf",
+                                trace_rows=int(len(rows)), mlp_rows=int(calc.gate_rows()))
+    calc.gate_unload()
+    # SQ4 component on the same vectors
+    calc.pq_unload()
+    calc.sq_load(w.graph, w.entry, w.sq)
+    sq_ep = 2 * ep
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = calc.sq_search(w.queries[:gq], 64, LARGE_REFINE, sq_mode=1, num_out=LARGE_REFINE, entry_points=sq_ep,
+                       expand_count=32, correction=1)
+    ids_r, d_r, c_r = calc.refine(0, w.queries[:gq], r["ids"], np.minimum(r["counts"], LARGE_REFINE), TOP_K)
+    sq_s = time.perf_counter() - t0
+    sq_rec = recall_at_k(ids_r, c_r, w.gt, TOP_K)
+    calc.sq_unload()
+    log(f"config5 sq4: {gq / sq_s:,.0f} QPS end to end, recall@10={sq_rec:.4f}")
+    return {"workload": args.large_workload, "n": cfg["n"], "dim": cfg["dim"], "pq": f"M={cfg['m']}x{cfg['ks']}",
+            "pq_trainer": "calculator_rover_pq_train (GPU, the reference's k-means bit for bit)",
+            "sq": f"{cfg['l1_bits']}-bit global codec + {cfg['sq_rbits']}-bit residuals",
+            "graph_degree": expand, "queries_per_step": nq, "recall_queries": gq,
+            "beam_L": f"uniform [{LARGE_L[0]}, {LARGE_L[1]}]", "top_k": TOP_K, "refine_budget": LARGE_REFINE,
+            "entry_points": ep, "calibration": table, "build_seconds": w.build_seconds, "forms": res,
+            "batched_over_plain": res["batched"]["qps"] / res["plain"]["qps"],
+            "gated_over_plain": res["gated"]["qps"] / res["plain"]["qps"],
+            "sq4": dict(queries=gq, L=64, entry_points=sq_ep, expand_count=32, refine=f"top {LARGE_REFINE} -> 10",
+                        e2e_qps=gq / sq_s, recall_at_10=sq_rec)}
 
 
 def timed_form(calc, args, w, q_d, L, kw, stream, dist, dev, world):

@@ -357,6 +357,99 @@ def navigable_graph(base: np.ndarray, candidates: int, degree: int, alpha: float
     return out
 
 
+def clustered_graph(base: np.ndarray, centers: np.ndarray, candidates: int, degree: int, alpha: float,
+                    long_edges: int = 8, probe: int = 3, device=None, margin: int = 16) -> np.ndarray:
+    """The navigable_graph recipe for indexes too large for an all-pairs
+    k-NN pass: every point belongs to its nearest centre's cluster, and its
+    ``candidates`` nearest neighbours are searched among the members of its
+    own cluster and of the ``probe - 1`` clusters whose centres are nearest
+    that cluster's centre (a TF32 Gram pass picks candidates + margin, exact
+    float32 differences order them, ties by lower id).  The lists are
+    alpha-pruned to ``degree - long_edges`` neighbours, and the remaining
+    slots hold representatives (the member nearest the centre) of the
+    nearest other clusters, each admitted only if no kept neighbour occludes
+    it (alpha * d(k, c) <= d(p, c)).  Fixture construction, not the search
+    path."""
+    dev = _device(device)
+    n, dim = base.shape
+    k_clusters = centers.shape[0]
+    knn = np.full((n, candidates), -1, dtype=np.int32)
+    with torch.no_grad():
+        x = torch.from_numpy(np.ascontiguousarray(base)).to(dev)
+        c = torch.from_numpy(np.ascontiguousarray(centers, dtype=np.float32)).to(dev)
+        cn = (c * c).sum(1)
+        labels = torch.empty(n, dtype=torch.long, device=dev)
+        for s in range(0, n, 1 << 16):
+            labels[s:s + (1 << 16)] = torch.argmin(cn[None, :] - 2.0 * (x[s:s + (1 << 16)] @ c.T), dim=1)
+        order = torch.argsort(labels, stable=True)
+        counts = torch.bincount(labels, minlength=k_clusters)
+        starts = torch.cumsum(counts, 0) - counts
+        near = torch.topk(torch.cdist(c, c), min(probe, k_clusters), dim=1, largest=False).indices
+        counts_h, starts_h, near_h = counts.cpu().numpy(), starts.cpu().numpy(), near.cpu().numpy()
+        old_tf32 = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = True
+        try:
+            for cl in range(k_clusters):
+                if counts_h[cl] == 0:
+                    continue
+                mine = order[starts_h[cl]:starts_h[cl] + counts_h[cl]]
+                pool = torch.cat([order[starts_h[o]:starts_h[o] + counts_h[o]] for o in near_h[cl]])
+                q, b = x[mine], x[pool]
+                d = (b * b).sum(1)[None, :] - 2.0 * (q @ b.T)
+                d[mine[:, None] == pool[None, :]] = float("inf")
+                kk = min(candidates + margin, pool.shape[0])
+                cand = pool[torch.topk(d, kk, dim=1, largest=False).indices]
+                diff = q[:, None, :] - x[cand]
+                exact = (diff * diff).sum(2)
+                exact[cand == mine[:, None]] = float("inf")
+                ids_sorted, perm = torch.sort(cand, dim=1)
+                exact = torch.gather(exact, 1, perm)
+                pick = torch.sort(exact, dim=1, stable=True).indices[:, :candidates]
+                best = torch.gather(ids_sorted, 1, pick)
+                bad = torch.gather(exact, 1, pick) == float("inf")
+                best[bad] = -1
+                got = best.shape[1]
+                knn[mine.cpu().numpy(), :got] = best.int().cpu().numpy()
+        finally:
+            torch.backends.cuda.matmul.allow_tf32 = old_tf32
+    intra = alpha_prune(base, knn, degree - long_edges, alpha, device=device)
+    out = np.full((n, degree), -1, dtype=np.int32)
+    out[:, :degree - long_edges] = intra
+    with torch.no_grad():
+        lab = labels
+        dc = ((x - c[lab]) ** 2).sum(1)
+        rep = torch.full((k_clusters,), -1, dtype=torch.long, device=dev)
+        order_d = torch.argsort(dc, descending=True)
+        rep[lab[order_d]] = order_d          # last write wins = nearest member
+        a2 = float(alpha) * float(alpha)
+        want = long_edges + 1
+        chunk = 16384
+        for s in range(0, n, chunk):
+            xs = x[s:s + chunk]
+            bsz = xs.shape[0]
+            nc = torch.topk(cn[None, :] - 2.0 * (xs @ c.T), min(want, k_clusters), dim=1, largest=False).indices
+            cand = rep[nc]
+            ids = torch.arange(s, s + bsz, device=dev)
+            cand = torch.where((cand == ids[:, None]) | (lab[s:s + bsz, None] == nc) | (cand < 0), -1, cand)
+            kept = torch.from_numpy(out[s:s + bsz]).to(dev).long()
+            dpc = ((x[cand.clamp_min(0)] - xs[:, None, :]) ** 2).sum(2)
+            cnt = (kept >= 0).sum(1)
+            for i in range(cand.shape[1]):
+                ci = cand[:, i]
+                cv = x[ci.clamp_min(0)]
+                kv = x[kept.clamp_min(0)]
+                dkc = ((kv - cv[:, None, :]) ** 2).sum(2)
+                occl = ((kept >= 0) & (a2 * dkc <= dpc[:, i:i + 1])).any(1)
+                dup = (kept == ci[:, None]).any(1)
+                take = (ci >= 0) & ~occl & ~dup & (cnt < degree)
+                rows = torch.nonzero(take, as_tuple=True)[0]
+                kept[rows, cnt[rows]] = ci[rows]
+                cnt = cnt + take.long()
+            out[s:s + bsz] = kept.int().cpu().numpy()
+        del x
+    return out
+
+
 def routed_graph(base: np.ndarray, candidates: int, degree: int, alpha: float, long_edges: int = 8,
                  clusters: int | None = None, entry: int | None = None, device=None) -> tuple[np.ndarray, int]:
     """``navigable_graph`` plus a two-level routing structure so that a beam

@@ -85,6 +85,74 @@ def build_sq(name: str, device=None, gt_k: int = 100) -> SqWorkload:
     return SqWorkload(name, queries, gt, graph, entry, bundle, time.time() - t0)
 
 
+# The large combined configuration: base n=10,000,000 d=128 from a
+# 4,096-component mixture (centres N(0, 4I), sigma 0.5) clipped to >= 0;
+# 100,000 queries (recall on the first 10,000, exact top-100 ground truth);
+# a degree-32 graph (48-NN within each point's and the two nearest other
+# clusters, alpha=1.2 pruned to 24, plus up to 8 long-range edges:
+# datasets.clustered_graph); PQ M=32 x 256 trained and encoded by the
+# library's own GPU trainer (calculator_rover_pq_train over 100,000
+# uniform-stride samples, 25 iterations; calculator_rover_pq_encode) with
+# 8-bit residuals; and over the same vectors the 4-bit global SQ codec with
+# 8-bit residuals.
+LARGE_CONFIGS = {
+    "pq_10m_d128": dict(n=10_000_000, dim=128, comps=4096, nq=100_000, gt_queries=10_000, cand=48, degree=32,
+                        alpha=1.2, probe=3, m=32, ks=256, iters=25, rbits=8, l1_bits=4, sq_rbits=8, seed=2026),
+    # the same recipe at 100K (parity tests against the compiled reference)
+    "pq_c5_100k": dict(n=100_000, dim=128, comps=256, nq=2_000, gt_queries=1_000, cand=48, degree=32,
+                       alpha=1.2, probe=3, m=32, ks=256, iters=10, rbits=8, l1_bits=4, sq_rbits=8, seed=2027),
+}
+
+
+@dataclass
+class LargeWorkload:
+    name: str
+    queries: np.ndarray
+    gt: np.ndarray            # [gt_queries][100]
+    graph: np.ndarray
+    entry: int
+    pq: B.PqBundle
+    sq: B.SqBundle
+    build_seconds: float = 0.0
+
+
+def build_large(name: str, calc, device=None, verbose: bool = True) -> LargeWorkload:
+    """The combined large configuration, built on the GPU (see LARGE_CONFIGS)."""
+    cfg = LARGE_CONFIGS[name]
+    t0 = time.time()
+    log = (lambda *a: print(f"[workload {name} {time.time() - t0:6.1f}s]", *a, file=sys.stderr, flush=True)) \
+        if verbose else (lambda *a: None)
+    n, dim = cfg["n"], cfg["dim"]
+    base, centers = D.gmm(n, dim, cfg["comps"], cfg["seed"], clip_nonneg=True, return_centers=True)
+    queries = D.gmm(cfg["nq"], dim, cfg["comps"], cfg["seed"] + 1, centers_seed=cfg["seed"], clip_nonneg=True)
+    log("vectors")
+    gt = D.exact_knn(queries[:cfg["gt_queries"]], base, 100, device=device)
+    log("ground truth")
+    graph = D.clustered_graph(base, np.maximum(centers, 0.0), cfg["cand"], cfg["degree"], cfg["alpha"],
+                              long_edges=8, probe=cfg["probe"], device=device)
+    entry = D.medoid(base, device=device)
+    log("graph", f"mean degree {float((graph >= 0).sum(1).mean()):.1f}")
+    sample = base[D.uniform_positions(n, min(n, 100_000))]
+    book = calc.pq_train(sample, cfg["m"], cfg["ks"], cfg["iters"])
+    codes = calc.pq_encode(base, book)
+    rcb = dim if cfg["rbits"] == 8 else (dim + 1) // 2
+    rows = np.empty((n, rcb), dtype=np.uint8)
+    qp = np.empty((n, 2), dtype=np.float32)
+    for s0 in range(0, n, 1 << 20):
+        sl = slice(s0, min(n, s0 + (1 << 20)))
+        rows[sl], qp[sl] = D.quantize_residual_rint(base[sl] - D.pq_reconstruct(codes[sl], book), cfg["rbits"])
+    md = B.PqMeta(hashlib.sha256(name.encode()).digest()[:16], n, dim, cfg["m"], cfg["ks"], dim // cfg["m"],
+                  B.pq_code_bytes(cfg["m"], cfg["ks"]), train_count=len(sample), kmeans_iters=cfg["iters"],
+                  seed=cfg["seed"])
+    pq = B.PqBundle(md, book, codes, cfg["rbits"], B.pack_residual_blocks(rows), qp)
+    del rows
+    log("pq codes + residuals (GPU trainer and encoder)")
+    scale, zero, l1, res, sqp = D.sq_encode(base, cfg["l1_bits"], cfg["sq_rbits"], chunk=1 << 18)
+    sq = B.SqBundle(n, dim, cfg["l1_bits"], scale, zero, l1, cfg["sq_rbits"], res, sqp)
+    log("sq4 codes + residuals")
+    return LargeWorkload(name, queries, gt, graph, entry, pq, sq, time.time() - t0)
+
+
 def _key(cfg: dict) -> str:
     return hashlib.sha256(json.dumps(cfg, sort_keys=True).encode()).hexdigest()[:16]
 
