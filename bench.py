@@ -901,7 +901,7 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
     # SQ4 component on the same vectors
     calc.pq_unload()
     calc.sq_load(w.graph, w.entry, w.sq)
-    sq_ep = 2 * ep
+    sq_ep = ep
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     r = calc.sq_search(w.queries[:gq], 64, LARGE_REFINE, sq_mode=1, num_out=LARGE_REFINE, entry_points=sq_ep,

@@ -67,6 +67,7 @@ def exact_knn(queries: np.ndarray, base: np.ndarray, k: int, exclude_self: bool 
             b = torch.from_numpy(np.ascontiguousarray(base)).to(dev)
             bn = (b * b).sum(1)
             kk = min(k + margin + (1 if exclude_self else 0), b.shape[0])
+            chunk = max(16, min(chunk, (1 << 30) // max(1, b.shape[0])))   # distance block <= 4 GB
             out = np.empty((queries.shape[0], k), dtype=np.int32)
             for s in range(0, queries.shape[0], chunk):
                 q = torch.from_numpy(np.ascontiguousarray(queries[s:s + chunk])).to(dev)
