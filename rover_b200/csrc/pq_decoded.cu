@@ -207,11 +207,17 @@ __global__ void pq_seed_gather_kernel(const float* __restrict__ decoded, int dim
   }
 }
 
-// One CTA per row: a radix select (8 bits per pass, MSB first) finds the
-// (m+1)-th smallest rank t; the ranks below t and the ones equal to it are
-// gathered as keys (rank, seed index), sorted, and the first m written.
-// Ranks are non-negative floats (the rank kernel clamps at zero), so their
-// bit patterns order as unsigned integers; a non-finite rank marks the row.
+// One CTA per row.  The ranks are non-negative floats (the rank kernel
+// clamps at zero), so their bit patterns order as unsigned integers.  A first
+// pass finds the row's smallest and largest bits; every rank shares their
+// common leading bits, so one 256-bin histogram of the next 8 bits finds the
+// bin b that holds the (m+1)-th smallest rank.  Every rank up to the end of
+// bin b is gathered as a key (rank, seed index) and sorted; the first m are
+// the row's m smallest, and the (m+1)-th is among them.  When bin b holds
+// too many ranks to gather, a radix select of 8 bits per pass (MSB first)
+// finds the (m+1)-th rank t exactly and the ranks <= t are gathered instead.
+// A non-finite rank, or more than kTopGather ranks <= t, marks the row for a
+// scan by the search kernel (empty keys, NaN next).
 constexpr int kTopThreads = 128;
 constexpr int kTopGather = 2048;   // gathered keys held in shared memory
 
@@ -221,6 +227,7 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
                                                                    float* __restrict__ next) {
   __shared__ unsigned hist[256];
   __shared__ unsigned s_prefix, s_mask, s_remaining, s_count;
+  __shared__ unsigned s_lo[kTopThreads / kWarp], s_hi[kTopThreads / kWarp];
   __shared__ uint64_t gathered[kTopGather];
   const int row = blockIdx.x;
   if (row >= rows) return;
@@ -228,16 +235,36 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
   const int tid = threadIdx.x;
   auto bits_at = [&](int e) -> uint32_t { return __float_as_uint(__ldg(r + e) + 0.0f); };
   bool bad = false;
-  for (int e = tid; e < n_seeds; e += kTopThreads) bad |= !(__ldg(r + e) < 3.0e38f);
+  uint32_t lo = 0xffffffffu, hi = 0u;
+  for (int e = tid; e < n_seeds; e += kTopThreads) {
+    const float x = __ldg(r + e);
+    bad |= !(x < 3.0e38f);
+    const uint32_t v = __float_as_uint(x + 0.0f);
+    lo = min(lo, v);
+    hi = max(hi, v);
+  }
   uint64_t* out = keys + static_cast<size_t>(row) * m;
   if (__syncthreads_or(bad)) {
     for (int i = tid; i < m; i += kTopThreads) out[i] = kEmptyKey;
     if (tid == 0) next[row] = __int_as_float(0x7fc00000);
     return;
   }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    lo = min(lo, __shfl_xor_sync(kFullMask, lo, off));
+    hi = max(hi, __shfl_xor_sync(kFullMask, hi, off));
+  }
+  if ((tid & 31) == 0) { s_lo[tid >> 5] = lo; s_hi[tid >> 5] = hi; }
+  __syncthreads();
+  lo = s_lo[0];
+  hi = s_hi[0];
+#pragma unroll
+  for (int w = 1; w < kTopThreads / kWarp; ++w) { lo = min(lo, s_lo[w]); hi = max(hi, s_hi[w]); }
   const int target = min(m + 1, n_seeds);   // rank (1-based) of the value to find
-  if (tid == 0) { s_prefix = 0u; s_mask = 0u; s_remaining = static_cast<unsigned>(target); }
-  for (int shift = 24; shift >= 0; shift -= 8) {
+
+  // One histogram pass over bits [shift, shift + 8) of the ranks matching
+  // (prefix, mask); narrows prefix / mask / remaining to the target's bin.
+  auto radix_pass = [&](int shift) {
     for (int i = tid; i < 256; i += kTopThreads) hist[i] = 0u;
     __syncthreads();
     const unsigned prefix = s_prefix, mask = s_mask;
@@ -275,19 +302,37 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
       }
     }
     __syncthreads();
-  }
-  const uint32_t t = s_prefix;   // the target-th smallest rank's bits
-  if (tid == 0) s_count = 0u;
-  __syncthreads();
-  for (int e = tid; e < n_seeds; e += kTopThreads) {
-    const uint32_t v = bits_at(e);
-    if (v <= t) {
-      const unsigned slot = atomicAdd(&s_count, 1u);
-      if (slot < kTopGather) gathered[slot] = (static_cast<uint64_t>(v) << 32) | static_cast<uint32_t>(e);
+  };
+  // Gathers every rank <= t as a key; returns how many there are.
+  auto gather = [&](uint32_t t) -> int {
+    if (tid == 0) s_count = 0u;
+    __syncthreads();
+    for (int e = tid; e < n_seeds; e += kTopThreads) {
+      const uint32_t v = bits_at(e);
+      if (v <= t) {
+        const unsigned slot = atomicAdd(&s_count, 1u);
+        if (slot < kTopGather) gathered[slot] = (static_cast<uint64_t>(v) << 32) | static_cast<uint32_t>(e);
+      }
     }
-  }
+    __syncthreads();
+    return static_cast<int>(s_count);
+  };
+
+  // the 8 bits below the leading bits every rank shares
+  const int common = lo == hi ? 32 : __clz(lo ^ hi);
+  const int first = max(0, 24 - common);
+  const unsigned top = first + 8 >= 32 ? 0u : (0xffffffffu << (first + 8));
+  if (tid == 0) { s_prefix = lo & top; s_mask = top; s_remaining = static_cast<unsigned>(target); }
   __syncthreads();
-  const int cnt = static_cast<int>(s_count);
+  radix_pass(first);
+  int cnt = gather(s_prefix | ((1u << first) - 1u));   // every rank up to the end of the target's bin
+  if (cnt > kTopGather) {
+    // a crowded bin: the exact (m+1)-th rank, 8 bits per pass from the top
+    if (tid == 0) { s_prefix = 0u; s_mask = 0u; s_remaining = static_cast<unsigned>(target); }
+    __syncthreads();
+    for (int shift = 24; shift >= 0; shift -= 8) radix_pass(shift);
+    cnt = gather(s_prefix);
+  }
   if (cnt > kTopGather) {   // a flood of equal ranks: let the search kernel scan the row
     for (int i = tid; i < m; i += kTopThreads) out[i] = kEmptyKey;
     if (tid == 0) next[row] = __int_as_float(0x7fc00000);
