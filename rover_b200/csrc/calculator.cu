@@ -535,9 +535,9 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
                             cudaStream_t stream) {
   PqDevice& pq = s.pq;
   if (ensure_seeds(s, pq, p->entry_points, p->seed) != AEE_SUCCESS) return AEE_ENOMEMORY;
-  // pools up to kMaxBatch: TF32-ranked seeds verified exactly in the kernel;
+  // pools up to kVerifyMaxPool: TF32-ranked seeds verified exactly in the kernel;
   // wider pools: every seed's exact distance up front
-  const bool verify = a.max_pool <= kMaxBatch;
+  const bool verify = a.max_pool <= kVerifyMaxPool;
   if (verify && ensure_seed_drows(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
   const SeedSet& ss = pq.seeds;
   PqDecodedArgs b{};
@@ -795,9 +795,9 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
   if (allow_smem(reinterpret_cast<const void*>(kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   const int max_blocks = resident_blocks(reinterpret_cast<const void*>(kernel), kSearchWarps * 32, smem, s.sms);
   // exact seed pools: verified from TF32 ranks of the seeds' decoded rows
-  // when every pool fits kMaxBatch (as the exact decoded search does), else
+  // when every pool fits kVerifyMaxPool (as the exact decoded search does), else
   // the all-seeds exact distance pass
-  const bool verify = !gated && !tracing && a.max_pool <= kMaxBatch;
+  const bool verify = !gated && !tracing && a.max_pool <= kVerifyMaxPool;
   const bool seed_pass = !gated && !verify;   // exact seed distances
   const bool rank_pass = rows;                // quantized seed distances (tensor cores)
   if (rank_pass && ensure_seed_recon(s, pq) != AEE_SUCCESS) return AEE_EFAILED;
@@ -1319,7 +1319,7 @@ struct PqPlanImpl : RoverPqPlan {
   DevBuf drows, drow_norms;             // exact plans: the seeds' decoded rows for the verified seed pool
   DevBuf seed_top, seed_top_next;       // per query: top-M seed ranks (verified and gated plans)
   int32_t top_m = 0;
-  bool verify_seeds = false;            // exact decoded plan with every pool <= kMaxBatch
+  bool verify_seeds = false;            // exact / batched decoded plan, every pool <= kVerifyMaxPool
   int32_t seed_stride = 0;              // floats per query row of seed_dists
   float drow_norm_max = 0.0f;
   size_t device_bytes() const {
@@ -1666,7 +1666,8 @@ AEEResult plan_inputs(State& s, PqPlanImpl& P) {
   CK(cudaMemcpyAsync(P.seed_ids.p, ss.ids.p, static_cast<size_t>(ss.count) * 4, cudaMemcpyDeviceToDevice, s.stream));
   CK(cudaMemcpyAsync(P.seed_bits.p, ss.bits.p, bits_bytes, cudaMemcpyDeviceToDevice, s.stream));
   if (!P.allow_decoded) return AEE_SUCCESS;
-  P.verify_seeds = P.p.mode == ROVER_MODE_EXACT && P.max_pool <= kMaxBatch && !P.gated;
+  P.verify_seeds = (P.p.mode == ROVER_MODE_EXACT || P.p.mode == ROVER_MODE_BATCHED) &&
+                  P.max_pool <= kVerifyMaxPool && !P.gated;
   P.seed_stride = P.verify_seeds ? (ss.count + 3) / 4 * 4 : ss.count;
   const size_t seed_bytes = static_cast<size_t>(P.nq) * P.seed_stride * sizeof(float);
   if (seed_bytes > kPlanSeedBytes) {

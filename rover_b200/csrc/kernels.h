@@ -12,6 +12,7 @@ namespace rover {
 constexpr int kSearchWarps = 4;   // query warps per CTA (default)
 constexpr int kMaxSearchWarps = 8;  // decoded / batched kernels take 1..8 warps per CTA (blockDim.x / 32)
 constexpr int kMaxBatch = 128;    // max neighbours scored per expansion
+constexpr int kVerifyMaxPool = 512;   // widest pool the verified seed pool serves (top-M of max(2L, L + 64))
 
 struct PqSearchArgs {
   PqIndexView ix;

@@ -320,7 +320,7 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       if (!tracing && b.seed_verify) {
         const float* arow = b.seed_dists + seed_row_index * b.seed_stride;
         if (st == kStatusOk) {
-          if (cap > kMaxBatch) st = kStatusBadParam;
+          if (cap > kVerifyMaxPool) st = kStatusBadParam;
           else if (!verified_seed_pool<D>(list, &size, cap, stage, batch, b, arow,
                                           b.seed_top ? b.seed_top + seed_row_index * b.top_m : nullptr,
                                           b.seed_top ? b.seed_top_next[seed_row_index] : 0.0f, q, dim, &cursor,

@@ -630,8 +630,8 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
     // ---- initial pool: top-L of the seed row under (distance, id)
     const float* drow = b.seed_dists + seed_row;
     if (b.seed_verify) {
-      // the host sets seed_verify only when every pool fits kMaxBatch
-      if (cap > kMaxBatch) st = kStatusBadParam;
+      // the host sets seed_verify only when every pool fits kVerifyMaxPool
+      if (cap > kVerifyMaxPool) st = kStatusBadParam;
       else if (!verified_seed_pool<D>(list, &size, cap, stage, batch, b, drow,
                                       b.seed_top ? b.seed_top + seed_row_index * b.top_m : nullptr,
                                       b.seed_top ? b.seed_top_next[seed_row_index] : 0.0f,

@@ -77,7 +77,7 @@ __device__ __forceinline__ bool exact_batch(uint64_t* list, int* size, int cap, 
   return true;
 }
 
-// The exact top-cap (cap <= kMaxBatch) of the seeds into list; false if an
+// The exact top-cap (cap <= kVerifyMaxPool) of the seeds into list; false if an
 // exact distance is non-finite (the query then fails as in the all-seeds
 // pass).  Keys of the first set and of the scans are (rank, seed index).
 // top / next: this query's top-M ranks from pq_seed_topm_kernel (null, or a
@@ -100,7 +100,8 @@ __device__ bool verified_seed_pool(uint64_t* list, int* size, int cap, uint64_t*
   if (have_top) {
     s1 = min(cap, n);
     last = key_cmp(top[s1 - 1]);
-    for (int k = lane; k < s1; k += kWarp) cand[k] = __ldg(b.seed_ids + key_id(top[k]));
+  } else if (!all && cap > kMaxBatch) {
+    all = true;   // no top-M list for a pool wider than one batch: compute every seed
   } else if (!all) {
     if (select_top_lanes(list, size, cap, stage, n, SeedIndexKeys{arow}, cursor, lane)) {
       s1 = *size;
@@ -114,7 +115,20 @@ __device__ bool verified_seed_pool(uint64_t* list, int* size, int cap, uint64_t*
   *size = 0;
   *cursor = 0;
   float U = 0.0f;
-  if (s1 > 0 && !exact_batch<D>(list, size, cap, stage, cand, s1, b.decoded, q, dim, cursor, &U, lane)) return false;
+  if (have_top) {
+    // the first set, kMaxBatch seeds at a time; U is the largest distance
+    for (int c0 = 0; c0 < s1; c0 += kMaxBatch) {
+      const int cn = min(kMaxBatch, s1 - c0);
+      for (int k = lane; k < cn; k += kWarp) cand[k] = __ldg(b.seed_ids + key_id(top[c0 + k]));
+      __syncwarp();
+      float u = 0.0f;
+      if (!exact_batch<D>(list, size, cap, stage, cand, cn, b.decoded, q, dim, cursor, &u, lane)) return false;
+      U = fmaxf(U, u);
+      __syncwarp();
+    }
+  } else if (s1 > 0 && !exact_batch<D>(list, size, cap, stage, cand, s1, b.decoded, q, dim, cursor, &U, lane)) {
+    return false;
+  }
   if (!all && s1 < cap) return true;   // every seed is in
   // With xmax the largest seed norm, A - eps <= U implies A <= T: one
   // comparison rules out almost every other seed; the few that pass take the

@@ -114,8 +114,9 @@ def test_tuned_plan_keeps_a_timed_candidate(calc):
     info = plan.describe()
     assert info["candidates"] >= 10
     assert 0 < info["tuned_ms"] <= info["default_ms"]
-    # bookkeeping x2, seed pass (decoded; plus the top-M selection when every pool fits 128), one per class
-    assert info["launches"] == 2 + (info["layout"] == DECODED) * (1 + (info["max_pool"] <= 128)) + info["classes"]
+    # bookkeeping x2, seed pass (decoded; plus the top-M selection when every pool fits the verified
+    # seed pool's 512), one per class
+    assert info["launches"] == 2 + (info["layout"] == DECODED) * (1 + (info["max_pool"] <= 512)) + info["classes"]
     _same(_run_plan(torch, plan, q_dev, nq, int(ks.max()), stride), _direct(calc, queries, pools, ks, stride))
     plan.destroy()
 
