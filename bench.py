@@ -902,12 +902,18 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
     calc.pq_unload()
     calc.sq_load(w.graph, w.entry, w.sq)
     sq_ep = ep
+
+    def sq_call():
+        r = calc.sq_search(w.queries[:gq], 64, LARGE_REFINE, sq_mode=1, num_out=LARGE_REFINE, entry_points=sq_ep,
+                           expand_count=32, correction=1)
+        return calc.refine(0, w.queries[:gq], r["ids"], np.minimum(r["counts"], LARGE_REFINE), TOP_K)
+
+    sq_call()                      # warm-up: scratch allocation and first launches
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    r = calc.sq_search(w.queries[:gq], 64, LARGE_REFINE, sq_mode=1, num_out=LARGE_REFINE, entry_points=sq_ep,
-                       expand_count=32, correction=1)
-    ids_r, d_r, c_r = calc.refine(0, w.queries[:gq], r["ids"], np.minimum(r["counts"], LARGE_REFINE), TOP_K)
-    sq_s = time.perf_counter() - t0
+    for _ in range(args.steps):
+        ids_r, d_r, c_r = sq_call()
+    sq_s = (time.perf_counter() - t0) / args.steps
     sq_rec = recall_at_k(ids_r, c_r, w.gt, TOP_K)
     calc.sq_unload()
     log(f"config5 sq4: {gq / sq_s:,.0f} QPS end to end, recall@10={sq_rec:.4f}")
