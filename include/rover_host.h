@@ -125,6 +125,17 @@ int rover_split_bias_open(const RoverBundle *b, const char *path, float **out);
 /* message of the last failed artifact call on this thread */
 const char *rover_artifact_error(void);
 
+/* ---- neighbourhood-aware layout ---- */
+/* The reference's clustered block ordering of a graph's ids (rover-layout,
+ * src/graph/layout_opt_kmeans.cpp:55-712): graph [n][degree] (-1 padded
+ * rows), one cluster label per node in [0, clusters); new_to_old[n]
+ * receives, per new id, the old id.  rrf_c, max_reverse (0 = no limit),
+ * use_cn / use_mnn as the tool's arguments; `threads` host threads.
+ * 0 on success, -1 on invalid input. */
+int rover_layout_order(const int32_t *graph, int32_t n, int32_t degree, const int32_t *labels, int32_t clusters,
+                       int32_t vectors_per_block, double rrf_c, int32_t max_reverse, int32_t use_cn,
+                       int32_t use_mnn, int32_t threads, int32_t *new_to_old);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ HOST_LIB = LIB_DIR / "librover_host.so"
 BIN_DIR = HERE / "bin"
 ROVER = BIN_DIR / "Rover"
 HOST_SOURCES = ["sha256.c", "json.c", "bundle.c", "artifacts.c"]
+HOST_CXX_SOURCES = ["layout.cpp"]
 
 SOURCES = ["calculator.cu", "pq_search.cu", "pq_decoded.cu", "pq_batched.cu", "gate_train.cu", "plan.cu", "sq_search.cu", "distance.cu", "sessions.cu", "seed_rank_tc.cu", "pq_train.cu", "rpcmem_compat.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -90,9 +91,18 @@ def build_host(force: bool = False) -> Path:
     include = HERE.parent / "include"
     headers = list(HOST_DIR.glob("*.h")) + list(include.glob("*.h"))
     srcs = [HOST_DIR / s for s in HOST_SOURCES]
+    cxx_srcs = [HOST_DIR / s for s in HOST_CXX_SOURCES]
     flags = ["-std=c11", "-O2", "-Wall", "-Wextra", "-Wno-unused-parameter", "-I", str(include), "-I", str(HOST_DIR)]
-    if force or _stale(HOST_LIB, [*srcs, *headers]):
-        subprocess.run([cc(), *flags, "-fPIC", "-shared", "-o", str(HOST_LIB), *map(str, srcs), "-lm"], check=True)
+    if force or _stale(HOST_LIB, [*srcs, *cxx_srcs, *headers]):
+        objs = []
+        for s_ in cxx_srcs:   # C++ parts (the layout tool) compiled apart, linked into the same library
+            o = LIB_DIR / (s_.stem + ".host.o")
+            subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-fPIC", "-c", str(s_), "-o", str(o)], check=True)
+            objs.append(str(o))
+        subprocess.run([cc(), *flags, "-fPIC", "-shared", "-o", str(HOST_LIB), *map(str, srcs), *objs, "-lm",
+                        "-lstdc++", "-lpthread"], check=True)
+        for o in objs:
+            Path(o).unlink()
     cli = HOST_DIR / "rover_cli.c"
     if force or _stale(ROVER, [cli, HOST_LIB, LIB, *headers]):
         subprocess.run([cc(), *flags, "-o", str(ROVER), str(cli), "-L", str(LIB_DIR), "-lrover_host", "-lcalculator",
