@@ -54,3 +54,24 @@ def permute_pq(w, new_to_old: np.ndarray):
                         B.pack_residual_blocks(rows), np.ascontiguousarray(b.qparams[n2o]))
     gt = np.where(w.gt >= 0, o2n[np.maximum(w.gt, 0)], -1).astype(np.int32)
     return replace(w, graph=graph, entry=int(o2n[w.entry]), bundle=bundle, gt=gt), new_to_old
+
+
+def gorder_workload(w, per_block: int = 32, threads: int | None = None):
+    """The workload's layout by gorder, clustered by the nearest mixture
+    centre (the mixture the workload was drawn from; rover_b200.workloads
+    CONFIGS).  Returns (workload, new_to_old)."""
+    import torch
+    from . import datasets as D
+    from .workloads import CONFIGS
+    cfg = CONFIGS[w.name]
+    base, centers = D.gmm(cfg["n"], cfg["dim"], cfg["comps"], cfg["seed"], clip_nonneg=cfg["clip"],
+                          normalize=cfg["normalize"], return_centers=True)
+    dev = torch.device("cuda" if torch.cuda.is_available() else "cpu")
+    with torch.no_grad():
+        x = torch.from_numpy(base).to(dev)
+        c = torch.from_numpy(np.ascontiguousarray(centers, dtype=np.float32)).to(dev)
+        cn = (c * c).sum(1)
+        labels = torch.cat([torch.argmin(cn[None, :] - 2.0 * (x[s:s + 65536] @ c.T), dim=1)
+                            for s in range(0, x.shape[0], 65536)]).int().cpu().numpy()
+    n2o = gorder(w.graph, labels, int(centers.shape[0]), per_block, threads=threads)
+    return permute_pq(w, n2o)

@@ -47,6 +47,8 @@ def main(argv=None) -> int:
     ap.add_argument("--W", type=int, default=2)
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--cache-dir", default=os.environ.get("ROVER_BENCH_CACHE", "/tmp/rover_bench_cache"))
+    ap.add_argument("--layout", default="original", choices=("original", "gorder"),
+                    help="gorder: the index in the neighbourhood-aware id order (rover_b200.layout)")
     args = ap.parse_args(argv)
 
     from . import workloads
@@ -54,6 +56,9 @@ def main(argv=None) -> int:
     if args.form in ("score", "refine"):
         return distance_case(args)
     w = workloads.build_pq(args.workload, cache_dir=args.cache_dir, verbose=False)
+    if args.layout == "gorder":
+        from .layout import gorder_workload
+        w, _ = gorder_workload(w)
     calc = Calculator()
     calc.pq_load(w.graph, w.entry, w.bundle)
     q = np.ascontiguousarray(w.queries[:args.queries])
@@ -75,12 +80,13 @@ def main(argv=None) -> int:
     warm = calc.launch_count() - l0
     calc.kernel_timing(True)
     for _ in range(args.repeat):
-        calc.pq_search(q, args.L, **kw)
+        r = calc.pq_search(q, args.L, **kw)
     times = {k: v[1] / args.repeat for k, v in calc.kernel_times().items() if v[0] > 0}
     calc.kernel_timing(False)
-    print(json.dumps(dict(form=args.form, workload=args.workload, queries=len(q), L=args.L, entry_points=args.ep,
-                          beam_width=args.W if args.form in ("batched", "gated") else None,
-                          warm_launches=warm, kernel_ms=times)), flush=True)
+    recall = workloads.recall_at_k(r["ids"], r["counts"], w.gt[:len(q)], 10) if args.repeat > 0 else None
+    print(json.dumps(dict(form=args.form, workload=args.workload, layout=args.layout, queries=len(q), L=args.L,
+                          entry_points=args.ep, beam_width=args.W if args.form in ("batched", "gated") else None,
+                          warm_launches=warm, kernel_ms=times, recall_at_10=recall)), flush=True)
     calc.close()
     return 0
 
