@@ -451,6 +451,7 @@ def main():
     ap.add_argument("--train-queries", type=int, default=TRAIN_QUERIES)
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch plan section")
     ap.add_argument("--no-sq", action="store_true", help="skip the SQ section")
+    ap.add_argument("--no-layout", action="store_true", help="skip the neighbourhood-aware layout section")
     ap.add_argument("--large-workload", default=LARGE_WORKLOAD, help="with --config5: workloads.LARGE_CONFIGS name")
     ap.add_argument("--config5", action="store_true",
                     help="only the large combined configuration (10M x 128, SQ4 + PQ32, uneven L): one JSON line")
@@ -560,6 +561,11 @@ def main():
     h2d = nq * md.dim * 4 + nq * 4
     d2h = nq * TOP_K * 8 + nq * 8
 
+    lay = None
+    if not args.no_layout:
+        lay = layout_section(calc, args, w, L, plain_kw, forms, stream, dist, dev, world)
+        calc.pq_load(w.graph, w.entry, w.bundle)      # the original id order for the sections below
+
     dk = None
     if rank == 0 and not args.no_distance_kernels:
         dk = distance_kernels(calc, w, args)
@@ -601,6 +607,7 @@ def main():
                    "gated_over_plain": head["qps"] / plain_qps if gated else None,
                    "forms": forms["report"] if forms else None,
                    "uneven": uneven,
+                   "layout_gorder": lay,
                    "sq": sq,
                    "parallelism": f"replicas x{world}",
                    "l2": "index (>800 MB with decoded rows) larger than L2; no flush"},
@@ -927,6 +934,32 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
             "gated_over_plain": res["gated"]["qps"] / res["plain"]["qps"],
             "sq4": dict(queries=gq, L=64, entry_points=sq_ep, expand_count=32, refine=f"top {LARGE_REFINE} -> 10",
                         e2e_qps=gq / sq_s, recall_at_10=sq_rec)}
+
+
+def layout_section(calc, args, w, L, plain_kw, forms, stream, dist, dev, world) -> dict:
+    """The plain and batched operating points on the same index in the
+    neighbourhood-aware id order (rover_b200.layout: the reference's
+    clustered block ordering, 32 ids per block, each vector clustered by its
+    nearest mixture centre).  The entry seeds are drawn over ids, so the
+    renumbered index searches from other seeds: recall is reported beside
+    each time."""
+    import torch
+    from rover_b200.layout import gorder_workload
+    t0 = time.time()
+    wg, _ = gorder_workload(w)
+    calc.pq_load(wg.graph, wg.entry, wg.bundle)
+    q_d = torch.from_numpy(np.ascontiguousarray(wg.queries)).to(dev)
+    out = {"order": "gorder: 32 ids per block, clusters = nearest mixture centre", "build_seconds": time.time() - t0}
+    points = [("plain", L, plain_kw)]
+    if forms:
+        points.append(("batched", forms["batched"]["L"], forms["batched"]["kw"]))
+    for label, L_, kw in points:
+        t = timed_form(calc, args, wg, q_d, L_, kw, stream, dist, dev, world)
+        out[label] = dict(qps=t["qps"], ms_per_step=t["steps"]["ms_per_step"], recall_at_10=t["recall"],
+                          kernel_ms_per_step={k: v[1] / args.steps for k, v in t["steps"]["kernels"].items()},
+                          expanded=float(t["stats"][:, 2].mean()), corrected=float(t["stats"][:, 1].mean()))
+        log(f"layout gorder {label}: {t['qps']:,.0f} QPS recall@10={t['recall']:.4f}")
+    return out
 
 
 def timed_form(calc, args, w, q_d, L, kw, stream, dist, dev, world):
