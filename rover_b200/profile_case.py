@@ -76,8 +76,9 @@ def main(argv=None) -> int:
                        refine_logit=-np.inf, stop_logit=np.inf)
         kw.update(mode=MODE_GATED, beam_width=args.W)
     l0 = calc.launch_count()
-    calc.pq_search(q, args.L, **kw)
+    first = calc.pq_search(q, args.L, **dict(kw, stats=True))
     warm = calc.launch_count() - l0
+    st = first["stats"].astype(np.float64).mean(axis=0)
     calc.kernel_timing(True)
     for _ in range(args.repeat):
         r = calc.pq_search(q, args.L, **kw)
@@ -86,7 +87,8 @@ def main(argv=None) -> int:
     recall = workloads.recall_at_k(r["ids"], r["counts"], w.gt[:len(q)], 10) if args.repeat > 0 else None
     print(json.dumps(dict(form=args.form, workload=args.workload, layout=args.layout, queries=len(q), L=args.L,
                           entry_points=args.ep, beam_width=args.W if args.form in ("batched", "gated") else None,
-                          warm_launches=warm, kernel_ms=times, recall_at_10=recall)), flush=True)
+                          warm_launches=warm, kernel_ms=times, recall_at_10=recall,
+                          scored=st[0], corrected=st[1], expanded=st[2])), flush=True)
     calc.close()
     return 0
 
