@@ -528,6 +528,10 @@ int rover_bundle_open_dir(const char* dir, int verify, RoverBundle** out) {
         }
         const char* layout = string_of(&doc, "residual_layout");
         if (layout && strcmp(layout, "a") && !member(files, "residual_map")) { fail("Index missing residual_map"); goto done; }
+        if (layout && strcmp(layout, "a")) {
+            fail("residual layout %s (a reordered residual file) is not supported; use residual layout a", layout);
+            goto done;
+        }
     }
     /* every member: inside the directory, a regular file, unique name, recorded size and digest */
     for (int i = 0; i < files->count; ++i) {

@@ -323,6 +323,11 @@ static int parse(int argc, char** argv) {
         c->search_mode = "db_pair";
     }
     c->refine_mode = c->refine ? 1 + (c->third_residual != 0) : 0;
+    /* A residual file in a storage order of its own (retrieval_rpc_demo_
+       reorder.c layouts B/C/D, read through --residual-map) is refused
+       rather than read as if it were in graph order. */
+    if (*c->residual_map)
+        return refuse("reordered residual files (--residual-map) are not supported; use residual layout a");
     if (c->third_residual) {
         /* the artifact must exist and hash (config.c:118); it is checked
            against the index when the refine opens it */

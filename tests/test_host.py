@@ -184,6 +184,15 @@ def test_bundle_loader_rejects_what_the_reference_rejects(host, tmp_path):
     (d / "index.json").write_text(json.dumps(idx)[:-3])
     rc, _, err = _open(host, d)
     assert rc != 0 and "JSON" in err
+    # a reordered residual layout: the map is required (index_bundle.py:204),
+    # and the reordered file itself is refused, not read in graph order
+    (d / "index.json").write_text(json.dumps(dict(idx, residual_layout="b")))
+    rc, _, err = _open(host, d)
+    assert rc != 0 and "Index missing residual_map" in err
+    idx["files"]["residual_map"] = dict(idx["files"]["graph"])
+    (d / "index.json").write_text(json.dumps(dict(idx, residual_layout="b")))
+    rc, _, err = _open(host, d)
+    assert rc != 0 and "residual layout b" in err
 
 
 def test_index_json_escapes_and_key_order(host, tmp_path):
@@ -238,3 +247,6 @@ def test_cli_options_and_checks(host):
     assert p.returncode == 2 and "search requires query, graph" in p.stderr
     p = _rover("build-index", "--n", "100", "--dim", "16", "--graph-degree", "8")
     assert p.returncode == 1 and "Construction" in p.stderr
+    # a residual file in its own storage order is refused, not read as graph order
+    p = _rover(*base, "--residual-map", "map.txt")
+    assert p.returncode == 2 and "reordered residual files" in p.stderr
