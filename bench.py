@@ -6,7 +6,11 @@ the learned-gate batched form against the plain drop-in.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Every form picks its operating point on 2,000 held-out calibration queries
+The index is searched in the reference's clustered block id order (the
+rover-layout ordering, 32 ids per block; --layout original keeps the ids as
+built); every arm, the reference's included, searches the same index, and
+``config.layout_other`` repeats the plain and batched points on the other
+order.  Every form picks its operating point on 2,000 held-out calibration queries
 (their own exact neighbours; target recall@10 0.95 plus a 0.003 margin) and
 is then timed, with its recall reported, on the 10,000 timed queries:
 
@@ -184,9 +188,32 @@ def seed_pass_bytes(nq: int, seeds: int, md, rcb: int, corrected: bool) -> int:
 
 
 def calibration_set(args):
-    """The held-out calibration queries and their exact neighbours."""
+    """The held-out calibration queries and their exact neighbours, in the
+    index's id order (args.old_to_new renumbers them for a reordered index)."""
     from rover_b200 import workloads
-    return workloads.held_out_set(args.workload, CALIBRATION_QUERIES, CALIBRATION_OFFSET, cache_dir=args.cache_dir)
+    q, gt = workloads.held_out_set(args.workload, CALIBRATION_QUERIES, CALIBRATION_OFFSET, cache_dir=args.cache_dir)
+    o2n = getattr(args, "old_to_new", None)
+    if o2n is not None:
+        gt = np.where(gt >= 0, o2n[np.maximum(gt, 0)], -1).astype(np.int32)
+    return q, gt
+
+
+def index_layout(args, w):
+    """The index the benchmark searches: the workload as built (original
+    ids) or renumbered into the reference's clustered block order
+    (rover_b200.layout.gorder_workload: rover-layout's ordering, 32 ids per
+    block, each vector clustered by its nearest mixture centre), as a
+    reordered bundle carries it.  Returns (index, the other order)."""
+    if args.layout == "original":
+        return w, None
+    from rover_b200.layout import gorder_workload
+    t0 = time.time()
+    wg, n2o = gorder_workload(w)
+    o2n = np.empty(len(n2o), dtype=np.int64)
+    o2n[np.asarray(n2o)] = np.arange(len(n2o))
+    args.old_to_new = o2n
+    log(f"index in the clustered block order ({time.time() - t0:.1f}s)")
+    return wg, w
 
 
 def calibrate(search, cal, comps, log_prefix=""):
@@ -260,7 +287,7 @@ def reference_arm(args, w, rank) -> dict:
         "value": qps, "unit": "queries/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * elapsed / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture)", "impl": "reference",
-        "config": {"workload": args.workload, "queries_per_step": sample, "beam_L": chosen,
+        "config": {"workload": args.workload, "layout": args.layout, "queries_per_step": sample, "beam_L": chosen,
                    "entry_points": ep_chosen, "calibration": table, "top_k": TOP_K,
                    "refine_budget": REFINE_BUDGET, "expand_count": expand, "correction": "online"},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "reference",
@@ -402,20 +429,27 @@ def device_steps(calc, args, step, stream, dist=None, dev=None):
 
 
 SEED_KERNELS = ("pq_seeds", "pq_seed_rank", "pq_seed_topm")
-# DRAM bytes per query of each form's search kernel, from one ncu capture of
-# a 2,000-query launch at the benchmark's operating point
+# DRAM bytes per query of each form's search kernel in each id order, from
+# one ncu capture of a 2,000-query launch at the benchmark's operating point
 # (dram__bytes_read.sum + dram__bytes_write.sum / 2,000); scaled to a launch
 # by its query count, since traffic grows with the queries searched.
 PROFILED_TRAFFIC = {
-    "plain": (219.8e3, "ncu DRAM bytes of pq_decoded_search_kernel<128>, 2,000 queries, L=40, 4,096 entry points"),
-    "batched": (184.3e3, "ncu DRAM bytes of pq_batched_search_kernel<128,kBatchFull>, 2,000 queries, W=3, L=24, "
-                         "8,192 entry points"),
-    "gated": (191.0e3, "ncu DRAM bytes of pq_batched_search_kernel<128,kBatchGated>, 2,000 queries, W=3, L=24, "
-                       "8,192 entry points"),
+    ("original", "plain"): (219.8e3, "ncu DRAM bytes of pq_decoded_search_kernel<128>, 2,000 queries, L=40, "
+                                     "4,096 entry points, ids as built"),
+    ("original", "batched"): (184.3e3, "ncu DRAM bytes of pq_batched_search_kernel<128,kBatchFull>, 2,000 queries, "
+                                       "W=3, L=24, 8,192 entry points, ids as built"),
+    ("original", "gated"): (191.0e3, "ncu DRAM bytes of pq_batched_search_kernel<128,kBatchGated>, 2,000 queries, "
+                                     "W=3, L=24, 8,192 entry points, ids as built"),
+    ("gorder", "plain"): (219.0e3, "ncu DRAM bytes of pq_decoded_search_kernel<128>, 2,000 queries, L=40, "
+                                   "4,096 entry points, clustered block order"),
+    ("gorder", "batched"): (182.7e3, "ncu DRAM bytes of pq_batched_search_kernel<128,kBatchFull>, 2,000 queries, "
+                                     "W=3, L=24, 8,192 entry points, clustered block order"),
+    ("gorder", "gated"): (188.6e3, "ncu DRAM bytes of pq_batched_search_kernel<128,kBatchGated>, 2,000 queries, "
+                                   "W=3, L=24, 8,192 entry points, clustered block order"),
 }
 
 
-def roofline(bytes_per_call, seed_bytes_per_call, kernels, steps, nq, label):
+def roofline(bytes_per_call, seed_bytes_per_call, kernels, steps, nq, label, layout):
     """The search kernel's roofline: its algorithmic bytes per launch (the
     call's bytes minus the seed pass's share) over its own mean launch
     duration; traffic = its measured DRAM bytes per query x nq."""
@@ -426,7 +460,7 @@ def roofline(bytes_per_call, seed_bytes_per_call, kernels, steps, nq, label):
     launch_s = total_ms / max(1, launches) / 1e3
     per_launch = (bytes_per_call - seed_bytes_per_call) * steps / max(1, launches)
     achieved = per_launch / launch_s / 1e9
-    per_query, source = PROFILED_TRAFFIC.get(label, (None, None))
+    per_query, source = PROFILED_TRAFFIC.get((layout, label), (None, None))
     traffic = per_query * nq * steps / max(1, launches) if per_query else None
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "traffic_source": source, "peak_kind": peak_kind, "kernel": top,
@@ -451,7 +485,9 @@ def main():
     ap.add_argument("--train-queries", type=int, default=TRAIN_QUERIES)
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch plan section")
     ap.add_argument("--no-sq", action="store_true", help="skip the SQ section")
-    ap.add_argument("--no-layout", action="store_true", help="skip the neighbourhood-aware layout section")
+    ap.add_argument("--layout", default="gorder", choices=("gorder", "original"),
+                    help="id order of the searched index: the reference's clustered block order, or as built")
+    ap.add_argument("--no-layout", action="store_true", help="skip the section on the other id order")
     ap.add_argument("--large-workload", default=LARGE_WORKLOAD, help="with --config5: workloads.LARGE_CONFIGS name")
     ap.add_argument("--config5", action="store_true",
                     help="only the large combined configuration (10M x 128, SQ4 + PQ32, uneven L): one JSON line")
@@ -487,6 +523,7 @@ def main():
     from rover_b200 import workloads
     w = workloads.build_pq(args.workload, cache_dir=args.cache_dir, verbose=rank == 0)
     log(f"workload ready in {w.build_seconds:.1f}s")
+    w, w_other = index_layout(args, w)
     if args.impl == "reference":
         print(json.dumps(reference_arm(args, w, rank)), flush=True)
         return 0
@@ -525,7 +562,8 @@ def main():
     plain = timed_form(calc, args, w, q_d, L, plain_kw, stream, dist, dev, world)
     plain_qps = plain["qps"]
     plain_seed = seed_pass_bytes(nq, min(ep, md.num_vectors), md, rcb, True)
-    plain_roof = roofline(plain_bytes, plain_seed, plain["steps"]["kernels"], args.steps, nq, "plain")
+    plain_roof = roofline(plain_bytes, plain_seed, plain["steps"]["kernels"], args.steps, nq, "plain",
+                          args.layout)
     log(f"plain {plain_qps:,.0f} QPS ({plain['steps']['ms_per_step']:.3f} ms/step)")
 
     # ---- batched form (no gate) and learned-gate batched form
@@ -563,8 +601,11 @@ def main():
 
     lay = None
     if not args.no_layout:
-        lay = layout_section(calc, args, w, L, plain_kw, forms, stream, dist, dev, world)
-        calc.pq_load(w.graph, w.entry, w.bundle)      # the original id order for the sections below
+        if w_other is None:
+            from rover_b200.layout import gorder_workload
+            w_other, _ = gorder_workload(w)
+        lay = layout_section(calc, args, w_other, L, plain_kw, forms, stream, dist, dev, world)
+        calc.pq_load(w.graph, w.entry, w.bundle)      # the headline index for the sections below
 
     dk = None
     if rank == 0 and not args.no_distance_kernels:
@@ -607,7 +648,10 @@ def main():
                    "gated_over_plain": head["qps"] / plain_qps if gated else None,
                    "forms": forms["report"] if forms else None,
                    "uneven": uneven,
-                   "layout_gorder": lay,
+                   "layout": ("clustered block order (rover-layout ordering: 32 ids per block, clusters = "
+                              "nearest mixture centre), the same index for every arm" if args.layout == "gorder"
+                              else "ids as built"),
+                   "layout_other": lay,
                    "sq": sq,
                    "parallelism": f"replicas x{world}",
                    "l2": "index (>800 MB with decoded rows) larger than L2; no flush"},
@@ -936,20 +980,17 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
                         e2e_qps=gq / sq_s, recall_at_10=sq_rec)}
 
 
-def layout_section(calc, args, w, L, plain_kw, forms, stream, dist, dev, world) -> dict:
-    """The plain and batched operating points on the same index in the
-    neighbourhood-aware id order (rover_b200.layout: the reference's
-    clustered block ordering, 32 ids per block, each vector clustered by its
-    nearest mixture centre).  The entry seeds are drawn over ids, so the
-    renumbered index searches from other seeds: recall is reported beside
-    each time."""
+def layout_section(calc, args, wg, L, plain_kw, forms, stream, dist, dev, world) -> dict:
+    """The plain and batched operating points on the same vectors in the
+    other id order (as built when the headline index is in the clustered
+    block order, and the other way round).  The entry seeds are drawn over
+    ids, so a renumbered index searches from other seeds: recall is reported
+    beside each time."""
     import torch
-    from rover_b200.layout import gorder_workload
-    t0 = time.time()
-    wg, _ = gorder_workload(w)
     calc.pq_load(wg.graph, wg.entry, wg.bundle)
     q_d = torch.from_numpy(np.ascontiguousarray(wg.queries)).to(dev)
-    out = {"order": "gorder: 32 ids per block, clusters = nearest mixture centre", "build_seconds": time.time() - t0}
+    out = {"order": "as built" if args.layout == "gorder" else
+           "clustered block order (rover-layout: 32 ids per block, clusters = nearest mixture centre)"}
     points = [("plain", L, plain_kw)]
     if forms:
         points.append(("batched", forms["batched"]["L"], forms["batched"]["kw"]))
@@ -958,7 +999,7 @@ def layout_section(calc, args, w, L, plain_kw, forms, stream, dist, dev, world) 
         out[label] = dict(qps=t["qps"], ms_per_step=t["steps"]["ms_per_step"], recall_at_10=t["recall"],
                           kernel_ms_per_step={k: v[1] / args.steps for k, v in t["steps"]["kernels"].items()},
                           expanded=float(t["stats"][:, 2].mean()), corrected=float(t["stats"][:, 1].mean()))
-        log(f"layout gorder {label}: {t['qps']:,.0f} QPS recall@10={t['recall']:.4f}")
+        log(f"other id order, {label}: {t['qps']:,.0f} QPS recall@10={t['recall']:.4f}")
     return out
 
 
@@ -1104,7 +1145,7 @@ def free_forms(calc, w, args, cal, ep, L, expand, q_d, stream, dist, dev, world,
         bbytes = algorithmic_bytes(b["stats"], b["counts"], md, w.bundle.residual_code_bytes, expand, md.dim)
         b["roof"] = roofline(bbytes, seed_pass_bytes(nq, min(bpick["entry_points"], md.num_vectors), md,
                                                      w.bundle.residual_code_bytes, True),
-                             b["steps"]["kernels"], args.steps, nq, "batched")
+                             b["steps"]["kernels"], args.steps, nq, "batched", args.layout)
         res["batched"] = b
         # equal point with the plain form: its L and entry points, W-wide steps
         bp = timed_form(calc, args, w, q_d, plain["L"], dict(plain["kw"], mode=MODE_BATCHED,
@@ -1129,7 +1170,7 @@ def free_forms(calc, w, args, cal, ep, L, expand, q_d, stream, dist, dev, world,
         gbytes = algorithmic_bytes(g["stats"], g["counts"], md, w.bundle.residual_code_bytes, expand, md.dim)
         g["roof"] = roofline(gbytes, seed_pass_bytes(nq, min(gpick["entry_points"], md.num_vectors), md,
                                                      w.bundle.residual_code_bytes, False),
-                             g["steps"]["kernels"], args.steps, nq, "gated")
+                             g["steps"]["kernels"], args.steps, nq, "gated", args.layout)
         res["gated"] = g
         # the same point with the network switched off
         bg = timed_form(calc, args, w, q_d, gpick["L"], kw_of(gpick, MODE_BATCHED), stream, dist, dev, world)

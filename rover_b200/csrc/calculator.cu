@@ -125,12 +125,17 @@ struct SqDevice {
   DevBuf graph, l1, residual, qparams;
   DevBuf e4_qparams, e4_blocks;   // ERROR4 artifact (calculator_rover_error4_load)
   DevBuf split_bias;              // SQ4 split-distance bias (calculator_rover_sq_split_load)
+  DevBuf entry_ids;               // entry ids of the last request (sq_entries)
+  bool entries_valid = false, entries_sqmd = false;
+  int32_t entries_target = 0, entry_count = 0;
+  uint32_t entries_seed = 0;
   SqIndexView view{};
   int32_t graph_entry = -1;
   bool loaded = false;
   void release() {
     graph.release(); l1.release(); residual.release(); qparams.release();
-    e4_qparams.release(); e4_blocks.release(); split_bias.release();
+    e4_qparams.release(); e4_blocks.release(); split_bias.release(); entry_ids.release();
+    entries_valid = false;
     view.e4 = Error4View{};
     view.split_bias = nullptr;
     loaded = false;
@@ -924,7 +929,62 @@ AEEResult download(T* dst, const void* src, size_t count, cudaStream_t s) {
   return AEE_SUCCESS;
 }
 
-AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSearchParams* p,
+// The entry ids of an SQ search request, shared by its queries (they depend
+// on the entry count, the graph entry and the seed only):
+//  * DSP and DB-pair searches, dsp_search_select_entry_id
+//    (retrieval_async_dsp_search.c:219): entry 0 is the graph entry when it is
+//    valid, the others LCG draws from 42 scaled to [0, n); repeats stay in the
+//    list (the search claims the first of each);
+//  * SQMD, retrieval_sqmd_make_seed_ids (retrieval_sqmd_seed.c:15): the graph
+//    entry, then (seed / 65536) % n LCG draws not yet in the list, at most
+//    64 per wanted seed + 1024 draws, then the lowest ids not in it.
+AEEResult sq_entries(State& s, SqDevice& sq, bool sqmd, int32_t entry_points, uint32_t seed) {
+  const int32_t n = sq.view.n;
+  const int32_t target = std::min(entry_points, n);
+  if (sq.entries_valid && sq.entries_sqmd == sqmd && sq.entries_target == target && sq.entries_seed == seed)
+    return AEE_SUCCESS;
+  sq.entries_valid = false;
+  std::vector<int32_t> ids;
+  ids.reserve(static_cast<size_t>(std::max(target, 0)));
+  const bool entry_ok = sq.graph_entry >= 0 && sq.graph_entry < n;
+  if (!sqmd) {
+    uint32_t lcg = 42u;
+    for (int32_t i = 0; i < target; ++i) {
+      if (i == 0 && entry_ok) {
+        ids.push_back(sq.graph_entry);
+        continue;
+      }
+      lcg = lcg * 1103515245u + 12345u;
+      ids.push_back(static_cast<int32_t>((static_cast<uint64_t>(lcg) * static_cast<uint64_t>(n)) >> 32));
+    }
+  } else if (target > 0) {
+    std::vector<uint8_t> taken(static_cast<size_t>(n), 0);
+    auto take = [&](int32_t id) {
+      if (taken[id]) return;
+      taken[id] = 1;
+      ids.push_back(id);
+    };
+    if (entry_ok) take(sq.graph_entry);
+    const uint64_t limit = static_cast<uint64_t>(target) * 64u + 1024u;
+    uint32_t lcg = seed;
+    for (uint64_t attempts = 0; static_cast<int32_t>(ids.size()) < target && attempts < limit; ++attempts) {
+      lcg = lcg * 1103515245u + 12345u;
+      take(static_cast<int32_t>((lcg / 65536u) % static_cast<uint32_t>(n)));
+    }
+    for (int32_t id = 0; id < n && static_cast<int32_t>(ids.size()) < target; ++id) take(id);
+  }
+  if (ids.empty()) ids.push_back(-1);   // never read: entry_count is 0
+  if (upload(sq.entry_ids, ids.data(), ids.size(), s.stream) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  CK(cudaStreamSynchronize(s.stream));
+  sq.entry_count = target > 0 ? static_cast<int32_t>(ids.size()) : 0;
+  sq.entries_sqmd = sqmd;
+  sq.entries_target = target;
+  sq.entries_seed = seed;
+  sq.entries_valid = true;
+  return AEE_SUCCESS;
+}
+
+AEEResult sq_search_core(State& s, SqDevice& sq, int mode, const RoverSearchParams* p,
                          const float* d_queries, int nq, const int32_t* d_pool,
                          const std::vector<int32_t>& h_pool, int num_out, int32_t* d_ids, float* d_dists,
                          int32_t out_stride, int32_t* d_counts, unsigned long long* d_stats,
@@ -962,8 +1022,18 @@ AEEResult sq_search_core(State& s, const SqDevice& sq, int mode, const RoverSear
   a.out_counts = d_counts;
   a.stats = d_stats;
   a.status = d_status;
-  const size_t per_warp = ((sq.view.dim * 4 + 15) & ~15) + ((sq.view.dim + 15) & ~15) + 64 * 8;
-  const size_t smem = per_warp * kSearchWarps;
+  if (sq_entries(s, sq, mode == kSqModeSqmd, p->entry_points, p->seed) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  a.entry_ids = sq.entry_ids.as<int32_t>();
+  a.entry_count = sq.entry_count;
+  // on-chip heap levels: with one block per SM enough for the batch, most of
+  // the shared memory; otherwise a share that keeps four blocks per SM
+  const bool few = nq <= s.sms * kSearchWarps;
+  const size_t fixed = sq_search_smem_per_warp(sq.view.dim, 0, 0);
+  const size_t budget = (few ? (200u << 10) : (48u << 10)) / kSearchWarps;
+  const size_t room = budget > fixed ? (budget - fixed) / 8u : 0u;
+  a.pool_split = static_cast<int32_t>(std::min<size_t>(static_cast<size_t>(max_pool), std::min<size_t>(room / 3u, few ? 1024u : 128u)));
+  a.front_split = static_cast<int32_t>(std::min<size_t>(static_cast<size_t>(fcap), room - static_cast<size_t>(a.pool_split)));
+  const size_t smem = sq_search_smem_per_warp(sq.view.dim, a.pool_split, a.front_split) * kSearchWarps;
   const SqSearchFn sq_kernel = sq_search_kernel_for(a.split != 0);
   if (allow_smem(reinterpret_cast<const void*>(sq_kernel), smem) != AEE_SUCCESS) return AEE_EFAILED;
   int blocks = std::max(1, std::min(resident_blocks(reinterpret_cast<const void*>(sq_kernel), kSearchWarps * 32, smem, s.sms),

@@ -286,9 +286,18 @@ struct SqSearchArgs {
   unsigned long long* visited; uint32_t visited_mask; uint32_t gen_base;
   uint64_t* heaps;               // per slot: max_pool + frontier_cap entries
   unsigned int* next_query;
+  // the request's entry ids, the same for every query (drawn on the host):
+  // DSP / DB-pair: entry_points ids in draw order, repeats included;
+  // SQMD: the distinct seeds of retrieval_sqmd_make_seed_ids
+  const int32_t* entry_ids; int32_t entry_count;
+  // heap entries kept in shared memory per warp (the rest at the same
+  // indices of the slot's global heaps)
+  int32_t pool_split, front_split;
 };
 
 using SqSearchFn = void (*)(SqSearchArgs);
+// Dynamic shared memory of one warp of the SQ search kernel.
+size_t sq_search_smem_per_warp(int dim, int pool_split, int front_split);
 // The SQ search kernel (a __global__ function): with the split distance
 // compiled in or out, so the plain searches keep their register budget.
 SqSearchFn sq_search_kernel_for(bool split);

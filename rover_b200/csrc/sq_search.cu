@@ -32,7 +32,19 @@ namespace rover {
 
 struct HeapEntry { int32_t id; float dist; };
 
-__device__ __forceinline__ void pool_sift_up(HeapEntry* p, int i) {
+// A heap whose first `split` entries sit in this warp's shared memory and
+// whose deeper entries sit at the same indices of its global scratch: the
+// levels every push and pop touches stay on chip, and a large frontier (the
+// SQMD bound is entry points + pool x expand) still fits.
+struct SplitHeap {
+  HeapEntry* sm;
+  HeapEntry* gl;
+  int split;
+  __device__ __forceinline__ HeapEntry& operator[](int i) const { return i < split ? sm[i] : gl[i]; }
+};
+
+template <class H>
+__device__ __forceinline__ void pool_sift_up(H p, int i) {
   HeapEntry t = p[i];
   while (i > 0) {
     const int parent = (i - 1) / 2;
@@ -43,7 +55,8 @@ __device__ __forceinline__ void pool_sift_up(HeapEntry* p, int i) {
   p[i] = t;
 }
 
-__device__ __forceinline__ void pool_sift_down(HeapEntry* p, int size, int i) {
+template <class H>
+__device__ __forceinline__ void pool_sift_down(H p, int size, int i) {
   HeapEntry t = p[i];
   for (;;) {
     int child = 2 * i + 1;
@@ -56,24 +69,24 @@ __device__ __forceinline__ void pool_sift_down(HeapEntry* p, int size, int i) {
   p[i] = t;
 }
 
-__device__ __forceinline__ bool pool_insert(HeapEntry* p, int* size, int cap, int32_t id, float d) {
+template <class H>
+__device__ __forceinline__ bool pool_insert(H p, int* size, int cap, int32_t id, float d) {
   if (*size < cap) {
-    p[*size].id = id;
-    p[*size].dist = d;
+    p[*size] = HeapEntry{id, d};
     pool_sift_up(p, *size);
     ++*size;
     return true;
   }
   if (d < p[0].dist) {
-    p[0].id = id;
-    p[0].dist = d;
+    p[0] = HeapEntry{id, d};
     pool_sift_down(p, *size, 0);
     return true;
   }
   return false;
 }
 
-__device__ __forceinline__ void front_sift_up(HeapEntry* f, int i) {
+template <class H>
+__device__ __forceinline__ void front_sift_up(H f, int i) {
   HeapEntry t = f[i];
   while (i > 0) {
     const int parent = (i - 1) / 2;
@@ -84,7 +97,8 @@ __device__ __forceinline__ void front_sift_up(HeapEntry* f, int i) {
   f[i] = t;
 }
 
-__device__ __forceinline__ void front_sift_down(HeapEntry* f, int size, int i) {
+template <class H>
+__device__ __forceinline__ void front_sift_down(H f, int size, int i) {
   HeapEntry t = f[i];
   for (;;) {
     int child = 2 * i + 1;
@@ -97,7 +111,8 @@ __device__ __forceinline__ void front_sift_down(HeapEntry* f, int size, int i) {
   f[i] = t;
 }
 
-__device__ __forceinline__ int32_t front_pop(HeapEntry* f, int* size) {
+template <class H>
+__device__ __forceinline__ int32_t front_pop(H f, int* size) {
   const int32_t top = f[0].id;
   --*size;
   if (*size > 0) {
@@ -165,11 +180,84 @@ __device__ __forceinline__ float sq_exact(const SqIndexView& ix, const float* q,
   return dist;
 }
 
+// Code of dimension j (0..15) of a 16-dimension group held in v: 4-bit codes
+// (64 bits, low nibble first) or 8-bit codes (128 bits).
+__device__ __forceinline__ uint32_t group_code(const uint4& v, bool four, int j) {
+  if (four) {
+    const uint32_t w = j < 8 ? v.x : v.y;
+    return (w >> ((j & 7) * 4)) & 15u;
+  }
+  const uint32_t w = j < 4 ? v.x : j < 8 ? v.y : j < 12 ? v.z : v.w;
+  return (w >> ((j & 3) * 8)) & 255u;
+}
+
+__device__ __forceinline__ uint4 group_load(const uint8_t* row, bool four, int g) {
+  if (four) {
+    const uint2 t = __ldg(reinterpret_cast<const uint2*>(row + g / 2));
+    return make_uint4(t.x, t.y, 0u, 0u);
+  }
+  return __ldg(reinterpret_cast<const uint4*>(row + g));
+}
+
+// sq_exact over 16-dimension groups read with 64/128-bit loads (rows whose
+// code and residual strides keep those loads aligned, dim % 16 == 0): the
+// same per-dimension arithmetic, in dimension order.
+__device__ __forceinline__ float sq_exact_vec(const SqIndexView& ix, const float* q, int32_t id) {
+  const uint8_t* l1 = ix.l1 + static_cast<size_t>(id) * ix.l1_code_bytes;
+  const uint8_t* res = ix.residual ? ix.residual + static_cast<size_t>(id) * ix.rcb : nullptr;
+  const bool c4 = ix.l1_bits == 4, r4 = ix.residual_bits == 4;
+  float rs = 0.0f, rz = 0.0f, dist = 0.0f;
+  if (res) {
+    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+    rs = qp.x;
+    rz = qp.y;
+  }
+  for (int g = 0; g < ix.dim; g += 16) {
+    const uint4 cv = group_load(l1, c4, g);
+    const uint4 rv = res ? group_load(res, r4, g) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      float value = fadd(fmul(u8f(group_code(cv, c4, j)), ix.l1_scale), ix.l1_zero);
+      if (res) value = fadd(value, fadd(fmul(u8f(group_code(rv, r4, j)), rs), rz));
+      const float diff = fsub(q[g + j], value);
+      dist = fadd(dist, fmul(diff, diff));
+    }
+  }
+  return dist;
+}
+
+// Whether the index's rows allow sq_exact_vec.
+__device__ __forceinline__ bool sq_rows_vectorizable(const SqIndexView& ix) {
+  if (ix.dim % 16 != 0) return false;
+  const int ca = ix.l1_bits == 4 ? 8 : 16;
+  if (ix.l1_code_bytes % ca != 0 || (reinterpret_cast<uintptr_t>(ix.l1) % ca) != 0) return false;
+  if (!ix.residual) return true;
+  const int ra = ix.residual_bits == 4 ? 8 : 16;
+  return ix.rcb % ra == 0 && (reinterpret_cast<uintptr_t>(ix.residual) % ra) == 0 &&
+         (reinterpret_cast<uintptr_t>(ix.qparams) % 8) == 0;
+}
+
+__device__ __forceinline__ float sq_exact_fast(const SqIndexView& ix, const float* q, int32_t id, bool vec) {
+  return vec ? sq_exact_vec(ix, q, id) : sq_exact(ix, q, id);
+}
+
 // First occurrence in lane order among lanes that hold the same id.
 __device__ __forceinline__ bool first_of_equal(bool active, int32_t id, int lane) {
   const unsigned act = __ballot_sync(kFullMask, active);
   const unsigned same = __match_any_sync(kFullMask, active ? id : -2 - lane) & act;
   return active && (__ffs(same) - 1) == lane;
+}
+
+// Shared memory of one warp of sq_search_kernel_t: the query, its codes, the
+// batch of scored candidates, then the pool's and the frontier's on-chip
+// levels (SqSearchArgs::pool_split / front_split entries).
+__host__ __device__ inline size_t sq_search_warp_smem(int dim, int pool_split, int front_split) {
+  return static_cast<size_t>(((dim * 4) + 15) & ~15) + static_cast<size_t>((dim + 15) & ~15) + 32 * 8 +
+         static_cast<size_t>(pool_split + front_split) * 8;
+}
+
+size_t sq_search_smem_per_warp(int dim, int pool_split, int front_split) {
+  return sq_search_warp_smem(dim, pool_split, front_split);
 }
 
 template <bool kSplit>
@@ -181,21 +269,59 @@ sq_search_kernel_t(SqSearchArgs a) {
   const SqIndexView& ix = a.ix;
   const int qbytes = ((ix.dim * 4) + 15) & ~15;
   const int cbytes = ((ix.dim + 15) & ~15);
-  uint8_t* base = smem + static_cast<size_t>(warp) * (qbytes + cbytes + 64 * 8);
+  uint8_t* base = smem + static_cast<size_t>(warp) * sq_search_warp_smem(ix.dim, a.pool_split, a.front_split);
   float* q = reinterpret_cast<float*>(base);
   uint8_t* qc = base + qbytes;
-  HeapEntry* work = reinterpret_cast<HeapEntry*>(base + qbytes + cbytes);  // 32 results
-  int32_t* seeds = reinterpret_cast<int32_t*>(work + 32);                   // 32 ids
+  HeapEntry* work = reinterpret_cast<HeapEntry*>(base + qbytes + cbytes);  // 32 scored candidates
   const int slot = blockIdx.x * kSearchWarps + warp;
-  HeapEntry* pool = reinterpret_cast<HeapEntry*>(a.heaps) +
-                    static_cast<size_t>(slot) * (a.max_pool + a.frontier_cap);
-  HeapEntry* front = pool + a.max_pool;
+  HeapEntry* gpool = reinterpret_cast<HeapEntry*>(a.heaps) +
+                     static_cast<size_t>(slot) * (a.max_pool + a.frontier_cap);
+  const SplitHeap pool{work + 32, gpool, a.pool_split};
+  const SplitHeap front{work + 32 + a.pool_split, gpool + a.max_pool, a.front_split};
   VisitedTable vt;
   vt.slots = a.visited + static_cast<size_t>(slot) * (a.visited_mask + 1ull);
   vt.mask = a.visited_mask;
   const bool sqmd = a.mode == kSqModeSqmd;
   const bool db = a.mode == kSqModeDb;
   const bool split = kSplit && sqmd && a.correction;   // the host checks the index supports it
+  const bool exact = (sqmd || db) && a.correction;
+  const bool vec = sq_rows_vectorizable(ix);
+
+  // Lane 0 applies the batch's scored candidates (work[0..cnt)) to the heaps
+  // in batch order.  keep marks the ones that can enter the pool: a full
+  // pool's worst only falls, so a candidate not below it at the start of the
+  // batch stays out (the strict '<' of sqmd_common.c:51-80), and skipping it
+  // changes nothing.
+  auto apply = [&](unsigned keep, int& psize, int& fsize, int cap, int fcap, int32_t& st) {
+    if (lane != 0) return;
+    for (; keep; keep &= keep - 1u) {
+      const int t = __ffs(keep) - 1;
+      const HeapEntry c = work[t];
+      if (pool_insert(pool, &psize, cap, c.id, c.dist)) {
+        if (fsize < fcap) {
+          front[fsize] = c;
+          front_sift_up(front, fsize);
+          ++fsize;
+        } else if (!sqmd) {
+          st = kStatusFrontierFull;
+        }
+      }
+    }
+  };
+  // The keep mask of a batch: lanes holding a scored candidate (fresh) whose
+  // distance may still enter the pool; each writes its entry at its rank.
+  auto stage = [&](bool fresh, int32_t id, float d, int psize, int cap) -> unsigned {
+    float worst = 0.0f;
+    if (lane == 0 && psize > 0) worst = pool[0].dist;
+    worst = __shfl_sync(kFullMask, worst, 0);
+    const int ps = __shfl_sync(kFullMask, psize, 0);
+    const bool keep = fresh && (ps < cap || d < worst);
+    const unsigned km = __ballot_sync(kFullMask, keep);
+    if (keep) work[__popc(km & ((1u << lane) - 1u))] = HeapEntry{id, d};
+    __syncwarp();
+    const int cnt = __popc(km);
+    return cnt == 32 ? 0xffffffffu : (1u << cnt) - 1u;
+  };
 
   for (;;) {
     int qi = 0;
@@ -253,97 +379,31 @@ sq_search_kernel_t(SqSearchArgs a) {
     int32_t st = kStatusOk;
     unsigned long long scored = 0, turns = 0, dedup = 0;
 
-    // ---- entries
-    const int entries = min(a.entry_points, ix.n);
-    uint32_t lcg = sqmd ? a.seed : 42u;
-    uint64_t attempts = 0;
-    const uint64_t attempt_limit = static_cast<uint64_t>(entries) * 64u + 1024u;
-    int sweep = 0;
-    bool graph_entry_used = false;
-    for (int base_e = 0; base_e < entries && st == kStatusOk; base_e += kWarp) {
-      // lane 0 produces the next chunk of entry ids in reference order
-      if (lane == 0) {
-        for (int t = 0; t < kWarp && base_e + t < entries; ++t) {
-          const int i = base_e + t;
-          int32_t id = -1;
-          if (!sqmd) {
-            if (i == 0 && a.graph_entry >= 0 && a.graph_entry < ix.n) {
-              id = a.graph_entry;
-            } else {
-              lcg = lcg * 1103515245u + 12345u;
-              id = static_cast<int32_t>((static_cast<uint64_t>(lcg) * static_cast<uint64_t>(ix.n)) >> 32);
-            }
-          } else {
-            // retrieval_sqmd_make_seed_ids: graph entry, LCG (seed/65536)%n
-            // with de-duplication, then an increasing sweep.  Seeds are
-            // claimed in the visited table as they are drawn, which is both
-            // the reference's de-duplication and sqmd_cpu_state_seed's claim.
-            if (!graph_entry_used && a.graph_entry >= 0 && a.graph_entry < ix.n) {
-              graph_entry_used = true;
-              const int r = visited_insert(vt, static_cast<uint32_t>(a.graph_entry));
-              if (r == 1) id = a.graph_entry;
-              else if (r < 0) st = kStatusTableFull;
-            }
-            while (id < 0 && st == kStatusOk && attempts < attempt_limit) {
-              lcg = lcg * 1103515245u + 12345u;
-              const int32_t cand = static_cast<int32_t>((lcg / 65536u) % static_cast<uint32_t>(ix.n));
-              ++attempts;
-              const int r = visited_insert(vt, static_cast<uint32_t>(cand));
-              if (r == 1) id = cand;
-              else if (r < 0) st = kStatusTableFull;
-            }
-            while (id < 0 && st == kStatusOk && sweep < ix.n) {
-              const int r = visited_insert(vt, static_cast<uint32_t>(sweep));
-              if (r == 1) id = sweep;
-              else if (r < 0) st = kStatusTableFull;
-              ++sweep;
-            }
-          }
-          seeds[t] = id;
-        }
-      }
-      st = __shfl_sync(kFullMask, st, 0);
-      __syncwarp();
+    // ---- entries: the request's entry list (the host draws it once for all
+    // queries, SqSearchArgs::entry_ids), claimed in list order
+    for (int base_e = 0; base_e < a.entry_count && st == kStatusOk; base_e += kWarp) {
       const int e = base_e + lane;
-      const bool active = e < entries && seeds[lane] >= 0;
-      const int32_t id = active ? seeds[lane] : -1;
+      const bool active = e < a.entry_count;
+      const int32_t id = active ? __ldg(a.entry_ids + e) : -1;
       bool fresh = false;
-      if (!sqmd) {
-        // DSP: claim in entry order; duplicates after the first are skipped
-        const bool first = first_of_equal(active, id, lane);
-        if (first) {
-          const int r = visited_insert(vt, static_cast<uint32_t>(id));
-          if (r < 0) st = kStatusTableFull;
-          fresh = r == 1;
-        }
-      } else {
-        // SQMD seeds were claimed while being drawn (unique by construction)
-        fresh = active;
+      // DSP: duplicates after the first are skipped; SQMD: the list holds
+      // distinct ids (the reference's de-duplication) claimed here as
+      // sqmd_cpu_state_seed does
+      const bool first = sqmd ? active : first_of_equal(active, id, lane);
+      if (first) {
+        const int r = visited_insert(vt, static_cast<uint32_t>(id));
+        if (r < 0) st = kStatusTableFull;
+        fresh = r == 1;
       }
       float d = 0.0f;
       if (fresh) {
         d = split ? split_seed_distance(ix, qc, sum_q, id, step)
-                  : (sqmd && a.correction) ? sq_exact(ix, q, id) : sq_coarse(ix, qc, id);
+                  : exact ? sq_exact_fast(ix, q, id, vec) : sq_coarse(ix, qc, id);
         if (sqmd && a.correction && (!isfinite(d) || d < 0.0f)) st = kStatusNumeric;
       }
       if (__any_sync(kFullMask, st != kStatusOk)) { st = st != kStatusOk ? st : kStatusNumeric; break; }
-      work[lane].id = fresh ? id : -1;
-      work[lane].dist = d;
-      __syncwarp();
-      if (lane == 0) {
-        for (int t = 0; t < kWarp; ++t) {
-          if (work[t].id < 0) continue;
-          if (pool_insert(pool, &psize, cap, work[t].id, work[t].dist)) {
-            if (fsize < fcap) {
-              front[fsize] = work[t];
-              front_sift_up(front, fsize);
-              ++fsize;
-            } else if (!sqmd) {
-              st = kStatusFrontierFull;
-            }
-          }
-        }
-      }
+      const unsigned keep = stage(fresh, id, d, psize, cap);
+      apply(keep, psize, fsize, cap, fcap, st);
       st = __shfl_sync(kFullMask, st, 0);
       __syncwarp();
     }
@@ -373,7 +433,6 @@ sq_search_kernel_t(SqSearchArgs a) {
           fresh = r == 1;
           if (r == 0) ++dedup;
         }
-        const unsigned fm = __ballot_sync(kFullMask, fresh);
         float d = 0.0f;
         bool dbad = false;
         if (fresh && split) {
@@ -383,32 +442,13 @@ sq_search_kernel_t(SqSearchArgs a) {
           d = split_sum(split_coarse(ix, qc, nid, step), dl);
           dbad = !isfinite(dl) || !isfinite(d) || d < 0.0f;
         } else if (fresh) {
-          d = sq_coarse(ix, qc, nid);
-          if ((sqmd || db) && a.correction) d = sq_exact(ix, q, nid);
+          d = exact ? sq_exact_fast(ix, q, nid, vec) : sq_coarse(ix, qc, nid);
         }
         if (split && __any_sync(kFullMask, dbad)) { st = kStatusNumeric; break; }
-        const int slot_i = __popc(fm & ((1u << lane) - 1u));
-        if (fresh) {
-          work[slot_i].id = nid;
-          work[slot_i].dist = d;
-        }
-        __syncwarp();
         if (__any_sync(kFullMask, st != kStatusOk)) { st = kStatusTableFull; break; }
-        const int cnt = __popc(fm);
-        if (lane == 0) {
-          for (int t = 0; t < cnt; ++t) {
-            if (pool_insert(pool, &psize, cap, work[t].id, work[t].dist)) {
-              if (fsize < fcap) {
-                front[fsize] = work[t];
-                front_sift_up(front, fsize);
-                ++fsize;
-              } else if (!sqmd) {
-                st = kStatusFrontierFull;
-              }
-            }
-          }
-        }
-        nw += cnt;
+        nw += __popc(__ballot_sync(kFullMask, fresh));
+        const unsigned keep = stage(fresh, nid, d, psize, cap);
+        apply(keep, psize, fsize, cap, fcap, st);
         st = __shfl_sync(kFullMask, st, 0);
         __syncwarp();
         if (st != kStatusOk) break;
@@ -437,8 +477,9 @@ sq_search_kernel_t(SqSearchArgs a) {
     const int limit = sqmd ? a.out_stride : a.num_out;
     const int outn = min(psize, min(limit, a.out_stride));
     for (int i = lane; i < outn; i += kWarp) {
-      a.out_ids[static_cast<size_t>(qi) * a.out_stride + i] = pool[i].id;
-      a.out_dists[static_cast<size_t>(qi) * a.out_stride + i] = pool[i].dist;
+      const HeapEntry e = pool[i];
+      a.out_ids[static_cast<size_t>(qi) * a.out_stride + i] = e.id;
+      a.out_dists[static_cast<size_t>(qi) * a.out_stride + i] = e.dist;
     }
     if (lane == 0) {
       a.out_counts[qi] = outn;
