@@ -15,6 +15,10 @@ residual rows), ``batched`` (W-wide steps, full correction) and ``gated``
 shortlisted seed and never stop -- the configuration bench.py's calibration
 keeps on the 1M x 128 workload).
 
+``--form sq`` runs the SQ drop-in's search (the 20,000 x 128 SQ8 workload,
+SQMD, L = 64, expand 32, exact residual correction, the top 20 returned) on
+--queries queries with --ep entry points.
+
 ``--form score --kind K`` runs one of the batched distance kernels of
 calculator_rover_score instead (K: 0 ADC, 1 packed residual, 2 SQ8 code
 distance, 3 SQ exact residual, 4 decoded-row rescore) on --queries queries x
@@ -36,7 +40,8 @@ import numpy as np
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--form", default="gated", choices=("plain", "packed", "batched", "gated", "score", "refine"))
+    ap.add_argument("--form", default="gated",
+                    choices=("plain", "packed", "batched", "gated", "score", "refine", "sq"))
     ap.add_argument("--kind", type=int, default=4)
     ap.add_argument("--ids", type=int, default=8192)
     ap.add_argument("--adc-n", type=int, default=0)
@@ -55,6 +60,8 @@ def main(argv=None) -> int:
     from .calculator import GATE_PARAMS, MODE_BATCHED, MODE_EXACT, MODE_GATED, Calculator
     if args.form in ("score", "refine"):
         return distance_case(args)
+    if args.form == "sq":
+        return sq_case(args)
     w = workloads.build_pq(args.workload, cache_dir=args.cache_dir, verbose=False)
     if args.layout == "gorder":
         from .layout import gorder_workload
@@ -89,6 +96,30 @@ def main(argv=None) -> int:
                           entry_points=args.ep, beam_width=args.W if args.form in ("batched", "gated") else None,
                           warm_launches=warm, kernel_ms=times, recall_at_10=recall,
                           scored=st[0], corrected=st[1], expanded=st[2])), flush=True)
+    calc.close()
+    return 0
+
+
+def sq_case(args) -> int:
+    """One warm-up SQMD search and --repeat timed ones on the SQ workload."""
+    from . import workloads
+    from .calculator import Calculator
+    w = workloads.build_sq("sq_20k_d128")
+    calc = Calculator()
+    calc.sq_load(w.graph, w.entry, w.bundle)
+    q = np.ascontiguousarray(w.queries[:args.queries])
+    kw = dict(sq_mode=1, num_out=20, entry_points=args.ep, expand_count=32, correction=1)
+    l0 = calc.launch_count()
+    r = calc.sq_search(q, 64, 20, **kw)
+    warm = calc.launch_count() - l0
+    calc.kernel_timing(True)
+    for _ in range(args.repeat):
+        r = calc.sq_search(q, 64, 20, **kw)
+    times = {k: v[1] / args.repeat for k, v in calc.kernel_times().items() if v[0] > 0}
+    calc.kernel_timing(False)
+    st = r["stats"].astype(np.float64).mean(axis=0)
+    print(json.dumps(dict(form="sq", workload="sq_20k_d128", queries=len(q), L=64, entry_points=args.ep,
+                          warm_launches=warm, kernel_ms=times, scored=st[0], turns=st[2])), flush=True)
     calc.close()
     return 0
 
