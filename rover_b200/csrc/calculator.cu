@@ -142,6 +142,32 @@ struct SqDevice {
   }
 };
 
+// Page-locked host memory that only grows (cudaHostAlloc).
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    const size_t want = std::max<size_t>(std::max<size_t>(b, 2 * bytes), 64);
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// A device-to-host copy the status fetch of a search enqueues with its own
+// (fetch_status): the results of a host-buffer call land in page-locked
+// staging in the same wait as the status.
+struct EarlyCopy {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+
 struct State {
   std::mutex mu;
   bool init = false;
@@ -171,6 +197,9 @@ struct State {
   DevBuf in_queries, in_pool, in_topk, in_ids, in_offsets;
   DevBuf out_ids, out_dists, out_counts, pool_ids, pool_dists, pool_counts;
   std::vector<int32_t> h_status;
+  PinnedBuf status_pin, stage;    // page-locked status and result staging (fetch_status, pq_search_host)
+  std::vector<EarlyCopy> early;   // result copies to enqueue with each status fetch of the current call
+  bool early_done = false;        // a status fetch of the current call enqueued them
 };
 
 State& st() {
@@ -295,6 +324,68 @@ AEEResult upload(DevBuf& b, const T* src, size_t count, cudaStream_t s) {
   if (count) CK(cudaMemcpyAsync(b.p, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
   return AEE_SUCCESS;
 }
+
+// The per-query statuses of a search, after everything enqueued on stream:
+// one page-locked copy (with the call's early result copies) and one wait.
+AEEResult fetch_status(State& s, const int32_t* d_status, int nq, cudaStream_t stream) {
+  for (const EarlyCopy& c : s.early)
+    CK(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, stream));
+  s.early_done = !s.early.empty();
+  CK(s.status_pin.ensure(static_cast<size_t>(nq) * sizeof(int32_t)));
+  CK(cudaMemcpyAsync(s.status_pin.p, d_status, static_cast<size_t>(nq) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                     stream));
+  CK(cudaStreamSynchronize(stream));
+  s.h_status.assign(s.status_pin.as<int32_t>(), s.status_pin.as<int32_t>() + nq);
+  return AEE_SUCCESS;
+}
+
+// The results of a host-buffer search: they travel to page-locked staging
+// within the search's own status fetch (one wait, no second round trip),
+// then to the caller's buffers.  add() the (caller, device) pairs, arm()
+// before the search, finish() after it succeeded.
+class ResultStage {
+ public:
+  explicit ResultStage(State& s) : s_(s) {}
+  ~ResultStage() {
+    s_.early.clear();
+    s_.early_done = false;
+  }
+  ResultStage(const ResultStage&) = delete;
+  ResultStage& operator=(const ResultStage&) = delete;
+  void add(void* user, const void* dev, size_t bytes) {
+    if (!user || !dev || !bytes) return;
+    parts_.push_back({user, dev, total_, bytes});
+    total_ += (bytes + 255) & ~static_cast<size_t>(255);
+  }
+  AEEResult arm() {
+    s_.early.clear();
+    s_.early_done = false;
+    if (!total_) return AEE_SUCCESS;
+    if (s_.stage.ensure(total_) != cudaSuccess) return AEE_ENOMEMORY;
+    for (const Part& x : parts_) s_.early.push_back({s_.stage.as<uint8_t>() + x.off, x.dev, x.bytes});
+    return AEE_SUCCESS;
+  }
+  AEEResult finish(cudaStream_t stream) {
+    if (!parts_.empty() && !s_.early_done) {
+      // a search path that returned without a status fetch: copy directly
+      for (const Part& x : parts_) CK(cudaMemcpyAsync(x.user, x.dev, x.bytes, cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      return AEE_SUCCESS;
+    }
+    for (const Part& x : parts_) std::memcpy(x.user, s_.stage.as<uint8_t>() + x.off, x.bytes);
+    return AEE_SUCCESS;
+  }
+
+ private:
+  struct Part {
+    void* user;
+    const void* dev;
+    size_t off, bytes;
+  };
+  State& s_;
+  std::vector<Part> parts_;
+  size_t total_ = 0;
+};
 
 uint32_t next_pow2(uint64_t v) {
   uint64_t p = 1;
@@ -618,9 +709,7 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
       CK(cudaGetLastError());
       ++g_launches;
     }
-    s.h_status.resize(nq);
-    CK(cudaMemcpyAsync(s.h_status.data(), a.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
+    if (fetch_status(s, a.status, nq, stream) != AEE_SUCCESS) return AEE_EFAILED;
     collect_timings();
     if (check_tc_err(s) != AEE_SUCCESS) return AEE_EFAILED;
     bool retry = false;
@@ -738,9 +827,7 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
     }
     CK(cudaGetLastError());
     ++g_launches;
-    s.h_status.resize(nq);
-    CK(cudaMemcpyAsync(s.h_status.data(), d_out.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
+    if (fetch_status(s, d_out.status, nq, stream) != AEE_SUCCESS) return AEE_EFAILED;
     collect_timings();
     bool retry = false;
     for (int i = 0; i < nq; ++i) retry |= s.h_status[i] == kStatusTableFull;
@@ -904,9 +991,7 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
       CK(cudaGetLastError());
       ++g_launches;
     }
-    s.h_status.resize(nq);
-    CK(cudaMemcpyAsync(s.h_status.data(), a.status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
+    if (fetch_status(s, a.status, nq, stream) != AEE_SUCCESS) return AEE_EFAILED;
     collect_timings();
     if (check_tc_err(s) != AEE_SUCCESS) return AEE_EFAILED;
     bool retry = false;
@@ -1070,9 +1155,7 @@ AEEResult sq_search_core(State& s, SqDevice& sq, int mode, const RoverSearchPara
     }
     CK(cudaGetLastError());
     ++g_launches;
-    s.h_status.resize(nq);
-    CK(cudaMemcpyAsync(s.h_status.data(), d_status, nq * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
+    if (fetch_status(s, d_status, nq, stream) != AEE_SUCCESS) return AEE_EFAILED;
     collect_timings();
     bool retry = false, widen = false;
     for (int i = 0; i < nq; ++i) {
@@ -1307,27 +1390,27 @@ AEEResult pq_search_host(State& s, const RoverSearchParams* p, const float* quer
   d.status = s.status.as<int32_t>();
   RoverSearchParams pp = *p;
   pp.pool_stride = p_stride;
+  ResultStage rs(s);
+  const size_t nk = static_cast<size_t>(nq) * k_stride, np = static_cast<size_t>(nq) * p_stride;
+  if (k_stride) {
+    rs.add(out->ids, d.ids, nk * sizeof(int32_t));
+    rs.add(out->dists, d.dists, nk * sizeof(float));
+    rs.add(out->counts, d.counts, static_cast<size_t>(nq) * sizeof(int32_t));
+  }
+  if (p_stride) {
+    rs.add(out->pool_ids, d.pool_ids, np * sizeof(int32_t));
+    rs.add(out->pool_dists, d.pool_dists, np * sizeof(float));
+    rs.add(out->pool_counts, d.pool_counts, static_cast<size_t>(nq) * sizeof(int32_t));
+  }
+  if (out->stats) rs.add(out->stats, d.stats, static_cast<size_t>(nq) * 4 * sizeof(uint64_t));
+  if (rs.arm() != AEE_SUCCESS) return AEE_ENOMEMORY;
   AEEResult r = pq_search_core(s, &pp, s.in_queries.as<float>(), nq, s.in_pool.as<int32_t>(),
                                top_ks ? s.in_topk.as<int32_t>() : nullptr, h_pool, d, strm);
   if (out->status) {
     std::copy(s.h_status.begin(), s.h_status.begin() + nq, out->status);
   }
   if (r != AEE_SUCCESS) return r;
-  if (k_stride) {
-    if (download(out->ids, d.ids, static_cast<size_t>(nq) * k_stride, strm) ||
-        download(out->dists, d.dists, static_cast<size_t>(nq) * k_stride, strm) ||
-        download(out->counts, d.counts, nq, strm))
-      return AEE_EFAILED;
-  }
-  if (p_stride) {
-    if (download(out->pool_ids, d.pool_ids, static_cast<size_t>(nq) * p_stride, strm) ||
-        download(out->pool_dists, d.pool_dists, static_cast<size_t>(nq) * p_stride, strm) ||
-        download(out->pool_counts, d.pool_counts, nq, strm))
-      return AEE_EFAILED;
-  }
-  if (out->stats && download(out->stats, d.stats, static_cast<size_t>(nq) * 4, strm)) return AEE_EFAILED;
-  CK(cudaStreamSynchronize(strm));
-  return AEE_SUCCESS;
+  return rs.finish(strm);
 }
 
 extern "C" AEEResult calculator_rover_pq_search(remote_handle64 h, const RoverSearchParams* p,
@@ -2846,19 +2929,19 @@ extern "C" AEEResult calculator_rover_sq_search(remote_handle64 h, const RoverSe
   CK(s.stats.ensure(static_cast<size_t>(nq) * 32));
   CK(s.status.ensure(nq * 4));
   const int mode = p->sq_mode == 1 ? kSqModeSqmd : p->sq_mode == 2 ? kSqModeDb : kSqModeDsp;
+  ResultStage rs(s);
+  rs.add(out->ids, s.out_ids.p, static_cast<size_t>(nq) * stride * sizeof(int32_t));
+  rs.add(out->dists, s.out_dists.p, static_cast<size_t>(nq) * stride * sizeof(float));
+  rs.add(out->counts, s.out_counts.p, static_cast<size_t>(nq) * sizeof(int32_t));
+  if (out->stats) rs.add(out->stats, s.stats.p, static_cast<size_t>(nq) * 4 * sizeof(uint64_t));
+  if (rs.arm() != AEE_SUCCESS) return AEE_ENOMEMORY;
   AEEResult r = sq_search_core(s, s.sq, mode, p, s.in_queries.as<float>(), nq,
                                s.in_pool.as<int32_t>(), h_pool, p->sq_mode == 1 ? stride : std::min(stride, p->top_k),
                                s.out_ids.as<int32_t>(), s.out_dists.as<float>(), stride, s.out_counts.as<int32_t>(),
                                s.stats.as<unsigned long long>(), s.status.as<int32_t>(), s.stream);
   if (out->status) std::copy(s.h_status.begin(), s.h_status.begin() + nq, out->status);
   if (r != AEE_SUCCESS) return r;
-  if (download(out->ids, s.out_ids.p, static_cast<size_t>(nq) * stride, s.stream) ||
-      download(out->dists, s.out_dists.p, static_cast<size_t>(nq) * stride, s.stream) ||
-      download(out->counts, s.out_counts.p, nq, s.stream) ||
-      (out->stats && download(out->stats, s.stats.p, static_cast<size_t>(nq) * 4, s.stream)))
-    return AEE_EFAILED;
-  CK(cudaStreamSynchronize(s.stream));
-  return AEE_SUCCESS;
+  return rs.finish(s.stream);
 }
 
 // ===========================================================================

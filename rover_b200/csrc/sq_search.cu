@@ -241,6 +241,47 @@ __device__ __forceinline__ float sq_exact_fast(const SqIndexView& ix, const floa
   return vec ? sq_exact_vec(ix, q, id) : sq_exact(ix, q, id);
 }
 
+// sq_exact of one candidate per group of 8 lanes (4 candidates per warp
+// step), for rows sq_exact_vec can read and dim % 128 == 0.  Each lane
+// squares 16 of every 128 dimensions; the sum then runs through the group's
+// lanes in dimension order (lane k adds its 16 squares, then hands the
+// partial sum to lane k + 1), so the FP32 additions are sq_exact's, in its
+// order.  All 32 lanes must call it; every lane of a group returns the sum.
+__device__ __forceinline__ float sq_exact_group(const SqIndexView& ix, const float* q, int32_t id, int lane) {
+  const int sub = lane & 7, leader = lane & ~7;
+  const uint8_t* l1 = ix.l1 + static_cast<size_t>(id) * ix.l1_code_bytes;
+  const uint8_t* res = ix.residual ? ix.residual + static_cast<size_t>(id) * ix.rcb : nullptr;
+  const bool c4 = ix.l1_bits == 4, r4 = ix.residual_bits == 4;
+  float rs = 0.0f, rz = 0.0f, acc = 0.0f;
+  if (res) {
+    const float2 qp = __ldg(reinterpret_cast<const float2*>(ix.qparams) + id);
+    rs = qp.x;
+    rz = qp.y;
+  }
+  for (int r = 0; r < ix.dim; r += 128) {
+    const int g = r + sub * 16;
+    const uint4 cv = group_load(l1, c4, g);
+    const uint4 rv = res ? group_load(res, r4, g) : make_uint4(0u, 0u, 0u, 0u);
+    float sq[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      float value = fadd(fmul(u8f(group_code(cv, c4, j)), ix.l1_scale), ix.l1_zero);
+      if (res) value = fadd(value, fadd(fmul(u8f(group_code(rv, r4, j)), rs), rz));
+      const float diff = fsub(q[g + j], value);
+      sq[j] = fmul(diff, diff);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (sub == k) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc = fadd(acc, sq[j]);
+      }
+      acc = __shfl_sync(kFullMask, acc, leader | k);
+    }
+  }
+  return acc;
+}
+
 // First occurrence in lane order among lanes that hold the same id.
 __device__ __forceinline__ bool first_of_equal(bool active, int32_t id, int lane) {
   const unsigned act = __ballot_sync(kFullMask, active);
@@ -260,8 +301,10 @@ size_t sq_search_smem_per_warp(int dim, int pool_split, int front_split) {
   return sq_search_warp_smem(dim, pool_split, front_split);
 }
 
+// Four CTAs per SM: the shared-memory share the host gives a CTA when one
+// per SM is not enough for the batch (sq_search_core) allows no more.
 template <bool kSplit>
-__global__ void __launch_bounds__(kSearchWarps * 32)
+__global__ void __launch_bounds__(kSearchWarps * 32, 4)
 sq_search_kernel_t(SqSearchArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int warp = threadIdx.x >> 5;
@@ -286,6 +329,7 @@ sq_search_kernel_t(SqSearchArgs a) {
   const bool split = kSplit && sqmd && a.correction;   // the host checks the index supports it
   const bool exact = (sqmd || db) && a.correction;
   const bool vec = sq_rows_vectorizable(ix);
+  const bool group_rows = vec && ix.dim % 128 == 0;
 
   // Lane 0 applies the batch's scored candidates (work[0..cnt)) to the heaps
   // in batch order.  keep marks the ones that can enter the pool: a full
@@ -397,8 +441,10 @@ sq_search_kernel_t(SqSearchArgs a) {
       }
       float d = 0.0f;
       if (fresh) {
+        // SQMD seeds carry the corrected distance (sqmd_make_seed); DSP and
+        // DB-pair entries the coarse one (db_search_state_init)
         d = split ? split_seed_distance(ix, qc, sum_q, id, step)
-                  : exact ? sq_exact_fast(ix, q, id, vec) : sq_coarse(ix, qc, id);
+                  : (sqmd && a.correction) ? sq_exact_fast(ix, q, id, vec) : sq_coarse(ix, qc, id);
         if (sqmd && a.correction && (!isfinite(d) || d < 0.0f)) st = kStatusNumeric;
       }
       if (__any_sync(kFullMask, st != kStatusOk)) { st = st != kStatusOk ? st : kStatusNumeric; break; }
@@ -441,6 +487,20 @@ sq_search_kernel_t(SqSearchArgs a) {
           const float dl = split_delta(ix, qc, sum_q, nid, step);
           d = split_sum(split_coarse(ix, qc, nid, step), dl);
           dbad = !isfinite(dl) || !isfinite(d) || d < 0.0f;
+        } else if (exact && group_rows && __popc(__ballot_sync(kFullMask, fresh)) <= 8) {
+          // few new neighbours (the usual case once the pool settles): a
+          // group of 8 lanes per candidate instead of a lane each
+          const unsigned fm = __ballot_sync(kFullMask, fresh);
+          const int nf = __popc(fm);
+          const int rank = __popc(fm & ((1u << lane) - 1u));
+          if (fresh) work[rank].id = nid;     // the candidates in lane order
+          __syncwarp();
+          for (int t0 = 0; t0 < nf; t0 += 4) {
+            const int t = t0 + (lane >> 3);
+            const float gd = sq_exact_group(ix, q, t < nf ? work[t].id : 0, lane);
+            const float mine = __shfl_sync(kFullMask, gd, ((rank - t0) & 3) * 8);
+            if (fresh && rank >= t0 && rank < t0 + 4) d = mine;
+          }
         } else if (fresh) {
           d = exact ? sq_exact_fast(ix, q, nid, vec) : sq_coarse(ix, qc, nid);
         }
