@@ -16,7 +16,7 @@ is then timed, with its recall reported, on the 10,000 timed queries:
 
 * plain drop-in: the exact mode (the reference's expansion order, every
   candidate corrected); entry points as multiples of the mixture's cluster
-  count x beam width L in {32, 40, 48, 64, 96, 128, 192, 256}; the
+  count x beam width L in {32, 40, 48, 56, 64, 80, 96, 128, 192, 256}; the
   least-work point reaching the target;
 * batched: W pool entries expanded per step, every candidate corrected, no
   network; the fastest point over W, entry points and L;
@@ -67,7 +67,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "pq_1m_d128"
-L_SWEEP = (32, 40, 48, 64, 96, 128, 192, 256)
+L_SWEEP = (32, 40, 48, 56, 64, 80, 96, 128, 192, 256)
 FREE_L_SWEEP = (16, 24) + L_SWEEP   # batched / gated forms may go below the plain grid
 EP_MULTIPLES = (0.25, 1, 2, 4)   # entry points as multiples of the mixture's cluster count
 TOP_K = 10

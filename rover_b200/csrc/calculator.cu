@@ -198,6 +198,12 @@ struct State {
   DevBuf out_ids, out_dists, out_counts, pool_ids, pool_dists, pool_counts;
   std::vector<int32_t> h_status;
   PinnedBuf status_pin, stage;    // page-locked status and result staging (fetch_status, pq_search_host)
+  // Queries uploaded in pieces on copy_stream (pq_search_host): rows
+  // [k arrival_rows, (k + 1) arrival_rows) are on the device once
+  // arrival_ev[k] completes.  arrival_pieces == 0: nothing in flight.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t arrival_ev[4] = {};
+  int arrival_rows = 0, arrival_pieces = 0;
   std::vector<EarlyCopy> early;   // result copies to enqueue with each status fetch of the current call
   bool early_done = false;        // a status fetch of the current call enqueued them
 };
@@ -303,6 +309,8 @@ AEEResult ensure_init(State& s) {
   }
   CK(cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&s.copy_stream, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : s.arrival_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   s.device = dev;
   s.init = true;
   return AEE_SUCCESS;
@@ -336,6 +344,47 @@ AEEResult fetch_status(State& s, const int32_t* d_status, int nq, cudaStream_t s
                      stream));
   CK(cudaStreamSynchronize(stream));
   s.h_status.assign(s.status_pin.as<int32_t>(), s.status_pin.as<int32_t>() + nq);
+  return AEE_SUCCESS;
+}
+
+// Makes stream wait until query rows [0, q_end) of a piecewise upload have
+// arrived (no-op without one).
+AEEResult await_rows(State& s, cudaStream_t stream, int q_end) {
+  if (!s.arrival_pieces || q_end <= 0) return AEE_SUCCESS;
+  const int k = std::min(s.arrival_pieces - 1, (q_end - 1) / s.arrival_rows);
+  CK(cudaStreamWaitEvent(stream, s.arrival_ev[k], 0));
+  return AEE_SUCCESS;
+}
+
+AEEResult seed_rank(State& s, const float* queries, int q0, int q1, int dim, const TcSeedMap& map,
+                    const DevBuf& rows, const DevBuf& norms, int n_seeds, float* out, int stride, cudaStream_t st);
+
+// TF32 ranks of queries [q0, q1) against the seed rows, then each query's
+// top_m smallest (pq_seed_topm_kernel), into rows (q - q0) of rank / top /
+// next.  With a piecewise query upload, each piece is ranked as soon as it
+// has arrived, so the upload of the next overlaps the work.
+AEEResult ranked_seeds(State& s, cudaStream_t stream, const float* queries, int q0, int q1, int dim,
+                       const TcSeedMap& map, const DevBuf& rows, const DevBuf& norms, int n_seeds, float* rank,
+                       int stride, int top_m, uint64_t* top, float* next) {
+  for (int p0 = q0; p0 < q1;) {
+    const int p1 = s.arrival_pieces ? std::min(q1, (p0 / s.arrival_rows + 1) * s.arrival_rows) : q1;
+    if (await_rows(s, stream, p1) != AEE_SUCCESS) return AEE_EFAILED;
+    const size_t off = static_cast<size_t>(p0 - q0);
+    {
+      TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
+      if (seed_rank(s, queries, p0, p1, dim, map, rows, norms, n_seeds, rank + off * stride, stride, stream) !=
+          AEE_SUCCESS)
+        return AEE_EFAILED;
+    }
+    {
+      TimedLaunch tl(ROVER_KERNEL_PQ_SEED_TOPM, stream);
+      launch_pq_seed_topm(rank + off * stride, stride, n_seeds, p1 - p0, top_m, top + off * top_m, next + off,
+                          stream);
+    }
+    CK(cudaGetLastError());
+    g_launches += 2;
+    p0 = p1;
+  }
   return AEE_SUCCESS;
 }
 
@@ -681,23 +730,20 @@ AEEResult pq_search_decoded(State& s, PqSearchArgs a, const RoverSearchParams* p
     for (int q0 = 0; q0 < nq; q0 += chunk) {
       const int q1 = std::min(nq, q0 + chunk);
       if (verify) {
-        {
-          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
-          if (seed_rank(s, a.queries, q0, q1, pq.view.dim, ss.drows_map, ss.drows_tc.p ? ss.drows_tc : ss.drows,
-                        ss.drow_norms, b.n_seeds, s.seed_dists.as<float>(), b.seed_stride, stream) != AEE_SUCCESS)
-            return AEE_EFAILED;
-        }
-        TimedLaunch tl(ROVER_KERNEL_PQ_SEED_TOPM, stream);
-        launch_pq_seed_topm(s.seed_dists.as<float>(), b.seed_stride, b.n_seeds, q1 - q0, b.top_m,
-                            s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
-        ++g_launches;
+        if (ranked_seeds(s, stream, a.queries, q0, q1, pq.view.dim, ss.drows_map,
+                         ss.drows_tc.p ? ss.drows_tc : ss.drows, ss.drow_norms, b.n_seeds, s.seed_dists.as<float>(),
+                         b.seed_stride, b.top_m, s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>()) !=
+            AEE_SUCCESS)
+          return AEE_EFAILED;
       } else {
+        if (await_rows(s, stream, q1) != AEE_SUCCESS) return AEE_EFAILED;
         TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream);
         launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
                              s.seed_dists.as<float>(), stream);
+        ++g_launches;
       }
       CK(cudaGetLastError());
-      ++g_launches;
+      if (await_rows(s, stream, q1) != AEE_SUCCESS) return AEE_EFAILED;
       b.q_begin = q0;
       b.q_end = q1;
       CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
@@ -810,6 +856,7 @@ AEEResult pq_search_core(State& s, const RoverSearchParams* p, const float* d_qu
   uint32_t entries = next_pow2(std::max<uint64_t>(4096, 2 * est));
   CK(s.counter.ensure(sizeof(unsigned int)));
   CK(cudaMemsetAsync(d_out.status, 0, nq * sizeof(int32_t), stream));
+  if (await_rows(s, stream, nq) != AEE_SUCCESS) return AEE_EFAILED;
   for (int attempt = 0; attempt < 8; ++attempt) {
     uint32_t gen_base = 0;
     if (reserve_visited(s, slots, entries, static_cast<uint32_t>(nq), &gen_base) != AEE_SUCCESS) return AEE_ENOMEMORY;
@@ -941,6 +988,7 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
     for (int q0 = 0; q0 < nq; q0 += chunk) {
       const int q1 = std::min(nq, q0 + chunk);
       if (seed_pass) {
+        if (await_rows(s, stream, q1) != AEE_SUCCESS) return AEE_EFAILED;
         {
           TimedLaunch tl(ROVER_KERNEL_PQ_SEEDS, stream);
           launch_pq_seed_dists(a.queries, q0, q1, pq.view.dim, b.decoded, b.seed_ids, b.n_seeds,
@@ -949,37 +997,18 @@ AEEResult pq_search_batched(State& s, PqSearchArgs a, const RoverSearchParams* p
         CK(cudaGetLastError());
         ++g_launches;
       }
-      if (verify) {
-        {
-          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
-          if (seed_rank(s, a.queries, q0, q1, pq.view.dim, ss.drows_map, ss.drows_tc.p ? ss.drows_tc : ss.drows,
-                        ss.drow_norms, b.n_seeds, s.seed_dists.as<float>(), b.seed_stride, stream) != AEE_SUCCESS)
-            return AEE_EFAILED;
-        }
-        {
-          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_TOPM, stream);
-          launch_pq_seed_topm(s.seed_dists.as<float>(), b.seed_stride, b.n_seeds, q1 - q0, b.top_m,
-                              s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
-        }
-        CK(cudaGetLastError());
-        g_launches += 2;
-      }
-      if (rank_pass) {
-        {
-          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream);
-          if (seed_rank(s, a.queries, q0, q1, pq.view.dim, pq.seeds.recon_map,
-                        pq.seeds.recon_tc.p ? pq.seeds.recon_tc : pq.seeds.recon, pq.seeds.recon_norms, b.n_seeds,
-                        s.seed_rank.as<float>(), c.rank_stride, stream) != AEE_SUCCESS)
-            return AEE_EFAILED;
-        }
-        {
-          TimedLaunch tl(ROVER_KERNEL_PQ_SEED_TOPM, stream);
-          launch_pq_seed_topm(s.seed_rank.as<float>(), c.rank_stride, b.n_seeds, q1 - q0, b.top_m,
-                              s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>(), stream);
-        }
-        CK(cudaGetLastError());
-        g_launches += 2;
-      }
+      if (verify &&
+          ranked_seeds(s, stream, a.queries, q0, q1, pq.view.dim, ss.drows_map,
+                       ss.drows_tc.p ? ss.drows_tc : ss.drows, ss.drow_norms, b.n_seeds, s.seed_dists.as<float>(),
+                       b.seed_stride, b.top_m, s.seed_top.as<uint64_t>(), s.seed_top_next.as<float>()) != AEE_SUCCESS)
+        return AEE_EFAILED;
+      if (rank_pass &&
+          ranked_seeds(s, stream, a.queries, q0, q1, pq.view.dim, pq.seeds.recon_map,
+                       pq.seeds.recon_tc.p ? pq.seeds.recon_tc : pq.seeds.recon, pq.seeds.recon_norms, b.n_seeds,
+                       s.seed_rank.as<float>(), c.rank_stride, b.top_m, s.seed_top.as<uint64_t>(),
+                       s.seed_top_next.as<float>()) != AEE_SUCCESS)
+        return AEE_EFAILED;
+      if (await_rows(s, stream, q1) != AEE_SUCCESS) return AEE_EFAILED;
       b.q_begin = q0;
       b.q_end = q1;
       CK(cudaMemsetAsync(a.next_query, 0, sizeof(unsigned int), stream));
@@ -1361,7 +1390,34 @@ AEEResult pq_search_host(State& s, const RoverSearchParams* p, const float* quer
   for (int v : h_pool) max_pool = std::max(max_pool, v);
   const int k_stride = out->ids ? out->out_stride : 0;
   const int p_stride = out->pool_ids ? p->pool_stride : 0;
-  if (upload(s.in_queries, queries, static_cast<size_t>(nq) * dim, strm) != AEE_SUCCESS) return AEE_ENOMEMORY;
+  // Large batches upload their queries in four pieces on the copy stream;
+  // the seed ranking of each piece starts when it has arrived (await_rows),
+  // so the upload overlaps the seed pass.
+  struct ArrivalScope {
+    State& s;
+    ~ArrivalScope() {
+      if (s.arrival_pieces) cudaStreamSynchronize(s.copy_stream);   // no copy from the caller's memory outlives the call
+      s.arrival_pieces = 0;
+    }
+  } arrival{s};
+  const int pieces = nq >= 2048 && s.copy_stream ? 4 : 1;
+  if (pieces > 1) {
+    const size_t bytes = static_cast<size_t>(nq) * dim * sizeof(float);
+    CK(s.in_queries.ensure(bytes));
+    const int rows = (((nq + pieces - 1) / pieces) + 127) / 128 * 128;   // whole 128-query tiles of the ranking
+    int k = 0;
+    for (int q0 = 0; q0 < nq; q0 += rows, ++k) {
+      const size_t n = static_cast<size_t>(std::min(nq, q0 + rows) - q0) * dim;
+      CK(cudaMemcpyAsync(s.in_queries.as<float>() + static_cast<size_t>(q0) * dim,
+                         queries + static_cast<size_t>(q0) * dim, n * sizeof(float), cudaMemcpyHostToDevice,
+                         s.copy_stream));
+      CK(cudaEventRecord(s.arrival_ev[k], s.copy_stream));
+    }
+    s.arrival_rows = rows;
+    s.arrival_pieces = k;
+  } else if (upload(s.in_queries, queries, static_cast<size_t>(nq) * dim, strm) != AEE_SUCCESS) {
+    return AEE_ENOMEMORY;
+  }
   if (upload(s.in_pool, pool_sizes, nq, strm) != AEE_SUCCESS) return AEE_ENOMEMORY;
   if (top_ks && upload(s.in_topk, top_ks, nq, strm) != AEE_SUCCESS) return AEE_ENOMEMORY;
   RoverSearchOutputs d{};

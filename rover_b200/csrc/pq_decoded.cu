@@ -233,16 +233,32 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
   if (row >= rows) return;
   const float* r = rank + static_cast<size_t>(row) * stride;
   const int tid = threadIdx.x;
-  auto bits_at = [&](int e) -> uint32_t { return __float_as_uint(__ldg(r + e) + 0.0f); };
+  // f(e, rank) over the row, 16 bytes per load when the rows allow it
+  const bool v4 = (stride & 3) == 0 && (reinterpret_cast<uintptr_t>(rank) & 15u) == 0;
+  auto each = [&](auto&& f) {
+    int e0 = 0;
+    if (v4) {
+      const int n4 = n_seeds >> 2;
+      const float4* r4 = reinterpret_cast<const float4*>(r);
+      for (int i = tid; i < n4; i += kTopThreads) {
+        const float4 x = __ldg(r4 + i);
+        f(4 * i, x.x);
+        f(4 * i + 1, x.y);
+        f(4 * i + 2, x.z);
+        f(4 * i + 3, x.w);
+      }
+      e0 = 4 * n4;
+    }
+    for (int e = e0 + tid; e < n_seeds; e += kTopThreads) f(e, __ldg(r + e));
+  };
   bool bad = false;
   uint32_t lo = 0xffffffffu, hi = 0u;
-  for (int e = tid; e < n_seeds; e += kTopThreads) {
-    const float x = __ldg(r + e);
+  each([&](int, float x) {
     bad |= !(x < 3.0e38f);
     const uint32_t v = __float_as_uint(x + 0.0f);
     lo = min(lo, v);
     hi = max(hi, v);
-  }
+  });
   uint64_t* out = keys + static_cast<size_t>(row) * m;
   if (__syncthreads_or(bad)) {
     for (int i = tid; i < m; i += kTopThreads) out[i] = kEmptyKey;
@@ -268,10 +284,10 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
     for (int i = tid; i < 256; i += kTopThreads) hist[i] = 0u;
     __syncthreads();
     const unsigned prefix = s_prefix, mask = s_mask;
-    for (int e = tid; e < n_seeds; e += kTopThreads) {
-      const uint32_t v = bits_at(e);
+    each([&](int, float x) {
+      const uint32_t v = __float_as_uint(x + 0.0f);
       if ((v & mask) == prefix) atomicAdd(&hist[(v >> shift) & 255u], 1u);
-    }
+    });
     __syncthreads();
     if (tid < kWarp) {
       // the bin holding the remaining-th element: lane l owns bins 8l..8l+7
@@ -307,13 +323,13 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
   auto gather = [&](uint32_t t) -> int {
     if (tid == 0) s_count = 0u;
     __syncthreads();
-    for (int e = tid; e < n_seeds; e += kTopThreads) {
-      const uint32_t v = bits_at(e);
+    each([&](int e, float x) {
+      const uint32_t v = __float_as_uint(x + 0.0f);
       if (v <= t) {
         const unsigned slot = atomicAdd(&s_count, 1u);
         if (slot < kTopGather) gathered[slot] = (static_cast<uint64_t>(v) << 32) | static_cast<uint32_t>(e);
       }
-    }
+    });
     __syncthreads();
     return static_cast<int>(s_count);
   };

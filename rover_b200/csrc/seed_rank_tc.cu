@@ -7,11 +7,15 @@
 // One CTA owns 128 queries and a run of 128-seed tiles:
 //   * warps 0-3 stage the 128 query rows, rounded to TF32, into shared
 //     memory in the 128-byte-swizzled K-major layout the MMA descriptors
-//     name, and sum |q|^2; later they are the epilogue: tcgen05.ld of their
-//     32 accumulator lanes, the rank formula, coalesced-per-row stores;
-//   * warp 4 streams the seed tiles with TMA (cp.async.bulk.tensor, one
+//     name, and sum |q|^2;
+//   * warps 0-7 are the epilogue: warp w reads accumulator lanes
+//     32 (w mod 4) .. +31 (its query rows) and columns 64 (w / 4) .. +63 of
+//     each tile with tcgen05.ld, applies the rank formula (the tile's seed
+//     norms read once per 32 columns and broadcast by shuffles) and stores
+//     the row segments;
+//   * warp 8 streams the seed tiles with TMA (cp.async.bulk.tensor, one
 //     32-float x 128-row box per 128-byte swizzle column) into two stages;
-//   * warp 5 allocates 256 tensor-memory columns (two accumulators) and one
+//   * warp 9 allocates 256 tensor-memory columns (two accumulators) and one
 //     of its threads issues the MMAs; tcgen05.commit hands each finished
 //     accumulator to the epilogue and each consumed stage back to TMA.
 // The seed rows come pre-rounded to TF32 (round to nearest, as cvt.rna),
@@ -37,7 +41,9 @@ namespace {
 
 constexpr int kTcM = 128;                 // queries per CTA (MMA M, TMEM lanes)
 constexpr int kTcN = 128;                 // seeds per tile (MMA N)
-constexpr int kTcThreads = 192;           // 4 epilogue warps, TMA warp, MMA warp
+constexpr int kTcEpiWarps = 8;            // two per accumulator lane quarter
+constexpr int kTmaWarp = kTcEpiWarps, kMmaWarp = kTcEpiWarps + 1;
+constexpr int kTcThreads = 32 * (kTcEpiWarps + 2);
 constexpr int kAtomBytes = 128 * 128;     // one 32-float column block of 128 rows
 constexpr uint32_t kWaitLimit = 1u << 22; // mbarrier polls before giving up
 
@@ -170,12 +176,12 @@ pq_seed_rank_tc_kernel(const __grid_constant__ CUtensorMap rows_map, const float
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
       mbar_init(accf0 + 8 * s, 1);
-      mbar_init(acce0 + 8 * s, 4);       // one arrival per epilogue warp
+      mbar_init(acce0 + 8 * s, kTcEpiWarps);   // one arrival per epilogue warp
     }
     *stop = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 5) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(256u)
                  : "memory");
@@ -205,7 +211,7 @@ pq_seed_rank_tc_kernel(const __grid_constant__ CUtensorMap rows_map, const float
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 4) {
+  if (warp == kTmaWarp) {
     if (lane == 0) {
       // TMA producer: seed tile t0 + i into stage i % 2
       int issued = 0;
@@ -222,7 +228,7 @@ pq_seed_rank_tc_kernel(const __grid_constant__ CUtensorMap rows_map, const float
       for (int i = max(0, issued - 2); i < issued; ++i)
         if (!mbar_wait(full0 + 8 * (i & 1), (i >> 1) & 1)) atomicExch(err, 1);
     }
-  } else if (warp == 5) {
+  } else if (warp == kMmaWarp) {
     if (lane == 0) {
       // MMA issuer: tile i into accumulator i % 2 (TMEM columns 128 (i % 2) ..)
       int committed = 0;
@@ -246,8 +252,10 @@ pq_seed_rank_tc_kernel(const __grid_constant__ CUtensorMap rows_map, const float
         atomicExch(err, 1);
     }
   } else {
-    // epilogue: accumulator lanes 32 warp .. 32 warp + 31 = this warp's query rows
-    const int r = warp * 32 + lane;
+    // epilogue: accumulator lanes 32 (warp mod 4) .. +31 = this warp's query
+    // rows; columns 64 (warp / 4) .. +63 of each tile
+    const int quarter = warp & 3, half = warp >> 2;
+    const int r = quarter * 32 + lane;
     const int qq = q0 + r;
     const float qv = qn[r];
     float* orow = out + static_cast<size_t>(qq - q_begin) * out_stride;
@@ -258,25 +266,22 @@ pq_seed_rank_tc_kernel(const __grid_constant__ CUtensorMap rows_map, const float
       tc_fence_after();
       const int u0 = (t0 + i) * kTcN;
 #pragma unroll 1
-      for (int c = 0; c < kTcN / 32; ++c) {
+      for (int c = 2 * half; c < 2 * half + 2; ++c) {
         float v[32];
-        tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(ab * kTcN + c * 32), v);
+        tmem_ld32(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(ab * kTcN + c * 32), v);
         const int ub = u0 + c * 32;
+        const float nl = ub + lane < n_seeds ? __ldg(norms + ub + lane) : 0.0f;   // this chunk's 32 seed norms
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = fmaxf(qv + __shfl_sync(kFullMask, nl, j) - 2.0f * v[j], 0.0f);
         if (qq < q_end) {
           if (vec && ub + 32 <= n_seeds) {
 #pragma unroll
-            for (int j = 0; j < 32; j += 4) {
-              float4 o;
-              o.x = fmaxf(qv + __ldg(norms + ub + j) - 2.0f * v[j], 0.0f);
-              o.y = fmaxf(qv + __ldg(norms + ub + j + 1) - 2.0f * v[j + 1], 0.0f);
-              o.z = fmaxf(qv + __ldg(norms + ub + j + 2) - 2.0f * v[j + 2], 0.0f);
-              o.w = fmaxf(qv + __ldg(norms + ub + j + 3) - 2.0f * v[j + 3], 0.0f);
-              *reinterpret_cast<float4*>(orow + ub + j) = o;
-            }
+            for (int j = 0; j < 32; j += 4)
+              *reinterpret_cast<float4*>(orow + ub + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
           } else {
 #pragma unroll
             for (int j = 0; j < 32; ++j)
-              if (ub + j < n_seeds) orow[ub + j] = fmaxf(qv + __ldg(norms + ub + j) - 2.0f * v[j], 0.0f);
+              if (ub + j < n_seeds) orow[ub + j] = v[j];
           }
         }
       }
@@ -287,7 +292,7 @@ pq_seed_rank_tc_kernel(const __grid_constant__ CUtensorMap rows_map, const float
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 5) {
+  if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
   }
@@ -367,10 +372,26 @@ bool launch_pq_seed_rank_tc(const TcSeedMap& m, const float* queries, int q_begi
   }
   const int qt = (q_end - q_begin + kTcM - 1) / kTcM;
   const int nt = (n_seeds + kTcN - 1) / kTcN;
-  // about two CTAs' worth of work per SM: split the seed tiles across CTAs
-  int splits = std::max(1, std::min(nt, (2 * std::max(sms, 1) + qt - 1) / qt));
-  const int per = (nt + splits - 1) / splits;
-  splits = (nt + per - 1) / per;
+  static int per_sm = 0;
+  if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pq_seed_rank_tc_kernel, kTcThreads, smem) !=
+                      cudaSuccess ||
+                  per_sm < 1))
+    per_sm = 1;
+  // Split the seed tiles of each 128-query tile across CTAs.  The time is
+  // about (waves of resident CTAs) x (tiles per CTA + the prologue, worth
+  // about two tiles: query staging, tensor-memory allocation, pipeline
+  // fill); take the split that minimises it.
+  const int slots = std::max(1, sms) * per_sm;
+  int per = nt;
+  long long best = -1;
+  for (int sp = 1; sp <= nt; ++sp) {
+    const int p = (nt + sp - 1) / sp;
+    const int used = (nt + p - 1) / p;
+    const long long waves = (static_cast<long long>(qt) * used + slots - 1) / slots;
+    const long long cost = waves * (p + 2);
+    if (best < 0 || cost < best) { best = cost; per = p; }
+  }
+  const int splits = (nt + per - 1) / per;
   CUtensorMap map;
   std::memcpy(&map, m.bytes, sizeof(map));
   pq_seed_rank_tc_kernel<<<dim3(splits, qt), kTcThreads, smem, s>>>(map, queries, q_begin, q_end, dim, norms,
