@@ -1193,7 +1193,8 @@ def free_forms(calc, w, args, cal, ep, L, expand, q_d, stream, dist, dev, world,
         "the learned gate is faster than the batched form without it" if res["gated"] and
         res["gated"]["qps"] > best_batched else
         "the learned gate does not beat the batched form without it on this workload: the speed-up over the "
-        "plain drop-in comes from the W-wide steps and the tensor-core seed ranking, not from the network")
+        "plain drop-in comes from the W-wide steps (whose gathers share DRAM pages on the clustered id order) "
+        "and the tensor-core seed ranking, not from the network")
     return res
 
 

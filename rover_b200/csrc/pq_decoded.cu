@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
                                                                    uint64_t* __restrict__ keys,
                                                                    float* __restrict__ next) {
   __shared__ unsigned hist[256];
-  __shared__ unsigned s_prefix, s_mask, s_remaining, s_count;
+  __shared__ unsigned s_prefix, s_mask, s_remaining, s_count, s_bin_count;
   __shared__ unsigned s_lo[kTopThreads / kWarp], s_hi[kTopThreads / kWarp];
   __shared__ uint64_t gathered[kTopGather];
   const int row = blockIdx.x;
@@ -305,14 +305,18 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
       const unsigned hit = __ballot_sync(kFullMask, incl >= rem0);
       const int owner = hit ? __ffs(hit) - 1 : kWarp - 1;
       if (lane == owner) {
-        unsigned rem = rem0 - (incl - sum), bin = 8u * lane;
+        unsigned rem = rem0 - (incl - sum), bin = 8u * lane, in_bin = own[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-          if (own[k] >= rem) break;
+          if (own[k] >= rem) {
+            in_bin = own[k];
+            break;
+          }
           rem -= own[k];
           ++bin;
         }
         s_remaining = rem;
+        s_bin_count = in_bin;
         s_prefix = prefix | (bin << shift);
         s_mask = mask | (255u << shift);
       }
@@ -341,7 +345,14 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
   if (tid == 0) { s_prefix = lo & top; s_mask = top; s_remaining = static_cast<unsigned>(target); }
   __syncthreads();
   radix_pass(first);
-  int cnt = gather(s_prefix | ((1u << first) - 1u));   // every rank up to the end of the target's bin
+  // narrow a crowded bin 8 bits at a time while that leaves more ranks up
+  // to its end than one warp sorts in registers
+  int shift = first;
+  while (shift >= 8 && static_cast<int>(target - s_remaining + s_bin_count) > 8 * kWarp) {
+    shift -= 8;
+    radix_pass(shift);
+  }
+  int cnt = gather(s_prefix | ((1u << shift) - 1u));   // every rank up to the end of the target's bin
   if (cnt > kTopGather) {
     // a crowded bin: the exact (m+1)-th rank, 8 bits per pass from the top
     if (tid == 0) { s_prefix = 0u; s_mask = 0u; s_remaining = static_cast<unsigned>(target); }
