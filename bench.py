@@ -641,7 +641,11 @@ def main():
                    "calibration_set": f"{CALIBRATION_QUERIES} held-out queries (seed offset {CALIBRATION_OFFSET}), "
                                       f"target recall@10 {TARGET_RECALL} + {CALIBRATION_MARGIN} margin; "
                                       "recall reported on the timed queries",
-                   "plain": {"qps": plain_qps, "ms_per_step": plain["steps"]["ms_per_step"], "recall_at_10": recall,
+                   "timed_steps": ("each form's search as a tuned search plan replayed from a CUDA graph "
+                                   "(the direct device-buffer call's time in direct_ms_per_step)"),
+                   "plain": {"qps": plain_qps, "ms_per_step": plain["steps"]["ms_per_step"],
+                             "direct_ms_per_step": plain["steps"]["direct_ms_per_step"],
+                             "plan_identical": plain["steps"]["plan_identical"], "recall_at_10": recall,
                              "entry_points": ep, "beam_L": L, "kernel_ms_per_step":
                                  {k: v[1] / args.steps for k, v in plain["steps"]["kernels"].items()},
                              "roofline": plain_roof, "calibration": table},
@@ -655,6 +659,8 @@ def main():
                    "sq": sq,
                    "parallelism": f"replicas x{world}",
                    "l2": "index (>800 MB with decoded rows) larger than L2; no flush"},
+        "direct_ms_per_step": steps.get("direct_ms_per_step"),
+        "plan_identical": steps.get("plan_identical"),
         "roofline": head["roof"],
         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in steps["kernels"].items()},
         "distance_kernels": dk,
@@ -1006,7 +1012,14 @@ def layout_section(calc, args, wg, L, plain_kw, forms, stream, dist, dev, world)
 def timed_form(calc, args, w, q_d, L, kw, stream, dist, dev, world):
     """One form at one operating point on the timed queries: a host-buffer
     search for recall and statistics, then the warm-up and timed device
-    steps (queries resident in HBM, outputs written to device buffers)."""
+    steps (queries resident in HBM, outputs written to device buffers).
+
+    The timed steps replay a search plan (calculator_rover_pq_plan_*, tuned
+    on the timed queries) from a CUDA graph: the same kernels as the direct
+    device-buffer call, without its per-call status wait, so that steps run
+    back to back.  The direct call is timed too; its per-kernel event times
+    give the kernel breakdown (a replayed graph records no library events),
+    and the plan's outputs must equal its outputs bit for bit."""
     import torch
     from rover_b200.workloads import recall_at_k
     nq = len(w.queries)
@@ -1025,7 +1038,22 @@ def timed_form(calc, args, w, q_d, L, kw, stream, dist, dev, world):
         calc.pq_search_device(q_d.data_ptr(), nq, pool_d.data_ptr(), ptrs, stream_ptr=stream.cuda_stream,
                               top_k=TOP_K, **kw)
 
-    steps = device_steps(calc, args, step, stream, dist, dev)
+    direct = device_steps(calc, args, step, stream, dist, dev)
+    torch.cuda.synchronize()
+    ref = {k: out[k].clone() for k in ("ids", "dists", "counts")}
+    plan = calc.pq_plan(nq, L, tune_queries_ptr=q_d.data_ptr(), top_k=TOP_K, **kw)
+    info = plan.describe()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        plan.launch(q_d.data_ptr(), ptrs, torch.cuda.current_stream().cuda_stream)
+    steps = device_steps(calc, args, graph.replay, stream, dist, dev)
+    torch.cuda.synchronize()
+    identical = all(torch.equal(out[k], ref[k]) for k in ref) and bool((out["status"] == 0).all())
+    del graph
+    plan.destroy()
+    steps.update(kernels=direct["kernels"], launches=info["launches"] * args.steps,
+                 direct_ms_per_step=direct["ms_per_step"], plan_identical=identical,
+                 plan={k: info[k] for k in ("classes", "warps_per_cta", "shared_visited_slots", "layout")})
     qps = nq * args.steps * world / (steps["total_ms"] / 1e3)
     return dict(qps=qps, steps=steps, recall=rec, stats=r["stats"], counts=r["counts"], kw=kw, L=L)
 
@@ -1151,7 +1179,9 @@ def free_forms(calc, w, args, cal, ep, L, expand, q_d, stream, dist, dev, world,
         bp = timed_form(calc, args, w, q_d, plain["L"], dict(plain["kw"], mode=MODE_BATCHED,
                                                                beam_width=bpick["beam_width"]),
                         stream, dist, dev, world)
-        rep["batched"] = dict(qps=b["qps"], ms_per_step=b["steps"]["ms_per_step"], recall_at_10=b["recall"],
+        rep["batched"] = dict(qps=b["qps"], ms_per_step=b["steps"]["ms_per_step"],
+                              direct_ms_per_step=b["steps"]["direct_ms_per_step"],
+                              plan_identical=b["steps"]["plan_identical"], recall_at_10=b["recall"],
                               beam_width=bpick["beam_width"], entry_points=bpick["entry_points"], L=bpick["L"],
                               calibration_ms=bpick["ms"])
         rep["batched_over_plain"] = b["qps"] / plain["qps"]
@@ -1174,7 +1204,9 @@ def free_forms(calc, w, args, cal, ep, L, expand, q_d, stream, dist, dev, world,
         res["gated"] = g
         # the same point with the network switched off
         bg = timed_form(calc, args, w, q_d, gpick["L"], kw_of(gpick, MODE_BATCHED), stream, dist, dev, world)
-        rep["gated"] = dict(qps=g["qps"], ms_per_step=g["steps"]["ms_per_step"], recall_at_10=g["recall"],
+        rep["gated"] = dict(qps=g["qps"], ms_per_step=g["steps"]["ms_per_step"],
+                            direct_ms_per_step=g["steps"]["direct_ms_per_step"],
+                            plan_identical=g["steps"]["plan_identical"], recall_at_10=g["recall"],
                             beam_width=gpick["beam_width"], entry_points=gpick["entry_points"], L=gpick["L"],
                             calibration_ms=gpick["ms"], mlp_rows_per_query=g_rows,
                             **{k: float(v) for k, v in thr.items()})
