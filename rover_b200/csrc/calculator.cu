@@ -2776,15 +2776,17 @@ extern "C" AEEResult calculator_rover_refine(remote_handle64 h, int32_t kind, co
   }
   CK(cudaGetLastError());
   ++g_launches;
-  std::vector<int32_t> hs(nq);
-  if (download(out_ids, s.out_ids.p, static_cast<size_t>(nq) * top_k, s.stream) ||
-      download(out_dists, s.out_dists.p, static_cast<size_t>(nq) * top_k, s.stream) ||
-      download(out_counts, s.out_counts.p, nq, s.stream) || download(hs.data(), s.status.p, nq, s.stream))
-    return AEE_EFAILED;
-  CK(cudaStreamSynchronize(s.stream));
+  ResultStage rs(s);
+  rs.add(out_ids, s.out_ids.p, static_cast<size_t>(nq) * top_k * sizeof(int32_t));
+  rs.add(out_dists, s.out_dists.p, static_cast<size_t>(nq) * top_k * sizeof(float));
+  rs.add(out_counts, s.out_counts.p, static_cast<size_t>(nq) * sizeof(int32_t));
+  if (rs.arm() != AEE_SUCCESS) return AEE_ENOMEMORY;
+  if (fetch_status(s, s.status.as<int32_t>(), nq, s.stream) != AEE_SUCCESS) return AEE_EFAILED;
   collect_timings();
-  if (out_status) std::copy(hs.begin(), hs.end(), out_status);
-  for (int32_t x : hs) if (x) { set_error("refine failed with status %d", x); return AEE_EFAILED; }
+  if (rs.finish(s.stream) != AEE_SUCCESS) return AEE_EFAILED;
+  if (out_status) std::copy(s.h_status.begin(), s.h_status.begin() + nq, out_status);
+  for (int i = 0; i < nq; ++i)
+    if (s.h_status[i]) { set_error("refine failed with status %d", s.h_status[i]); return AEE_EFAILED; }
   return AEE_SUCCESS;
 }
 

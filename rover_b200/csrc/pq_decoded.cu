@@ -235,17 +235,29 @@ __global__ void __launch_bounds__(kTopThreads) pq_seed_topm_kernel(const float* 
   const int tid = threadIdx.x;
   // f(e, rank) over the row, 16 bytes per load when the rows allow it
   const bool v4 = (stride & 3) == 0 && (reinterpret_cast<uintptr_t>(rank) & 15u) == 0;
+  // (four loads in flight per thread before any is used)
   auto each = [&](auto&& f) {
     int e0 = 0;
     if (v4) {
       const int n4 = n_seeds >> 2;
       const float4* r4 = reinterpret_cast<const float4*>(r);
-      for (int i = tid; i < n4; i += kTopThreads) {
-        const float4 x = __ldg(r4 + i);
-        f(4 * i, x.x);
-        f(4 * i + 1, x.y);
-        f(4 * i + 2, x.z);
-        f(4 * i + 3, x.w);
+      for (int i = tid; i < n4; i += 4 * kTopThreads) {
+        float4 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = i + u * kTopThreads;
+          x[u] = j < n4 ? __ldg(r4 + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int j = i + u * kTopThreads;
+          if (j < n4) {
+            f(4 * j, x[u].x);
+            f(4 * j + 1, x[u].y);
+            f(4 * j + 2, x[u].z);
+            f(4 * j + 3, x[u].w);
+          }
+        }
       }
       e0 = 4 * n4;
     }
