@@ -784,6 +784,9 @@ def uneven_section(calc, args, stream, dist, dev, world):
     from rover_b200 import replicas, workloads
     t0 = time.time()
     w = workloads.build_pq(UNEVEN_WORKLOAD, cache_dir=args.cache_dir, verbose=False)
+    if args.layout == "gorder":          # the same id order as the headline index
+        from rover_b200.layout import gorder_workload
+        w, _ = gorder_workload(w)
     calc.pq_load(w.graph, w.entry, w.bundle)
     nq = len(w.queries)
     expand = int(w.graph.shape[1])
@@ -866,6 +869,7 @@ def uneven_section(calc, args, stream, dist, dev, world):
         f"{info['warps_per_cta']} warps, {info['shared_visited_slots']} slots, layout {info['layout']}), direct "
         f"{direct_qps:,.0f} QPS, identical={identical}, recall@k={rk:.4f}")
     return {"workload": UNEVEN_WORKLOAD, "n": int(w.bundle.meta.num_vectors), "dim": int(w.bundle.meta.dim),
+            "layout": args.layout,
             "pq": f"M={w.bundle.meta.m}x{w.bundle.meta.ks}", "graph_degree": expand, "queries_per_step": nq,
             "beam_L": f"log-uniform [{UNEVEN_L[0]}, {UNEVEN_L[1]}], L >= k", "top_k": list(UNEVEN_K),
             "refine_budget": UNEVEN_REFINE, "entry_points": ep, "calibration": table,
