@@ -902,6 +902,13 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
     w = workloads.build_large(args.large_workload, calc)
     cfg = workloads.LARGE_CONFIGS[args.large_workload]
     log(f"config5 workload ready in {w.build_seconds:.1f}s")
+    order_s = None
+    if args.layout == "gorder":          # the same id order as the headline index
+        from rover_b200.layout import gorder_large
+        t0 = time.time()
+        w, _ = gorder_large(w)
+        order_s = time.time() - t0
+        log(f"config5 index in the clustered block order ({order_s:.1f}s)")
     calc.pq_load(w.graph, w.entry, w.pq)
     nq, gq = len(w.queries), len(w.gt)
     expand = int(w.graph.shape[1])
@@ -979,6 +986,7 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
     calc.sq_unload()
     log(f"config5 sq4: {gq / sq_s:,.0f} QPS end to end, recall@10={sq_rec:.4f}")
     return {"workload": args.large_workload, "n": cfg["n"], "dim": cfg["dim"], "pq": f"M={cfg['m']}x{cfg['ks']}",
+            "layout": args.layout, "layout_seconds": order_s,
             "pq_trainer": "calculator_rover_pq_train (GPU, the reference's k-means bit for bit)",
             "sq": f"{cfg['l1_bits']}-bit global codec + {cfg['sq_rbits']}-bit residuals",
             "graph_degree": expand, "queries_per_step": nq, "recall_queries": gq,

@@ -56,22 +56,58 @@ def permute_pq(w, new_to_old: np.ndarray):
     return replace(w, graph=graph, entry=int(o2n[w.entry]), bundle=bundle, gt=gt), new_to_old
 
 
+def nearest_centre(base: np.ndarray, centers: np.ndarray) -> np.ndarray:
+    """Index of each vector's nearest centre (squared L2; torch, on the GPU
+    when there is one), 65,536 vectors at a time."""
+    import torch
+    dev = torch.device("cuda" if torch.cuda.is_available() else "cpu")
+    with torch.no_grad():
+        c = torch.from_numpy(np.ascontiguousarray(centers, dtype=np.float32)).to(dev)
+        cn = (c * c).sum(1)
+        parts = []
+        for s in range(0, base.shape[0], 65536):
+            x = torch.from_numpy(np.ascontiguousarray(base[s:s + 65536], dtype=np.float32)).to(dev)
+            parts.append(torch.argmin(cn[None, :] - 2.0 * (x @ c.T), dim=1).int().cpu())
+        return torch.cat(parts).numpy()
+
+
 def gorder_workload(w, per_block: int = 32, threads: int | None = None):
     """The workload's layout by gorder, clustered by the nearest mixture
     centre (the mixture the workload was drawn from; rover_b200.workloads
     CONFIGS).  Returns (workload, new_to_old)."""
-    import torch
     from . import datasets as D
     from .workloads import CONFIGS
     cfg = CONFIGS[w.name]
     base, centers = D.gmm(cfg["n"], cfg["dim"], cfg["comps"], cfg["seed"], clip_nonneg=cfg["clip"],
                           normalize=cfg["normalize"], return_centers=True)
-    dev = torch.device("cuda" if torch.cuda.is_available() else "cpu")
-    with torch.no_grad():
-        x = torch.from_numpy(base).to(dev)
-        c = torch.from_numpy(np.ascontiguousarray(centers, dtype=np.float32)).to(dev)
-        cn = (c * c).sum(1)
-        labels = torch.cat([torch.argmin(cn[None, :] - 2.0 * (x[s:s + 65536] @ c.T), dim=1)
-                            for s in range(0, x.shape[0], 65536)]).int().cpu().numpy()
+    labels = nearest_centre(base, centers)
     n2o = gorder(w.graph, labels, int(centers.shape[0]), per_block, threads=threads)
     return permute_pq(w, n2o)
+
+
+def permute_large(w, new_to_old: np.ndarray):
+    """The large combined workload (workloads.LargeWorkload) with its ids in
+    the new order: graph renumbered, the PQ bundle's and the SQ bundle's rows
+    moved, ground truth and entry renumbered.  Returns (workload,
+    new_to_old)."""
+    n2o = np.asarray(new_to_old, dtype=np.int64)
+    o2n = np.empty_like(n2o)
+    o2n[n2o] = np.arange(len(n2o))
+    g = w.graph[n2o]
+    graph = np.where(g >= 0, o2n[np.maximum(g, 0)], -1).astype(np.int32)
+    del g
+    p = w.pq
+    pq = B.PqBundle(p.meta, p.codebook, np.ascontiguousarray(p.codes[n2o]), p.residual_bits,
+                    B.pack_residual_blocks(p.residual_rows()[n2o]), np.ascontiguousarray(p.qparams[n2o]))
+    q = w.sq
+    sq = B.SqBundle(q.num_vectors, q.dim, q.l1_bits, q.l1_scale, q.l1_zero, np.ascontiguousarray(q.l1[n2o]),
+                    q.residual_bits, np.ascontiguousarray(q.residual_rows[n2o]), np.ascontiguousarray(q.qparams[n2o]))
+    gt = np.where(w.gt >= 0, o2n[np.maximum(w.gt, 0)], -1).astype(np.int32)
+    return replace(w, graph=graph, entry=int(o2n[w.entry]), pq=pq, sq=sq, gt=gt, labels=None), new_to_old
+
+
+def gorder_large(w, per_block: int = 32, threads: int | None = None):
+    """The large workload's layout by gorder, clustered by the labels its
+    build recorded (nearest mixture centre)."""
+    n2o = gorder(w.graph, w.labels, int(w.labels.max()) + 1, per_block, threads=threads)
+    return permute_large(w, n2o)

@@ -114,6 +114,7 @@ class LargeWorkload:
     pq: B.PqBundle
     sq: B.SqBundle
     build_seconds: float = 0.0
+    labels: np.ndarray | None = None   # nearest mixture centre of each vector (layout.gorder_large)
 
 
 def build_large(name: str, calc, device=None, verbose: bool = True) -> LargeWorkload:
@@ -132,6 +133,8 @@ def build_large(name: str, calc, device=None, verbose: bool = True) -> LargeWork
                               long_edges=8, probe=cfg["probe"], device=device)
     entry = D.medoid(base, device=device)
     log("graph", f"mean degree {float((graph >= 0).sum(1).mean()):.1f}")
+    from .layout import nearest_centre
+    labels = nearest_centre(base, centers)
     sample = base[D.uniform_positions(n, min(n, 100_000))]
     book = calc.pq_train(sample, cfg["m"], cfg["ks"], cfg["iters"])
     codes = calc.pq_encode(base, book)
@@ -150,7 +153,7 @@ def build_large(name: str, calc, device=None, verbose: bool = True) -> LargeWork
     scale, zero, l1, res, sqp = D.sq_encode(base, cfg["l1_bits"], cfg["sq_rbits"], chunk=1 << 18)
     sq = B.SqBundle(n, dim, cfg["l1_bits"], scale, zero, l1, cfg["sq_rbits"], res, sqp)
     log("sq4 codes + residuals")
-    return LargeWorkload(name, queries, gt, graph, entry, pq, sq, time.time() - t0)
+    return LargeWorkload(name, queries, gt, graph, entry, pq, sq, time.time() - t0, labels)
 
 
 def _key(cfg: dict) -> str:

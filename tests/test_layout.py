@@ -102,3 +102,33 @@ def test_permuted_workload_is_the_same_index(tmp_path):
     assert p.entry == o2n[data["graph_entry"]]
     back = np.where(p.graph >= 0, n2o[np.maximum(p.graph, 0)], -1)
     assert np.array_equal(back, graph[n2o])
+
+
+def test_permuted_large_workload_moves_both_bundles():
+    """The large combined workload renumbered: the PQ and SQ rows, the
+    graph, the ground truth and the entry move together."""
+    from rover_b200 import bundle as B
+    from rover_b200 import datasets as D
+    from rover_b200.layout import gorder_large
+    from rover_b200.workloads import LargeWorkload
+    data, graph, pq, _, _ = load_fixture("pq8_d64")
+    n, dim = data["n"], data["dim"]
+    base = D.gmm(n, dim, 8, 3)
+    scale, zero, l1, res, qp = D.sq_encode(base, 4, 8)
+    sq = B.SqBundle(n, dim, 4, scale, zero, l1, 8, res, qp)
+    labels = (np.arange(n) * 5 % 7).astype(np.int32)
+    gt = np.random.default_rng(1).integers(-1, n, size=(6, 100)).astype(np.int32)
+    w = LargeWorkload("t", np.zeros((6, dim), np.float32), gt, graph, data["graph_entry"], pq, sq, 0.0, labels)
+    p, n2o = gorder_large(w, per_block=16, threads=2)
+    assert np.array_equal(np.sort(n2o), np.arange(n))
+    assert p.labels is None
+    assert np.array_equal(p.pq.codes, pq.codes[n2o])
+    assert np.array_equal(p.pq.residual_rows(), pq.residual_rows()[n2o])
+    assert np.array_equal(p.sq.l1, sq.l1[n2o])
+    assert np.array_equal(p.sq.residual_rows, sq.residual_rows[n2o])
+    assert np.array_equal(p.sq.qparams, sq.qparams[n2o])
+    o2n = np.argsort(n2o)
+    assert p.entry == o2n[data["graph_entry"]]
+    assert np.array_equal(np.where(p.gt >= 0, n2o[np.maximum(p.gt, 0)], -1), gt)
+    back = np.where(p.graph >= 0, n2o[np.maximum(p.graph, 0)], -1)
+    assert np.array_equal(back, graph[n2o])
