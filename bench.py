@@ -784,9 +784,6 @@ def uneven_section(calc, args, stream, dist, dev, world):
     from rover_b200 import replicas, workloads
     t0 = time.time()
     w = workloads.build_pq(UNEVEN_WORKLOAD, cache_dir=args.cache_dir, verbose=False)
-    if args.layout == "gorder":          # the same id order as the headline index
-        from rover_b200.layout import gorder_workload
-        w, _ = gorder_workload(w)
     calc.pq_load(w.graph, w.entry, w.bundle)
     nq = len(w.queries)
     expand = int(w.graph.shape[1])
@@ -869,7 +866,6 @@ def uneven_section(calc, args, stream, dist, dev, world):
         f"{info['warps_per_cta']} warps, {info['shared_visited_slots']} slots, layout {info['layout']}), direct "
         f"{direct_qps:,.0f} QPS, identical={identical}, recall@k={rk:.4f}")
     return {"workload": UNEVEN_WORKLOAD, "n": int(w.bundle.meta.num_vectors), "dim": int(w.bundle.meta.dim),
-            "layout": args.layout,
             "pq": f"M={w.bundle.meta.m}x{w.bundle.meta.ks}", "graph_degree": expand, "queries_per_step": nq,
             "beam_L": f"log-uniform [{UNEVEN_L[0]}, {UNEVEN_L[1]}], L >= k", "top_k": list(UNEVEN_K),
             "refine_budget": UNEVEN_REFINE, "entry_points": ep, "calibration": table,
@@ -903,12 +899,17 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
     cfg = workloads.LARGE_CONFIGS[args.large_workload]
     log(f"config5 workload ready in {w.build_seconds:.1f}s")
     order_s = None
+    # The SQ4 component keeps the ids as built: the SQMD seeds are
+    # (seed / 65536) mod n of an LCG (retrieval_sqmd_seed.c:15), ids below
+    # 65,536 only, which the clustered order would put in a few clusters.
+    from dataclasses import replace
+    w_sq = replace(w, pq=None)
     if args.layout == "gorder":          # the same id order as the headline index
         from rover_b200.layout import gorder_large
         t0 = time.time()
         w, _ = gorder_large(w)
         order_s = time.time() - t0
-        log(f"config5 index in the clustered block order ({order_s:.1f}s)")
+        log(f"config5 PQ index in the clustered block order ({order_s:.1f}s)")
     calc.pq_load(w.graph, w.entry, w.pq)
     nq, gq = len(w.queries), len(w.gt)
     expand = int(w.graph.shape[1])
@@ -966,8 +967,10 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
     res["gated"]["gate"] = dict(band=[model.band_lo, model.band_hi], refine_logit=0.0, stop_logit="inf",
                                 trace_rows=int(len(rows)), mlp_rows=int(calc.gate_rows()))
     calc.gate_unload()
-    # SQ4 component on the same vectors
+    # SQ4 component on the same vectors, ids as built
     calc.pq_unload()
+    del w
+    w = w_sq
     calc.sq_load(w.graph, w.entry, w.sq)
     sq_ep = ep
 
@@ -986,7 +989,8 @@ def config5_section(calc, args, stream, dist, dev, world) -> dict:
     calc.sq_unload()
     log(f"config5 sq4: {gq / sq_s:,.0f} QPS end to end, recall@10={sq_rec:.4f}")
     return {"workload": args.large_workload, "n": cfg["n"], "dim": cfg["dim"], "pq": f"M={cfg['m']}x{cfg['ks']}",
-            "layout": args.layout, "layout_seconds": order_s,
+            "layout": f"{args.layout} (PQ forms); ids as built (SQ4: its LCG seeds are ids < 65,536)",
+            "layout_seconds": order_s,
             "pq_trainer": "calculator_rover_pq_train (GPU, the reference's k-means bit for bit)",
             "sq": f"{cfg['l1_bits']}-bit global codec + {cfg['sq_rbits']}-bit residuals",
             "graph_degree": expand, "queries_per_step": nq, "recall_queries": gq,
