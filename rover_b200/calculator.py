@@ -390,15 +390,22 @@ class Calculator:
         return p
 
     def pq_search(self, queries, pool_sizes, top_k=10, top_ks=None, pool_stride=0, stats=True, check=True,
-                  **kw) -> dict:
+                  out: dict | None = None, **kw) -> dict:
+        """Host-buffer search (calculator_rover_pq_search).  out: arrays from
+        an earlier call's result to write into again (ids, dists, counts,
+        status of the same shapes), so that repeated calls allocate nothing;
+        the call fills every row it returns (counts give the valid prefix)."""
         q = np.ascontiguousarray(queries, dtype=np.float32)
         nq = q.shape[0]
         pools = np.ascontiguousarray(np.broadcast_to(np.asarray(pool_sizes, dtype=np.int32), (nq,)))
         tks = None if top_ks is None else np.ascontiguousarray(np.broadcast_to(np.asarray(top_ks, dtype=np.int32), (nq,)))
         stride = top_k if tks is None else int(tks.max())
         p = self.params(top_k=top_k, pool_stride=pool_stride, **kw)
-        r = dict(ids=np.full((nq, stride), -1, np.int32), dists=np.zeros((nq, stride), np.float32),
-                 counts=np.zeros(nq, np.int32), status=np.zeros(nq, np.int32))
+        if out is not None and not pool_stride and not stats and out["ids"].shape == (nq, stride):
+            r = {k: out[k] for k in ("ids", "dists", "counts", "status")}
+        else:
+            r = dict(ids=np.full((nq, stride), -1, np.int32), dists=np.zeros((nq, stride), np.float32),
+                     counts=np.zeros(nq, np.int32), status=np.zeros(nq, np.int32))
         if pool_stride:
             r.update(pool_ids=np.full((nq, pool_stride), -1, np.int32),
                      pool_dists=np.zeros((nq, pool_stride), np.float32), pool_counts=np.zeros(nq, np.int32))

@@ -388,10 +388,11 @@ AEEResult ranked_seeds(State& s, cudaStream_t stream, const float* queries, int 
   return AEE_SUCCESS;
 }
 
-// The results of a host-buffer search: they travel to page-locked staging
-// within the search's own status fetch (one wait, no second round trip),
-// then to the caller's buffers.  add() the (caller, device) pairs, arm()
-// before the search, finish() after it succeeded.
+// The results of a host-buffer search: they travel within the search's own
+// status fetch (one wait, no second round trip), straight into caller
+// buffers that are page-locked, through page-locked staging into the
+// others.  add() the (caller, device) pairs, arm() before the search,
+// finish() after it succeeded.
 class ResultStage {
  public:
   explicit ResultStage(State& s) : s_(s) {}
@@ -401,17 +402,21 @@ class ResultStage {
   }
   ResultStage(const ResultStage&) = delete;
   ResultStage& operator=(const ResultStage&) = delete;
+  // A caller buffer in page-locked memory receives its copy directly.
   void add(void* user, const void* dev, size_t bytes) {
     if (!user || !dev || !bytes) return;
-    parts_.push_back({user, dev, total_, bytes});
-    total_ += (bytes + 255) & ~static_cast<size_t>(255);
+    cudaPointerAttributes at{};
+    const bool pinned = cudaPointerGetAttributes(&at, user) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    if (!pinned) cudaGetLastError();
+    parts_.push_back({user, dev, pinned ? 0 : total_, bytes, pinned});
+    if (!pinned) total_ += (bytes + 255) & ~static_cast<size_t>(255);
   }
   AEEResult arm() {
     s_.early.clear();
     s_.early_done = false;
-    if (!total_) return AEE_SUCCESS;
-    if (s_.stage.ensure(total_) != cudaSuccess) return AEE_ENOMEMORY;
-    for (const Part& x : parts_) s_.early.push_back({s_.stage.as<uint8_t>() + x.off, x.dev, x.bytes});
+    if (total_ && s_.stage.ensure(total_) != cudaSuccess) return AEE_ENOMEMORY;
+    for (const Part& x : parts_)
+      s_.early.push_back({x.pinned ? x.user : s_.stage.as<uint8_t>() + x.off, x.dev, x.bytes});
     return AEE_SUCCESS;
   }
   AEEResult finish(cudaStream_t stream) {
@@ -421,7 +426,8 @@ class ResultStage {
       CK(cudaStreamSynchronize(stream));
       return AEE_SUCCESS;
     }
-    for (const Part& x : parts_) std::memcpy(x.user, s_.stage.as<uint8_t>() + x.off, x.bytes);
+    for (const Part& x : parts_)
+      if (!x.pinned) std::memcpy(x.user, s_.stage.as<uint8_t>() + x.off, x.bytes);
     return AEE_SUCCESS;
   }
 
@@ -430,6 +436,7 @@ class ResultStage {
     void* user;
     const void* dev;
     size_t off, bytes;
+    bool pinned;
   };
   State& s_;
   std::vector<Part> parts_;

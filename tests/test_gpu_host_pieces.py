@@ -63,3 +63,24 @@ def test_piecewise_upload_matches_device_entry(calc, big, form):
     assert np.array_equal(h["ids"], d["ids"])
     assert np.array_equal(h["dists"].view(np.uint32), d["dists"].view(np.uint32))
     assert np.array_equal(h["stats"].astype(np.int64), d["stats"])
+
+
+def test_results_into_page_locked_buffers(calc, big):
+    """Page-locked result arrays passed back in (out=) receive the copies
+    directly; the results equal those of a call with fresh pageable arrays,
+    on two calls in a row."""
+    import torch
+    w, q = big
+    calc.pq_load(w.graph, w.entry, w.bundle)
+    kw = dict(entry_points=2048, expand_count=int(w.graph.shape[1]), correction=1, refine_budget=20)
+    nq = len(q)
+    want = calc.pq_search(q, 32, top_k=TOP_K, stats=False, **kw)
+    out = {k: torch.empty(shape, dtype=dt).pin_memory().numpy() for k, shape, dt in
+           (("ids", (nq, TOP_K), torch.int32), ("dists", (nq, TOP_K), torch.float32),
+            ("counts", (nq,), torch.int32), ("status", (nq,), torch.int32))}
+    for _ in range(2):
+        got = calc.pq_search(q, np.full(nq, 32, np.int32), top_k=TOP_K, stats=False, out=out, **kw)
+        assert got["ids"] is out["ids"]
+        for k in ("counts", "ids", "status"):
+            assert np.array_equal(got[k], want[k]), k
+        assert np.array_equal(got["dists"].view(np.uint32), want["dists"].view(np.uint32))
