@@ -78,6 +78,8 @@ def test_results_into_page_locked_buffers(calc, big):
     out = {k: torch.empty(shape, dtype=dt).pin_memory().numpy() for k, shape, dt in
            (("ids", (nq, TOP_K), torch.int32), ("dists", (nq, TOP_K), torch.float32),
             ("counts", (nq,), torch.int32), ("status", (nq,), torch.int32))}
+    out["ids"][:] = -1                      # as a fresh result's rows past its count
+    out["dists"][:] = 0.0
     for _ in range(2):
         got = calc.pq_search(q, np.full(nq, 32, np.int32), top_k=TOP_K, stats=False, out=out, **kw)
         assert got["ids"] is out["ids"]
