@@ -140,6 +140,21 @@ def uniform_positions(population: int, count: int) -> np.ndarray:
     return (np.arange(count, dtype=np.int64) * (population - 1)) // (count - 1)
 
 
+def cluster_sums(x, labels, k: int):
+    """Per-cluster sums and counts of x's rows, the same bits on every run:
+    rows in label order (a stable sort), a float64 running sum, differences
+    at the cluster boundaries -- no floating-point atomics, whose order (and
+    so the k-means centroids, and the index built from them) would change
+    from run to run."""
+    order = torch.sort(labels, stable=True).indices
+    cs = torch.cumsum(x[order].double(), 0)
+    cnt = torch.bincount(labels, minlength=k)
+    ends = torch.cumsum(cnt, 0)
+    cs0 = torch.cat([torch.zeros((1, x.shape[1]), dtype=torch.float64, device=x.device), cs], 0)
+    sums = cs0[ends] - cs0[ends - cnt]
+    return sums.to(x.dtype), cnt.to(x.dtype)
+
+
 def train_pq(base: np.ndarray, m: int, ks: int, iters: int, train_max: int = 100000,
              device=None) -> np.ndarray:
     """Per-subspace k-means codebook [m][ks][subdim] (float32)."""
@@ -156,8 +171,7 @@ def train_pq(base: np.ndarray, m: int, ks: int, iters: int, train_max: int = 100
                 d = ((x[:, None, :] - cent[None, :, :]) ** 2).sum(2) if x.shape[0] * ks <= (1 << 24) \
                     else torch.cdist(x, cent) ** 2
                 a = torch.argmin(d, dim=1)
-                sums = torch.zeros_like(cent).index_add_(0, a, x)
-                cnt = torch.bincount(a, minlength=ks).to(x.dtype)
+                sums, cnt = cluster_sums(x, a, ks)
                 pop = cnt > 0
                 cent[pop] = sums[pop] / cnt[pop, None]
             book[s] = cent.cpu().numpy()
@@ -297,8 +311,7 @@ def kmeans_centroids(base: np.ndarray, k: int, iters: int = 10, device=None, see
                 xs = x[s:s + 65536]
                 parts.append(torch.argmin(cn[None, :] - 2.0 * (xs @ cent.T), dim=1))
             labels = torch.cat(parts)
-            sums = torch.zeros_like(cent).index_add_(0, labels, x)
-            cnt = torch.bincount(labels, minlength=k).to(x.dtype)
+            sums, cnt = cluster_sums(x, labels, k)
             pop = cnt > 0
             cent[pop] = sums[pop] / cnt[pop, None]
         return cent.cpu().numpy(), labels.cpu().numpy()
