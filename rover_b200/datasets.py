@@ -155,6 +155,21 @@ def cluster_sums(x, labels, k: int):
     return sums.to(x.dtype), cnt.to(x.dtype)
 
 
+def representatives(dc, lab, k: int):
+    """rep[j] = the member of cluster j nearest its centre (dc: each point's
+    distance to its own centre), ties to the lower id, -1 for an empty
+    cluster.  Two stable sorts, no scatter with repeated indices (whose
+    winning write the GPU does not fix)."""
+    by_d = torch.sort(dc, stable=True).indices
+    by_c = by_d[torch.sort(lab[by_d], stable=True).indices]
+    cnt = torch.bincount(lab, minlength=k)
+    start = torch.cumsum(cnt, 0) - cnt
+    rep = torch.full((k,), -1, dtype=torch.long, device=dc.device)
+    has = cnt > 0
+    rep[has] = by_c[start[has]]
+    return rep
+
+
 def train_pq(base: np.ndarray, m: int, ks: int, iters: int, train_max: int = 100000,
              device=None) -> np.ndarray:
     """Per-subspace k-means codebook [m][ks][subdim] (float32)."""
@@ -340,9 +355,7 @@ def navigable_graph(base: np.ndarray, candidates: int, degree: int, alpha: float
         lab = torch.from_numpy(labels).to(dev).long()
         # representative of each cluster: member nearest its centroid
         dc = ((x - c[lab]) ** 2).sum(1)
-        rep = torch.full((clusters,), -1, dtype=torch.long, device=dev)
-        order = torch.argsort(dc, descending=True)
-        rep[lab[order]] = order            # last write wins = nearest member
+        rep = representatives(dc, lab, clusters)
         cn = (c * c).sum(1)
         a2 = float(alpha) * float(alpha)
         want = long_edges + 1
@@ -432,9 +445,7 @@ def clustered_graph(base: np.ndarray, centers: np.ndarray, candidates: int, degr
     with torch.no_grad():
         lab = labels
         dc = ((x - c[lab]) ** 2).sum(1)
-        rep = torch.full((k_clusters,), -1, dtype=torch.long, device=dev)
-        order_d = torch.argsort(dc, descending=True)
-        rep[lab[order_d]] = order_d          # last write wins = nearest member
+        rep = representatives(dc, lab, k_clusters)
         a2 = float(alpha) * float(alpha)
         want = long_edges + 1
         chunk = 16384
@@ -484,9 +495,7 @@ def routed_graph(base: np.ndarray, candidates: int, degree: int, alpha: float, l
         c = torch.from_numpy(cent).to(dev)
         lab = torch.from_numpy(labels).to(dev).long()
         dc = ((x - c[lab]) ** 2).sum(1)
-        order = torch.argsort(dc, descending=True)
-        rep = torch.full((clusters,), -1, dtype=torch.long, device=dev)
-        rep[lab[order]] = order
+        rep = representatives(dc, lab, clusters)
         reps = [int(r) for r in rep.cpu().numpy() if r >= 0 and r != entry]
         # hubs: the nodes nearest the entry that are not representatives
         taken = set(reps) | {entry}

@@ -29,3 +29,19 @@ def test_training_is_repeatable():
     ca, la = D.kmeans_centroids(base, 12, iters=4, device="cpu")
     cb, lb = D.kmeans_centroids(base, 12, iters=4, device="cpu")
     assert np.array_equal(ca, cb) and np.array_equal(la, lb)
+
+
+def test_representatives_are_each_clusters_nearest_member():
+    from rover_b200.datasets import representatives
+    g = torch.Generator().manual_seed(9)
+    lab = torch.randint(0, 6, (400,), generator=g)
+    lab[lab == 4] = 5                                # an empty cluster
+    dc = torch.randint(0, 50, (400,), generator=g).float()   # with ties
+    rep = representatives(dc, lab, 7)
+    for j in range(7):
+        members = torch.nonzero(lab == j).flatten()
+        if len(members) == 0:
+            assert rep[j] == -1
+            continue
+        best = members[dc[members] == dc[members].min()].min()   # nearest, then lowest id
+        assert rep[j] == best
