@@ -1533,6 +1533,10 @@ struct PqPlanImpl : RoverPqPlan {
   GateParams gate{};
   DevBuf pool, topk, order, ctl, visited, seed_ids, seed_bits, recon, recon_norms, seed_dists, seed_rank, gate_buf;
   DevBuf drows, drow_norms;             // exact plans: the seeds' decoded rows for the verified seed pool
+  // TF32-rounded copies of drows / recon named by TMA descriptors: the
+  // plan ranks its seeds on the tensor cores (valid == 0: mma.sync)
+  DevBuf drows_tc, recon_tc;
+  TcSeedMap drows_map{}, recon_map{};
   DevBuf seed_top, seed_top_next;       // per query: top-M seed ranks (verified and gated plans)
   int32_t top_m = 0;
   bool verify_seeds = false;            // exact / batched decoded plan, every pool <= kVerifyMaxPool
@@ -1659,6 +1663,7 @@ PqDecodedArgs plan_decoded_args(const State& s, const PqPlanImpl& P) {
     b.seed_top_next = P.seed_top_next.as<float>();
     b.top_m = P.top_m;
   }
+  if (P.drows_map.valid || P.recon_map.valid) b.seed_err = s.tc_err.as<int>();
   return b;
 }
 
@@ -1761,11 +1766,18 @@ AEEResult plan_enqueue(State& s, PqPlanImpl& P, const float* queries, const Rove
   CK(cudaGetLastError());
   ++g_launches;
   const bool decoded = P.cfg.layout != ROVER_LAYOUT_PACKED;
+  // seed ranks on the tensor cores when the rows have a descriptor
+  auto rank = [&](const TcSeedMap& map, const DevBuf& rows, const DevBuf& norms, float* out, int stride) {
+    if (map.valid && launch_pq_seed_rank_tc(map, queries, 0, P.nq, pq.view.dim, norms.as<float>(), P.n_seeds, out,
+                                            stride, s.tc_err.as<int>(), s.sms, stream))
+      return;
+    launch_pq_seed_rank(queries, 0, P.nq, pq.view.dim, rows.as<float>(), norms.as<float>(), P.n_seeds, out, stream,
+                        stride);
+  };
   if (decoded && P.verify_seeds) {
     {
       TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream, timed);
-      launch_pq_seed_rank(queries, 0, P.nq, pq.view.dim, P.drows.as<float>(), P.drow_norms.as<float>(), P.n_seeds,
-                          P.seed_dists.as<float>(), stream, P.seed_stride);
+      rank(P.drows_map, P.drows, P.drow_norms, P.seed_dists.as<float>(), P.seed_stride);
       launch_pq_seed_topm(P.seed_dists.as<float>(), P.seed_stride, P.n_seeds, P.nq, P.top_m,
                           P.seed_top.as<uint64_t>(), P.seed_top_next.as<float>(), stream);
     }
@@ -1783,8 +1795,7 @@ AEEResult plan_enqueue(State& s, PqPlanImpl& P, const float* queries, const Rove
   if (decoded && P.gated) {
     {
       TimedLaunch tl(ROVER_KERNEL_PQ_SEED_RANK, stream, timed);
-      launch_pq_seed_rank(queries, 0, P.nq, pq.view.dim, P.recon.as<float>(), P.recon_norms.as<float>(), P.n_seeds,
-                          P.seed_rank.as<float>(), stream);
+      rank(P.recon_map, P.recon, P.recon_norms, P.seed_rank.as<float>(), P.n_seeds);
       launch_pq_seed_topm(P.seed_rank.as<float>(), P.n_seeds, P.n_seeds, P.nq, P.top_m, P.seed_top.as<uint64_t>(),
                           P.seed_top_next.as<float>(), stream);
     }
@@ -1904,6 +1915,7 @@ AEEResult plan_inputs(State& s, PqPlanImpl& P) {
     CK(cudaMemcpyAsync(P.recon.p, ss.recon.p, rb, cudaMemcpyDeviceToDevice, s.stream));
     CK(cudaMemcpyAsync(P.recon_norms.p, ss.recon_norms.p, static_cast<size_t>(ss.count) * sizeof(float),
                        cudaMemcpyDeviceToDevice, s.stream));
+    if (make_tc_rows(s, P.recon, ss.count, pq.view.dim, P.recon_tc, P.recon_map) != AEE_SUCCESS) return AEE_EFAILED;
     CK(P.seed_rank.ensure(seed_bytes));
     // the gate's weights move with the plan: rebase its pointers
     CK(P.gate_buf.ensure(s.gate_buf.bytes));
@@ -1932,6 +1944,8 @@ AEEResult plan_inputs(State& s, PqPlanImpl& P) {
       CK(cudaMemcpyAsync(P.drow_norms.p, ss.drow_norms.p, static_cast<size_t>(ss.count) * sizeof(float),
                          cudaMemcpyDeviceToDevice, s.stream));
       P.drow_norm_max = ss.drow_norm_max;
+      if (make_tc_rows(s, P.drows, ss.count, pq.view.dim, P.drows_tc, P.drows_map) != AEE_SUCCESS)
+        return AEE_EFAILED;
     }
   }
   CK(cudaStreamSynchronize(s.stream));

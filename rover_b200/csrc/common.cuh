@@ -22,6 +22,7 @@ enum QueryStatus : int32_t {
   kStatusTableFull = 3,     // visited table exceeded its load limit
   kStatusBadParam = 4,      // request out of range (pool, k, expand, ids)
   kStatusFrontierFull = 5,  // SQ frontier exceeded the reference's bound
+  kStatusSeedRank = 6,      // the tensor-core seed ranking of the launch gave up waiting (bounded waits)
 };
 
 // The final refine's third-level ERROR4 term (retrieval_final_refine.c:

@@ -97,6 +97,10 @@ struct PqDecodedArgs {
   const uint64_t* seed_top;
   const float* seed_top_next;
   int32_t top_m;
+  // set by the tensor-core seed ranking when one of its bounded waits ran
+  // out (search plans, which have no host check between the ranking and the
+  // search): every query of the launch then fails with kStatusSeedRank
+  const int* seed_err;
 };
 
 using PqDecodedFn = void (*)(PqSearchArgs, PqDecodedArgs);

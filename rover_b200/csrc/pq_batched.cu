@@ -245,6 +245,10 @@ pq_batched_search_kernel(PqSearchArgs a, PqDecodedArgs b, PqBatchArgs c) {
       if (lane == 0) *status = kStatusBadParam;
       continue;
     }
+    if (b.seed_err && *reinterpret_cast<const volatile int*>(b.seed_err)) {
+      if (lane == 0) *status = kStatusSeedRank;
+      continue;
+    }
     float qsq = 0.0f;
     {
       const float4* src = reinterpret_cast<const float4*>(a.queries + static_cast<size_t>(qi) * dim);

@@ -628,6 +628,10 @@ pq_decoded_search_kernel(PqSearchArgs a, PqDecodedArgs b) {
       if (lane == 0) *status = kStatusBadParam;
       continue;
     }
+    if (b.seed_err && *reinterpret_cast<const volatile int*>(b.seed_err)) {
+      if (lane == 0) *status = kStatusSeedRank;
+      continue;
+    }
     {
       const float4* src = reinterpret_cast<const float4*>(a.queries + static_cast<size_t>(qi) * dim);
       for (int t = lane; t < dim / 4; t += kWarp) reinterpret_cast<float4*>(q)[t] = __ldg(src + t);
