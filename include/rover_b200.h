@@ -28,6 +28,7 @@ extern "C" {
 #define ROVER_QUERY_TABLE_FULL 3     /* internal: retried with a larger table  */
 #define ROVER_QUERY_BAD_PARAM 4
 #define ROVER_QUERY_FRONTIER_FULL 5
+#define ROVER_QUERY_SEED_RANK 6      /* a plan's tensor-core seed ranking gave up waiting */
 
 /* Search modes. */
 #define ROVER_MODE_EXACT 0    /* reference expansion order, bit-exact results */
