@@ -394,6 +394,10 @@ bool launch_pq_seed_rank_tc(const TcSeedMap& m, const float* queries, int q_begi
   const int splits = (nt + per - 1) / per;
   CUtensorMap map;
   std::memcpy(&map, m.bytes, sizeof(map));
+  // a failure left behind by an earlier call that tolerated it (an occupancy
+  // or attribute probe) must not read as this launch's: the caller would
+  // then rank the seeds a second time on mma.sync
+  cudaGetLastError();
   pq_seed_rank_tc_kernel<<<dim3(splits, qt), kTcThreads, smem, s>>>(map, queries, q_begin, q_end, dim, norms,
                                                                    n_seeds, per, out, out_stride ? out_stride : n_seeds,
                                                                    err);
