@@ -648,7 +648,9 @@ def main():
                                       f"target recall@10 {TARGET_RECALL} + {CALIBRATION_MARGIN} margin; "
                                       "recall reported on the timed queries",
                    "timed_steps": ("each form's search as a tuned search plan replayed from a CUDA graph "
-                                   "(the direct device-buffer call's time in direct_ms_per_step)"),
+                                   "(the direct device-buffer call's time in direct_ms_per_step); plans rank "
+                                   "seeds on tcgen05 except gated ones (mma.sync), the kernel breakdown is the "
+                                   "direct call's (tcgen05)"),
                    "plain": {"qps": plain_qps, "ms_per_step": plain["steps"]["ms_per_step"],
                              "direct_ms_per_step": plain["steps"]["direct_ms_per_step"],
                              "plan_identical": plain["steps"]["plan_identical"], "recall_at_10": recall,
