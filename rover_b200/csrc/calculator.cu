@@ -1922,8 +1922,8 @@ AEEResult plan_inputs(State& s, PqPlanImpl& P) {
     CK(cudaMemcpyAsync(P.recon_norms.p, ss.recon_norms.p, static_cast<size_t>(ss.count) * sizeof(float),
                        cudaMemcpyDeviceToDevice, s.stream));
     // (gated plans keep the mma.sync ranking: inside a plan the tcgen05 ranking
-    // of the reconstructions measured slower, 0.77 against 0.53 ms with the
-    // top-M selection per 10,000 queries x 8,192 seeds)
+    // of the reconstructions measured 0.52 ms against 0.29 ms on mma.sync per
+    // 10,000 queries x 8,192 seeds, for a cause not found yet)
     CK(P.seed_rank.ensure(seed_bytes));
     // the gate's weights move with the plan: rebase its pointers
     CK(P.gate_buf.ensure(s.gate_buf.bytes));
